@@ -1,0 +1,206 @@
+/*
+ * xpbd_b200.h -- C ABI of libxpbd_b200.so, the sm_100a XPBD substep.
+ *
+ * Every buffer is a device pointer owned by the caller (the library never
+ * allocates on these entry points).  Arrays documented as [n][4] hold four
+ * floats per element and must be 16-byte aligned.  All launches go to the
+ * given stream; no entry point synchronises, so every call may be captured
+ * into a CUDA graph.  Return value: XPBD_OK or a negative XPBD_ERR_* code
+ * (xpbd_error_string() describes the last failure on the calling thread).
+ *
+ * Each entry point names the reference (chunleili/rlmuscleV2) code it
+ * replaces.  The reference launches one Warp kernel per constraint type per
+ * iteration and scatters with float atomics into dP/dPw; this library keeps
+ * the same arithmetic but projects all constraints of a tet in one pass over
+ * Morton-ordered tiles (see XpbdTiles).
+ */
+#ifndef XPBD_B200_H
+#define XPBD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* xpbd_stream_t; /* a cudaStream_t */
+
+enum {
+    XPBD_OK = 0,
+    XPBD_ERR_ARG = -1,    /* null pointer / bad size / bad enum */
+    XPBD_ERR_ALIGN = -2,  /* a [n][4] array is not 16-byte aligned */
+    XPBD_ERR_CUDA = -3,   /* a CUDA runtime call failed */
+    XPBD_ERR_LIMIT = -4,  /* a size exceeds a documented maximum */
+};
+
+#define XPBD_MAX_MATERIALS 64
+#define XPBD_MAX_ATTACH_MATERIALS 16
+#define XPBD_MAX_TILE_VERTS 4096
+
+/* Material flags: which constraints a tet carries (constraint types of
+ * src/muscle/defs.py:20-36). */
+enum {
+    XPBD_MAT_ARAPSVD = 1 << 0, /* TETARAPSVD   solve_kernels.py:1194 */
+    XPBD_MAT_VOLUME = 1 << 1,  /* TETVOLUME    solve_kernels.py:553  */
+    XPBD_MAT_ANISO = 1 << 2,   /* TETARAPANISO solve_kernels.py:1310 */
+    XPBD_MAT_SNH = 1 << 3,     /* TETSNH       solve_kernels.py:1587 */
+    XPBD_MAT_DAMPED = 1 << 4,  /* a constraint of this material reads pprev */
+};
+
+typedef struct XpbdMaterial {
+    uint32_t flags;
+    float arap_k;             /* TETARAPSVD stiffness (c_stiffness) */
+    float vol_k, vol_damp;    /* TETVOLUME stiffness, dampingratio */
+    float aniso_k;            /* TETARAPANISO stiffness */
+    float snh_mu, snh_lam;    /* TETSNH c_stiffness, c_restdir[0] */
+    float snh_damp;           /* TETSNH dampingratio */
+} XpbdMaterial;
+
+typedef struct XpbdAttachMaterial {
+    float k;    /* ATTACH stiffness */
+    float damp; /* ATTACH dampingratio */
+} XpbdAttachMaterial;
+
+typedef struct XpbdParams {
+    float dt;                    /* substep dt */
+    float gravity[3];            /* gravity vector (engine.py:799-803) */
+    float veldamping;            /* integrate_kernel velocity damping */
+    int32_t quasi_static;        /* integrate_kernel quasi_static */
+    float omega;                 /* Jacobi relaxation of the averaged correction; 1 = reference */
+    float contraction_ratio;     /* aniso_arap activation scale */
+    float fiber_stiffness_scale; /* aniso_arap stiffness multiplier */
+    int32_t n_materials;
+    int32_t n_attach_materials;
+    int32_t reserved;
+    XpbdMaterial materials[XPBD_MAX_MATERIALS];
+    XpbdAttachMaterial attach[XPBD_MAX_ATTACH_MATERIALS];
+} XpbdParams;
+
+/* Per-vertex state, in the library's (tile-grouped Morton) vertex order. */
+typedef struct XpbdVerts {
+    int32_t n;
+    int32_t reserved;
+    float* pos;                 /* [n][4] x, y, z, inverse mass (0 = stopped/massless) */
+    float* pprev;               /* [n][4] x, y, z, unused */
+    float* vel;                 /* [n][4] vx, vy, vz, stopped flag (0/1) */
+    const float* mass;          /* [n] lumped mass */
+    const float* force;         /* [n][4] external force or NULL */
+    float* accum;               /* [n][4] Jacobi accumulator dP.xyz, dPw; zero between iterations */
+    const int32_t* vflags;      /* [n] or NULL: bits 0-7 attach material+1 (0 = none), bit 8 pin */
+    const float* attach_target; /* [n][4] x, y, z, restlength (ATTACH c_restvector / c_restlength) */
+    const float* pin_target;    /* [n][4] x, y, z, active (target_pos + rest_offset, pin_active) */
+} XpbdVerts;
+
+#define XPBD_VF_ATTACH_MASK 0xff
+#define XPBD_VF_PIN (1 << 8)
+
+/* Morton tiles of tets.  Tile t owns tets [tile_tptr[t], tile_tptr[t+1]) and
+ * the vertex list tile_verts[tile_vptr[t] .. tile_vptr[t+1]); the first
+ * tile_nint[t] of those are interior (touched by no other tile), the rest
+ * are tile-boundary vertices.  tet_q[t] = {l0 | l1<<16, l2 | l3<<16,
+ * material, bits of the signed rest volume V0}, l* being tile-local vertex
+ * indices (reference order pts[0..3], pts[3] the rest-matrix reference
+ * vertex).  The rest matrix B = inv(Dm) is row-major over
+ * tet_b0 = {B00,B01,B02,B10}, tet_b1 = {B11,B12,B20,B21}, tet_b2 = {B22}. */
+typedef struct XpbdTiles {
+    int32_t n_tets, n_tiles, n_boundary, max_tile_verts;
+    const int32_t* tile_vptr;  /* [n_tiles+1] */
+    const int32_t* tile_nint;  /* [n_tiles] */
+    const int32_t* tile_tptr;  /* [n_tiles+1] */
+    const int32_t* tile_verts; /* [tile_vptr[n_tiles]] global vertex ids */
+    const uint32_t* tet_q;     /* [n_tets][4] */
+    const float* tet_b0;       /* [n_tets][4] */
+    const float* tet_b1;       /* [n_tets][4] */
+    const float* tet_b2;       /* [n_tets] */
+    const float* tet_fiber;    /* [n_tets][4] f0.xyz, tendonmask; NULL without aniso */
+    const float* tet_act;      /* [n_tets] activation; NULL without aniso */
+    const int32_t* bnd_verts;  /* [n_boundary] boundary vertex ids */
+} XpbdTiles;
+
+/* Grid signed-distance field of the bones, phi[z][y][x], x fastest. */
+typedef struct XpbdSdf {
+    const float* phi;
+    int32_t nx, ny, nz;
+    float origin[3];
+    float h;               /* cell size (grid node spacing) */
+    float contact_offset;  /* push out until phi >= contact_offset */
+    float max_push;        /* > 0: ignore contacts deeper than this; <= 0: push all */
+    int32_t reserved;
+} XpbdSdf;
+
+typedef struct XpbdMetrics {
+    double vol_sum;        /* sum of signed tet volumes (calc_vol_error_kernel, engine.py:701) */
+    double resid_sq_sum;   /* sum of ARAP C^2 (arap_residual_accum_kernel, mg/kernel.py:86) */
+    float resid_max;       /* max ARAP C = ||sigma - 1|| */
+    int32_t n_inverted;    /* tets with det F <= 0 (count_inverted_tets_kernel, engine.py:410) */
+    int32_t n_nonfinite;   /* tets touching a non-finite position */
+    int32_t reserved;
+} XpbdMetrics;
+
+/* vertex_step ops, applied in this order to each vertex. */
+enum {
+    XPBD_OP_SDF = 1 << 0,      /* bone push-out (solve_mesh_contact_pos_kernel, sdf/kernel.py:122-170) */
+    XPBD_OP_VELOCITY = 1 << 1, /* update_velocities_kernel, engine.py:582-605 */
+    XPBD_OP_PREDICT = 1 << 2,  /* integrate_kernel, engine.py:431-464 */
+    XPBD_OP_PIN = 1 << 3,      /* pintotarget_overwrite_masked_kernel, mg/kernel.py:211-225 */
+};
+
+/* apply ops for xpbd_apply_all / xpbd_apply_boundary. */
+enum {
+    XPBD_APPLY_ATTACH = 1 << 0, /* add ATTACH corrections (solve_attach_kernel, solve_kernels.py:892) to accum */
+    XPBD_APPLY_DIVIDE = 1 << 1, /* pos += omega * dP / dPw (apply_dP_kernel, engine.py:689-698) */
+    XPBD_APPLY_PIN = 1 << 2,    /* pin overwrite (mg/kernel.py:211-225) */
+    XPBD_APPLY_CLEAR = 1 << 3,  /* zero accum after reading (clear_dP_kernel, engine.py:664) */
+};
+
+/* project modes */
+enum {
+    XPBD_PROJECT_FUSED = 0,      /* apply interior vertices in place, accumulate boundary ones */
+    XPBD_PROJECT_ACCUMULATE = 1, /* accumulate every vertex into accum (reference dP/dPw) */
+};
+
+int xpbd_abi_version(void);
+const char* xpbd_error_string(void);
+
+/* Fused per-vertex substep boundary: [push-out] -> [velocity] -> [predict] -> [pin].
+ * Replaces XpbdEngine.integrate (engine.py:798-809), update_velocities
+ * (engine.py:811-829), MultiGridSim.apply_pintotarget (mg/mg.py:1251-1261)
+ * and the AnimatedBoneMeshCollider push-out (example/humanV2.py:400-406). */
+int xpbd_vertex_step(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, const XpbdSdf* sdf,
+                     xpbd_stream_t stream);
+
+/* One Jacobi projection of every tet constraint.  Replaces
+ * XpbdEngine.solve_constraints / _dispatch_constraints (engine.py:1029-1052,
+ * 890-1027) and, in FUSED mode, apply_dP (engine.py:865) for interior
+ * vertices. */
+int xpbd_project(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v, int32_t mode,
+                 xpbd_stream_t stream);
+
+/* Finish a FUSED projection on the tile-boundary vertices: ATTACH, divide,
+ * pin, clear (apply ops as above). */
+int xpbd_apply_boundary(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v, uint32_t ops,
+                        xpbd_stream_t stream);
+
+/* Apply ops over every vertex (the unfused engine primitives: ATTACH
+ * accumulation of solve_constraints, apply_dP, apply_pintotarget, clear). */
+int xpbd_apply_all(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, xpbd_stream_t stream);
+
+/* Masked hard pin in the reference's own layout: pos4[pts[i]].xyz =
+ * target[i] + offset[i] where active[i] != 0 (target/offset are [n][3]).
+ * pintotarget_overwrite_masked_kernel, mg/kernel.py:211-225. */
+int xpbd_pin_overwrite_masked(int32_t n, const int32_t* pts, const float* target, const float* offset,
+                              const int32_t* active, float* pos4, xpbd_stream_t stream);
+
+/* Mesh metrics into out (device XpbdMetrics, zeroed by this call). */
+int xpbd_metrics(const XpbdTiles* tiles, const XpbdVerts* v, XpbdMetrics* out, xpbd_stream_t stream);
+
+/* Stream capture helpers (a captured substep replays as one graph launch). */
+int xpbd_graph_begin(xpbd_stream_t stream);
+int xpbd_graph_end(xpbd_stream_t stream, void** exec_out);
+int xpbd_graph_launch(void* exec, xpbd_stream_t stream);
+int xpbd_graph_destroy(void* exec);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XPBD_B200_H */

@@ -1,0 +1,124 @@
+"""ctypes binding of libxpbd_b200.so (include/xpbd_b200.h).
+
+The library is the product's only compute path: importing this module on a
+machine with a GPU and no built library raises instead of falling back to any
+Python or CPU implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+MAX_MATERIALS = 64
+MAX_ATTACH_MATERIALS = 16
+MAX_TILE_VERTS = 4096
+
+OK = 0
+MAT_ARAPSVD, MAT_VOLUME, MAT_ANISO, MAT_SNH, MAT_DAMPED = 1, 2, 4, 8, 16
+VF_ATTACH_MASK, VF_PIN = 0xFF, 1 << 8
+OP_SDF, OP_VELOCITY, OP_PREDICT, OP_PIN = 1, 2, 4, 8
+APPLY_ATTACH, APPLY_DIVIDE, APPLY_PIN, APPLY_CLEAR = 1, 2, 4, 8
+PROJECT_FUSED, PROJECT_ACCUMULATE = 0, 1
+
+
+class XpbdMaterial(C.Structure):
+    _fields_ = [("flags", C.c_uint32), ("arap_k", C.c_float), ("vol_k", C.c_float), ("vol_damp", C.c_float),
+                ("aniso_k", C.c_float), ("snh_mu", C.c_float), ("snh_lam", C.c_float), ("snh_damp", C.c_float)]
+
+
+class XpbdAttachMaterial(C.Structure):
+    _fields_ = [("k", C.c_float), ("damp", C.c_float)]
+
+
+class XpbdParams(C.Structure):
+    _fields_ = [("dt", C.c_float), ("gravity", C.c_float * 3), ("veldamping", C.c_float),
+                ("quasi_static", C.c_int32), ("omega", C.c_float), ("contraction_ratio", C.c_float),
+                ("fiber_stiffness_scale", C.c_float), ("n_materials", C.c_int32),
+                ("n_attach_materials", C.c_int32), ("reserved", C.c_int32),
+                ("materials", XpbdMaterial * MAX_MATERIALS),
+                ("attach", XpbdAttachMaterial * MAX_ATTACH_MATERIALS)]
+
+
+class XpbdVerts(C.Structure):
+    _fields_ = [("n", C.c_int32), ("reserved", C.c_int32), ("pos", C.c_void_p), ("pprev", C.c_void_p),
+                ("vel", C.c_void_p), ("mass", C.c_void_p), ("force", C.c_void_p), ("accum", C.c_void_p),
+                ("vflags", C.c_void_p), ("attach_target", C.c_void_p), ("pin_target", C.c_void_p)]
+
+
+class XpbdTiles(C.Structure):
+    _fields_ = [("n_tets", C.c_int32), ("n_tiles", C.c_int32), ("n_boundary", C.c_int32),
+                ("max_tile_verts", C.c_int32), ("tile_vptr", C.c_void_p), ("tile_nint", C.c_void_p),
+                ("tile_tptr", C.c_void_p), ("tile_verts", C.c_void_p), ("tet_q", C.c_void_p),
+                ("tet_b0", C.c_void_p), ("tet_b1", C.c_void_p), ("tet_b2", C.c_void_p),
+                ("tet_fiber", C.c_void_p), ("tet_act", C.c_void_p), ("bnd_verts", C.c_void_p)]
+
+
+class XpbdSdf(C.Structure):
+    _fields_ = [("phi", C.c_void_p), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("origin", C.c_float * 3), ("h", C.c_float), ("contact_offset", C.c_float),
+                ("max_push", C.c_float), ("reserved", C.c_int32)]
+
+
+class XpbdMetrics(C.Structure):
+    _fields_ = [("vol_sum", C.c_double), ("resid_sq_sum", C.c_double), ("resid_max", C.c_float),
+                ("n_inverted", C.c_int32), ("n_nonfinite", C.c_int32), ("reserved", C.c_int32)]
+
+
+P = C.c_void_p
+_SIGS = {
+    "xpbd_abi_version": ([], C.c_int),
+    "xpbd_error_string": ([], C.c_char_p),
+    "xpbd_vertex_step": ([C.POINTER(XpbdParams), C.POINTER(XpbdVerts), C.c_uint32, C.POINTER(XpbdSdf), P], C.c_int),
+    "xpbd_project": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), C.c_int32, P], C.c_int),
+    "xpbd_apply_boundary": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), C.c_uint32, P],
+                            C.c_int),
+    "xpbd_apply_all": ([C.POINTER(XpbdParams), C.POINTER(XpbdVerts), C.c_uint32, P], C.c_int),
+    "xpbd_pin_overwrite_masked": ([C.c_int32, P, P, P, P, P, P], C.c_int),
+    "xpbd_metrics": ([C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), P, P], C.c_int),
+    "xpbd_graph_begin": ([P], C.c_int),
+    "xpbd_graph_end": ([P, C.POINTER(C.c_void_p)], C.c_int),
+    "xpbd_graph_launch": ([P, P], C.c_int),
+    "xpbd_graph_destroy": ([P], C.c_int),
+}
+
+_LIB = None
+
+
+def lib_path() -> Path:
+    return Path(__file__).resolve().parent / "lib" / "libxpbd_b200.so"
+
+
+def load(build_if_missing: bool = False) -> C.CDLL:
+    """Load the CUDA library; raise if it is missing (there is no fallback)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = lib_path()
+    if not path.exists():
+        if build_if_missing:
+            from .build import build
+            build()
+        if not path.exists():
+            raise RuntimeError(f"{path} is not built; run `python -m rlmusclev2_b200.build` "
+                               "(the XPBD substep has no CPU fallback)")
+    lib = C.CDLL(str(path))
+    for name, (args, res) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIB = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+class XpbdError(RuntimeError):
+    pass
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        msg = load().xpbd_error_string()
+        raise XpbdError(f"libxpbd_b200 error {rc}: {msg.decode() if msg else ''}")

@@ -1,0 +1,556 @@
+// Core XPBD substep kernels for sm_100a and their C ABI (include/xpbd_b200.h).
+//
+// Hot loop per Jacobi iteration: k_project_tiles (one CTA per Morton tile of
+// tets: stage the tile's vertices in shared memory, project every constraint
+// of every tet, accumulate with shared-memory atomics, apply interior
+// vertices in place, push tile-boundary sums to a global float4 accumulator
+// with one vector reduction each) followed by k_apply_boundary (finish the
+// boundary vertices and clear their accumulator slots).  Between substeps a
+// single per-vertex kernel fuses push-out, velocity update, prediction and
+// pinning.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/xpbd_b200.h"
+#include "xpbd_device.cuh"
+
+using namespace xpbd;
+
+namespace {
+
+thread_local char g_err[256] = "";
+
+int fail(int code, const char* fmt, const char* detail = "") {
+    snprintf(g_err, sizeof(g_err), fmt, detail);
+    return code;
+}
+int cuda_check(const char* where) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
+        return XPBD_ERR_CUDA;
+    }
+    return XPBD_OK;
+}
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+constexpr int kTileThreads = 256;
+constexpr int kVertThreads = 256;
+
+// ---------------------------------------------------------------------------
+// Per-vertex finish of a Jacobi iteration: ATTACH, divide, pin.
+__device__ __forceinline__ void finish_vertex(const XpbdParams& prm, const XpbdVerts& V, int g, float4& p, float4 a,
+                                              uint32_t ops) {
+    int f = 0;
+    if (V.vflags) f = V.vflags[g];
+    if ((ops & XPBD_APPLY_ATTACH) && (f & XPBD_VF_ATTACH_MASK) && (f & XPBD_VF_ATTACH_MASK) <= prm.n_attach_materials) {
+        const XpbdAttachMaterial& M = prm.attach[(f & XPBD_VF_ATTACH_MASK) - 1];
+        if (M.k > 0.f) {
+            const float4 at = reinterpret_cast<const float4*>(V.attach_target)[g];
+            float3 prev = make_float3(0.f, 0.f, 0.f);
+            if (M.damp > 0.f) prev = f3(reinterpret_cast<const float4*>(V.pprev)[g]);
+            float3 d;
+            if (con_attach(p, prev, f3(at), at.w, M.k, M.damp, prm.dt, d)) {
+                a.x += d.x;
+                a.y += d.y;
+                a.z += d.z;
+                a.w += 1.f;
+            }
+        }
+    }
+    if ((ops & XPBD_APPLY_DIVIDE) && a.w > 1e-9f) {
+        float3 d = make_float3(a.x / a.w, a.y / a.w, a.z / a.w);
+        if (prm.omega != 1.f) d = prm.omega * d;
+        p.x += d.x;
+        p.y += d.y;
+        p.z += d.z;
+    }
+    if ((ops & XPBD_APPLY_PIN) && (f & XPBD_VF_PIN)) {
+        const float4 t = reinterpret_cast<const float4*>(V.pin_target)[g];
+        if (t.w != 0.f) {
+            p.x = t.x;
+            p.y = t.y;
+            p.z = t.z;
+        }
+    }
+}
+
+__device__ __forceinline__ void smem_add(float4* acc, int l, float3 d) {
+    atomicAdd(&acc[l].x, d.x);
+    atomicAdd(&acc[l].y, d.y);
+    atomicAdd(&acc[l].z, d.z);
+    atomicAdd(&acc[l].w, 1.f);
+}
+
+// ---------------------------------------------------------------------------
+template <int MODE, bool DAMP>
+__global__ void __launch_bounds__(kTileThreads, 2)
+    k_project_tiles(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdTiles T,
+                    const __grid_constant__ XpbdVerts V, uint32_t finish_ops) {
+    extern __shared__ float4 smem[];
+    const int tile = blockIdx.x;
+    const int vbeg = T.tile_vptr[tile];
+    const int nvt = T.tile_vptr[tile + 1] - vbeg;
+    const int nint = (MODE == XPBD_PROJECT_FUSED) ? T.tile_nint[tile] : 0;
+    float4* s_pos = smem;
+    float4* s_acc = smem + T.max_tile_verts;
+    float4* s_prev = smem + 2 * T.max_tile_verts;
+    const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
+    const float4* prev4 = reinterpret_cast<const float4*>(V.pprev);
+    for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
+        const int g = T.tile_verts[vbeg + i];
+        s_pos[i] = pos4[g];
+        s_acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (DAMP) s_prev[i] = prev4[g];
+    }
+    __syncthreads();
+
+    const int t1 = T.tile_tptr[tile + 1];
+    const uint4* tq = reinterpret_cast<const uint4*>(T.tet_q);
+    const float4* tb0 = reinterpret_cast<const float4*>(T.tet_b0);
+    const float4* tb1 = reinterpret_cast<const float4*>(T.tet_b1);
+    for (int t = T.tile_tptr[tile] + threadIdx.x; t < t1; t += blockDim.x) {
+        const uint4 q = tq[t];
+        const float4 b0 = tb0[t], b1 = tb1[t];
+        const float b2 = T.tet_b2[t];
+        const int l[4] = {int(q.x & 0xffffu), int(q.x >> 16), int(q.y & 0xffffu), int(q.y >> 16)};
+        const XpbdMaterial& m = prm.materials[min(int(q.z & 0xffu), XPBD_MAX_MATERIALS - 1)];
+        const float V0 = __uint_as_float(q.w);
+        M3 B;
+        B.m[0][0] = b0.x; B.m[0][1] = b0.y; B.m[0][2] = b0.z;
+        B.m[1][0] = b0.w; B.m[1][1] = b1.x; B.m[1][2] = b1.y;
+        B.m[2][0] = b1.z; B.m[2][1] = b1.w; B.m[2][2] = b2;
+        float4 p[4], pq[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            p[i] = s_pos[l[i]];
+            if (DAMP) pq[i] = s_prev[l[i]];
+        }
+        const float3 p3 = f3(p[3]);
+        const M3 F = deformation(f3(p[0]) - p3, f3(p[1]) - p3, f3(p[2]) - p3, B);
+        Corr4 c;
+        const uint32_t fl = m.flags;
+        // Same type order as the reference table (ascending ConstraintType tag).
+        if (fl & XPBD_MAT_SNH) {
+            if (con_snh(p, pq, B, F, V0, m.snh_mu, m.snh_lam, m.snh_damp, prm.dt, c))
+#pragma unroll
+                for (int i = 0; i < 4; ++i) smem_add(s_acc, l[i], c.d[i]);
+        }
+        if (fl & XPBD_MAT_VOLUME) {
+            if (con_volume(p, pq, V0, m.vol_k, m.vol_damp, prm.dt, c))
+#pragma unroll
+                for (int i = 0; i < 4; ++i) smem_add(s_acc, l[i], c.d[i]);
+        }
+        if (fl & XPBD_MAT_ANISO) {
+            const float4 fb = reinterpret_cast<const float4*>(T.tet_fiber)[t];
+            if (con_aniso(p, B, F, f3(fb), fb.w, T.tet_act[t], m.aniso_k, prm.contraction_ratio,
+                          prm.fiber_stiffness_scale, prm.dt, c))
+#pragma unroll
+                for (int i = 0; i < 4; ++i) smem_add(s_acc, l[i], c.d[i]);
+        }
+        if (fl & XPBD_MAT_ARAPSVD) {
+            if (con_arapsvd(p, B, F, m.arap_k, prm.dt, c))
+#pragma unroll
+                for (int i = 0; i < 4; ++i) smem_add(s_acc, l[i], c.d[i]);
+        }
+    }
+    __syncthreads();
+
+    float4* pos4w = reinterpret_cast<float4*>(V.pos);
+    float4* acc4 = reinterpret_cast<float4*>(V.accum);
+    if (MODE == XPBD_PROJECT_FUSED) {
+        // Interior vertices: every incident constraint lives in this tile, so
+        // the shared sum is complete and no other CTA reads this position.
+        for (int i = threadIdx.x; i < nint; i += blockDim.x) {
+            const int g = T.tile_verts[vbeg + i];
+            float4 pp = s_pos[i];
+            finish_vertex(prm, V, g, pp, s_acc[i], finish_ops);
+            pos4w[g] = pp;
+        }
+    }
+    for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
+        const float4 a = s_acc[i];
+        if (a.w != 0.f) atomicAdd(&acc4[T.tile_verts[vbeg + i]], a);
+    }
+}
+
+__global__ void __launch_bounds__(kVertThreads)
+    k_apply_list(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdVerts V, const int32_t* list,
+                 int n, uint32_t ops) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int g = list ? list[i] : i;
+    float4* acc4 = reinterpret_cast<float4*>(V.accum);
+    float4* pos4 = reinterpret_cast<float4*>(V.pos);
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ops & (XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_CLEAR)) a = acc4[g];
+    if (ops & XPBD_APPLY_CLEAR) {
+        if (a.x != 0.f || a.y != 0.f || a.z != 0.f || a.w != 0.f) acc4[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    float4 p = pos4[g];
+    const float4 p0 = p;
+    if ((ops & XPBD_APPLY_ATTACH) && !(ops & XPBD_APPLY_DIVIDE)) {
+        // accumulate-only: add the ATTACH term to the reference dP/dPw
+        const int f = V.vflags ? V.vflags[g] : 0;
+        if ((f & XPBD_VF_ATTACH_MASK) && (f & XPBD_VF_ATTACH_MASK) <= prm.n_attach_materials) {
+            const XpbdAttachMaterial& M = prm.attach[(f & XPBD_VF_ATTACH_MASK) - 1];
+            const float4 at = reinterpret_cast<const float4*>(V.attach_target)[g];
+            float3 prev = make_float3(0.f, 0.f, 0.f);
+            if (M.damp > 0.f) prev = f3(reinterpret_cast<const float4*>(V.pprev)[g]);
+            float3 d;
+            if (M.k > 0.f && con_attach(p, prev, f3(at), at.w, M.k, M.damp, prm.dt, d))
+                acc4[g] = make_float4(a.x + d.x, a.y + d.y, a.z + d.z, a.w + 1.f);
+        }
+        return;
+    }
+    finish_vertex(prm, V, g, p, a, ops);
+    if (p.x != p0.x || p.y != p0.y || p.z != p0.z) pos4[g] = p;
+}
+
+// ---------------------------------------------------------------------------
+// Trilinear grid SDF sample and gradient (phi at nodes origin + h*(i,j,k)).
+__device__ __forceinline__ bool sdf_sample(const XpbdSdf& S, float3 x, float& phi, float3& grad) {
+    const float inv_h = 1.f / S.h;
+    const float gx = (x.x - S.origin[0]) * inv_h, gy = (x.y - S.origin[1]) * inv_h, gz = (x.z - S.origin[2]) * inv_h;
+    if (!(gx >= 0.f && gy >= 0.f && gz >= 0.f && gx <= float(S.nx - 1) && gy <= float(S.ny - 1) && gz <= float(S.nz - 1)))
+        return false;
+    int ix = min(int(gx), S.nx - 2), iy = min(int(gy), S.ny - 2), iz = min(int(gz), S.nz - 2);
+    const float fx = gx - float(ix), fy = gy - float(iy), fz = gz - float(iz);
+    const size_t sx = 1, sy = size_t(S.nx), sz = size_t(S.nx) * size_t(S.ny);
+    const float* b = S.phi + size_t(iz) * sz + size_t(iy) * sy + size_t(ix);
+    const float c000 = __ldg(b), c100 = __ldg(b + sx), c010 = __ldg(b + sy), c110 = __ldg(b + sy + sx);
+    const float c001 = __ldg(b + sz), c101 = __ldg(b + sz + sx), c011 = __ldg(b + sz + sy), c111 = __ldg(b + sz + sy + sx);
+    const float c00 = c000 + fx * (c100 - c000), c10 = c010 + fx * (c110 - c010);
+    const float c01 = c001 + fx * (c101 - c001), c11 = c011 + fx * (c111 - c011);
+    const float c0 = c00 + fy * (c10 - c00), c1 = c01 + fy * (c11 - c01);
+    phi = c0 + fz * (c1 - c0);
+    // analytic gradient of the trilinear interpolant
+    const float dx0 = (c100 - c000) + fy * ((c110 - c010) - (c100 - c000));
+    const float dx1 = (c101 - c001) + fy * ((c111 - c011) - (c101 - c001));
+    const float dy0 = (c010 - c000) + fx * ((c110 - c100) - (c010 - c000));
+    const float dy1 = (c011 - c001) + fx * ((c111 - c101) - (c011 - c001));
+    grad = make_float3((dx0 + fz * (dx1 - dx0)) * inv_h, (dy0 + fz * (dy1 - dy0)) * inv_h, (c1 - c0) * inv_h);
+    return true;
+}
+
+// Push-out of one vertex (solve_mesh_contact_pos_kernel semantics with the
+// bone mesh query replaced by the grid SDF): err = phi - offset; if err < 0
+// (and depth <= max_push when max_push > 0) move along the outward normal.
+__device__ __forceinline__ void sdf_push(const XpbdSdf& S, float4& p) {
+    if (p.w == 0.f) return;
+    float phi;
+    float3 gr;
+    if (!sdf_sample(S, f3(p), phi, gr)) return;
+    const float gl = len(gr);
+    if (!(gl > 1e-12f)) return;
+    const float err = phi - S.contact_offset;
+    if (err < 0.f && (S.max_push <= 0.f || -err <= S.max_push)) {
+        const float3 n = gr / gl;
+        p.x -= n.x * err;
+        p.y -= n.y * err;
+        p.z -= n.z * err;
+    }
+}
+
+__global__ void __launch_bounds__(kVertThreads)
+    k_vertex_step(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdVerts V, uint32_t ops,
+                  const __grid_constant__ XpbdSdf S) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= V.n) return;
+    float4* pos4 = reinterpret_cast<float4*>(V.pos);
+    float4* prev4 = reinterpret_cast<float4*>(V.pprev);
+    float4* vel4 = reinterpret_cast<float4*>(V.vel);
+    float4 p = pos4[g];
+    float4 v = vel4[g];
+    float4 q;
+    const float dt = prm.dt;
+    if (ops & XPBD_OP_SDF) sdf_push(S, p);
+    if (ops & XPBD_OP_VELOCITY) {
+        q = prev4[g];
+        v.x = (p.x - q.x) / dt;
+        v.y = (p.y - q.y) / dt;
+        v.z = (p.z - q.z) / dt;
+    }
+    if (ops & XPBD_OP_PREDICT) {
+        q = make_float4(p.x, p.y, p.z, 0.f);
+        if (v.w != 0.f) {
+            v.x = v.y = v.z = 0.f;
+        } else {
+            float3 ext = make_float3(prm.gravity[0], prm.gravity[1], prm.gravity[2]);
+            const float m = V.mass[g];
+            if (V.force && m > 1.0e-12f) ext = ext + f3(reinterpret_cast<const float4*>(V.force)[g]) / m;
+            if (prm.quasi_static) {
+                const float dt2 = dt * dt;
+                p.x += dt2 * ext.x;
+                p.y += dt2 * ext.y;
+                p.z += dt2 * ext.z;
+                v.x = v.y = v.z = 0.f;
+            } else {
+                const float damp = 1.f - prm.veldamping;
+                v.x = damp * v.x + dt * ext.x;
+                v.y = damp * v.y + dt * ext.y;
+                v.z = damp * v.z + dt * ext.z;
+                p.x += dt * v.x;
+                p.y += dt * v.y;
+                p.z += dt * v.z;
+            }
+        }
+        prev4[g] = q;
+    }
+    if ((ops & XPBD_OP_PIN) && V.vflags && (V.vflags[g] & XPBD_VF_PIN)) {
+        const float4 t = reinterpret_cast<const float4*>(V.pin_target)[g];
+        if (t.w != 0.f) {
+            p.x = t.x;
+            p.y = t.y;
+            p.z = t.z;
+        }
+    }
+    pos4[g] = p;
+    if (ops & (XPBD_OP_VELOCITY | XPBD_OP_PREDICT)) vel4[g] = v;
+}
+
+__global__ void k_pin_masked(int n, const int32_t* pts, const float* target, const float* offset,
+                             const int32_t* active, float4* pos4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (active && active[i] == 0) return;
+    const int v = pts[i];
+    float4 p = pos4[v];
+    p.x = target[3 * i] + offset[3 * i];
+    p.y = target[3 * i + 1] + offset[3 * i + 1];
+    p.z = target[3 * i + 2] + offset[3 * i + 2];
+    pos4[v] = p;
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTileThreads)
+    k_metrics(const __grid_constant__ XpbdTiles T, const __grid_constant__ XpbdVerts V, XpbdMetrics* out) {
+    extern __shared__ float4 smem[];
+    const int tile = blockIdx.x;
+    const int vbeg = T.tile_vptr[tile];
+    const int nvt = T.tile_vptr[tile + 1] - vbeg;
+    const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
+    for (int i = threadIdx.x; i < nvt; i += blockDim.x) smem[i] = pos4[T.tile_verts[vbeg + i]];
+    __syncthreads();
+    double vol = 0.0, rsq = 0.0;
+    float rmax = 0.f;
+    int ninv = 0, nnan = 0;
+    const uint4* tq = reinterpret_cast<const uint4*>(T.tet_q);
+    const float4* tb0 = reinterpret_cast<const float4*>(T.tet_b0);
+    const float4* tb1 = reinterpret_cast<const float4*>(T.tet_b1);
+    for (int t = T.tile_tptr[tile] + threadIdx.x; t < T.tile_tptr[tile + 1]; t += blockDim.x) {
+        const uint4 q = tq[t];
+        const float4 b0 = tb0[t], b1 = tb1[t];
+        M3 B;
+        B.m[0][0] = b0.x; B.m[0][1] = b0.y; B.m[0][2] = b0.z;
+        B.m[1][0] = b0.w; B.m[1][1] = b1.x; B.m[1][2] = b1.y;
+        B.m[2][0] = b1.z; B.m[2][1] = b1.w; B.m[2][2] = T.tet_b2[t];
+        const float3 p0 = f3(smem[q.x & 0xffffu]), p1 = f3(smem[q.x >> 16]), p2 = f3(smem[q.y & 0xffffu]),
+                     p3 = f3(smem[q.y >> 16]);
+        const float s = p0.x + p0.y + p0.z + p1.x + p1.y + p1.z + p2.x + p2.y + p2.z + p3.x + p3.y + p3.z;
+        if (!isfinite(s)) {
+            ++nnan;
+            continue;
+        }
+        const M3 F = deformation(p0 - p3, p1 - p3, p2 - p3, B);
+        if (det3(F) <= 0.f) ++ninv;
+        const float3 d1 = p1 - p0, d2 = p2 - p0, d3 = p3 - p0;
+        vol += double(dot(cross(d2, d1), d3) / 6.f);
+        const Svd3 sv = svd3(F);
+        const float a = sv.s0 - 1.f, b = sv.s1 - 1.f, c = sv.s2 - 1.f;
+        const float csq = a * a + b * b + c * c;
+        rsq += double(csq);
+        rmax = fmaxf(rmax, sqrtf(csq));
+    }
+    // warp reduce then one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) {
+        vol += __shfl_down_sync(0xffffffffu, vol, o);
+        rsq += __shfl_down_sync(0xffffffffu, rsq, o);
+        rmax = fmaxf(rmax, __shfl_down_sync(0xffffffffu, rmax, o));
+        ninv += __shfl_down_sync(0xffffffffu, ninv, o);
+        nnan += __shfl_down_sync(0xffffffffu, nnan, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&out->vol_sum, vol);
+        atomicAdd(&out->resid_sq_sum, rsq);
+        atomicMax(reinterpret_cast<int*>(&out->resid_max), __float_as_int(rmax));  // rmax >= 0
+        atomicAdd(&out->n_inverted, ninv);
+        atomicAdd(&out->n_nonfinite, nnan);
+    }
+}
+
+int check_verts(const XpbdVerts* v) {
+    if (!v || v->n <= 0 || !v->pos) return fail(XPBD_ERR_ARG, "XpbdVerts: null or empty%s");
+    if (!aligned16(v->pos) || !aligned16(v->pprev) || !aligned16(v->vel) || !aligned16(v->accum) ||
+        !aligned16(v->force) || !aligned16(v->attach_target) || !aligned16(v->pin_target))
+        return fail(XPBD_ERR_ALIGN, "XpbdVerts: a [n][4] array is not 16-byte aligned%s");
+    if (v->vflags && (!v->attach_target || !v->pin_target))
+        return fail(XPBD_ERR_ARG, "XpbdVerts: vflags given without attach_target/pin_target%s");
+    return XPBD_OK;
+}
+int check_params(const XpbdParams* p) {
+    if (!p) return fail(XPBD_ERR_ARG, "XpbdParams: null%s");
+    if (p->n_materials < 0 || p->n_materials > XPBD_MAX_MATERIALS || p->n_attach_materials < 0 ||
+        p->n_attach_materials > XPBD_MAX_ATTACH_MATERIALS)
+        return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range%s");
+    if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0%s");
+    return XPBD_OK;
+}
+int check_tiles(const XpbdTiles* t) {
+    if (!t || t->n_tiles <= 0 || !t->tile_vptr || !t->tile_nint || !t->tile_tptr || !t->tile_verts || !t->tet_q ||
+        !t->tet_b0 || !t->tet_b1 || !t->tet_b2)
+        return fail(XPBD_ERR_ARG, "XpbdTiles: null member%s");
+    if (t->max_tile_verts <= 0 || t->max_tile_verts > XPBD_MAX_TILE_VERTS)
+        return fail(XPBD_ERR_LIMIT, "XpbdTiles: max_tile_verts out of range%s");
+    if (!aligned16(t->tet_q) || !aligned16(t->tet_b0) || !aligned16(t->tet_b1) || !aligned16(t->tet_fiber))
+        return fail(XPBD_ERR_ALIGN, "XpbdTiles: a [n][4] array is not 16-byte aligned%s");
+    return XPBD_OK;
+}
+
+bool any_damped(const XpbdParams* p) {
+    for (int i = 0; i < p->n_materials; ++i)
+        if (p->materials[i].flags & XPBD_MAT_DAMPED) return true;
+    return false;
+}
+bool any_aniso(const XpbdParams* p) {
+    for (int i = 0; i < p->n_materials; ++i)
+        if (p->materials[i].flags & XPBD_MAT_ANISO) return true;
+    return false;
+}
+
+template <int MODE, bool DAMP>
+int launch_project(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
+    const size_t smem = size_t(T->max_tile_verts) * sizeof(float4) * (DAMP ? 3 : 2);
+    if (smem > 48 * 1024) {
+        static unsigned char done[64];
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64 || !done[dev]) {
+            cudaFuncSetAttribute(k_project_tiles<MODE, DAMP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(XPBD_MAX_TILE_VERTS * sizeof(float4) * 3));
+            if (dev >= 0 && dev < 64) done[dev] = 1;
+        }
+    }
+    k_project_tiles<MODE, DAMP><<<T->n_tiles, kTileThreads, smem, s>>>(*prm, *T, *V, fops);
+    return cuda_check("xpbd_project");
+}
+
+}  // namespace
+
+extern "C" {
+
+int xpbd_abi_version(void) { return 1; }
+const char* xpbd_error_string(void) { return g_err; }
+
+int xpbd_vertex_step(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, const XpbdSdf* sdf,
+                     xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_params(prm)) || (rc = check_verts(v))) return rc;
+    if ((ops & XPBD_OP_SDF) && (!sdf || !sdf->phi || sdf->nx < 2 || sdf->ny < 2 || sdf->nz < 2 || !(sdf->h > 0.f)))
+        return fail(XPBD_ERR_ARG, "xpbd_vertex_step: XPBD_OP_SDF needs a valid XpbdSdf%s");
+    if ((ops & (XPBD_OP_VELOCITY | XPBD_OP_PREDICT)) && (!v->pprev || !v->vel))
+        return fail(XPBD_ERR_ARG, "xpbd_vertex_step: pprev/vel required%s");
+    if ((ops & XPBD_OP_PREDICT) && !v->mass) return fail(XPBD_ERR_ARG, "xpbd_vertex_step: mass required%s");
+    XpbdSdf S;
+    memset(&S, 0, sizeof(S));
+    if (sdf) S = *sdf;
+    k_vertex_step<<<(v->n + kVertThreads - 1) / kVertThreads, kVertThreads, 0, (cudaStream_t)stream>>>(*prm, *v, ops, S);
+    return cuda_check("xpbd_vertex_step");
+}
+
+int xpbd_project(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v, int32_t mode,
+                 xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_params(prm)) || (rc = check_tiles(tiles)) || (rc = check_verts(v))) return rc;
+    if (!v->accum) return fail(XPBD_ERR_ARG, "xpbd_project: accum required%s");
+    if (any_aniso(prm) && (!tiles->tet_fiber || !tiles->tet_act))
+        return fail(XPBD_ERR_ARG, "xpbd_project: aniso materials need tet_fiber and tet_act%s");
+    const bool damp = any_damped(prm);
+    if (damp && !v->pprev) return fail(XPBD_ERR_ARG, "xpbd_project: damped materials need pprev%s");
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t fops = XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_PIN;
+    if (mode == XPBD_PROJECT_FUSED)
+        return damp ? launch_project<XPBD_PROJECT_FUSED, true>(prm, tiles, v, fops, s)
+                    : launch_project<XPBD_PROJECT_FUSED, false>(prm, tiles, v, fops, s);
+    if (mode == XPBD_PROJECT_ACCUMULATE)
+        return damp ? launch_project<XPBD_PROJECT_ACCUMULATE, true>(prm, tiles, v, 0, s)
+                    : launch_project<XPBD_PROJECT_ACCUMULATE, false>(prm, tiles, v, 0, s);
+    return fail(XPBD_ERR_ARG, "xpbd_project: unknown mode%s");
+}
+
+int xpbd_apply_boundary(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v, uint32_t ops,
+                        xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_params(prm)) || (rc = check_verts(v))) return rc;
+    if (!tiles || (tiles->n_boundary > 0 && !tiles->bnd_verts)) return fail(XPBD_ERR_ARG, "xpbd_apply_boundary: tiles%s");
+    if (!v->accum) return fail(XPBD_ERR_ARG, "xpbd_apply_boundary: accum required%s");
+    if (tiles->n_boundary == 0) return XPBD_OK;
+    k_apply_list<<<(tiles->n_boundary + kVertThreads - 1) / kVertThreads, kVertThreads, 0, (cudaStream_t)stream>>>(
+        *prm, *v, tiles->bnd_verts, tiles->n_boundary, ops);
+    return cuda_check("xpbd_apply_boundary");
+}
+
+int xpbd_apply_all(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_params(prm)) || (rc = check_verts(v))) return rc;
+    if ((ops & (XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_CLEAR)) && !v->accum)
+        return fail(XPBD_ERR_ARG, "xpbd_apply_all: accum required%s");
+    k_apply_list<<<(v->n + kVertThreads - 1) / kVertThreads, kVertThreads, 0, (cudaStream_t)stream>>>(*prm, *v, nullptr,
+                                                                                                       v->n, ops);
+    return cuda_check("xpbd_apply_all");
+}
+
+int xpbd_pin_overwrite_masked(int32_t n, const int32_t* pts, const float* target, const float* offset,
+                              const int32_t* active, float* pos4, xpbd_stream_t stream) {
+    if (n < 0 || (n > 0 && (!pts || !target || !offset || !pos4)))
+        return fail(XPBD_ERR_ARG, "xpbd_pin_overwrite_masked: bad arguments%s");
+    if (!aligned16(pos4)) return fail(XPBD_ERR_ALIGN, "xpbd_pin_overwrite_masked: pos4 alignment%s");
+    if (n == 0) return XPBD_OK;
+    k_pin_masked<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, pts, target, offset, active,
+                                                                    reinterpret_cast<float4*>(pos4));
+    return cuda_check("xpbd_pin_overwrite_masked");
+}
+
+int xpbd_metrics(const XpbdTiles* tiles, const XpbdVerts* v, XpbdMetrics* out, xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_tiles(tiles)) || (rc = check_verts(v))) return rc;
+    if (!out) return fail(XPBD_ERR_ARG, "xpbd_metrics: out%s");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemsetAsync(out, 0, sizeof(XpbdMetrics), s) != cudaSuccess) return cuda_check("xpbd_metrics memset");
+    const size_t smem = size_t(tiles->max_tile_verts) * sizeof(float4);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_metrics, cudaFuncAttributeMaxDynamicSharedMemorySize, int(XPBD_MAX_TILE_VERTS * sizeof(float4)));
+    k_metrics<<<tiles->n_tiles, kTileThreads, smem, s>>>(*tiles, *v, out);
+    return cuda_check("xpbd_metrics");
+}
+
+int xpbd_graph_begin(xpbd_stream_t stream) {
+    if (cudaStreamBeginCapture((cudaStream_t)stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return cuda_check("xpbd_graph_begin");
+    return XPBD_OK;
+}
+int xpbd_graph_end(xpbd_stream_t stream, void** exec_out) {
+    if (!exec_out) return fail(XPBD_ERR_ARG, "xpbd_graph_end: exec_out%s");
+    cudaGraph_t g = nullptr;
+    if (cudaStreamEndCapture((cudaStream_t)stream, &g) != cudaSuccess) return cuda_check("xpbd_graph_end");
+    cudaGraphExec_t e = nullptr;
+    cudaError_t err = cudaGraphInstantiate(&e, g, 0);
+    cudaGraphDestroy(g);
+    if (err != cudaSuccess) return cuda_check("xpbd_graph_end instantiate");
+    *exec_out = e;
+    return XPBD_OK;
+}
+int xpbd_graph_launch(void* exec, xpbd_stream_t stream) {
+    if (!exec) return fail(XPBD_ERR_ARG, "xpbd_graph_launch: exec%s");
+    if (cudaGraphLaunch((cudaGraphExec_t)exec, (cudaStream_t)stream) != cudaSuccess)
+        return cuda_check("xpbd_graph_launch");
+    return XPBD_OK;
+}
+int xpbd_graph_destroy(void* exec) {
+    if (!exec) return XPBD_OK;
+    if (cudaGraphExecDestroy((cudaGraphExec_t)exec) != cudaSuccess) return cuda_check("xpbd_graph_destroy");
+    return XPBD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,363 @@
+// Device math and per-constraint XPBD projections for sm_100a.
+//
+// Each constraint function restates one reference Warp kernel
+// (chunleili/rlmuscleV2 src/muscle/constraint/solve_kernels.py) for the
+// Jacobi path (use_jacobi=1, Lagrange multipliers zeroed every iteration so
+// L == 0), returning the per-vertex position deltas that the reference
+// passes to update_dP (solve_kernels.py:52-56).  Positions arrive as float4
+// with the inverse mass in .w (get_inv_mass_fn, solve_kernels.py:71-80, is
+// folded into that lane at upload time).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace xpbd {
+
+struct M3 { float m[3][3]; };
+
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return make_float3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float3 operator/(float3 a, float s) { return make_float3(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross(float3 a, float3 b) {
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float len(float3 a) { return sqrtf(dot(a, a)); }
+
+// F = Ds * B with Ds columns (c0, c1, c2) -- engine.py / solve_kernels.py layout.
+__device__ __forceinline__ M3 deformation(float3 c0, float3 c1, float3 c2, const M3& B) {
+    const float d[3][3] = {{c0.x, c1.x, c2.x}, {c0.y, c1.y, c2.y}, {c0.z, c1.z, c2.z}};
+    M3 F;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) F.m[i][j] = d[i][0] * B.m[0][j] + d[i][1] * B.m[1][j] + d[i][2] * B.m[2][j];
+    return F;
+}
+
+__device__ __forceinline__ float det3(const M3& M) {
+    return M.m[0][0] * (M.m[1][1] * M.m[2][2] - M.m[1][2] * M.m[2][1])
+         - M.m[0][1] * (M.m[1][0] * M.m[2][2] - M.m[1][2] * M.m[2][0])
+         + M.m[0][2] * (M.m[1][0] * M.m[2][1] - M.m[1][1] * M.m[2][0]);
+}
+
+// grad_k[a] = sum_j G[a][j] * B[k][j]   (solve_kernels.py:1276-1288)
+__device__ __forceinline__ float3 grad_row(const M3& G, const M3& B, int k) {
+    return make_float3(G.m[0][0] * B.m[k][0] + G.m[0][1] * B.m[k][1] + G.m[0][2] * B.m[k][2],
+                       G.m[1][0] * B.m[k][0] + G.m[1][1] * B.m[k][1] + G.m[1][2] * B.m[k][2],
+                       G.m[2][0] * B.m[k][0] + G.m[2][1] * B.m[k][1] + G.m[2][2] * B.m[k][2]);
+}
+
+// ---------------------------------------------------------------------------
+// Sign-fixed 3x3 SVD: F = U diag(s) V^T with U, V rotations, s0 >= s1 >= |s2|,
+// sign(s2) = sign(det F) -- the factorisation ssvd_fn (solve_kernels.py:85-112)
+// produces.  Method: cyclic Jacobi eigen-decomposition of the symmetric
+// S = F^T F (Jacobi rotations with the Rutishauser update formulas, Golub &
+// Van Loan sec. 8.5), eigenvalues sorted descending, then U is built from
+// F V: u0 = F v0/|F v0|, u1 by Gram-Schmidt, u2 = u0 x u1, so U is a rotation
+// by construction and s2 = u2 . (F v2) carries the sign of det F.  Singular
+// values are read off |F v_k| (second-order accurate in the eigenvector
+// error), not sqrt of the eigenvalues.
+struct Svd3 {
+    float3 u0, u1, u2;  // columns of U
+    float3 v0, v1, v2;  // columns of V
+    float s0, s1, s2;
+};
+
+__device__ __forceinline__ void jacobi_rot(float& spp, float& sqq, float& spq, float& srp, float& srq,
+                                           float3& vp, float3& vq) {
+    if (spq == 0.f) return;
+    const float theta = (sqq - spp) / (2.f * spq);
+    const float t = copysignf(1.f, theta) / (fabsf(theta) + sqrtf(fmaf(theta, theta, 1.f)));
+    const float c = 1.f / sqrtf(fmaf(t, t, 1.f));
+    const float s = t * c;
+    spp = fmaf(-t, spq, spp);
+    sqq = fmaf(t, spq, sqq);
+    spq = 0.f;
+    const float rp = srp, rq = srq;
+    srp = c * rp - s * rq;
+    srq = s * rp + c * rq;
+    const float3 a = vp, b = vq;
+    vp = make_float3(c * a.x - s * b.x, c * a.y - s * b.y, c * a.z - s * b.z);
+    vq = make_float3(s * a.x + c * b.x, s * a.y + c * b.y, s * a.z + c * b.z);
+}
+
+__device__ __forceinline__ void swap3(float3& a, float3& b) { float3 t = a; a = b; b = t; }
+
+__device__ __forceinline__ Svd3 svd3(const M3& F) {
+    // S = F^T F (upper triangle)
+    float s00 = F.m[0][0] * F.m[0][0] + F.m[1][0] * F.m[1][0] + F.m[2][0] * F.m[2][0];
+    float s01 = F.m[0][0] * F.m[0][1] + F.m[1][0] * F.m[1][1] + F.m[2][0] * F.m[2][1];
+    float s02 = F.m[0][0] * F.m[0][2] + F.m[1][0] * F.m[1][2] + F.m[2][0] * F.m[2][2];
+    float s11 = F.m[0][1] * F.m[0][1] + F.m[1][1] * F.m[1][1] + F.m[2][1] * F.m[2][1];
+    float s12 = F.m[0][1] * F.m[0][2] + F.m[1][1] * F.m[1][2] + F.m[2][1] * F.m[2][2];
+    float s22 = F.m[0][2] * F.m[0][2] + F.m[1][2] * F.m[1][2] + F.m[2][2] * F.m[2][2];
+    Svd3 r;
+    r.v0 = make_float3(1.f, 0.f, 0.f);
+    r.v1 = make_float3(0.f, 1.f, 0.f);
+    r.v2 = make_float3(0.f, 0.f, 1.f);
+#pragma unroll 1
+    for (int sweep = 0; sweep < 5; ++sweep) {
+        const float off = s01 * s01 + s02 * s02 + s12 * s12;
+        const float dia = s00 * s00 + s11 * s11 + s22 * s22;
+        if (off <= 1e-15f * dia) break;
+        // plane (0,1), third index 2: s20=s02, s21=s12
+        jacobi_rot(s00, s11, s01, s02, s12, r.v0, r.v1);
+        // plane (0,2), third index 1: s10=s01, s12
+        jacobi_rot(s00, s22, s02, s01, s12, r.v0, r.v2);
+        // plane (1,2), third index 0: s01, s02
+        jacobi_rot(s11, s22, s12, s01, s02, r.v1, r.v2);
+    }
+    // sort eigenvalues descending (columns of V follow)
+    float l0 = s00, l1 = s11, l2 = s22, tl;
+    if (l1 > l0) { tl = l0; l0 = l1; l1 = tl; swap3(r.v0, r.v1); }
+    if (l2 > l0) { tl = l0; l0 = l2; l2 = tl; swap3(r.v0, r.v2); }
+    if (l2 > l1) { tl = l1; l1 = l2; l2 = tl; swap3(r.v1, r.v2); }
+    if (dot(r.v0, cross(r.v1, r.v2)) < 0.f) r.v2 = -r.v2;
+    auto Fv = [&](float3 v) {
+        return make_float3(F.m[0][0] * v.x + F.m[0][1] * v.y + F.m[0][2] * v.z,
+                           F.m[1][0] * v.x + F.m[1][1] * v.y + F.m[1][2] * v.z,
+                           F.m[2][0] * v.x + F.m[2][1] * v.y + F.m[2][2] * v.z);
+    };
+    const float3 b0 = Fv(r.v0), b1 = Fv(r.v1), b2 = Fv(r.v2);
+    const float n0 = len(b0);
+    r.u0 = n0 > 1e-30f ? b0 / n0 : make_float3(1.f, 0.f, 0.f);
+    r.s0 = n0;
+    const float pr = dot(r.u0, b1);
+    const float3 w = b1 - pr * r.u0;
+    const float n1 = len(w);
+    if (n1 > 1e-30f * fmaxf(n0, 1.f)) {
+        r.u1 = w / n1;
+    } else {
+        const float a0 = fabsf(r.u0.x), a1 = fabsf(r.u0.y), a2 = fabsf(r.u0.z);
+        float3 e = (a0 <= a1 && a0 <= a2) ? make_float3(1.f, 0.f, 0.f)
+                   : (a1 <= a2 ? make_float3(0.f, 1.f, 0.f) : make_float3(0.f, 0.f, 1.f));
+        float3 c = cross(r.u0, e);
+        r.u1 = c / len(c);
+    }
+    r.s1 = dot(r.u1, b1);
+    r.u2 = cross(r.u0, r.u1);
+    r.s2 = dot(r.u2, b2);
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Material table entry (constraints a tet carries and their parameters).
+enum : uint32_t {
+    MAT_ARAPSVD = 1u << 0,
+    MAT_VOLUME = 1u << 1,
+    MAT_ANISO = 1u << 2,
+    MAT_SNH = 1u << 3,
+    MAT_DAMPED = 1u << 4,  // some constraint of this material reads pprev
+};
+
+struct Corr4 {
+    float3 d[4];
+};
+
+// solve_tetarap_svd_kernel, solve_kernels.py:1194-1307 (Jacobi branch).
+__device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float k, float dt, Corr4& out) {
+    const Svd3 s = svd3(F);
+    const float a = s.s0 - 1.f, b = s.s1 - 1.f, c = s.s2 - 1.f;
+    const float ssq = a * a + b * b + c * c;
+    if (ssq < 1.0e-12f) return false;
+    const float C = sqrtf(ssq);
+    const float invC = 1.f / C;
+    const float d0 = invC * a, d1 = invC * b, d2 = invC * c;
+    const float U[3][3] = {{s.u0.x, s.u1.x, s.u2.x}, {s.u0.y, s.u1.y, s.u2.y}, {s.u0.z, s.u1.z, s.u2.z}};
+    const float V[3][3] = {{s.v0.x, s.v1.x, s.v2.x}, {s.v0.y, s.v1.y, s.v2.y}, {s.v0.z, s.v1.z, s.v2.z}};
+    M3 G;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) G.m[i][j] = U[i][0] * V[j][0] * d0 + U[i][1] * V[j][1] * d1 + U[i][2] * V[j][2] * d2;
+    float3 g[4];
+    g[0] = grad_row(G, B, 0);
+    g[1] = grad_row(G, B, 1);
+    g[2] = grad_row(G, B, 2);
+    g[3] = (-g[0] - g[1]) - g[2];
+    const float wsum = p[0].w * dot(g[0], g[0]) + p[1].w * dot(g[1], g[1]) + p[2].w * dot(g[2], g[2]) + p[3].w * dot(g[3], g[3]);
+    if (wsum == 0.f) return false;
+    const float alpha = 1.f / k;
+    const float at = alpha / (dt * dt);
+    const float dL = -C / (wsum + at);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out.d[i] = (dL * p[i].w) * g[i];
+    return true;
+}
+
+// solve_tetvolume_kernel + tet_volume_update_xpbd_fn, solve_kernels.py:553-585, 187-281.
+__device__ __forceinline__ bool con_volume(const float4 p[4], const float4* q, float V0, float k, float kd, float dt,
+                                           Corr4& out) {
+    const float3 p3 = f3(p[3]);
+    const float3 d0 = f3(p[0]) - p3, d1 = f3(p[1]) - p3, d2 = f3(p[2]) - p3;
+    float3 g[4];
+    g[0] = cross(d1, d2) / 6.f;
+    g[1] = cross(d2, d0) / 6.f;
+    g[2] = cross(d0, d1) / 6.f;
+    g[3] = -((g[0] + g[1]) + g[2]);
+    const float ws = p[0].w * dot(g[0], g[0]) + p[1].w * dot(g[1], g[1]) + p[2].w * dot(g[2], g[2]) + p[3].w * dot(g[3], g[3]);
+    if (!(ws > 1e-9f)) return false;
+    const float volume = dot(cross(d0, d1), d2) / 6.f;
+    float alpha = 1.f / k;
+    alpha = alpha / (dt * dt);
+    const float C = volume - V0;
+    float dsum = 0.f, gamma = 1.f;
+    if (kd > 0.f) {
+        const float beta = k * kd * dt * dt;
+        gamma = alpha * beta / dt;
+        dsum = dot(g[0], f3(p[0]) - f3(q[0])) + dot(g[1], f3(p[1]) - f3(q[1])) + dot(g[2], f3(p[2]) - f3(q[2])) +
+               dot(g[3], f3(p[3]) - f3(q[3]));
+        dsum = dsum * gamma;
+        gamma = gamma + 1.f;
+    }
+    const float dl = (-C - dsum) / (gamma * ws + alpha);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out.d[i] = (dl * p[i].w) * g[i];
+    return true;
+}
+
+// solve_tet_aniso_arap_kernel, solve_kernels.py:1310-1426.  f0 is the
+// normalised mean fiber direction of the tet's 4 vertices (static, built at
+// upload); a zero f0 marks a tet whose mean fiber vanished (fn < 1e-9).
+__device__ __forceinline__ bool con_aniso(const float4 p[4], const M3& B, const M3& F, float3 f0, float tendon,
+                                          float act, float k, float ratio, float kscale, float dt, Corr4& out) {
+    const float3 d = make_float3(F.m[0][0] * f0.x + F.m[0][1] * f0.y + F.m[0][2] * f0.z,
+                                 F.m[1][0] * f0.x + F.m[1][1] * f0.y + F.m[1][2] * f0.z,
+                                 F.m[2][0] * f0.x + F.m[2][1] * f0.y + F.m[2][2] * f0.z);
+    const float s = len(d);
+    if (s < 1.0e-9f) return false;
+    const float detF = det3(F);
+    if (detF <= 0.f || s > 1.5f) return false;
+    const float belly = 1.f - tendon;
+    const float fiberscale = 1.f - belly * act * ratio;
+    const float diff = s - fiberscale;
+    const float C = 0.5f * diff * diff;
+    const float gs = diff / s;
+    const float dd[3] = {d.x, d.y, d.z}, ff[3] = {f0.x, f0.y, f0.z};
+    M3 G;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) G.m[i][j] = gs * (dd[i] * ff[j]);
+    float3 g[4];
+    g[0] = grad_row(G, B, 0);
+    g[1] = grad_row(G, B, 1);
+    g[2] = grad_row(G, B, 2);
+    g[3] = (-g[0] - g[1]) - g[2];
+    const float wsum = p[0].w * dot(g[0], g[0]) + p[1].w * dot(g[1], g[1]) + p[2].w * dot(g[2], g[2]) + p[3].w * dot(g[3], g[3]);
+    if (wsum < 1.0e-20f) return false;
+    const float sv = k * kscale;
+    const float at = (1.f / sv) / (dt * dt);
+    const float dL = -C / (wsum + at);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out.d[i] = (dL * p[i].w) * g[i];
+    return true;
+}
+
+// solve_tetsnh_kernel + tet_snh_update_xpbd_fn, solve_kernels.py:1587-1617, 1429-1584.
+__device__ __forceinline__ bool con_snh(const float4 p[4], const float4* q, const M3& B, const M3& F, float V0,
+                                        float mu, float lam, float kd, float dt, Corr4& out) {
+    float Ic = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Ic += F.m[i][j] * F.m[i][j];
+    const float rs = sqrtf(fmaxf(Ic, 1.0e-12f));
+    const float dC = rs - 1.7320508075688772f;
+    if (rs < 1.0e-6f) return false;
+    const float inv_rs = 1.f / rs;
+    M3 Fn;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Fn.m[i][j] = F.m[i][j] * inv_rs;
+    float3 dg[4], hg[4];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        dg[k] = make_float3(B.m[k][0] * Fn.m[0][0] + B.m[k][1] * Fn.m[0][1] + B.m[k][2] * Fn.m[0][2],
+                            B.m[k][0] * Fn.m[1][0] + B.m[k][1] * Fn.m[1][1] + B.m[k][2] * Fn.m[1][2],
+                            B.m[k][0] * Fn.m[2][0] + B.m[k][1] * Fn.m[2][1] + B.m[k][2] * Fn.m[2][2]);
+    dg[3] = (-dg[0] - dg[1]) - dg[2];
+    float dsw = 0.f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dsw += p[i].w * dot(dg[i], dg[i]);
+    if (dsw == 0.f) return false;
+    const float asnh = 1.f + mu / lam;
+    const float hC = det3(F) - asnh;
+    const float3 p3 = f3(p[3]);
+    const float3 c0 = f3(p[0]) - p3, c1 = f3(p[1]) - p3, c2 = f3(p[2]) - p3;
+    const float av = fmaxf(fabsf(V0), 1.0e-20f);
+    const float inv_detDm = 1.f / fmaxf(fabsf(V0) * 6.f, 1.0e-20f);
+    hg[0] = inv_detDm * cross(c1, c2);
+    hg[1] = inv_detDm * cross(c2, c0);
+    hg[2] = inv_detDm * cross(c0, c1);
+    hg[3] = (-hg[0] - hg[1]) - hg[2];
+    float hsw = 0.f, dh = 0.f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) hsw += p[i].w * dot(hg[i], hg[i]);
+    if (hsw == 0.f) return false;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dh += p[i].w * dot(dg[i], hg[i]);
+    const float dalpha = 1.f / (mu * av * dt * dt);
+    const float halpha = 1.f / (lam * av * dt * dt);
+    float ddamp = 0.f, dgam = 1.f, hdamp = 0.f, hgam = 1.f;
+    if (kd > 0.f) {
+        const float dbeta = mu * av * kd * dt * dt, hbeta = lam * av * kd * dt * dt;
+        dgam = dalpha * dbeta / dt;
+        hgam = halpha * hbeta / dt;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float3 dv = f3(p[i]) - f3(q[i]);
+            ddamp += dot(dg[i], dv);
+            hdamp += dot(hg[i], dv);
+        }
+        ddamp = ddamp * dgam;
+        hdamp = hdamp * hgam;
+        dgam = dgam + 1.f;
+        hgam = hgam + 1.f;
+    }
+    const float Axx = dgam * dsw + dalpha, Ayy = hgam * hsw + halpha;
+    const float detA = Axx * Ayy - dh * dh;
+    if (detA < 1.0e-8f) return false;
+    const float invd = 1.f / detA;
+    const float db = -dC - ddamp;
+    const float hb = -hC - hdamp;
+    const float ddL = invd * (Ayy * db - dh * hb);
+    const float hdL = invd * (Axx * hb - dh * db);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out.d[i] = p[i].w * (ddL * dg[i] + hdL * hg[i]);
+    return true;
+}
+
+// attach_bilateral_update_fn (Jacobi branch), solve_kernels.py:462-526, for
+// restlength-parameterised point attachment to a target.  Returns the delta
+// for the attached vertex.
+__device__ __forceinline__ bool con_attach(float4 p, float3 prev, float3 tgt, float restlength, float k, float kd,
+                                           float dt, float3& out) {
+    const float im = p.w;
+    if (im == 0.f) return false;
+    float3 n = f3(p) - tgt;
+    const float d = len(n);
+    if (!(d >= 1.0e-6f)) return false;
+    float alpha = 1.f / k;
+    alpha = alpha / (dt * dt);
+    const float C = d - restlength;
+    n = n / d;
+    float dsum = 0.f, gamma = 1.f;
+    if (kd > 0.f) {
+        const float beta = k * kd * dt * dt;
+        gamma = alpha * beta / dt;
+        dsum = gamma * dot(n, f3(p) - prev);
+        gamma = gamma + 1.f;
+    }
+    const float dL = (-C - dsum) / (gamma * im + alpha);
+    const float3 dp = (-dL) * n;
+    out = (-im) * dp;
+    return true;
+}
+
+}  // namespace xpbd

@@ -1,0 +1,155 @@
+"""MuscleSim on the sm_100a engine (reference: src/muscle/musclesim.py).
+
+``MuscleSim.from_procedural`` (musclesim.py:181-287) is the no-asset entry
+point; file-based construction needs the reference's Houdini/USD readers,
+which are not part of this project.
+"""
+from __future__ import annotations
+
+from types import SimpleNamespace
+
+import numpy as np
+
+from . import _capi as capi
+from .builder import collect_raw_constraints, lumped_mass
+from .engine import XpbdEngine
+
+
+class MuscleSim(XpbdEngine):
+    """XPBD muscle simulator: one Jacobi projection per substep."""
+
+    def __init__(self, cfg):
+        raise NotImplementedError("MuscleSim(cfg) loads .geo/.usd assets, which this project does not read; "
+                                  "use MuscleSim.from_procedural(...)")
+
+    @classmethod
+    def from_procedural(cls, vertices, tets, fiber_dirs_per_tet, bone_targets=None, *, constraint_configs, dts,
+                        num_substeps=1, device="cuda:0", density=1060.0, veldamping=0.02, gravity=0.0, sigma0=0.0,
+                        lambda_opt=1.0, contraction_ratio=0.0, fiber_stiffness_scale=1.0, v_max_norm=0.0,
+                        d_damp=0.0, stopped=None, relaxation=1.0, tile_tets=None, tet_masks=None):
+        """Build a MuscleSim from mesh arrays (musclesim.py:181-287).
+
+        Extra keywords beyond the reference: ``stopped`` (per-vertex kinematic
+        flags, equivalent to assigning ``sim.stopped`` afterwards),
+        ``relaxation`` (scale of the averaged Jacobi correction; 1 reproduces
+        the reference's apply_dP), ``tile_tets`` (tile size of the tet pass)
+        and ``tet_masks`` (restrict a named constraint config to a tet subset).
+        """
+        if float(sigma0) > 0.0:
+            raise NotImplementedError("explicit active fiber force (sigma0 > 0) is not on the sm_100a path")
+        vertices = np.asarray(vertices, dtype=np.float32)
+        tets = np.asarray(tets, dtype=np.int32)
+        n_v = vertices.shape[0]
+        fd = np.asarray(fiber_dirs_per_tet, dtype=np.float32).reshape(-1, 3)
+        # per-tet -> per-vertex fiber average (musclesim.py:226-234)
+        vf = np.zeros((n_v, 3), dtype=np.float32)
+        vc = np.zeros(n_v, dtype=np.float32)
+        np.add.at(vf, tets.reshape(-1), np.repeat(fd, 4, axis=0))
+        np.add.at(vc, tets.reshape(-1), np.float32(1.0))
+        vc = np.maximum(vc, np.float32(1.0))
+        vf /= vc[:, None]
+        vf /= np.maximum(np.linalg.norm(vf, axis=1, keepdims=True), np.float32(1e-8))
+        cfg = SimpleNamespace(
+            geo_path="<procedural>", bone_geo_path="<none>", gui=False, render_mode="none",
+            constraints=list(constraint_configs), dt=dts, num_substeps=num_substeps, gravity=gravity,
+            density=density, veldamping=veldamping, contraction_ratio=contraction_ratio,
+            fiber_stiffness_scale=fiber_stiffness_scale, HAS_compressstiffness=False, arch=device,
+            activation=0.0, nsteps=1, sigma0=sigma0, lambda_opt=lambda_opt, v_max_norm=v_max_norm, d_damp=d_damp,
+            relaxation=relaxation)
+        sim = object.__new__(cls)
+        sim.cfg = cfg
+        sim.constraint_configs = cfg.constraints
+        sim.pos0_np = vertices
+        sim.tet_np = tets
+        sim.v_fiber_np = vf
+        sim.v_tendonmask_np = None
+        sim.n_verts = n_v
+        sim.bone_pos = (np.asarray(bone_targets, np.float32) if bone_targets is not None
+                        else np.zeros((0, 3), np.float32))
+        sim.use_jacobi = True
+        sim.use_colored_gs = False
+        sim.contraction_ratio = contraction_ratio
+        sim.fiber_stiffness_scale = fiber_stiffness_scale
+        sim.has_compressstiffness = False
+        sim.num_substeps = int(num_substeps)
+        sim.quasi_static = False
+        sim.step_cnt = 0
+        sim.renderer = None
+        mass, rest_volume = lumped_mass(vertices, tets, density)
+        sim.rest_volume_np = rest_volume
+        sim.total_rest_volume = float(rest_volume.astype(np.float64).sum())
+        table = collect_raw_constraints(vertices, tets, sim.constraint_configs, tet_masks).sorted_by_type()
+        sim.raw_constraints = table
+        st = np.zeros(n_v, np.int32) if stopped is None else np.asarray(stopped, np.int32)
+        sim._setup_device(device, mass=mass, stopped=st, table=table, v_fiber=vf, tet_tendonmask=None,
+                          dt=float(dts) / int(num_substeps), gravity_vec=(0.0, float(gravity), 0.0),
+                          veldamping=float(veldamping), quasi_static=False, omega=float(relaxation),
+                          contraction_ratio=contraction_ratio, fiber_stiffness_scale=fiber_stiffness_scale,
+                          tile_tets=tile_tets)
+        return sim
+
+    # ---------------------------------------------------------------- program
+    def build_program(self):
+        """Default program (musclesim.py:107-130): integrate_phase, solve_phase,
+        finalize_phase."""
+        s = self
+
+        def integrate_phase():
+            s.integrate()
+            s.apply_pintotarget()
+            s.clear()
+
+        def solve_phase():
+            s.solve_constraints(run_extras=False)
+            s.apply_dP()
+            s.solve_extras()
+
+        def finalize_phase():
+            s.post_smooth()
+            s.freeze_near_inverted()
+            s.repair_inverted_tets()
+            s.apply_pintotarget()
+            s.update_velocities()
+
+        self.program = [integrate_phase, solve_phase, finalize_phase]
+
+    def _hooks(self) -> bool:
+        return bool(getattr(self, "constraint_solvers", None)) or int(getattr(self, "post_smooth_iters", 0)) > 0
+
+    def _frame_fused(self) -> None:
+        """One frame, fused: [predict] (tile pass + boundary finish) ... with the
+        velocity update of substep s folded into the prediction of s+1."""
+        n = self.num_substeps
+        for sub in range(n):
+            ops = capi.OP_PREDICT | (capi.OP_VELOCITY if sub > 0 else 0)
+            self._vstep(ops)
+            if self.n_cons > 0:
+                self._fused_iteration()
+        self._vstep(capi.OP_VELOCITY)
+
+    def step(self):
+        """One frame (musclesim.py:136-142)."""
+        if self._hooks():
+            if getattr(self, "program", None) is None:
+                self.build_program()
+            self.run_program()
+        else:
+            self._graph("frame", self._frame_fused)
+        self.step_cnt += 1
+
+    def step_eager(self):
+        """One frame through the phase program (no graph, unfused primitives)."""
+        if getattr(self, "program", None) is None:
+            self.build_program()
+        self.run_program()
+        self.step_cnt += 1
+
+    def set_fiber_activation(self, acti_np) -> None:
+        """Per-tet activation in the user's tet order (mg.py:1098-1111)."""
+        if self._t_act is None:
+            raise RuntimeError("set_fiber_activation requires an aniso_arap constraint")
+        import torch
+        a = np.ascontiguousarray(np.asarray(acti_np, np.float32)[self.layout.tet_perm])
+        with torch.cuda.stream(self._stream):
+            self._t_act.copy_(torch.from_numpy(a).to(self.device), non_blocking=False)
+        self._stream.synchronize()

@@ -1,0 +1,58 @@
+"""The C-ABI library loads without a GPU and exports every declared symbol."""
+import ctypes
+import re
+from pathlib import Path
+
+from rlmusclev2_b200 import _capi as capi
+from rlmusclev2_b200.build import build, lib_path
+
+HEADERS = sorted((Path(__file__).resolve().parents[1] / "include").glob("*.h"))
+
+
+def _declared():
+    names = set()
+    for h in HEADERS:
+        txt = h.read_text()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        names |= set(re.findall(r"^\s*(?:int|const char\*|int32_t)\s+(xpbd_\w+)\s*\(", txt, flags=re.M))
+    return names
+
+
+def test_library_loads_and_exports_declared_symbols():
+    build()
+    lib = ctypes.CDLL(str(lib_path()))
+    declared = _declared()
+    assert "xpbd_project" in declared and "xpbd_vertex_step" in declared
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(capi.exported_symbols()) <= declared | set()
+    assert lib.xpbd_abi_version() == 1
+
+
+def test_struct_sizes_match_header_layout():
+    assert ctypes.sizeof(capi.XpbdMaterial) == 32
+    assert ctypes.sizeof(capi.XpbdParams) == 48 + 32 * capi.MAX_MATERIALS + 8 * capi.MAX_ATTACH_MATERIALS
+    assert ctypes.sizeof(capi.XpbdMetrics) == 32
+
+
+def test_ctypes_offsets_match_c_compiler(tmp_path):
+    """Every ctypes mirror has the field offsets gcc computes from the header."""
+    import subprocess
+    structs = [capi.XpbdMaterial, capi.XpbdAttachMaterial, capi.XpbdParams, capi.XpbdVerts, capi.XpbdTiles,
+               capi.XpbdSdf, capi.XpbdMetrics]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "xpbd_b200.h"', 'int main(void){']
+    for s in structs:
+        lines.append(f'printf("{s.__name__} %zu\\n", sizeof({s.__name__}));')
+        for f, _ in s._fields_:
+            lines.append(f'printf("{s.__name__}.{f} %zu\\n", offsetof({s.__name__}, {f}));')
+    lines.append("return 0;}")
+    src = tmp_path / "abi.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "abi"
+    subprocess.run(["gcc", "-I", str(HEADERS[0].parent), str(src), "-o", str(exe)], check=True)
+    out = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                         check=True).stdout.splitlines())
+    for s in structs:
+        assert int(out[s.__name__]) == ctypes.sizeof(s), s.__name__
+        for f, _ in s._fields_:
+            assert int(out[f"{s.__name__}.{f}"]) == getattr(s, f).offset, (s.__name__, f)
