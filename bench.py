@@ -1,0 +1,390 @@
+"""Benchmark: ms/frame of the XPBD substep at 535k tets (synthetic humanV2 scene).
+
+Workload: rlmusclev2_b200/configs/humanv2_synth.json -- 40 ellipsoidal
+muscles + fascia shell (~129k verts / ~535k tets), 20 moving capsule bones,
+ARAP-SVD + belly attach + tendon pins + aniso_arap on one muscle, 256^3 bone
+SDF push-out, 10 substeps x 20 Jacobi iterations per frame, FP32.  A step is
+one frame.  Inputs of every frame (bone poses, activation) are seeded
+synthetic data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  ``value`` is device time per frame with the
+frame inputs already on the GPU (CUDA events on the engine stream, max over
+ranks); ``e2e`` is the same frame through the public API (host activation and
+bone poses uploaded, positions read back every frame).  Multi-GPU runs are
+independent replicas (the single-mesh path does not shard).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+CONFIG = ROOT / "rlmusclev2_b200" / "configs" / "humanv2_synth.json"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC = ROOT / "profiles" / "ncu_traffic.json"
+FALLBACK_HBM_GBS = 6650.0
+WORKLOAD = "humanv2_synth_535k_tets (10 substeps x 20 Jacobi iterations, SDF push-out)"
+
+
+def _peak_hbm():
+    try:
+        return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 4 + k and r[4 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+class CpuBaseline:
+    """The CPU oracle (OpenMP, all host threads) on the same mesh and constraint
+    set; a step times a bounded sample (``sample_iters`` Jacobi iterations of the
+    full mesh plus one predict/velocity pass) scaled to one frame."""
+
+    def __init__(self, cfg, scene):
+        from oracle import oracle as O
+        from rlmusclev2_b200.builder import tet_rest_data
+        from rlmusclev2_b200.mg import find_constraint
+        verts, tets = scene.verts, scene.tets
+        _, V0, valid = tet_rest_data(verts, tets)
+        rho = float(cfg["total_mass"]) / float(V0[valid].astype(np.float64).sum())
+        rv, B, mass, tot = O.precompute_rest(verts, tets, rho, "f32")
+        arap = find_constraint(cfg, "arap")
+        fib = find_constraint(cfg, "fiber")
+        cons = [dict(type="tetarapsvd", name="arap", stiffness=arap["stiffness"],
+                     dampingratio=arap.get("dampingratio", 0.0))]
+        masks = {}
+        if fib:
+            cons.append(dict(type="aniso_arap", name="fiber", stiffness=fib["stiffness"]))
+            masks["fiber"] = scene.tet_part == scene.aniso_muscle
+        t = O.table_from_configs(verts, tets, cons, masks)
+        belly = find_constraint(cfg, "belly_attach")
+        if belly:
+            src = np.nonzero(scene.v_tendon <= 0.5)[0]
+            rvv = np.ones((src.shape[0], 4))
+            rvv[:, :3] = verts[src]
+            pts = np.full((src.shape[0], 4), -1, np.int32)
+            pts[:, 0] = src
+            t.add(O.T_ATTACH, pts, belly["stiffness"], belly.get("dampingratio", 0.0), np.full(src.shape[0], -1),
+                  np.zeros(src.shape[0]), restvector=rvv)
+        t.finalize()
+        dt = float(cfg["delta_t"]) / int(cfg["nsubsteps"])
+        self.s = O.OracleSolver(verts, tets, t, mass, np.zeros(verts.shape[0], np.int32), B, dt=dt,
+                                gravity_vec=(0, 0, 0), v_fiber=scene.v_fiber, tendonmask=np.zeros(tets.shape[0]),
+                                contraction_ratio=0.4, prec="f32")
+        self.s.pos += np.float32(1e-4) * np.sin(np.arange(self.s.pos.size, dtype=np.float32)).reshape(self.s.pos.shape)
+        self.n_iter = int(cfg["nsubsteps"]) * int(cfg["fine_iterations"])
+        self.nsub = int(cfg["nsubsteps"])
+        self.n_tets = int(tets.shape[0])
+        self.s.project()  # first touch of the scratch buffers
+
+    def sample(self, sample_iters: int = 1) -> float:
+        s = self.s
+        t0 = time.perf_counter()
+        for _ in range(sample_iters):
+            s.project()
+            s.apply_dP()
+        t_iter = (time.perf_counter() - t0) / sample_iters
+        t1 = time.perf_counter()
+        s.integrate()
+        s.update_velocities()
+        t_vert = time.perf_counter() - t1
+        return (t_iter * self.n_iter + t_vert * self.nsub) * 1e3
+
+    def describe(self, value: float, sample_iters: int) -> dict:
+        return {"value": round(value, 3), "unit": "ms/frame", "cores": _omp_threads(), "kind": "port",
+                "sample": f"{sample_iters} Jacobi iteration(s) + 1 predict/velocity pass of the full {self.n_tets}-tet "
+                          f"mesh on the FP32 oracle, scaled to {self.n_iter} iterations and {self.nsub} substeps/frame"}
+
+
+def _omp_threads() -> int:
+    v = os.environ.get("OMP_NUM_THREADS")
+    return int(v) if v else (os.cpu_count() or 1)
+
+
+def _dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from rlmusclev2_b200.mg import load_config, scene_from_cfg
+    cfg = load_config(str(CONFIG))
+    scene = scene_from_cfg(cfg)
+    cb = CpuBaseline(cfg, scene)
+    for _ in range(args.warmup):
+        cb.sample(1)
+    vals = [cb.sample(1) for _ in range(max(1, args.steps))]
+    v = float(np.median(vals))
+    line = {"impl": "reference", "metric": "ms/frame", "value": round(v, 3), "unit": "ms/frame", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_verts": int(scene.verts.shape[0]), "n_tets": int(scene.tets.shape[0])},
+            "cpu_baseline": cb.describe(v, 1),
+            "e2e": {"value": round(v, 3), "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference runs on NVIDIA Warp, which cannot be installed here; its CPU path is restated "
+                    "by the C oracle (OpenMP) and timed on a bounded sample scaled to one frame"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import ctypes as C
+    import torch
+
+    from rlmusclev2_b200 import _capi as capi
+    from rlmusclev2_b200.mg import MultiGridSim, load_config
+
+    world, rank, local = _dist_setup()
+    torch.cuda.set_device(local)
+    cfg = load_config(str(CONFIG))
+    sim = MultiGridSim(cfg, device=f"cuda:{local}")
+    sc = sim.scene
+    nf = args.warmup + args.steps
+    frames = [sim.start_frame + f for f in range(nf)]
+    stream = sim._stream
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    # ---- device-resident inputs: all frames' bone poses and activations on the GPU
+    trs = torch.from_numpy(np.stack([sc.bone_transforms(f).reshape(sc.n_bones, 12) for f in frames]).astype(
+        np.float32)).to(sim.device)
+    acts_user = torch.from_numpy(np.stack([sc.activation(f) for f in frames])).to(sim.device)
+    perm_d = sim._tet_perm_d
+
+    def frame_resident(i):
+        with torch.cuda.stream(stream):
+            sim._bone_tr.copy_(trs[i])
+        capi.check(sim._lib.xpbd_gather(sim.NT, 1, C.c_void_p(perm_d.data_ptr()),
+                                        C.c_void_p(acts_user[i].data_ptr()), 1, C.c_void_p(sim._t_act.data_ptr()), 1,
+                                        sim._sp))
+        sim._frame_loaded = frames[i]
+        sim.step_frame(frames[i])
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=sim.device)  # 256 MB > L2 (126 MB)
+
+    def flush_l2():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+
+    for i in range(args.warmup):
+        frame_resident(i)
+    stream.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    evs = [(ev(), ev()) for _ in range(args.steps)]
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for k, i in enumerate(range(args.warmup, nf)):
+            flush_l2()
+            evs[k][0].record(stream)
+            frame_resident(i)
+            evs[k][1].record(stream)
+        stream.synchronize()
+    ms_frame = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+    if world > 1:
+        t = torch.tensor([ms_frame], device=sim.device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_frame = float(t.item())
+
+    # ---- e2e through the public API: host inputs in, positions out, every frame
+    for i in range(min(args.warmup, 3)):
+        sim.set_fiber_activation(sc.activation(frames[i]))
+        sim.step_frame(frames[i])
+        sim.positions_np()
+    stream.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    h2d = sim.NT * 4 + sc.n_bones * 12 * 4
+    d2h = sim.NV * 3 * 4
+    evs2 = [(ev(), ev()) for _ in range(args.steps)]
+    for k, i in enumerate(range(args.warmup, nf)):
+        flush_l2()
+        evs2[k][0].record(stream)
+        sim.set_fiber_activation(sc.activation(frames[i]))
+        sim.step_frame(frames[i])
+        _ = sim.positions_np()
+        evs2[k][1].record(stream)
+    stream.synchronize()
+    ms_e2e = sum(a.elapsed_time(b) for a, b in evs2) / args.steps
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=sim.device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+
+    # ---- roofline of the dominant kernel, measured inside a real frame: one
+    # frame replayed launch by launch with events around every Jacobi iteration
+    # (tile pass + boundary finish) on the engine stream.
+    L = sim.layout
+    flush_l2()
+    frame_resident(nf - 1)
+    iters = []
+    sim._targets_kernel()
+    sim.collision_solvers[0].bake() if sim.collision_solvers else None
+    for sub in range(sim.nsubsteps):
+        sim._vstep(capi.OP_PREDICT | (capi.OP_PIN if sim._has_pins else 0))
+        for _ in range(sim.fine_iters):
+            a, b = ev(), ev()
+            a.record(stream)
+            sim._fused_iteration()
+            b.record(stream)
+            iters.append((a, b))
+    stream.synchronize()
+    it_ms = float(np.mean([a.elapsed_time(b) for a, b in iters]))
+    alg_bytes = L.n_tets * 56 + L.n_verts * 40
+    achieved = alg_bytes / (it_ms * 1e-3) / 1e9
+    peak, peak_kind = _peak_hbm()
+    traffic = None
+    try:
+        tr = json.loads(TRAFFIC.read_text())
+        traffic = tr.get("bytes_per_iteration")
+    except Exception:
+        pass
+    launches_per_frame = 1 + (1 if sim.collision_solvers else 0) + (1 if sim._has_pins else 0) + sim.nsubsteps * (
+        1 + 2 * sim.fine_iters) + 1
+    n_iter = sim.nsubsteps * sim.fine_iters
+    line = {
+        "metric": "ms/frame", "value": round(ms_frame, 4), "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_frame, 4), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD,
+                   "n_verts": L.n_verts, "n_tets": L.n_tets, "n_tiles": L.n_tiles, "fine_iterations": sim.fine_iters,
+                   "nsubsteps": sim.nsubsteps, "parallelism": f"replicas x{world}",
+                   "l2": "working set < L2 (126 MB); no flush: frames run back to back like a real rollout"},
+        "substeps_per_s": round(1e3 * sim.nsubsteps / ms_frame, 1),
+        "tets_per_s": round(L.n_tets * n_iter / (ms_frame * 1e-3), 1),
+        "e2e": {"value": round(ms_e2e, 4), "unit": "ms/frame", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_project_tiles + k_apply_list (one Jacobi iteration, timed inside a frame)",
+                     "algorithmic_bytes": alg_bytes, "iteration_us": round(it_ms * 1e3, 2),
+                     "frame_roofline_ms": round(alg_bytes * n_iter / (peak * 1e9) * 1e3, 4)},
+        "clocks": clk.summary(),
+        "gpu_launches": (launches_per_frame + 1) * args.steps,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = CpuBaseline(cfg, sc)
+        line["cpu_baseline"] = cb.describe(cb.sample(2), 2)
+    sim.release_graphs()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_profile_case(args):
+    """Small deterministic workloads for ncu (no timing, no output line).
+
+    humanv2: ``--steps`` frames of the benchmark configuration through the
+    frame graph.  box3m: a 64x64x120-hex box (2.95M tets, ~150 MB of tet
+    streams, larger than L2) and ``--steps`` Jacobi iterations of its tet pass."""
+    import torch
+    if args.profile_case == "humanv2":
+        from rlmusclev2_b200.mg import MultiGridSim, load_config
+        sim = MultiGridSim(load_config(str(CONFIG)))
+        for f in range(sim.start_frame, sim.start_frame + args.steps):
+            sim.set_fiber_activation(sim.scene.activation(f))
+            sim.step_frame(f)
+        sim.synchronize()
+    elif args.profile_case == "box3m":
+        from rlmusclev2_b200 import MuscleSim
+        from rlmusclev2_b200.meshgen import box_muscle
+        m = box_muscle(nx=64, ny=64, nz=120, spacing=0.0025, seed=0)
+        cons = [{"type": "tetarapsvd", "name": "arap", "compliance": 1e-7},
+                {"type": "volume", "name": "volume", "compliance": 0.0}]
+        sim = MuscleSim.from_procedural(m.verts, m.tets, m.fiber_per_tet, constraint_configs=cons,
+                                        device="cuda:0", stopped=m.stopped, dts=1 / 24, num_substeps=10,
+                                        gravity=-9.8)
+        sim.integrate()
+        for _ in range(args.steps):
+            sim._fused_iteration()
+        sim.synchronize()
+    torch.cuda.synchronize()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", choices=["humanv2", "box3m"], default=None,
+                    help="run a small fixed workload for ncu and exit")
+    args = ap.parse_args()
+    if args.profile_case:
+        return run_profile_case(args)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

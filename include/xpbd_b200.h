@@ -194,6 +194,35 @@ int xpbd_pin_overwrite_masked(int32_t n, const int32_t* pts, const float* target
 /* Mesh metrics into out (device XpbdMetrics, zeroed by this call). */
 int xpbd_metrics(const XpbdTiles* tiles, const XpbdVerts* v, XpbdMetrics* out, xpbd_stream_t stream);
 
+/* Per-frame kinematic targets of bone-bound vertices.  transforms is
+ * [n_bones][12] = row-major 3x4 [R | t]; vertex i (library order) has bone
+ * vert_bone[i] and rest position rest4[i] (x,y,z,-); target = R x + t is
+ * written to pin_target[i].xyz and attach_target[i].xyz (their .w lanes are
+ * kept).  Replaces the per-frame target refresh of MultiGridSim
+ * (load_frame_targets / _update_belly_attach_targets, mg/mg.py:1386-1407,
+ * 725-734) without the reference's device->host->device round trip. */
+int xpbd_bone_targets(int32_t n, int32_t n_bones, const float* transforms, const int32_t* vert_bone,
+                      const float* rest4, float* pin_target, float* attach_target, xpbd_stream_t stream);
+
+/* Capsule bone, rest pose: centre, unit axis, half segment length, radius. */
+typedef struct XpbdCapsule {
+    float center[3];
+    float half;
+    float axis[3];
+    float radius;
+} XpbdCapsule;
+
+/* Bake the grid SDF of the union of n capsules, each moved by its
+ * transforms[bone] ([n][12], NULL = rest pose), into sdf->phi.  Values are
+ * exact distances within band of a capsule surface and clamped to band
+ * elsewhere (band > 0; push-out only reads phi near zero). */
+int xpbd_sdf_bake_capsules(const XpbdSdf* sdf, int32_t n_caps, const XpbdCapsule* caps, const float* transforms,
+                           float band, xpbd_stream_t stream);
+
+/* dst[i] = src[idx[i]] for float lanes of width `width` (1..4). */
+int xpbd_gather(int32_t n, int32_t width, const int32_t* idx, const float* src, int32_t src_stride, float* dst,
+                int32_t dst_stride, xpbd_stream_t stream);
+
 /* Stream capture helpers (a captured substep replays as one graph launch). */
 int xpbd_graph_begin(xpbd_stream_t stream);
 int xpbd_graph_end(xpbd_stream_t stream, void** exec_out);

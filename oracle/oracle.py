@@ -292,3 +292,148 @@ class OracleMuscleSim(OracleSolver):
     def step(self):
         for _ in range(self.num_substeps):
             self.substep()
+
+
+def sdf_bake(nxyz, origin, h, caps, transforms, band, prec="f32"):
+    """Capsule-union SDF on the grid, clamped to band (see orc_sdf_bake_capsules)."""
+    P = Prec(prec)
+    nx, ny, nz = nxyz
+    phi = np.zeros((nz, ny, nx), P.dt)
+    f = P.fn("orc_sdf_bake_capsules")
+    f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, P.ct, C.c_int, C.c_void_p, C.c_void_p, P.ct, C.c_void_p]
+    o = P.arr(origin)
+    cp = P.arr(caps)
+    tr = None if transforms is None else P.arr(transforms)
+    f(nx, ny, nz, _p(o), P.ct(h), cp.shape[0], _p(cp), _p(tr), P.ct(band), _p(phi))
+    return phi
+
+
+def sdf_push(pos, inv_mass, phi, origin, h, offset, max_push, prec="f32"):
+    P = Prec(prec)
+    nz, ny, nx = phi.shape
+    f = P.fn("orc_sdf_push")
+    f.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, P.ct, P.ct, P.ct]
+    o = P.arr(origin)
+    f(pos.shape[0], _p(pos), _p(P.arr(inv_mass)), _p(P.arr(phi)), nx, ny, nz, _p(o), P.ct(h), P.ct(offset),
+      P.ct(max_push))
+
+
+def _find(cfg, name):
+    for c in cfg.get("constraints", []):
+        if c.get("name") == name:
+            return c if c.get("enable", True) else None
+    return None
+
+
+class OracleMultiGridSim(OracleSolver):
+    """MultiGridSim's program (mg/mg.py:1322-1418) on the oracle, for a synthetic
+    scene whose vertices ride capsule bones rigidly (rest_offset = 0)."""
+
+    def __init__(self, cfg, scene, prec="f32", sdf_margin=0.02, band_cells=3.0):
+        self.cfg, self.scene = cfg, scene
+        verts, tets = scene.verts.astype(np.float32), scene.tets.astype(np.int32)
+        nv, nt = verts.shape[0], tets.shape[0]
+        arap = _find(cfg, "arap")
+        snh = _find(cfg, "snh")
+        fib = _find(cfg, "fiber")
+        vol = _find(cfg, "volume")
+        fascia = scene.tet_part < 0
+        cons, masks = [], {}
+        if snh:
+            cons.append(dict(type="snh", name="snh", mu=float(snh.get("mu", snh.get("stiffness", arap["stiffness"]))),
+                             lam=float(snh.get("lam", 1e8)), dampingratio=float(snh.get("dampingratio", 0.0))))
+            if snh.get("region", "all") == "fascia":
+                masks["snh"], masks["arap"] = fascia, ~fascia
+                cons.append(dict(type="tetarapsvd", name="arap", stiffness=arap["stiffness"]))
+        else:
+            cons.append(dict(type="tetarapsvd", name="arap", stiffness=arap["stiffness"]))
+        if vol and not (snh and snh.get("region", "all") == "all"):
+            cons.append(dict(type="volume", name="volume", stiffness=vol["stiffness"],
+                             dampingratio=vol.get("dampingratio", 0.0)))
+            if snh:
+                masks["volume"] = ~fascia
+        if fib:
+            cons.append(dict(type="aniso_arap", name="fiber", stiffness=float(fib.get("stiffness", 1e8))))
+            if fib.get("region", "all") == "aniso_muscle":
+                masks["fiber"] = scene.tet_part == scene.aniso_muscle
+        self.contraction = float((fib or {}).get("contraction_ratio", 0.4))
+        t = table_from_configs(verts, tets, cons, masks)
+        V0, valid = signed_rest_volume(verts, tets)
+        rho = float(cfg["total_mass"]) / float(V0[valid].astype(np.float64).sum())
+        rv, B, mass, tot = precompute_rest(verts, tets, rho, prec)
+        self.total_rest_volume = tot
+        pin = _find(cfg, "muscleToBonePin")
+        self.active = np.zeros(nv, bool)
+        if pin is not None and pin.get("region", "tendonmask") == "tendonmask":
+            self.active = scene.v_tendon > float(pin["tendon_pin_threshold"])
+        elif pin is not None and pin.get("region") == "full":
+            self.active[:] = True
+        belly = _find(cfg, "belly_attach")
+        self.belly_src = np.nonzero(~self.active)[0] if belly else np.zeros(0, np.int64)
+        if belly and self.belly_src.size:
+            n = self.belly_src.shape[0]
+            pts = np.full((n, 4), -1, np.int32)
+            pts[:, 0] = self.belly_src
+            t.add(T_ATTACH, pts, float(belly["stiffness"]), float(belly.get("dampingratio", 0.0)), np.full(n, -1),
+                  np.zeros(n), restvector=np.ones((n, 4)))
+        t.finalize()
+        tendon_tet = (scene.v_tendon[tets].astype(np.float32).sum(1) / np.float32(4.0)).astype(np.float32)
+        self.nsub = int(cfg["nsubsteps"])
+        self.fine_iters = int(cfg["fine_iterations"])
+        super().__init__(verts, tets, t, mass, np.zeros(nv, np.int32), B, dt=float(cfg["delta_t"]) / self.nsub,
+                         gravity_vec=cfg.get("gravity", [0, 0, 0]), veldamping=float(cfg.get("veldamping", 0.0)),
+                         quasi_static=bool(cfg.get("quasi_static", False)), v_fiber=scene.v_fiber,
+                         tendonmask=tendon_tet, contraction_ratio=self.contraction, prec=prec)
+        if t.n:
+            self.attach_rows = np.nonzero(self.c_type == T_ATTACH)[0]
+            order = np.argsort(self.c_pts[self.attach_rows, 0])
+            self.attach_rows = self.attach_rows[order]
+        coll = (cfg.get("demo") or {}).get("collision") or {}
+        self.coll = coll if coll.get("enabled", False) else None
+        if self.coll:
+            lo, hi = verts.min(0) - sdf_margin, verts.max(0) + sdf_margin
+            res = int(coll.get("sdf_res", 256))
+            self.sdf_h = float((hi - lo).max()) / (res - 1)
+            self.sdf_origin = lo.astype(np.float64)
+            self.sdf_res = res
+            self.band = band_cells * self.sdf_h
+            self.caps = np.concatenate([scene.bone_center, scene.bone_half[:, None], scene.bone_axis,
+                                        scene.bone_radius[:, None]], 1)
+        self.inv_mass = np.where(self.mass > 0, 1.0 / np.where(self.mass > 0, self.mass, 1), 0).astype(self.P.dt)
+        self.target = None
+
+    def targets(self, frame):
+        T = self.scene.bone_transforms(frame).astype(np.float32)
+        b = self.scene.vert_bone
+        x = self.scene.verts.astype(np.float32)
+        Tb = T[b]
+        out = np.empty_like(x)
+        for r in range(3):
+            out[:, r] = ((Tb[:, r, 0] * x[:, 0] + Tb[:, r, 1] * x[:, 1]) + Tb[:, r, 2] * x[:, 2]) + Tb[:, r, 3]
+        return out, T.reshape(-1, 12)
+
+    def apply_pins(self):
+        self.pos[self.active] = self.target[self.active]
+
+    def step_frame(self, frame):
+        self.target, T = self.targets(frame)
+        if self.table.n and self.attach_rows.size:
+            self.c_rv[self.attach_rows, :3] = self.target[self.c_pts[self.attach_rows, 0]]
+        if self.scene.tet_part is not None and hasattr(self.scene, "activation"):
+            self.activation[:] = self.scene.activation(frame)
+        self.apply_pins()
+        if self.coll:
+            r = self.sdf_res
+            self.phi = sdf_bake((r, r, r), self.sdf_origin, self.sdf_h, self.caps, T, self.band, self.P.name)
+        for _ in range(self.nsub):
+            self.integrate()
+            self.apply_pins()
+            for _ in range(self.fine_iters):
+                self.project()
+                self.apply_dP()
+                self.apply_pins()
+            if self.coll:
+                sdf_push(self.pos, self.inv_mass, self.phi, self.sdf_origin, self.sdf_h,
+                         float(self.coll.get("contact_offset", 0.0)), float(self.coll.get("max_push", -1.0)),
+                         self.P.name)
+            self.update_velocities()

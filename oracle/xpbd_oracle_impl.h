@@ -644,6 +644,100 @@ void FN(orc_arap_residual)(int nt, const int* tets, const REAL* pos, const REAL*
     }
 }
 
+
+/* ------------------------------------------------------------------------ */
+/* Bone push-out on a grid SDF.  The reference queries the bone triangle mesh
+ * (solve_mesh_contact_pos_kernel, sdf/kernel.py:122-170): err = dist - offset;
+ * if err < 0 (and -err <= max_push when max_push > 0) pos -= n * err, n the
+ * outward normal; inverse-mass-0 vertices are skipped.  With capsule bones the
+ * distance comes from the baked grid: trilinear phi, n = normalised analytic
+ * gradient of the trilinear interpolant. */
+static REAL FN(cap_phi)(const REAL* a, const REAL* b, REAL r, const REAL* x) {
+    REAL ab[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, ax[3] = {x[0] - a[0], x[1] - a[1], x[2] - a[2]};
+    REAL L2 = ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2];
+    REAL t = 0;
+    if (L2 > 0) {
+        t = (ax[0] * ab[0] + ax[1] * ab[1] + ax[2] * ab[2]) / L2;
+        t = t < 0 ? 0 : (t > 1 ? 1 : t);
+    }
+    REAL d[3] = {ax[0] - t * ab[0], ax[1] - t * ab[1], ax[2] - t * ab[2]};
+    return SQRT(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) - r;
+}
+
+/* caps: [n][8] = center xyz, half, axis xyz, radius; transforms [n][12] or NULL. */
+void FN(orc_sdf_bake_capsules)(int nx, int ny, int nz, const REAL* origin, REAL h, int ncaps, const REAL* caps,
+                               const REAL* transforms, REAL band, REAL* phi) {
+    REAL* seg = (REAL*)malloc(sizeof(REAL) * 7 * (size_t)(ncaps > 0 ? ncaps : 1));
+    for (int c = 0; c < ncaps; ++c) {
+        const REAL* K = caps + 8 * c;
+        REAL a[3], b[3];
+        for (int k = 0; k < 3; ++k) {
+            a[k] = K[k] - K[3] * K[4 + k];
+            b[k] = K[k] + K[3] * K[4 + k];
+        }
+        if (transforms) {
+            const REAL* T = transforms + 12 * c;
+            REAL a0[3] = {a[0], a[1], a[2]}, b0[3] = {b[0], b[1], b[2]};
+            for (int r = 0; r < 3; ++r) {
+                a[r] = T[4 * r] * a0[0] + T[4 * r + 1] * a0[1] + T[4 * r + 2] * a0[2] + T[4 * r + 3];
+                b[r] = T[4 * r] * b0[0] + T[4 * r + 1] * b0[1] + T[4 * r + 2] * b0[2] + T[4 * r + 3];
+            }
+        }
+        for (int k = 0; k < 3; ++k) { seg[7 * c + k] = a[k]; seg[7 * c + 3 + k] = b[k]; }
+        seg[7 * c + 6] = K[7];
+    }
+#pragma omp parallel for schedule(static)
+    for (int iz = 0; iz < nz; ++iz)
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                REAL x[3] = {origin[0] + h * (REAL)ix, origin[1] + h * (REAL)iy, origin[2] + h * (REAL)iz};
+                REAL v = band;
+                for (int c = 0; c < ncaps; ++c) {
+                    REAL pc = FN(cap_phi)(seg + 7 * c, seg + 7 * c + 3, seg[7 * c + 6], x);
+                    if (pc < v) v = pc;
+                }
+                phi[((size_t)iz * ny + iy) * nx + ix] = v;
+            }
+    free(seg);
+}
+
+void FN(orc_sdf_push)(int nv, REAL* pos, const REAL* inv_mass, const REAL* phi, int nx, int ny, int nz,
+                      const REAL* origin, REAL h, REAL offset, REAL max_push) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nv; ++i) {
+        if (inv_mass[i] == (REAL)0) continue;
+        REAL inv_h = (REAL)1 / h;
+        REAL gx = (pos[3 * i] - origin[0]) * inv_h, gy = (pos[3 * i + 1] - origin[1]) * inv_h,
+             gz = (pos[3 * i + 2] - origin[2]) * inv_h;
+        if (!(gx >= 0 && gy >= 0 && gz >= 0 && gx <= (REAL)(nx - 1) && gy <= (REAL)(ny - 1) && gz <= (REAL)(nz - 1)))
+            continue;
+        int ix = (int)gx, iy = (int)gy, iz = (int)gz;
+        if (ix > nx - 2) ix = nx - 2;
+        if (iy > ny - 2) iy = ny - 2;
+        if (iz > nz - 2) iz = nz - 2;
+        REAL fx = gx - (REAL)ix, fy = gy - (REAL)iy, fz = gz - (REAL)iz;
+        size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+        const REAL* b = phi + iz * sz + iy * sy + ix;
+        REAL c000 = b[0], c100 = b[1], c010 = b[sy], c110 = b[sy + 1];
+        REAL c001 = b[sz], c101 = b[sz + 1], c011 = b[sz + sy], c111 = b[sz + sy + 1];
+        REAL c00 = c000 + fx * (c100 - c000), c10 = c010 + fx * (c110 - c010);
+        REAL c01 = c001 + fx * (c101 - c001), c11 = c011 + fx * (c111 - c011);
+        REAL c0 = c00 + fy * (c10 - c00), c1 = c01 + fy * (c11 - c01);
+        REAL ph = c0 + fz * (c1 - c0);
+        REAL dx0 = (c100 - c000) + fy * ((c110 - c010) - (c100 - c000));
+        REAL dx1 = (c101 - c001) + fy * ((c111 - c011) - (c101 - c001));
+        REAL dy0 = (c010 - c000) + fx * ((c110 - c100) - (c010 - c000));
+        REAL dy1 = (c011 - c001) + fx * ((c111 - c101) - (c011 - c001));
+        REAL g[3] = {(dx0 + fz * (dx1 - dx0)) * inv_h, (dy0 + fz * (dy1 - dy0)) * inv_h, (c1 - c0) * inv_h};
+        REAL gl = SQRT(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+        if (!(gl > (REAL)1e-12)) continue;
+        REAL err = ph - offset;
+        if (err < 0 && (max_push <= 0 || -err <= max_push)) {
+            for (int k = 0; k < 3; ++k) pos[3 * i + k] -= (g[k] / gl) * err;
+        }
+    }
+}
+
 #undef VEC
 #undef MAT
 #undef SQRT

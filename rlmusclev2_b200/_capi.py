@@ -59,6 +59,10 @@ class XpbdSdf(C.Structure):
                 ("max_push", C.c_float), ("reserved", C.c_int32)]
 
 
+class XpbdCapsule(C.Structure):
+    _fields_ = [("center", C.c_float * 3), ("half", C.c_float), ("axis", C.c_float * 3), ("radius", C.c_float)]
+
+
 class XpbdMetrics(C.Structure):
     _fields_ = [("vol_sum", C.c_double), ("resid_sq_sum", C.c_double), ("resid_max", C.c_float),
                 ("n_inverted", C.c_int32), ("n_nonfinite", C.c_int32), ("reserved", C.c_int32)]
@@ -75,6 +79,9 @@ _SIGS = {
     "xpbd_apply_all": ([C.POINTER(XpbdParams), C.POINTER(XpbdVerts), C.c_uint32, P], C.c_int),
     "xpbd_pin_overwrite_masked": ([C.c_int32, P, P, P, P, P, P], C.c_int),
     "xpbd_metrics": ([C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), P, P], C.c_int),
+    "xpbd_bone_targets": ([C.c_int32, C.c_int32, P, P, P, P, P, P], C.c_int),
+    "xpbd_sdf_bake_capsules": ([C.POINTER(XpbdSdf), C.c_int32, P, P, C.c_float, P], C.c_int),
+    "xpbd_gather": ([C.c_int32, C.c_int32, P, P, C.c_int32, P, C.c_int32, P], C.c_int),
     "xpbd_graph_begin": ([P], C.c_int),
     "xpbd_graph_end": ([P, C.POINTER(C.c_void_p)], C.c_int),
     "xpbd_graph_launch": ([P, P], C.c_int),

@@ -13,27 +13,19 @@
 #include <string.h>
 
 #include "../../include/xpbd_b200.h"
+#include "xpbd_common.cuh"
 #include "xpbd_device.cuh"
 
 using namespace xpbd;
 
+namespace xpbd {
+char* err_buffer() {
+    static thread_local char buf[256] = "";
+    return buf;
+}
+}  // namespace xpbd
+
 namespace {
-
-thread_local char g_err[256] = "";
-
-int fail(int code, const char* fmt, const char* detail = "") {
-    snprintf(g_err, sizeof(g_err), fmt, detail);
-    return code;
-}
-int cuda_check(const char* where) {
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
-        return XPBD_ERR_CUDA;
-    }
-    return XPBD_OK;
-}
-bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 constexpr int kTileThreads = 256;
 constexpr int kVertThreads = 256;
@@ -74,13 +66,6 @@ __device__ __forceinline__ void finish_vertex(const XpbdParams& prm, const XpbdV
             p.z = t.z;
         }
     }
-}
-
-__device__ __forceinline__ void smem_add(float4* acc, int l, float3 d) {
-    atomicAdd(&acc[l].x, d.x);
-    atomicAdd(&acc[l].y, d.y);
-    atomicAdd(&acc[l].z, d.z);
-    atomicAdd(&acc[l].w, 1.f);
 }
 
 // ---------------------------------------------------------------------------
@@ -129,30 +114,38 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         }
         const float3 p3 = f3(p[3]);
         const M3 F = deformation(f3(p[0]) - p3, f3(p[1]) - p3, f3(p[2]) - p3, B);
+        // All constraints of the tet read the same positions (Jacobi), so their
+        // deltas are summed in registers and pushed with one set of shared
+        // atomics; each active constraint adds 1 to dPw of all four vertices.
         Corr4 c;
+        float3 d[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) d[i] = make_float3(0.f, 0.f, 0.f);
+        float nact = 0.f;
+        auto add = [&](const Corr4& cc) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) d[i] = d[i] + cc.d[i];
+            nact += 1.f;
+        };
         const uint32_t fl = m.flags;
         // Same type order as the reference table (ascending ConstraintType tag).
-        if (fl & XPBD_MAT_SNH) {
-            if (con_snh(p, pq, B, F, V0, m.snh_mu, m.snh_lam, m.snh_damp, prm.dt, c))
-#pragma unroll
-                for (int i = 0; i < 4; ++i) smem_add(s_acc, l[i], c.d[i]);
-        }
-        if (fl & XPBD_MAT_VOLUME) {
-            if (con_volume(p, pq, V0, m.vol_k, m.vol_damp, prm.dt, c))
-#pragma unroll
-                for (int i = 0; i < 4; ++i) smem_add(s_acc, l[i], c.d[i]);
-        }
+        if ((fl & XPBD_MAT_SNH) && con_snh(p, pq, B, F, V0, m.snh_mu, m.snh_lam, m.snh_damp, prm.dt, c)) add(c);
+        if ((fl & XPBD_MAT_VOLUME) && con_volume(p, pq, V0, m.vol_k, m.vol_damp, prm.dt, c)) add(c);
         if (fl & XPBD_MAT_ANISO) {
             const float4 fb = reinterpret_cast<const float4*>(T.tet_fiber)[t];
             if (con_aniso(p, B, F, f3(fb), fb.w, T.tet_act[t], m.aniso_k, prm.contraction_ratio,
                           prm.fiber_stiffness_scale, prm.dt, c))
-#pragma unroll
-                for (int i = 0; i < 4; ++i) smem_add(s_acc, l[i], c.d[i]);
+                add(c);
         }
-        if (fl & XPBD_MAT_ARAPSVD) {
-            if (con_arapsvd(p, B, F, m.arap_k, prm.dt, c))
+        if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, m.arap_k, prm.dt, c)) add(c);
+        if (nact != 0.f) {
 #pragma unroll
-                for (int i = 0; i < 4; ++i) smem_add(s_acc, l[i], c.d[i]);
+            for (int i = 0; i < 4; ++i) {
+                atomicAdd(&s_acc[l[i]].x, d[i].x);
+                atomicAdd(&s_acc[l[i]].y, d[i].y);
+                atomicAdd(&s_acc[l[i]].z, d[i].z);
+                atomicAdd(&s_acc[l[i]].w, nact);
+            }
         }
     }
     __syncthreads();
@@ -381,30 +374,30 @@ __global__ void __launch_bounds__(kTileThreads)
 }
 
 int check_verts(const XpbdVerts* v) {
-    if (!v || v->n <= 0 || !v->pos) return fail(XPBD_ERR_ARG, "XpbdVerts: null or empty%s");
+    if (!v || v->n <= 0 || !v->pos) return fail(XPBD_ERR_ARG, "XpbdVerts: null or empty");
     if (!aligned16(v->pos) || !aligned16(v->pprev) || !aligned16(v->vel) || !aligned16(v->accum) ||
         !aligned16(v->force) || !aligned16(v->attach_target) || !aligned16(v->pin_target))
-        return fail(XPBD_ERR_ALIGN, "XpbdVerts: a [n][4] array is not 16-byte aligned%s");
+        return fail(XPBD_ERR_ALIGN, "XpbdVerts: a [n][4] array is not 16-byte aligned");
     if (v->vflags && (!v->attach_target || !v->pin_target))
-        return fail(XPBD_ERR_ARG, "XpbdVerts: vflags given without attach_target/pin_target%s");
+        return fail(XPBD_ERR_ARG, "XpbdVerts: vflags given without attach_target/pin_target");
     return XPBD_OK;
 }
 int check_params(const XpbdParams* p) {
-    if (!p) return fail(XPBD_ERR_ARG, "XpbdParams: null%s");
+    if (!p) return fail(XPBD_ERR_ARG, "XpbdParams: null");
     if (p->n_materials < 0 || p->n_materials > XPBD_MAX_MATERIALS || p->n_attach_materials < 0 ||
         p->n_attach_materials > XPBD_MAX_ATTACH_MATERIALS)
-        return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range%s");
-    if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0%s");
+        return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range");
+    if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0");
     return XPBD_OK;
 }
 int check_tiles(const XpbdTiles* t) {
     if (!t || t->n_tiles <= 0 || !t->tile_vptr || !t->tile_nint || !t->tile_tptr || !t->tile_verts || !t->tet_q ||
         !t->tet_b0 || !t->tet_b1 || !t->tet_b2)
-        return fail(XPBD_ERR_ARG, "XpbdTiles: null member%s");
+        return fail(XPBD_ERR_ARG, "XpbdTiles: null member");
     if (t->max_tile_verts <= 0 || t->max_tile_verts > XPBD_MAX_TILE_VERTS)
-        return fail(XPBD_ERR_LIMIT, "XpbdTiles: max_tile_verts out of range%s");
+        return fail(XPBD_ERR_LIMIT, "XpbdTiles: max_tile_verts out of range");
     if (!aligned16(t->tet_q) || !aligned16(t->tet_b0) || !aligned16(t->tet_b1) || !aligned16(t->tet_fiber))
-        return fail(XPBD_ERR_ALIGN, "XpbdTiles: a [n][4] array is not 16-byte aligned%s");
+        return fail(XPBD_ERR_ALIGN, "XpbdTiles: a [n][4] array is not 16-byte aligned");
     return XPBD_OK;
 }
 
@@ -441,17 +434,17 @@ int launch_project(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V
 extern "C" {
 
 int xpbd_abi_version(void) { return 1; }
-const char* xpbd_error_string(void) { return g_err; }
+const char* xpbd_error_string(void) { return err_buffer(); }
 
 int xpbd_vertex_step(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, const XpbdSdf* sdf,
                      xpbd_stream_t stream) {
     int rc;
     if ((rc = check_params(prm)) || (rc = check_verts(v))) return rc;
     if ((ops & XPBD_OP_SDF) && (!sdf || !sdf->phi || sdf->nx < 2 || sdf->ny < 2 || sdf->nz < 2 || !(sdf->h > 0.f)))
-        return fail(XPBD_ERR_ARG, "xpbd_vertex_step: XPBD_OP_SDF needs a valid XpbdSdf%s");
+        return fail(XPBD_ERR_ARG, "xpbd_vertex_step: XPBD_OP_SDF needs a valid XpbdSdf");
     if ((ops & (XPBD_OP_VELOCITY | XPBD_OP_PREDICT)) && (!v->pprev || !v->vel))
-        return fail(XPBD_ERR_ARG, "xpbd_vertex_step: pprev/vel required%s");
-    if ((ops & XPBD_OP_PREDICT) && !v->mass) return fail(XPBD_ERR_ARG, "xpbd_vertex_step: mass required%s");
+        return fail(XPBD_ERR_ARG, "xpbd_vertex_step: pprev/vel required");
+    if ((ops & XPBD_OP_PREDICT) && !v->mass) return fail(XPBD_ERR_ARG, "xpbd_vertex_step: mass required");
     XpbdSdf S;
     memset(&S, 0, sizeof(S));
     if (sdf) S = *sdf;
@@ -463,11 +456,11 @@ int xpbd_project(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts*
                  xpbd_stream_t stream) {
     int rc;
     if ((rc = check_params(prm)) || (rc = check_tiles(tiles)) || (rc = check_verts(v))) return rc;
-    if (!v->accum) return fail(XPBD_ERR_ARG, "xpbd_project: accum required%s");
+    if (!v->accum) return fail(XPBD_ERR_ARG, "xpbd_project: accum required");
     if (any_aniso(prm) && (!tiles->tet_fiber || !tiles->tet_act))
-        return fail(XPBD_ERR_ARG, "xpbd_project: aniso materials need tet_fiber and tet_act%s");
+        return fail(XPBD_ERR_ARG, "xpbd_project: aniso materials need tet_fiber and tet_act");
     const bool damp = any_damped(prm);
-    if (damp && !v->pprev) return fail(XPBD_ERR_ARG, "xpbd_project: damped materials need pprev%s");
+    if (damp && !v->pprev) return fail(XPBD_ERR_ARG, "xpbd_project: damped materials need pprev");
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t fops = XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_PIN;
     if (mode == XPBD_PROJECT_FUSED)
@@ -476,15 +469,15 @@ int xpbd_project(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts*
     if (mode == XPBD_PROJECT_ACCUMULATE)
         return damp ? launch_project<XPBD_PROJECT_ACCUMULATE, true>(prm, tiles, v, 0, s)
                     : launch_project<XPBD_PROJECT_ACCUMULATE, false>(prm, tiles, v, 0, s);
-    return fail(XPBD_ERR_ARG, "xpbd_project: unknown mode%s");
+    return fail(XPBD_ERR_ARG, "xpbd_project: unknown mode");
 }
 
 int xpbd_apply_boundary(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v, uint32_t ops,
                         xpbd_stream_t stream) {
     int rc;
     if ((rc = check_params(prm)) || (rc = check_verts(v))) return rc;
-    if (!tiles || (tiles->n_boundary > 0 && !tiles->bnd_verts)) return fail(XPBD_ERR_ARG, "xpbd_apply_boundary: tiles%s");
-    if (!v->accum) return fail(XPBD_ERR_ARG, "xpbd_apply_boundary: accum required%s");
+    if (!tiles || (tiles->n_boundary > 0 && !tiles->bnd_verts)) return fail(XPBD_ERR_ARG, "xpbd_apply_boundary: tiles");
+    if (!v->accum) return fail(XPBD_ERR_ARG, "xpbd_apply_boundary: accum required");
     if (tiles->n_boundary == 0) return XPBD_OK;
     k_apply_list<<<(tiles->n_boundary + kVertThreads - 1) / kVertThreads, kVertThreads, 0, (cudaStream_t)stream>>>(
         *prm, *v, tiles->bnd_verts, tiles->n_boundary, ops);
@@ -495,7 +488,7 @@ int xpbd_apply_all(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, xpbd
     int rc;
     if ((rc = check_params(prm)) || (rc = check_verts(v))) return rc;
     if ((ops & (XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_CLEAR)) && !v->accum)
-        return fail(XPBD_ERR_ARG, "xpbd_apply_all: accum required%s");
+        return fail(XPBD_ERR_ARG, "xpbd_apply_all: accum required");
     k_apply_list<<<(v->n + kVertThreads - 1) / kVertThreads, kVertThreads, 0, (cudaStream_t)stream>>>(*prm, *v, nullptr,
                                                                                                        v->n, ops);
     return cuda_check("xpbd_apply_all");
@@ -504,8 +497,8 @@ int xpbd_apply_all(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, xpbd
 int xpbd_pin_overwrite_masked(int32_t n, const int32_t* pts, const float* target, const float* offset,
                               const int32_t* active, float* pos4, xpbd_stream_t stream) {
     if (n < 0 || (n > 0 && (!pts || !target || !offset || !pos4)))
-        return fail(XPBD_ERR_ARG, "xpbd_pin_overwrite_masked: bad arguments%s");
-    if (!aligned16(pos4)) return fail(XPBD_ERR_ALIGN, "xpbd_pin_overwrite_masked: pos4 alignment%s");
+        return fail(XPBD_ERR_ARG, "xpbd_pin_overwrite_masked: bad arguments");
+    if (!aligned16(pos4)) return fail(XPBD_ERR_ALIGN, "xpbd_pin_overwrite_masked: pos4 alignment");
     if (n == 0) return XPBD_OK;
     k_pin_masked<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, pts, target, offset, active,
                                                                     reinterpret_cast<float4*>(pos4));
@@ -515,7 +508,7 @@ int xpbd_pin_overwrite_masked(int32_t n, const int32_t* pts, const float* target
 int xpbd_metrics(const XpbdTiles* tiles, const XpbdVerts* v, XpbdMetrics* out, xpbd_stream_t stream) {
     int rc;
     if ((rc = check_tiles(tiles)) || (rc = check_verts(v))) return rc;
-    if (!out) return fail(XPBD_ERR_ARG, "xpbd_metrics: out%s");
+    if (!out) return fail(XPBD_ERR_ARG, "xpbd_metrics: out");
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(out, 0, sizeof(XpbdMetrics), s) != cudaSuccess) return cuda_check("xpbd_metrics memset");
     const size_t smem = size_t(tiles->max_tile_verts) * sizeof(float4);
@@ -531,7 +524,7 @@ int xpbd_graph_begin(xpbd_stream_t stream) {
     return XPBD_OK;
 }
 int xpbd_graph_end(xpbd_stream_t stream, void** exec_out) {
-    if (!exec_out) return fail(XPBD_ERR_ARG, "xpbd_graph_end: exec_out%s");
+    if (!exec_out) return fail(XPBD_ERR_ARG, "xpbd_graph_end: exec_out");
     cudaGraph_t g = nullptr;
     if (cudaStreamEndCapture((cudaStream_t)stream, &g) != cudaSuccess) return cuda_check("xpbd_graph_end");
     cudaGraphExec_t e = nullptr;
@@ -542,7 +535,7 @@ int xpbd_graph_end(xpbd_stream_t stream, void** exec_out) {
     return XPBD_OK;
 }
 int xpbd_graph_launch(void* exec, xpbd_stream_t stream) {
-    if (!exec) return fail(XPBD_ERR_ARG, "xpbd_graph_launch: exec%s");
+    if (!exec) return fail(XPBD_ERR_ARG, "xpbd_graph_launch: exec");
     if (cudaGraphLaunch((cudaGraphExec_t)exec, (cudaStream_t)stream) != cudaSuccess)
         return cuda_check("xpbd_graph_launch");
     return XPBD_OK;

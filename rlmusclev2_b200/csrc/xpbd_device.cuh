@@ -69,10 +69,15 @@ struct Svd3 {
 
 __device__ __forceinline__ void jacobi_rot(float& spp, float& sqq, float& spq, float& srp, float& srq,
                                            float3& vp, float3& vq) {
-    if (spq == 0.f) return;
-    const float theta = (sqq - spp) / (2.f * spq);
-    const float t = copysignf(1.f, theta) / (fabsf(theta) + sqrtf(fmaf(theta, theta, 1.f)));
-    const float c = 1.f / sqrtf(fmaf(t, t, 1.f));
+    // tan of the rotation angle, t = sign(theta)/(|theta| + sqrt(theta^2 + 1)) with
+    // theta = (sqq - spp)/(2 spq), written without dividing by spq:
+    // t = spq / (h + sign(h) sqrt(h^2 + spq^2)), h = (sqq - spp)/2.  Branch-free;
+    // t = 0 when spq = 0 and h = 0.
+    const float h = 0.5f * (sqq - spp);
+    const float r = sqrtf(fmaf(h, h, spq * spq));
+    const float den = h + copysignf(r, h);
+    const float t = den != 0.f ? __fdividef(spq, den) : 0.f;
+    const float c = rsqrtf(fmaf(t, t, 1.f));
     const float s = t * c;
     spp = fmaf(-t, spq, spp);
     sqq = fmaf(t, spq, sqq);
@@ -100,10 +105,11 @@ __device__ __forceinline__ Svd3 svd3(const M3& F) {
     r.v1 = make_float3(0.f, 1.f, 0.f);
     r.v2 = make_float3(0.f, 0.f, 1.f);
 #pragma unroll 1
-    for (int sweep = 0; sweep < 5; ++sweep) {
+    for (int sweep = 0; sweep < 4; ++sweep) {
+        // converged when the off-diagonal mass is at FP32 rounding level
         const float off = s01 * s01 + s02 * s02 + s12 * s12;
         const float dia = s00 * s00 + s11 * s11 + s22 * s22;
-        if (off <= 1e-15f * dia) break;
+        if (off <= 1e-13f * dia) break;
         // plane (0,1), third index 2: s20=s02, s21=s12
         jacobi_rot(s00, s11, s01, s02, s12, r.v0, r.v1);
         // plane (0,2), third index 1: s10=s01, s12
@@ -124,13 +130,13 @@ __device__ __forceinline__ Svd3 svd3(const M3& F) {
     };
     const float3 b0 = Fv(r.v0), b1 = Fv(r.v1), b2 = Fv(r.v2);
     const float n0 = len(b0);
-    r.u0 = n0 > 1e-30f ? b0 / n0 : make_float3(1.f, 0.f, 0.f);
+    r.u0 = n0 > 1e-30f ? rsqrtf(dot(b0, b0)) * b0 : make_float3(1.f, 0.f, 0.f);
     r.s0 = n0;
     const float pr = dot(r.u0, b1);
     const float3 w = b1 - pr * r.u0;
     const float n1 = len(w);
     if (n1 > 1e-30f * fmaxf(n0, 1.f)) {
-        r.u1 = w / n1;
+        r.u1 = rsqrtf(dot(w, w)) * w;
     } else {
         const float a0 = fabsf(r.u0.x), a1 = fabsf(r.u0.y), a2 = fabsf(r.u0.z);
         float3 e = (a0 <= a1 && a0 <= a2) ? make_float3(1.f, 0.f, 0.f)

@@ -68,3 +68,279 @@ def box_muscle(nx=8, ny=8, nz=32, spacing=0.0025, jitter=0.0002, seed=0, pin_fra
     zr = (z - z.min()) / (z.max() - z.min())
     stopped = ((zr < pin_frac) | (zr > 1.0 - pin_frac)).astype(np.int32)
     return BoxMuscle(verts, tets, fiber, stopped, dict(nx=nx, ny=ny, nz=nz, spacing=spacing, seed=seed))
+
+
+# --------------------------------------------------------------------------
+# humanV2-scale scene: ellipsoidal muscles + fascia shell + capsule bones
+
+
+def _seg_dist(p0, p1, q0, q1) -> float:
+    """Distance between segments p0p1 and q0q1 (clamped closest points)."""
+    d1, d2, r = p1 - p0, q1 - q0, p0 - q0
+    a, e, f = d1 @ d1, d2 @ d2, d2 @ r
+    c, b = d1 @ r, d1 @ d2
+    den = a * e - b * b
+    s = np.clip((b * f - c * e) / den, 0.0, 1.0) if den > 1e-18 else 0.0
+    t = (b * s + f) / e if e > 1e-18 else 0.0
+    if t < 0.0:
+        t, s = 0.0, np.clip(-c / a, 0.0, 1.0) if a > 1e-18 else 0.0
+    elif t > 1.0:
+        t, s = 1.0, np.clip((b - c) / a, 0.0, 1.0) if a > 1e-18 else 0.0
+    return float(np.linalg.norm((p0 + d1 * s) - (q0 + d2 * t)))
+
+
+def _rand_rot(rng) -> np.ndarray:
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+def axis_angle(axis: np.ndarray, ang: float) -> np.ndarray:
+    a = axis / np.linalg.norm(axis)
+    K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    return np.eye(3) + np.sin(ang) * K + (1 - np.cos(ang)) * (K @ K)
+
+
+def clipped_ellipsoid_lattice(L: float, r1: float, r2: float, h: float):
+    """Hex lattice over the ellipsoid's box, cells with centre inside kept,
+    6 tets per cell.  Returns local verts (x along the long axis) and tets."""
+    nx = max(2, int(np.ceil(L / h)))
+    ny = max(2, int(np.ceil(2 * r1 / h)))
+    nz = max(2, int(np.ceil(2 * r2 / h)))
+    hx, hy, hz = L / nx, 2 * r1 / ny, 2 * r2 / nz
+    ci, cj, ck = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
+    cx = -L / 2 + (ci + 0.5) * hx
+    cy = -r1 + (cj + 0.5) * hy
+    cz = -r2 + (ck + 0.5) * hz
+    keep = (cx / (L / 2)) ** 2 + (cy / r1) ** 2 + (cz / r2) ** 2 <= 1.0
+    ci, cj, ck = ci[keep], cj[keep], ck[keep]
+    gid = lambda i, j, k: (i * (ny + 1) + j) * (nz + 1) + k  # noqa: E731
+    tets = hex_to_tets(lambda dx, dy, dz: gid(ci + dx, cj + dy, ck + dz))
+    used, tets = np.unique(tets, return_inverse=True)
+    tets = tets.reshape(-1, 4)
+    gi = used // ((ny + 1) * (nz + 1))
+    gj = (used // (nz + 1)) % (ny + 1)
+    gk = used % (nz + 1)
+    verts = np.stack([-L / 2 + gi * hx, -r1 + gj * hy, -r2 + gk * hz], 1)
+    return verts, tets
+
+
+def boundary_faces(tets: np.ndarray) -> np.ndarray:
+    """Faces used by exactly one tet, wound outward (right-hand normal points
+    away from the tet's fourth vertex)."""
+    f = np.concatenate([tets[:, [0, 1, 2]], tets[:, [0, 1, 3]], tets[:, [0, 2, 3]], tets[:, [1, 2, 3]]])
+    opp = np.concatenate([tets[:, 3], tets[:, 2], tets[:, 1], tets[:, 0]])
+    key = np.sort(f, axis=1)
+    _, idx, cnt = np.unique(key, axis=0, return_index=True, return_counts=True)
+    sel = idx[cnt == 1]
+    return f[sel], opp[sel]
+
+
+def orient_faces_outward(pos: np.ndarray, faces: np.ndarray, opp: np.ndarray) -> np.ndarray:
+    a, b, c = pos[faces[:, 0]], pos[faces[:, 1]], pos[faces[:, 2]]
+    n = np.cross(b - a, c - a)
+    inward = np.einsum("ij,ij->i", n, pos[opp] - a) > 0
+    out = faces.copy()
+    out[inward, 1], out[inward, 2] = faces[inward, 2], faces[inward, 1]
+    return out
+
+
+def extrude_shell(pos: np.ndarray, faces: np.ndarray, thickness: float):
+    """Prism shell outward of a closed surface: new inner and outer vertex
+    layers, 3 tets per prism with the vertex-id diagonal rule (conforming)."""
+    sv, inv = np.unique(faces, return_inverse=True)
+    tri = inv.reshape(-1, 3)
+    p = pos[sv]
+    a, b, c = p[tri[:, 0]], p[tri[:, 1]], p[tri[:, 2]]
+    fn = np.cross(b - a, c - a)
+    vn = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(vn, tri[:, k], fn)
+    vn /= np.maximum(np.linalg.norm(vn, axis=1, keepdims=True), 1e-30)
+    n = p.shape[0]
+    verts = np.concatenate([p, p + thickness * vn])
+    t = np.sort(tri, axis=1)
+    a0, b0, c0 = t[:, 0], t[:, 1], t[:, 2]
+    a1, b1, c1 = a0 + n, b0 + n, c0 + n
+    tets = np.concatenate([np.stack([a0, b0, c0, c1], 1), np.stack([a0, b0, b1, c1], 1),
+                           np.stack([a0, a1, b1, c1], 1)])
+    return verts, tets, sv
+
+
+@dataclass
+class Scene:
+    verts: np.ndarray            # (NV,3) float32, metres
+    tets: np.ndarray             # (NT,4) int32, positively oriented (pt3 reference)
+    tet_part: np.ndarray         # (NT,) muscle index, or -1 for fascia tets
+    vert_part: np.ndarray        # (NV,) muscle index, or -1 for fascia verts
+    v_tendon: np.ndarray         # (NV,) 1 on tendon verts (end 5% of a muscle's axis)
+    v_fiber: np.ndarray          # (NV,3) unit fiber direction
+    surface_tris: np.ndarray     # (NTRI,3) outward muscle surface triangles
+    bone_center: np.ndarray      # (NB,3)
+    bone_axis: np.ndarray        # (NB,3) unit
+    bone_half: np.ndarray        # (NB,) half segment length
+    bone_radius: np.ndarray      # (NB,)
+    vert_bone: np.ndarray        # (NV,) nearest bone per vertex
+    traj: dict                   # bone trajectory parameters
+    aniso_muscle: int
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_bones(self) -> int:
+        return int(self.bone_center.shape[0])
+
+    def bone_transforms(self, frame: float) -> np.ndarray:
+        """(NB,3,4) rigid transforms [R | t] at ``frame``: x -> R (x - c) + c + d,
+        the identity at the start frame (targets bind to the rest pose there)."""
+        tr = self.traj
+        f = float(frame) - float(tr.get("start_frame", 1))
+        out = np.zeros((self.n_bones, 3, 4))
+        for b in range(self.n_bones):
+            ang = tr["rot_amp"][b] * (np.sin(tr["rot_w"][b] * f + tr["rot_phase"][b]) - np.sin(tr["rot_phase"][b]))
+            R = axis_angle(tr["rot_axis"][b], ang)
+            d = tr["tr_amp"][b] * (np.sin(tr["tr_w"][b] * f + tr["tr_phase"][b]) - np.sin(tr["tr_phase"][b])) \
+                * tr["tr_dir"][b]
+            c = self.bone_center[b]
+            out[b, :, :3] = R
+            out[b, :, 3] = c + d - R @ c
+        return out
+
+    def activation(self, frame: int, start: int = 1, end: int = 50) -> np.ndarray:
+        """RampActivationSource (util/activation.py:28-44) on the aniso muscle's tets."""
+        a = min(1.0, max(0.0, (int(frame) - start) / max(1, end - start)))
+        return (a * (self.tet_part == self.aniso_muscle)).astype(np.float32)
+
+
+def capsule_sdf(x: np.ndarray, c: np.ndarray, axis: np.ndarray, half: float, r: float) -> np.ndarray:
+    d = x - c
+    t = np.clip(d @ axis, -half, half)
+    return np.linalg.norm(d - t[..., None] * axis, axis=-1) - r
+
+
+def humanv2_scene(seed: int = 0, n_muscles: int = 40, n_bones: int = 20, target_tets: int = 468_000,
+                  fascia_tets: int = 67_000, fascia_thickness: float = 0.0015, tendon_frac: float = 0.05,
+                  box=(0.7, 0.9, 0.7)) -> Scene:
+    """Synthetic humanV2-scale muscle scene (~172.7k verts / ~535k tets at the
+    defaults): ``n_muscles`` ellipsoids with length U(80,300) mm and radii
+    U(10,40) mm, clipped 6-tet hex lattices, a ``fascia_thickness`` extruded
+    shell over the first muscles' surfaces up to ``fascia_tets`` tets, and
+    ``n_bones`` capsules (radius U(8,20) mm, length U(150,400) mm) on smooth
+    rigid trajectories of at most 5 deg and 10 mm per frame."""
+    rng = np.random.default_rng(seed)
+    box = np.asarray(box)
+    L = rng.uniform(0.080, 0.300, n_muscles)
+    R1 = rng.uniform(0.010, 0.040, n_muscles)
+    R2 = rng.uniform(0.010, 0.040, n_muscles)
+    rots, cents, segs = [], [], []
+    margin = 0.004
+    for i in range(n_muscles):
+        for _ in range(20000):
+            Rm = _rand_rot(rng)
+            c = rng.uniform(0, 1, 3) * box
+            ax = Rm[:, 0]
+            p0, p1 = c - ax * L[i] / 2, c + ax * L[i] / 2
+            ri = max(R1[i], R2[i])
+            if all(_seg_dist(p0, p1, q0, q1) > ri + rj + margin for (q0, q1, rj) in segs):
+                break
+        else:
+            raise RuntimeError("could not place muscles; enlarge the box")
+        rots.append(Rm)
+        cents.append(c)
+        segs.append((p0, p1, ri))
+    bc, ba, bh, br = [], [], [], []
+    for b in range(n_bones):
+        for _ in range(20000):
+            r = rng.uniform(0.008, 0.020)
+            half = rng.uniform(0.150, 0.400) / 2
+            c = rng.uniform(0, 1, 3) * box
+            ax = rng.normal(size=3)
+            ax /= np.linalg.norm(ax)
+            p0, p1 = c - ax * half, c + ax * half
+            ok = all(_seg_dist(p0, p1, q0, q1) > r + rj + 2 * margin for (q0, q1, rj) in segs)
+            ok = ok and all(_seg_dist(p0, p1, bc[k] - ba[k] * bh[k], bc[k] + ba[k] * bh[k]) > r + br[k] + margin
+                            for k in range(len(bc)))
+            if ok:
+                break
+        else:
+            raise RuntimeError("could not place bones; enlarge the box")
+        bc.append(c)
+        ba.append(ax)
+        bh.append(half)
+        br.append(r)
+    bc, ba, bh, br = map(np.asarray, (bc, ba, bh, br))
+    # lattice spacing for the muscle tet budget
+    vol = 4.0 / 3.0 * np.pi * (L / 2) * R1 * R2
+    h = (6.0 * vol.sum() / target_tets) ** (1.0 / 3.0)
+    for _ in range(3):
+        nt = sum(clipped_ellipsoid_lattice(L[i], R1[i], R2[i], h)[1].shape[0] for i in range(n_muscles))
+        h *= (nt / target_tets) ** (1.0 / 3.0)
+    verts, tets, tpart, vpart, vlocal_x, vlen = [], [], [], [], [], []
+    off = 0
+    for i in range(n_muscles):
+        lv, lt = clipped_ellipsoid_lattice(L[i], R1[i], R2[i], h)
+        wv = lv @ rots[i].T + cents[i]
+        verts.append(wv)
+        tets.append(lt + off)
+        tpart.append(np.full(lt.shape[0], i))
+        vpart.append(np.full(lv.shape[0], i))
+        vlocal_x.append(lv[:, 0])
+        vlen.append(np.full(lv.shape[0], L[i]))
+        off += lv.shape[0]
+    mverts = np.concatenate(verts)
+    mtets = orient_tets(mverts, np.concatenate(tets))
+    tpart = np.concatenate(tpart)
+    vpart = np.concatenate(vpart)
+    lx, lL = np.concatenate(vlocal_x), np.concatenate(vlen)
+    xr = (lx + lL / 2) / lL
+    tendon = ((xr < tendon_frac) | (xr > 1 - tendon_frac)).astype(np.float32)
+    faces, opp = boundary_faces(mtets)
+    surf = orient_faces_outward(mverts, faces, opp)
+    # fascia shell over the first muscles' surfaces, up to the tet budget
+    face_part = vpart[surf[:, 0]]
+    chosen, acc = [], 0
+    for i in range(n_muscles):
+        nf = int((face_part == i).sum())
+        if acc + 3 * nf > fascia_tets * 1.05 and chosen:
+            continue
+        chosen.append(i)
+        acc += 3 * nf
+        if acc >= fascia_tets * 0.95:
+            break
+    fsel = np.isin(face_part, chosen)
+    fverts, ftets, _ = extrude_shell(mverts, surf[fsel], fascia_thickness)
+    nmv = mverts.shape[0]
+    allv = np.concatenate([mverts, fverts]).astype(np.float32)
+    ftets = orient_tets(allv, ftets + nmv)
+    alltets = np.concatenate([mtets, ftets]).astype(np.int32)
+    tet_part = np.concatenate([tpart, np.full(ftets.shape[0], -1)]).astype(np.int32)
+    vert_part = np.concatenate([vpart, np.full(fverts.shape[0], -1)]).astype(np.int32)
+    v_tendon = np.concatenate([tendon, np.zeros(fverts.shape[0], np.float32)])
+    # fibers: each muscle's long axis with N(0, 10 deg) per-vertex noise
+    fib = np.zeros((allv.shape[0], 3))
+    for i in range(n_muscles):
+        sel = np.nonzero(vpart == i)[0]
+        ax = rots[i][:, 0]
+        perp = np.cross(ax, rng.normal(size=(sel.shape[0], 3)))
+        perp /= np.maximum(np.linalg.norm(perp, axis=1, keepdims=True), 1e-12)
+        ang = np.deg2rad(rng.normal(0.0, 10.0, sel.shape[0]))
+        fib[sel] = np.cos(ang)[:, None] * ax + np.sin(ang)[:, None] * perp
+    fib[vert_part < 0] = [1.0, 0.0, 0.0]
+    # nearest bone per vertex (surface distance of the capsule)
+    dist = np.stack([capsule_sdf(allv.astype(np.float64), bc[b], ba[b], bh[b], br[b]) for b in range(n_bones)], 1)
+    vert_bone = dist.argmin(1).astype(np.int32)
+    aniso = int(np.argmax(L * R1 * R2))
+    traj = dict(rot_axis=rng.normal(size=(n_bones, 3)), rot_amp=np.deg2rad(rng.uniform(10, 25, n_bones)),
+                rot_w=rng.uniform(0.05, 0.12, n_bones), rot_phase=rng.uniform(0, 2 * np.pi, n_bones),
+                tr_dir=rng.normal(size=(n_bones, 3)), tr_amp=rng.uniform(0.01, 0.04, n_bones),
+                tr_w=rng.uniform(0.05, 0.12, n_bones), tr_phase=rng.uniform(0, 2 * np.pi, n_bones))
+    traj["tr_dir"] /= np.linalg.norm(traj["tr_dir"], axis=1, keepdims=True)
+    traj["start_frame"] = 1
+    return Scene(verts=allv, tets=alltets, tet_part=tet_part, vert_part=vert_part, v_tendon=v_tendon,
+                 v_fiber=fib.astype(np.float32), surface_tris=surf.astype(np.int32), bone_center=bc, bone_axis=ba,
+                 bone_half=bh, bone_radius=br, vert_bone=vert_bone, traj=traj, aniso_muscle=aniso,
+                 meta=dict(seed=seed, h=h, n_muscle_verts=nmv, n_muscle_tets=mtets.shape[0],
+                           n_fascia_tets=ftets.shape[0], fascia_muscles=chosen))

@@ -1,0 +1,361 @@
+"""MultiGridSim (the reference's OneWaySim successor, src/muscle/mg/mg.py:85-1443)
+on the sm_100a engine.
+
+Same JSON schema (``constraints[]`` blocks looked up by name with ``enable``
+toggles, solver keys at the top level).  The rest mesh comes from a seeded
+synthetic generator (``cfg["synthetic"]``) because the reference's humanV2
+assets are not available; each vertex is bound to its nearest capsule bone and
+its target rides that bone rigidly (the reference's target_mode="mesh"
+binding with sliding off).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _capi as capi
+from .builder import ConstraintTable, collect_raw_constraints, create_attach_constraints, lumped_mass, tet_rest_data
+from .collision import GridSdfCollider
+from .meshgen import Scene, humanv2_scene
+from .musclesim import MuscleSim
+
+
+def find_constraint(cfg: dict, name: str) -> dict | None:
+    """mg.py:71-82: the constraint block named ``name`` unless ``enable`` is false."""
+    for c in cfg.get("constraints", []):
+        if c.get("name") == name:
+            return c if c.get("enable", True) else None
+    return None
+
+
+def load_config(config_path: str) -> dict:
+    """mg.py:1437-1443: JSON scene config with cwd-resolved relative paths."""
+    cfg = json.load(open(config_path))
+    for key in ("geo_dir", "cons_dir", "rest_path", "fascia_path"):
+        if key in cfg and not Path(cfg[key]).is_absolute():
+            cfg[key] = str(Path.cwd() / cfg[key])
+    return cfg
+
+
+def scene_from_cfg(cfg: dict) -> Scene:
+    syn = dict(cfg.get("synthetic") or {})
+    kind = syn.pop("kind", "humanv2")
+    if kind != "humanv2":
+        raise ValueError(f"unknown synthetic scene kind {kind!r}")
+    return humanv2_scene(**syn)
+
+
+class MultiGridSim(MuscleSim):
+    """One-way pin-to-target XPBD solver (mg.py:85)."""
+
+    def __init__(self, cfg: dict, device: str | None = "cuda:0", scene: Scene | None = None):
+        self.cfg = cfg
+        self._device_str = device or "cuda:0"
+        self.quasi_static = bool(cfg.get("quasi_static", False))
+        self._gravity_vec = tuple(float(x) for x in cfg.get("gravity", [0.0, 0.0, 0.0]))
+        _arap = find_constraint(cfg, "arap")
+        if _arap is None:
+            raise ValueError("constraints[] must define an 'arap' entry (the muscle ARAP-SVD shape match)")
+        self.mu = float(_arap["stiffness"])
+        self._arap_damp = float(_arap.get("dampingratio", 0.0))
+        _snh = find_constraint(cfg, "snh")
+        self.use_snh = _snh is not None
+        self.snh_mu = float(_snh.get("mu", _snh.get("stiffness", self.mu))) if _snh else 0.0
+        self.snh_lam = float(_snh.get("lam", 1.0e8)) if _snh else 0.0
+        self.snh_damp = float(_snh.get("dampingratio", self._arap_damp)) if _snh else 0.0
+        self.snh_region = str(_snh.get("region", "all")) if _snh else "all"
+        self.omega = float(cfg["omega"])
+        self.dt_frame = float(cfg["delta_t"])
+        self.nsubsteps = int(cfg["nsubsteps"])
+        self.num_substeps = self.nsubsteps
+        self.presubframe_pintotarget = float(cfg.get("presubframe_pintotarget", 0.0))
+        if self.presubframe_pintotarget > 0.0:
+            raise NotImplementedError("presubframe_pintotarget > 0 is not on the sm_100a path")
+        self.fine_iters = int(cfg["fine_iterations"])
+        self.total_mass = float(cfg["total_mass"])
+        self.dt = self.dt_frame / self.nsubsteps
+        self.end_frame = int(cfg.get("end_frame", 90))
+        self.start_frame = int(cfg.get("start_frame", 1))
+        self.use_multigrid = bool(cfg.get("use_multigrid", False))
+        self.mg_mode = str(cfg.get("mg_mode", "hpbd")).lower()
+        if self.mg_mode not in ("projection", "hpbd"):
+            raise ValueError(f"mg_mode must be 'projection' or 'hpbd', got {self.mg_mode!r}")
+        self.mg_coarse_iters = int(cfg.get("mg_coarse_iters", 15))
+        _vol = find_constraint(cfg, "volume")
+        self.use_volume = _vol is not None
+        self.volume_stiffness = float(_vol["stiffness"]) if _vol else 1.0e10
+        self.volume_damp = float(_vol.get("dampingratio", 0.0)) if _vol else 0.0
+        _fib = find_constraint(cfg, "fiber")
+        self.use_fiber = _fib is not None
+        self.fiber_model = str((_fib or {}).get("fiber_model", "aniso_arap"))
+        self.fiber_stiffness = float((_fib or {}).get("stiffness", 1.0e8))
+        self.fiber_damp = float((_fib or {}).get("dampingratio", 0.0))
+        self.contraction_ratio = float((_fib or {}).get("contraction_ratio", 0.4))
+        self.fiber_region = str((_fib or {}).get("region", "all"))
+        if self.use_fiber and self.fiber_model != "aniso_arap":
+            raise NotImplementedError(f"fiber_model={self.fiber_model!r} is not on the sm_100a path "
+                                      "(supported: 'aniso_arap')")
+        if cfg.get("rest_path") and Path(cfg["rest_path"]).exists() and scene is None and "synthetic" not in cfg:
+            raise NotImplementedError("loading .geo/.usd rest meshes is not part of this project; "
+                                      "provide cfg['synthetic'] or a Scene")
+        self.scene = scene if scene is not None else scene_from_cfg(cfg)
+        sc = self.scene
+        self.pos0_np = sc.verts.astype(np.float32)
+        self.tet_np = sc.tets.astype(np.int32)
+        self.NV = self.n_verts = int(self.pos0_np.shape[0])
+        self.NT = int(self.tet_np.shape[0])
+        self.use_jacobi = True
+        self.use_colored_gs = False
+        self.has_compressstiffness = False
+        self.fiber_stiffness_scale = 1.0
+        self.step_cnt = 0
+        # constraint set (mg.py:374-399): SNH or ARAP-SVD, optional volume and fiber
+        fascia = sc.tet_part < 0
+        masks = {}
+        if self.use_snh:
+            cons = [dict(type="snh", name="snh", mu=self.snh_mu, lam=self.snh_lam, dampingratio=self.snh_damp)]
+            if self.snh_region == "fascia":
+                masks["snh"] = fascia
+                masks["arap"] = ~fascia
+                cons.append(dict(type="tetarapsvd", name="arap", stiffness=self.mu, dampingratio=self._arap_damp))
+            elif self.snh_region != "all":
+                raise ValueError(f"snh region must be 'all' or 'fascia', got {self.snh_region!r}")
+        else:
+            cons = [dict(type="tetarapsvd", name="arap", stiffness=self.mu, dampingratio=self._arap_damp)]
+        if self.use_volume and not (self.use_snh and self.snh_region == "all"):
+            cons.append(dict(type="volume", name="volume", stiffness=self.volume_stiffness,
+                             dampingratio=self.volume_damp))
+            if self.use_snh:
+                masks["volume"] = ~fascia
+        if self.use_fiber:
+            cons.append(dict(type="aniso_arap", name="fiber", stiffness=self.fiber_stiffness,
+                             dampingratio=self.fiber_damp))
+            if self.fiber_region == "aniso_muscle":
+                masks["fiber"] = sc.tet_part == sc.aniso_muscle
+            elif self.fiber_region != "all":
+                raise ValueError(f"fiber region must be 'all' or 'aniso_muscle', got {self.fiber_region!r}")
+        self.constraint_configs = cons
+        table = collect_raw_constraints(self.pos0_np, self.tet_np, cons, tet_masks=masks)
+        # density = total_mass / sum(signed V0) (mg.py:736-740), mass = |V| rho / 4
+        _, V0, valid = tet_rest_data(self.pos0_np, self.tet_np)
+        self.density = self.total_mass / float(max(V0[valid].astype(np.float64).sum(), 1e-30))
+        mass, rest_volume = lumped_mass(self.pos0_np, self.tet_np, self.density)
+        self.total_rest_volume = float(rest_volume.astype(np.float64).sum())
+        # pins (muscleToBonePin, mg.py:486-535) and belly attach (mg.py:700-723)
+        self.NCONS = self.NV
+        self._pin_pts_np = np.arange(self.NV, dtype=np.int64)
+        _pin = find_constraint(cfg, "muscleToBonePin")
+        active = np.zeros(self.NV, np.int32)
+        if _pin is not None:
+            region = str(_pin.get("region", "tendonmask")).lower()
+            if region == "full":
+                active[:] = 1
+            elif region == "tendonmask":
+                thr = _pin.get("tendon_pin_threshold")
+                if thr is None:
+                    raise ValueError("muscleToBonePin region='tendonmask' requires tendon_pin_threshold")
+                active = (sc.v_tendon > float(thr)).astype(np.int32)
+            elif region == "pinmask":
+                active[:] = 0  # the synthetic rest carries no authored pinmask
+            else:
+                raise ValueError(f"muscleToBonePin 'region' must be 'full', 'tendonmask' or 'pinmask', got {region!r}")
+        self.pin_active_np = active
+        _belly = find_constraint(cfg, "belly_attach")
+        self._belly_enabled = _belly is not None
+        self.pin_attach_stiffness = float(_belly["stiffness"]) if _belly else 0.0
+        self.pin_attach_damp = float(_belly.get("dampingratio", 0.0)) if _belly else 0.0
+        self.rest_offset_np = np.zeros((self.NV, 3), np.float32)
+        target0 = self._host_targets(self.start_frame)
+        parts = [table]
+        if self._belly_enabled:
+            belly = np.nonzero(active == 0)[0]
+            parts.append(create_attach_constraints(belly, target0[belly] + self.rest_offset_np[belly], 0.0,
+                                                   self.pin_attach_stiffness, self.pin_attach_damp))
+        table = ConstraintTable.concat(parts).sorted_by_type()
+        self.raw_constraints = table
+        self._pin_user = (active != 0, target0 + self.rest_offset_np, active)
+        self._has_pins = bool(active.any())
+        tendon_tet = (sc.v_tendon[self.tet_np].astype(np.float32).sum(1) / np.float32(4.0)).astype(np.float32)
+        self._setup_device(self._device_str, mass=mass, stopped=np.zeros(self.NV, np.int32), table=table,
+                           v_fiber=sc.v_fiber, tet_tendonmask=tendon_tet, dt=self.dt,
+                           gravity_vec=self._gravity_vec, veldamping=float(cfg.get("veldamping", 0.0)),
+                           quasi_static=self.quasi_static, omega=1.0, contraction_ratio=self.contraction_ratio,
+                           fiber_stiffness_scale=self.fiber_stiffness_scale, tile_tets=cfg.get("tile_tets"))
+        self._setup_kinematics()
+        self.collision_solvers = []
+        self.collision_solvers_iter = []
+        coll = (cfg.get("demo") or {}).get("collision") or {}
+        if coll.get("enabled", False):
+            self.bone_collider = GridSdfCollider(
+                self, sc.bone_center, sc.bone_axis, sc.bone_half, sc.bone_radius, res=int(coll.get("sdf_res", 256)),
+                contact_offset=float(coll.get("contact_offset", 0.0)), max_push=float(coll.get("max_push", -1.0)))
+            self.bone_collider.transforms = self._bone_tr
+            self.collision_solvers.append(self.bone_collider)
+        self._frame_loaded = None
+
+    # ----------------------------------------------------------- kinematics
+    def _host_targets(self, frame: float) -> np.ndarray:
+        T = self.scene.bone_transforms(frame)
+        b = self.scene.vert_bone
+        x = self.pos0_np.astype(np.float64)
+        return (np.einsum("nij,nj->ni", T[b, :, :3], x) + T[b, :, 3]).astype(np.float32)
+
+    def _setup_kinematics(self) -> None:
+        L = self.layout
+        dev = self.device
+        nb = self.scene.n_bones
+        self._bone_tr = torch.zeros((nb, 12), dtype=torch.float32, device=dev)
+        self._bone_tr_host = torch.zeros((nb, 12), dtype=torch.float32).pin_memory()
+        self._vert_bone = torch.from_numpy(self.scene.vert_bone[L.perm].astype(np.int32)).to(dev)
+        r4 = np.zeros((self.NV, 4), np.float32)
+        r4[:, :3] = self.pos0_np
+        self._rest4 = torch.from_numpy(r4[L.perm]).to(dev)
+        self._tet_perm_d = torch.from_numpy(L.tet_perm.astype(np.int32)).to(dev)
+        self._vinv_d = torch.from_numpy(L.inv.astype(np.int32)).to(dev)
+        self._act_user = torch.zeros(self.NT, dtype=torch.float32, device=dev)
+        self._act_host = torch.zeros(self.NT, dtype=torch.float32).pin_memory()
+        self._pos_user = torch.zeros((self.NV, 3), dtype=torch.float32, device=dev)
+        self._pos_host = torch.zeros((self.NV, 3), dtype=torch.float32).pin_memory()
+        self._h2d_event = torch.cuda.Event()
+        self._h2d_event.record(self._stream)
+
+    def load_frame_targets(self, frame: float) -> None:
+        """Bone poses of ``frame`` -> device (one pinned H2D copy), then the
+        per-vertex pin/attach targets on the device (mg.py:1386-1407)."""
+        T = self.scene.bone_transforms(frame).reshape(self.scene.n_bones, 12).astype(np.float32)
+        self._h2d_event.synchronize()  # the previous copy has consumed the pinned buffer
+        self._bone_tr_host.numpy()[:] = T
+        with torch.cuda.stream(self._stream):
+            self._bone_tr.copy_(self._bone_tr_host, non_blocking=True)
+        self._h2d_event.record(self._stream)
+        self._frame_loaded = frame
+
+    def _targets_kernel(self) -> None:
+        v = self._verts
+        capi.check(self._lib.xpbd_bone_targets(self.NV, self.scene.n_bones, C.c_void_p(self._bone_tr.data_ptr()),
+                                               C.c_void_p(self._vert_bone.data_ptr()),
+                                               C.c_void_p(self._rest4.data_ptr()), v.pin_target, v.attach_target,
+                                               self._sp))
+
+    def set_fiber_activation(self, acti_np) -> None:
+        """Per-tet activation in user tet order (mg.py:1098-1111): pinned H2D copy,
+        then a device gather into the library's tet order."""
+        if not self.use_fiber or self._t_act is None:
+            raise RuntimeError("set_fiber_activation requires use_fiber=True.")
+        a = np.asarray(acti_np, np.float32).reshape(-1)
+        if a.shape[0] != self.NT:
+            raise ValueError(f"activation has {a.shape[0]} entries, expected NT={self.NT}")
+        self._h2d_event.synchronize()
+        self._act_host.numpy()[:] = a
+        with torch.cuda.stream(self._stream):
+            self._act_user.copy_(self._act_host, non_blocking=True)
+        self._h2d_event.record(self._stream)
+        capi.check(self._lib.xpbd_gather(self.NT, 1, C.c_void_p(self._tet_perm_d.data_ptr()),
+                                         C.c_void_p(self._act_user.data_ptr()), 1, C.c_void_p(self._t_act.data_ptr()),
+                                         1, self._sp))
+
+    def positions_np(self) -> np.ndarray:
+        """Positions in the user's vertex order: device gather, one D2H copy."""
+        capi.check(self._lib.xpbd_gather(self.NV, 3, C.c_void_p(self._vinv_d.data_ptr()),
+                                         C.c_void_p(self._pos4.data_ptr()), 4, C.c_void_p(self._pos_user.data_ptr()),
+                                         3, self._sp))
+        with torch.cuda.stream(self._stream):
+            self._pos_host.copy_(self._pos_user, non_blocking=True)
+        self._stream.synchronize()
+        return self._pos_host.numpy().copy()
+
+    # -------------------------------------------------------------- program
+    def apply_pintotarget(self) -> None:
+        """Hard pin of the active tendon verts (mg.py:1251-1261)."""
+        if self._has_pins:
+            self._apply_all(capi.APPLY_PIN)
+
+    def _vstep_sdf_only(self, coll) -> None:
+        sdf = coll.struct()
+        capi.check(self._lib.xpbd_vertex_step(C.byref(self._prm), C.byref(self._verts), capi.OP_SDF, C.byref(sdf),
+                                              self._sp))
+
+    def build_program(self):
+        """mg.py:1322-1378: pre_phase, iter_phase, post_phase."""
+        s = self
+
+        def pre_phase():
+            s.integrate()
+            if s.use_multigrid:
+                s._multigrid_pre()
+            s.apply_pintotarget()
+
+        def iter_phase():
+            for it in range(s.fine_iters):
+                s.clear()
+                s.solve_constraints(run_extras=False)
+                s.apply_dP()
+                s.apply_pintotarget()
+                for fn in getattr(s, "collision_solvers_iter", None) or []:
+                    fn(it)
+
+        def post_phase():
+            for fn in getattr(s, "collision_solvers", None) or []:
+                fn()
+            s.update_velocities()
+
+        self.program = [pre_phase, iter_phase, post_phase]
+
+    def substep(self) -> None:
+        if getattr(self, "program", None) is None:
+            self.build_program()
+        for phase in self.program:
+            phase()
+
+    def _multigrid_pre(self) -> None:
+        raise NotImplementedError("multigrid is enabled but the coarse cage is not built")
+
+    def _kinematic_step(self, t: float) -> None:
+        """mg.py:1396-1407: targets for frame t, hard pin (presubframe soft pin is 0)."""
+        if self._frame_loaded != t:
+            self.load_frame_targets(t)
+        self._targets_kernel()
+        if getattr(self, "bone_collider", None) is not None:
+            self.bone_collider.bake()
+        self.apply_pintotarget()
+
+    def _fusable(self) -> bool:
+        cs = getattr(self, "collision_solvers", None) or []
+        return (not getattr(self, "collision_solvers_iter", None) and not getattr(self, "constraint_solvers", None)
+                and all(isinstance(c, GridSdfCollider) for c in cs) and len(cs) <= 1 and not self.use_multigrid
+                and getattr(self, "program", None) is None)
+
+    def _frame_fused(self) -> None:
+        self._targets_kernel()
+        sdf = self.collision_solvers[0] if self.collision_solvers else None
+        if sdf is not None:
+            sdf.bake()
+        self._sdf = sdf
+        pin = capi.OP_PIN if self._has_pins else 0
+        if pin:
+            self._vstep(capi.OP_PIN)
+        vel = 0 if self.quasi_static else capi.OP_VELOCITY
+        push = capi.OP_SDF if sdf is not None else 0
+        for sub in range(self.nsubsteps):
+            ops = capi.OP_PREDICT | pin | ((push | vel) if sub > 0 else 0)
+            self._vstep(ops)
+            for _ in range(self.fine_iters):
+                self._fused_iteration()
+        if push | vel:
+            self._vstep(push | vel)
+
+    def step_frame(self, frame: int) -> None:
+        """mg.py:1409-1418: kinematic step then nsubsteps substeps at that pose."""
+        if self._frame_loaded != frame:
+            self.load_frame_targets(frame)
+        if self._fusable():
+            self._graph("frame", self._frame_fused)
+        else:
+            self._kinematic_step(frame)
+            for _ in range(self.nsubsteps):
+                self.substep()
+        self.step_cnt += 1
