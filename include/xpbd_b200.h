@@ -71,7 +71,7 @@ typedef struct XpbdParams {
     float fiber_stiffness_scale; /* aniso_arap stiffness multiplier */
     int32_t n_materials;
     int32_t n_attach_materials;
-    int32_t reserved;
+    int32_t tile_variant;        /* tile-pass build: 0 = 2 CTAs/SM (128 regs), 1 = 3 CTAs/SM (80 regs) */
     XpbdMaterial materials[XPBD_MAX_MATERIALS];
     XpbdAttachMaterial attach[XPBD_MAX_ATTACH_MATERIALS];
 } XpbdParams;
@@ -115,6 +115,8 @@ typedef struct XpbdTiles {
     const float* tet_fiber;    /* [n_tets][4] f0.xyz, tendonmask; NULL without aniso */
     const float* tet_act;      /* [n_tets] activation; NULL without aniso */
     const int32_t* bnd_verts;  /* [n_boundary] boundary vertex ids */
+    const int32_t* vert_ntiles; /* [n_verts] number of tiles touching each vertex (FUSED_LAST mode) */
+    int32_t* arrive;            /* [n_verts] arrival counters, zero between iterations (FUSED_LAST mode) */
 } XpbdTiles;
 
 /* Grid signed-distance field of the bones, phi[z][y][x], x fastest. */
@@ -157,6 +159,8 @@ enum {
 enum {
     XPBD_PROJECT_FUSED = 0,      /* apply interior vertices in place, accumulate boundary ones */
     XPBD_PROJECT_ACCUMULATE = 1, /* accumulate every vertex into accum (reference dP/dPw) */
+    XPBD_PROJECT_FUSED_LAST = 2, /* FUSED, and the last tile to reach a boundary vertex finishes it:
+                                    a whole Jacobi iteration in one launch (needs vert_ntiles, arrive) */
 };
 
 int xpbd_abi_version(void);
@@ -222,6 +226,38 @@ int xpbd_sdf_bake_capsules(const XpbdSdf* sdf, int32_t n_caps, const XpbdCapsule
 /* dst[i] = src[idx[i]] for float lanes of width `width` (1..4). */
 int xpbd_gather(int32_t n, int32_t width, const int32_t* idx, const float* src, int32_t src_stride, float* dst,
                 int32_t dst_stride, xpbd_stream_t stream);
+
+/* Two-level multigrid transfer (hpbd V-cycle, mg/mg.py:1064-1079).  Coarse
+ * vertex ids in the restriction/blocks are the cage's own ids (cage order);
+ * coarse_lib maps them to the coarse engine's library order.  Fine ids are
+ * fine library ids. */
+typedef struct XpbdCage {
+    int32_t n_fine, n_coarse, n_blocks, max_block;
+    const int32_t* r_ptr;      /* [n_coarse+1] restriction CSR per coarse vertex (cage order) */
+    const int32_t* r_fine;     /* [nnz] fine vertex */
+    const float* r_w;          /* [nnz] prolongation weight of that fine vertex on this coarse vertex */
+    const int32_t* blk_ptr;    /* [n_blocks+1] coarse vertices of block b: [blk_ptr[b], blk_ptr[b+1]) */
+    const int32_t* blk_moff;   /* [n_blocks] offset of the block's dim x dim row-major (P^T P)^-1 in minv */
+    const float* minv;
+    const int32_t* coarse_lib; /* [n_coarse] cage order -> coarse library order */
+    const int32_t* p_idx;      /* [n_fine][4] coarse library ids of the embedding tet, -1 = not embedded */
+    const float* p_w;          /* [n_fine][4] barycentric weights (1-u-v-w, u, v, w) */
+} XpbdCage;
+
+/* Galerkin restriction x_c = (P^T P)^-1 P^T x_f of the xyz lanes of fine4
+ * into coarse4 (restrict_galerkin_scatter_kernel + block_solve_kernel,
+ * mg/kernel.py:137-178).  Optional: coarse_prev4 receives the same values
+ * (the q_j snapshot, mg/mg.py:1077), and where coarse_pin4[c].w != 0 the
+ * coarse position is overwritten by coarse_pin4[c].xyz (the coarse kinematic
+ * pin, mg/mg.py:1013-1026).  One CTA per block, no atomics. */
+int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, float* coarse_prev4,
+                     const float* coarse_pin4, xpbd_stream_t stream);
+
+/* fine4.xyz += sum_k w_k (coarse4 - coarse_prev4)[p_idx_k] (prolong_delta_kernel,
+ * mg/kernel.py:8-39), then the fine pin overwrite where vflags has
+ * XPBD_VF_PIN and pin_target.w != 0 (vflags/pin_target may be NULL). */
+int xpbd_mg_prolong_delta(const XpbdCage* cage, const float* coarse4, const float* coarse_prev4, float* fine4,
+                          const int32_t* vflags, const float* pin_target, xpbd_stream_t stream);
 
 /* Stream capture helpers (a captured substep replays as one graph launch). */
 int xpbd_graph_begin(xpbd_stream_t stream);

@@ -401,6 +401,79 @@ class OracleMultiGridSim(OracleSolver):
                                         scene.bone_radius[:, None]], 1)
         self.inv_mass = np.where(self.mass > 0, 1.0 / np.where(self.mass > 0, self.mass, 1), 0).astype(self.P.dt)
         self.target = None
+        self.mg = None
+        if cfg.get("use_multigrid", False):
+            self._init_mg(float(arap["stiffness"]))
+
+    # ---- multigrid (mg/mg.py:744-1079, mg/kernel.py:8-178) --------------------
+    def _init_mg(self, mu):
+        from rlmusclev2_b200.meshgen import build_cage  # synthetic input geometry only
+        cfg, P = self.cfg, self.P
+        cage = build_cage(self.scene, spacing=float(cfg.get("mg_cage_spacing", 0.016)))
+        self.cage = cage
+        emb = np.nonzero(cage.cage_idx >= 0)[0]
+        self.mg_emb = emb
+        self.mg_t = cage.coarse_tet[cage.cage_idx[emb]]
+        u = cage.uvw[emb].astype(P.dt)
+        self.mg_w = np.concatenate([(P.dt(1) - u[:, 0] - u[:, 1] - u[:, 2])[:, None], u], 1)
+        nc = cage.coarse_pos.shape[0]
+        starts = np.nonzero(np.r_[True, np.diff(cage.blk_base) != 0])[0]
+        self.mg_blocks = [(int(cage.blk_base[s0]), int(cage.blk_dim[s0]),
+                           cage.minv_flat[cage.blk_matoff[s0]:cage.blk_matoff[s0] + cage.blk_dim[s0] ** 2]
+                           .astype(P.dt).reshape(cage.blk_dim[s0], cage.blk_dim[s0])) for s0 in starts]
+        q0 = self.restrict(self.scene.verts.astype(P.dt)).astype(np.float32)
+        r = q0[cage.coarse_tet].astype(np.float64)  # _rest_B_p3ref (mg.py:43-53)
+        Dm = np.stack([r[:, 0] - r[:, 3], r[:, 1] - r[:, 3], r[:, 2] - r[:, 3]], axis=-1)
+        B = np.linalg.inv(Dm).astype(np.float32)
+        rp = cage.coarse_pos[cage.coarse_tet].astype(np.float64)  # _node_mass_redistribute (mg.py:56-68)
+        vol = np.abs(np.linalg.det(np.stack([rp[:, 1] - rp[:, 0], rp[:, 2] - rp[:, 0], rp[:, 3] - rp[:, 0]], -1))) / 6
+        m = np.zeros(nc)
+        np.add.at(m, cage.coarse_tet.reshape(-1), np.repeat(vol / 4.0, 4))
+        m *= float(cfg["total_mass"]) / m.sum()
+        w4 = np.abs(self.mg_w.astype(np.float64))
+        wacc, pacc = np.zeros(nc), np.zeros(nc)
+        np.add.at(wacc, self.mg_t.reshape(-1), w4.reshape(-1))
+        np.add.at(pacc, self.mg_t.reshape(-1), (self.active[emb].astype(np.float64)[:, None] * w4).reshape(-1))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            frac = np.where(wacc > 1e-9, pacc / wacc, 0.0)
+        pin = ((frac >= float(cfg.get("mg_coarse_pin_frac", 0.5))) & (wacc > 1e-9)).astype(np.int32)
+        self.mg_pin = pin.astype(bool)
+        t = Table()
+        V0, _ = signed_rest_volume(q0, cage.coarse_tet)
+        t.add(T_TETARAPSVD, cage.coarse_tet, mu, 0.0, np.arange(cage.coarse_tet.shape[0]), V0)
+        t.finalize()
+        self.mg = OracleSolver(q0, cage.coarse_tet, t, m.astype(np.float32), pin, B, dt=self.dt, gravity_vec=(0, 0, 0),
+                               prec=P.name)
+        self.mg_iters = int(cfg.get("mg_coarse_iters", 15))
+
+    def restrict(self, x):
+        """restrict_galerkin_scatter_kernel + block_solve_kernel (serial scatter in fine order)."""
+        P = self.P
+        nc = self.cage.coarse_pos.shape[0]
+        b = np.zeros((nc, 3), P.dt)
+        xe = x[self.mg_emb].astype(P.dt)
+        for k in range(4):
+            np.add.at(b, self.mg_t[:, k], self.mg_w[:, k:k + 1] * xe)
+        out = np.zeros_like(b)
+        for base, dim, M in self.mg_blocks:
+            out[base:base + dim] = M @ b[base:base + dim]
+        return out
+
+    def vcycle(self):
+        """_hpbd_vcycle (mg.py:1064-1079) with beta = 0 (no coarse soft attach)."""
+        co = self.mg
+        co.pos[:] = self.restrict(self.pos)
+        prev = co.pos.copy()
+        tgt = self.restrict(self.target)
+        co.pos[self.mg_pin] = tgt[self.mg_pin]
+        for _ in range(self.mg_iters):
+            co.project()
+            co.apply_dP()
+        d = co.pos - prev
+        e = self.mg_emb
+        w = self.mg_w
+        self.pos[e] += ((w[:, 0:1] * d[self.mg_t[:, 0]] + w[:, 1:2] * d[self.mg_t[:, 1]]) + w[:, 2:3] * d[self.mg_t[:, 2]]) \
+            + w[:, 3:4] * d[self.mg_t[:, 3]]
 
     def targets(self, frame):
         T = self.scene.bone_transforms(frame).astype(np.float32)
@@ -427,6 +500,8 @@ class OracleMultiGridSim(OracleSolver):
             self.phi = sdf_bake((r, r, r), self.sdf_origin, self.sdf_h, self.caps, T, self.band, self.P.name)
         for _ in range(self.nsub):
             self.integrate()
+            if self.mg is not None:
+                self.vcycle()
             self.apply_pins()
             for _ in range(self.fine_iters):
                 self.project()

@@ -18,7 +18,7 @@ MAT_ARAPSVD, MAT_VOLUME, MAT_ANISO, MAT_SNH, MAT_DAMPED = 1, 2, 4, 8, 16
 VF_ATTACH_MASK, VF_PIN = 0xFF, 1 << 8
 OP_SDF, OP_VELOCITY, OP_PREDICT, OP_PIN = 1, 2, 4, 8
 APPLY_ATTACH, APPLY_DIVIDE, APPLY_PIN, APPLY_CLEAR = 1, 2, 4, 8
-PROJECT_FUSED, PROJECT_ACCUMULATE = 0, 1
+PROJECT_FUSED, PROJECT_ACCUMULATE, PROJECT_FUSED_LAST = 0, 1, 2
 
 
 class XpbdMaterial(C.Structure):
@@ -34,7 +34,7 @@ class XpbdParams(C.Structure):
     _fields_ = [("dt", C.c_float), ("gravity", C.c_float * 3), ("veldamping", C.c_float),
                 ("quasi_static", C.c_int32), ("omega", C.c_float), ("contraction_ratio", C.c_float),
                 ("fiber_stiffness_scale", C.c_float), ("n_materials", C.c_int32),
-                ("n_attach_materials", C.c_int32), ("reserved", C.c_int32),
+                ("n_attach_materials", C.c_int32), ("tile_variant", C.c_int32),
                 ("materials", XpbdMaterial * MAX_MATERIALS),
                 ("attach", XpbdAttachMaterial * MAX_ATTACH_MATERIALS)]
 
@@ -50,7 +50,8 @@ class XpbdTiles(C.Structure):
                 ("max_tile_verts", C.c_int32), ("tile_vptr", C.c_void_p), ("tile_nint", C.c_void_p),
                 ("tile_tptr", C.c_void_p), ("tile_verts", C.c_void_p), ("tet_q", C.c_void_p),
                 ("tet_b0", C.c_void_p), ("tet_b1", C.c_void_p), ("tet_b2", C.c_void_p),
-                ("tet_fiber", C.c_void_p), ("tet_act", C.c_void_p), ("bnd_verts", C.c_void_p)]
+                ("tet_fiber", C.c_void_p), ("tet_act", C.c_void_p), ("bnd_verts", C.c_void_p),
+                ("vert_ntiles", C.c_void_p), ("arrive", C.c_void_p)]
 
 
 class XpbdSdf(C.Structure):
@@ -61,6 +62,13 @@ class XpbdSdf(C.Structure):
 
 class XpbdCapsule(C.Structure):
     _fields_ = [("center", C.c_float * 3), ("half", C.c_float), ("axis", C.c_float * 3), ("radius", C.c_float)]
+
+
+class XpbdCage(C.Structure):
+    _fields_ = [("n_fine", C.c_int32), ("n_coarse", C.c_int32), ("n_blocks", C.c_int32), ("max_block", C.c_int32),
+                ("r_ptr", C.c_void_p), ("r_fine", C.c_void_p), ("r_w", C.c_void_p), ("blk_ptr", C.c_void_p),
+                ("blk_moff", C.c_void_p), ("minv", C.c_void_p), ("coarse_lib", C.c_void_p), ("p_idx", C.c_void_p),
+                ("p_w", C.c_void_p)]
 
 
 class XpbdMetrics(C.Structure):
@@ -82,6 +90,8 @@ _SIGS = {
     "xpbd_bone_targets": ([C.c_int32, C.c_int32, P, P, P, P, P, P], C.c_int),
     "xpbd_sdf_bake_capsules": ([C.POINTER(XpbdSdf), C.c_int32, P, P, C.c_float, P], C.c_int),
     "xpbd_gather": ([C.c_int32, C.c_int32, P, P, C.c_int32, P, C.c_int32, P], C.c_int),
+    "xpbd_mg_restrict": ([C.POINTER(XpbdCage), P, P, P, P, P], C.c_int),
+    "xpbd_mg_prolong_delta": ([C.POINTER(XpbdCage), P, P, P, P, P, P], C.c_int),
     "xpbd_graph_begin": ([P], C.c_int),
     "xpbd_graph_end": ([P, C.POINTER(C.c_void_p)], C.c_int),
     "xpbd_graph_launch": ([P, P], C.c_int),

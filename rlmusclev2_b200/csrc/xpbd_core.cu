@@ -69,24 +69,34 @@ __device__ __forceinline__ void finish_vertex(const XpbdParams& prm, const XpbdV
 }
 
 // ---------------------------------------------------------------------------
-template <int MODE, bool DAMP>
-__global__ void __launch_bounds__(kTileThreads, 2)
+template <int MODE, bool DAMP, int MINB>
+__global__ void __launch_bounds__(kTileThreads, MINB)
     k_project_tiles(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdTiles T,
                     const __grid_constant__ XpbdVerts V, uint32_t finish_ops) {
     extern __shared__ float4 smem[];
     const int tile = blockIdx.x;
     const int vbeg = T.tile_vptr[tile];
     const int nvt = T.tile_vptr[tile + 1] - vbeg;
-    const int nint = (MODE == XPBD_PROJECT_FUSED) ? T.tile_nint[tile] : 0;
+    const int nint = (MODE != XPBD_PROJECT_ACCUMULATE) ? T.tile_nint[tile] : 0;
+    // Shared layout: positions (float4), previous positions (float4, damped
+    // materials only), and the accumulator as four separate float arrays so
+    // that atomics on random vertices spread over all 32 banks.
+    const int mtv = T.max_tile_verts;
     float4* s_pos = smem;
-    float4* s_acc = smem + T.max_tile_verts;
-    float4* s_prev = smem + 2 * T.max_tile_verts;
+    float4* s_prev = smem + mtv;
+    float* s_ax = reinterpret_cast<float*>(smem + (DAMP ? 2 : 1) * mtv);
+    float* s_ay = s_ax + mtv;
+    float* s_az = s_ay + mtv;
+    float* s_aw = s_az + mtv;
     const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
     const float4* prev4 = reinterpret_cast<const float4*>(V.pprev);
     for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
         const int g = T.tile_verts[vbeg + i];
         s_pos[i] = pos4[g];
-        s_acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        s_ax[i] = 0.f;
+        s_ay[i] = 0.f;
+        s_az[i] = 0.f;
+        s_aw[i] = 0.f;
         if (DAMP) s_prev[i] = prev4[g];
     }
     __syncthreads();
@@ -141,10 +151,10 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         if (nact != 0.f) {
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                atomicAdd(&s_acc[l[i]].x, d[i].x);
-                atomicAdd(&s_acc[l[i]].y, d[i].y);
-                atomicAdd(&s_acc[l[i]].z, d[i].z);
-                atomicAdd(&s_acc[l[i]].w, nact);
+                atomicAdd(&s_ax[l[i]], d[i].x);
+                atomicAdd(&s_ay[l[i]], d[i].y);
+                atomicAdd(&s_az[l[i]], d[i].z);
+                atomicAdd(&s_aw[l[i]], nact);
             }
         }
     }
@@ -152,19 +162,41 @@ __global__ void __launch_bounds__(kTileThreads, 2)
 
     float4* pos4w = reinterpret_cast<float4*>(V.pos);
     float4* acc4 = reinterpret_cast<float4*>(V.accum);
-    if (MODE == XPBD_PROJECT_FUSED) {
+    if (MODE != XPBD_PROJECT_ACCUMULATE) {
         // Interior vertices: every incident constraint lives in this tile, so
         // the shared sum is complete and no other CTA reads this position.
         for (int i = threadIdx.x; i < nint; i += blockDim.x) {
             const int g = T.tile_verts[vbeg + i];
             float4 pp = s_pos[i];
-            finish_vertex(prm, V, g, pp, s_acc[i], finish_ops);
+            finish_vertex(prm, V, g, pp, make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]), finish_ops);
             pos4w[g] = pp;
         }
     }
     for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
-        const float4 a = s_acc[i];
-        if (a.w != 0.f) atomicAdd(&acc4[T.tile_verts[vbeg + i]], a);
+        const float4 a = make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]);
+        const int g = T.tile_verts[vbeg + i];
+        if (MODE != XPBD_PROJECT_FUSED_LAST) {
+            if (a.w != 0.f) atomicAdd(&acc4[g], a);
+            continue;
+        }
+        // Every tile touching g adds its partial sum, then counts its arrival;
+        // the fence orders the sum before the count.  The tile that arrives
+        // last sees all partial sums (fence + L2 load), finishes g from its own
+        // staged copy of the old position and resets the slots.  All tiles
+        // touching g staged pos[g] before accumulating, so the write cannot be
+        // observed by this launch.
+        if (a.w != 0.f) atomicAdd(&acc4[g], a);
+        __threadfence();
+        const int arrived = atomicAdd(&T.arrive[g], 1) + 1;
+        if (arrived == T.vert_ntiles[g]) {
+            __threadfence();
+            const float4 tot = __ldcg(&acc4[g]);
+            acc4[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+            T.arrive[g] = 0;
+            float4 pp = s_pos[i];
+            finish_vertex(prm, V, g, pp, tot, finish_ops);
+            pos4w[g] = pp;
+        }
     }
 }
 
@@ -388,6 +420,7 @@ int check_params(const XpbdParams* p) {
         p->n_attach_materials > XPBD_MAX_ATTACH_MATERIALS)
         return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range");
     if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0");
+    if (p->tile_variant < 0 || p->tile_variant > 1) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be 0 or 1");
     return XPBD_OK;
 }
 int check_tiles(const XpbdTiles* t) {
@@ -412,21 +445,27 @@ bool any_aniso(const XpbdParams* p) {
     return false;
 }
 
-template <int MODE, bool DAMP>
-int launch_project(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
-    const size_t smem = size_t(T->max_tile_verts) * sizeof(float4) * (DAMP ? 3 : 2);
+template <int MODE, bool DAMP, int MINB>
+int launch_project_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
+    const size_t smem = size_t(T->max_tile_verts) * sizeof(float4) * (DAMP ? 3 : 2);  // pos, [prev], 4 x float acc
     if (smem > 48 * 1024) {
         static unsigned char done[64];
         int dev = 0;
         cudaGetDevice(&dev);
         if (dev < 0 || dev >= 64 || !done[dev]) {
-            cudaFuncSetAttribute(k_project_tiles<MODE, DAMP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_project_tiles<MODE, DAMP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(XPBD_MAX_TILE_VERTS * sizeof(float4) * 3));
             if (dev >= 0 && dev < 64) done[dev] = 1;
         }
     }
-    k_project_tiles<MODE, DAMP><<<T->n_tiles, kTileThreads, smem, s>>>(*prm, *T, *V, fops);
+    k_project_tiles<MODE, DAMP, MINB><<<T->n_tiles, kTileThreads, smem, s>>>(*prm, *T, *V, fops);
     return cuda_check("xpbd_project");
+}
+
+template <int MODE, bool DAMP>
+int launch_project(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
+    if (prm->tile_variant == 1) return launch_project_v<MODE, DAMP, 3>(prm, T, V, fops, s);
+    return launch_project_v<MODE, DAMP, 2>(prm, T, V, fops, s);
 }
 
 }  // namespace
@@ -466,6 +505,12 @@ int xpbd_project(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts*
     if (mode == XPBD_PROJECT_FUSED)
         return damp ? launch_project<XPBD_PROJECT_FUSED, true>(prm, tiles, v, fops, s)
                     : launch_project<XPBD_PROJECT_FUSED, false>(prm, tiles, v, fops, s);
+    if (mode == XPBD_PROJECT_FUSED_LAST) {
+        if (!tiles->vert_ntiles || !tiles->arrive)
+            return fail(XPBD_ERR_ARG, "xpbd_project: FUSED_LAST needs vert_ntiles and arrive");
+        return damp ? launch_project<XPBD_PROJECT_FUSED_LAST, true>(prm, tiles, v, fops, s)
+                    : launch_project<XPBD_PROJECT_FUSED_LAST, false>(prm, tiles, v, fops, s);
+    }
     if (mode == XPBD_PROJECT_ACCUMULATE)
         return damp ? launch_project<XPBD_PROJECT_ACCUMULATE, true>(prm, tiles, v, 0, s)
                     : launch_project<XPBD_PROJECT_ACCUMULATE, false>(prm, tiles, v, 0, s);

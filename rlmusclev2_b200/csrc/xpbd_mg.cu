@@ -1,0 +1,145 @@
+// Two-level multigrid transfers between the fine mesh and the coarse cage.
+#include <cuda_runtime.h>
+
+#include "xpbd_common.cuh"
+#include "xpbd_device.cuh"
+
+using namespace xpbd;
+
+namespace {
+
+constexpr int kMgThreads = 256;
+
+// One CTA per Galerkin block: b_j = sum_e w_e x_f[e] for the block's coarse
+// vertices (CSR gather into shared memory), then each warp computes rows
+// x_c[r] = sum_j Minv[r][j] b_j with lanes striding j (coalesced rows).
+__global__ void __launch_bounds__(kMgThreads)
+    k_mg_restrict(const __grid_constant__ XpbdCage G, const float4* __restrict__ fine, float4* coarse, float4* prev,
+                  const float4* __restrict__ pin) {
+    extern __shared__ float4 sb[];
+    const int blk = blockIdx.x;
+    const int c0 = G.blk_ptr[blk];
+    const int dim = G.blk_ptr[blk + 1] - c0;
+    for (int j = threadIdx.x; j < dim; j += blockDim.x) {
+        const int c = c0 + j;
+        float3 acc = make_float3(0.f, 0.f, 0.f);
+        for (int e = G.r_ptr[c]; e < G.r_ptr[c + 1]; ++e) {
+            const float w = G.r_w[e];
+            const float4 x = fine[G.r_fine[e]];
+            acc.x += w * x.x;
+            acc.y += w * x.y;
+            acc.z += w * x.z;
+        }
+        sb[j] = make_float4(acc.x, acc.y, acc.z, 0.f);
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    const float* M = G.minv + G.blk_moff[blk];
+    for (int r = warp; r < dim; r += nwarp) {
+        const float* row = M + size_t(r) * dim;
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        for (int j = lane; j < dim; j += 32) {
+            const float m = row[j];
+            const float4 b = sb[j];
+            ax += m * b.x;
+            ay += m * b.y;
+            az += m * b.z;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            ax += __shfl_xor_sync(0xffffffffu, ax, o);
+            ay += __shfl_xor_sync(0xffffffffu, ay, o);
+            az += __shfl_xor_sync(0xffffffffu, az, o);
+        }
+        if (lane == 0) {
+            const int cl = G.coarse_lib[c0 + r];
+            float4 p = coarse[cl];
+            p.x = ax;
+            p.y = ay;
+            p.z = az;
+            if (prev) prev[cl] = make_float4(ax, ay, az, 0.f);
+            if (pin) {
+                const float4 t = pin[cl];
+                if (t.w != 0.f) {
+                    p.x = t.x;
+                    p.y = t.y;
+                    p.z = t.z;
+                }
+            }
+            coarse[cl] = p;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kMgThreads)
+    k_mg_prolong_delta(const __grid_constant__ XpbdCage G, const float4* __restrict__ coarse,
+                       const float4* __restrict__ prev, float4* fine, const int32_t* __restrict__ vflags,
+                       const float4* __restrict__ pin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G.n_fine) return;
+    const int4 id = reinterpret_cast<const int4*>(G.p_idx)[i];
+    float4 p = fine[i];
+    bool wr = false;
+    if (id.x >= 0) {
+        const float4 w = reinterpret_cast<const float4*>(G.p_w)[i];
+        const float4 a0 = coarse[id.x], b0 = prev[id.x], a1 = coarse[id.y], b1 = prev[id.y];
+        const float4 a2 = coarse[id.z], b2 = prev[id.z], a3 = coarse[id.w], b3 = prev[id.w];
+        p.x += ((w.x * (a0.x - b0.x) + w.y * (a1.x - b1.x)) + w.z * (a2.x - b2.x)) + w.w * (a3.x - b3.x);
+        p.y += ((w.x * (a0.y - b0.y) + w.y * (a1.y - b1.y)) + w.z * (a2.y - b2.y)) + w.w * (a3.y - b3.y);
+        p.z += ((w.x * (a0.z - b0.z) + w.y * (a1.z - b1.z)) + w.z * (a2.z - b2.z)) + w.w * (a3.z - b3.z);
+        wr = true;
+    }
+    if (vflags && pin && (vflags[i] & XPBD_VF_PIN)) {
+        const float4 t = pin[i];
+        if (t.w != 0.f) {
+            p.x = t.x;
+            p.y = t.y;
+            p.z = t.z;
+            wr = true;
+        }
+    }
+    if (wr) fine[i] = p;
+}
+
+int check_cage(const XpbdCage* g) {
+    if (!g || g->n_fine <= 0 || g->n_coarse <= 0 || g->n_blocks <= 0 || !g->r_ptr || !g->r_fine || !g->r_w ||
+        !g->blk_ptr || !g->blk_moff || !g->minv || !g->coarse_lib || !g->p_idx || !g->p_w)
+        return fail(XPBD_ERR_ARG, "XpbdCage: null member or empty size");
+    if (g->max_block <= 0 || g->max_block > 8192) return fail(XPBD_ERR_LIMIT, "XpbdCage: max_block must be in 1..8192");
+    if (!aligned16(g->p_idx) || !aligned16(g->p_w)) return fail(XPBD_ERR_ALIGN, "XpbdCage: p_idx/p_w alignment");
+    return XPBD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, float* coarse_prev4,
+                     const float* coarse_pin4, xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_cage(cage))) return rc;
+    if (!fine4 || !coarse4) return fail(XPBD_ERR_ARG, "xpbd_mg_restrict: null buffer");
+    if (!aligned16(fine4) || !aligned16(coarse4) || !aligned16(coarse_prev4) || !aligned16(coarse_pin4))
+        return fail(XPBD_ERR_ALIGN, "xpbd_mg_restrict: [n][4] buffers must be 16-byte aligned");
+    const size_t smem = size_t(cage->max_block) * sizeof(float4);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_mg_restrict, cudaFuncAttributeMaxDynamicSharedMemorySize, int(8192 * sizeof(float4)));
+    k_mg_restrict<<<cage->n_blocks, kMgThreads, smem, (cudaStream_t)stream>>>(
+        *cage, reinterpret_cast<const float4*>(fine4), reinterpret_cast<float4*>(coarse4),
+        reinterpret_cast<float4*>(coarse_prev4), reinterpret_cast<const float4*>(coarse_pin4));
+    return cuda_check("xpbd_mg_restrict");
+}
+
+int xpbd_mg_prolong_delta(const XpbdCage* cage, const float* coarse4, const float* coarse_prev4, float* fine4,
+                          const int32_t* vflags, const float* pin_target, xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_cage(cage))) return rc;
+    if (!coarse4 || !coarse_prev4 || !fine4) return fail(XPBD_ERR_ARG, "xpbd_mg_prolong_delta: null buffer");
+    if (!aligned16(coarse4) || !aligned16(coarse_prev4) || !aligned16(fine4) || !aligned16(pin_target))
+        return fail(XPBD_ERR_ALIGN, "xpbd_mg_prolong_delta: [n][4] buffers must be 16-byte aligned");
+    k_mg_prolong_delta<<<(cage->n_fine + kMgThreads - 1) / kMgThreads, kMgThreads, 0, (cudaStream_t)stream>>>(
+        *cage, reinterpret_cast<const float4*>(coarse4), reinterpret_cast<const float4*>(coarse_prev4),
+        reinterpret_cast<float4*>(fine4), vflags, reinterpret_cast<const float4*>(pin_target));
+    return cuda_check("xpbd_mg_prolong_delta");
+}
+
+}  // extern "C"

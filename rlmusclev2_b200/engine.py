@@ -36,6 +36,10 @@ def _ptr(t) -> int | None:
 class XpbdEngine:
     """State-independent substep primitives plus the program runner."""
 
+    #: fused Jacobi iteration: PROJECT_FUSED_LAST (one launch) or PROJECT_FUSED
+    #: (tile pass + boundary finish launch)
+    fused_mode = capi.PROJECT_FUSED_LAST
+
     # subclasses fill these before calling _setup_device()
     pos0_np: np.ndarray
     tet_np: np.ndarray
@@ -46,7 +50,7 @@ class XpbdEngine:
                       v_fiber: np.ndarray | None, tet_tendonmask: np.ndarray | None, dt: float,
                       gravity_vec, veldamping: float, quasi_static: bool, omega: float = 1.0,
                       contraction_ratio: float = 0.0, fiber_stiffness_scale: float = 1.0,
-                      tile_tets: int | None = None) -> None:
+                      tile_tets: int | None = None, stream=None) -> None:
         self._lib = capi.load()
         self.device = torch.device(device)
         if self.device.type != "cuda":
@@ -54,7 +58,7 @@ class XpbdEngine:
                                "pass device='cuda:0'")
         if not torch.cuda.is_available():
             raise RuntimeError("CUDA is not available")
-        self._stream = torch.cuda.Stream(self.device)
+        self._stream = stream if stream is not None else torch.cuda.Stream(self.device)
         self._sp = C.c_void_p(self._stream.cuda_stream)
         self.table = table
         self.n_cons = table.n
@@ -96,6 +100,9 @@ class XpbdEngine:
         self._t_fiber = T(L.tet_fiber) if L.tet_fiber is not None else None
         self._t_act = torch.zeros(L.n_tets, dtype=f32, device=dev) if L.tet_fiber is not None else None
         self._t_bnd = T(L.bnd_verts) if L.n_boundary else torch.zeros(1, dtype=torch.int32, device=dev)
+        self._t_ntiles = T(L.vert_ntiles)
+        self._t_arrive = torch.zeros(nv, dtype=torch.int32, device=dev)
+        self._t_orph = T(L.orphans) if L.orphans.shape[0] else None
         # vertex constraints (attach, pin) in library order
         self._vflags = None
         self._attach_tgt = None
@@ -120,6 +127,7 @@ class XpbdEngine:
             prm.attach[i].k = k
             prm.attach[i].damp = d
         self._prm = prm
+        self.dt = float(dt)
         self._sdf = None
         self._graphs: dict = {}
         self._refresh_structs()
@@ -184,7 +192,16 @@ class XpbdEngine:
         t.tet_b0, t.tet_b1, t.tet_b2 = _ptr(self._t_b0), _ptr(self._t_b1), _ptr(self._t_b2)
         t.tet_fiber, t.tet_act = _ptr(self._t_fiber), _ptr(self._t_act)
         t.bnd_verts = _ptr(self._t_bnd)
+        t.vert_ntiles, t.arrive = _ptr(self._t_ntiles), _ptr(self._t_arrive)
         self._tiles = t
+        # orphan vertices (in no tet) still take ATTACH/pin in the fused pass
+        to = capi.XpbdTiles()
+        C.memmove(C.addressof(to), C.addressof(t), C.sizeof(t))
+        if self._t_orph is not None:
+            to.n_boundary, to.bnd_verts = int(self._t_orph.shape[0]), _ptr(self._t_orph)
+        else:
+            to.n_boundary = 0
+        self._tiles_orph = to
         for g in self._graphs.values():
             capi.check(self._lib.xpbd_graph_destroy(g))
         self._graphs = {}
@@ -214,6 +231,14 @@ class XpbdEngine:
         uses); a preceding unfused solve may have left sums behind."""
         if self._accum_dirty:
             self.clear()
+        if self.fused_mode == capi.PROJECT_FUSED_LAST:
+            self._project(capi.PROJECT_FUSED_LAST)
+            if self._t_orph is not None and self._vflags is not None:
+                capi.check(self._lib.xpbd_apply_boundary(C.byref(self._prm), C.byref(self._tiles_orph),
+                                                         C.byref(self._verts),
+                                                         capi.APPLY_ATTACH | capi.APPLY_DIVIDE | capi.APPLY_PIN
+                                                         | capi.APPLY_CLEAR, self._sp))
+            return
         self._project(capi.PROJECT_FUSED)
         self._apply_boundary(capi.APPLY_ATTACH | capi.APPLY_DIVIDE | capi.APPLY_PIN | capi.APPLY_CLEAR)
 
@@ -221,10 +246,6 @@ class XpbdEngine:
         self._stream.synchronize()
 
     # ------------------------------------------- reference engine primitives
-    @property
-    def dt(self) -> float:
-        return float(self._prm.dt)
-
     def integrate(self) -> None:
         """XpbdEngine.integrate (engine.py:798-809)."""
         self._vstep(capi.OP_PREDICT)
@@ -428,7 +449,7 @@ class XpbdSolver(XpbdEngine):
     def __init__(self, verts, tets, table: ConstraintTable, *, mass, dt, stopped=None, gravity=(0.0, 0.0, 0.0),
                  veldamping=0.0, quasi_static=False, relaxation=1.0, v_fiber=None, tet_tendonmask=None,
                  contraction_ratio=0.0, fiber_stiffness_scale=1.0, device="cuda:0", tile_tets=None, pins=None,
-                 num_substeps=1, total_rest_volume=None):
+                 num_substeps=1, total_rest_volume=None, stream=None):
         self.pos0_np = np.asarray(verts, np.float32)
         self.tet_np = np.asarray(tets, np.int32)
         self.n_verts = self.pos0_np.shape[0]
@@ -445,7 +466,7 @@ class XpbdSolver(XpbdEngine):
         self._setup_device(device, mass=mass, stopped=st, table=table, v_fiber=v_fiber,
                            tet_tendonmask=tet_tendonmask, dt=dt, gravity_vec=gravity, veldamping=veldamping,
                            quasi_static=quasi_static, omega=relaxation, contraction_ratio=contraction_ratio,
-                           fiber_stiffness_scale=fiber_stiffness_scale, tile_tets=tile_tets)
+                           fiber_stiffness_scale=fiber_stiffness_scale, tile_tets=tile_tets, stream=stream)
 
     def project_once(self) -> None:
         """clear -> solve_constraints -> apply_dP -> apply_pintotarget (unfused primitives)."""

@@ -188,6 +188,9 @@ class Scene:
     traj: dict                   # bone trajectory parameters
     aniso_muscle: int
     meta: dict = field(default_factory=dict)
+    muscle_rot: np.ndarray | None = None     # (M,3,3) local->world rotation (column 0 = long axis)
+    muscle_center: np.ndarray | None = None  # (M,3)
+    muscle_len: np.ndarray | None = None     # (M,)
 
     @property
     def n_bones(self) -> int:
@@ -342,5 +345,125 @@ def humanv2_scene(seed: int = 0, n_muscles: int = 40, n_bones: int = 20, target_
     return Scene(verts=allv, tets=alltets, tet_part=tet_part, vert_part=vert_part, v_tendon=v_tendon,
                  v_fiber=fib.astype(np.float32), surface_tris=surf.astype(np.int32), bone_center=bc, bone_axis=ba,
                  bone_half=bh, bone_radius=br, vert_bone=vert_bone, traj=traj, aniso_muscle=aniso,
+                 muscle_rot=np.stack(rots), muscle_center=np.stack(cents), muscle_len=L,
                  meta=dict(seed=seed, h=h, n_muscle_verts=nmv, n_muscle_tets=mtets.shape[0],
                            n_fascia_tets=ftets.shape[0], fascia_muscles=chosen))
+
+
+# --------------------------------------------------------------------------
+# Coarse cage for the two-level multigrid
+
+
+@dataclass
+class Cage:
+    """Per-muscle coarse hex cage (6 tets per cell) enclosing the fine muscle
+    vertices, with the same arrays as the reference's baked cage npz
+    (mg/mg.py:744-800): fine vertex -> coarse tet (cage_idx, -1 = not
+    embedded) and barycentric uvw, and the Galerkin restriction
+    (P^T P)^-1 stored per muscle block (minv_flat, blk_base, blk_dim,
+    blk_matoff)."""
+    coarse_pos: np.ndarray
+    coarse_tet: np.ndarray
+    cage_idx: np.ndarray
+    uvw: np.ndarray
+    minv_flat: np.ndarray
+    blk_base: np.ndarray
+    blk_dim: np.ndarray
+    blk_matoff: np.ndarray
+    mg_fine_nv: int
+
+
+def _bary(p, a, b, c, d):
+    T = np.stack([b - a, c - a, d - a], axis=-1)
+    w = np.linalg.solve(T, (p - a)[..., None])[..., 0]
+    return np.concatenate([(1.0 - w.sum(-1))[..., None], w], -1)
+
+
+def build_cage(scene: "Scene", spacing: float = 0.016) -> Cage:
+    """Coarse cage: for every muscle a ``spacing`` hex lattice in the muscle's
+    local frame over the cells that hold its fine vertices; fascia vertices are
+    not embedded."""
+    nv = scene.verts.shape[0]
+    cage_idx = np.full(nv, -1, np.int64)
+    uvw = np.zeros((nv, 3))
+    cpos_all, ctet_all, blocks = [], [], []
+    voff = toff = 0
+    x64 = scene.verts.astype(np.float64)
+    for m in range(scene.muscle_rot.shape[0]):
+        sel = np.nonzero(scene.vert_part == m)[0]
+        R, c = scene.muscle_rot[m], scene.muscle_center[m]
+        loc = (x64[sel] - c) @ R
+        lo = loc.min(0) - 1e-9
+        cell = np.floor((loc - lo) / spacing).astype(np.int64)
+        dims = cell.max(0) + 1
+        key = (cell[:, 0] * dims[1] + cell[:, 1]) * dims[2] + cell[:, 2]
+        ucell, cell_of = np.unique(key, return_inverse=True)
+        ci = ucell // (dims[1] * dims[2])
+        cj = (ucell // dims[2]) % dims[1]
+        ck = ucell % dims[2]
+        gid = lambda i, j, k: (i * (dims[1] + 1) + j) * (dims[2] + 1) + k  # noqa: E731
+        tets = hex_to_tets(lambda dx, dy, dz: gid(ci + dx, cj + dy, ck + dz))  # (6*ncell,4), perm-major
+        used, tl = np.unique(tets, return_inverse=True)
+        tl = tl.reshape(-1, 4)
+        gi = used // ((dims[1] + 1) * (dims[2] + 1))
+        gj = (used // (dims[2] + 1)) % (dims[1] + 1)
+        gk = used % (dims[2] + 1)
+        cl = lo + spacing * np.stack([gi, gj, gk], 1)
+        cw = cl @ R.T + c
+        ncell = ucell.shape[0]
+        # the 6 tets of cell q are rows q + r*ncell
+        best_w = np.full((sel.shape[0], 4), -np.inf)
+        best_t = np.zeros(sel.shape[0], np.int64)
+        for r in range(6):
+            t = cell_of + r * ncell
+            w = _bary(loc, cl[tl[t, 0]], cl[tl[t, 1]], cl[tl[t, 2]], cl[tl[t, 3]])
+            better = w.min(1) > best_w.min(1)
+            best_w[better] = w[better]
+            best_t[better] = t[better]
+        # keep only the coarse tets that embed a fine vertex, and their corners
+        # (every kept corner then carries prolongation weight, so the Galerkin
+        # restriction defines it)
+        kept, best_t = np.unique(best_t, return_inverse=True)
+        tl = tl[kept]
+        usedv, tl = np.unique(tl, return_inverse=True)
+        tl = tl.reshape(-1, 4)
+        cw = cw[usedv]
+        cage_idx[sel] = best_t + toff
+        uvw[sel] = best_w[:, 1:]
+        # Galerkin block (P^T P)^-1 over this muscle's coarse verts
+        n = cw.shape[0]
+        Pm = np.zeros((sel.shape[0], n))
+        rows = np.repeat(np.arange(sel.shape[0]), 4)
+        np.add.at(Pm, (rows, tl[best_t].reshape(-1)), best_w.reshape(-1))
+        blocks.append(np.linalg.pinv(Pm.T @ Pm, rcond=1e-8))  # cutoff of tools/gen_coarse_cage.py:221
+        cpos_all.append(cw)
+        ctet_all.append(tl + voff)
+        voff += n
+        toff += tl.shape[0]
+    coarse_pos = np.concatenate(cpos_all).astype(np.float32)
+    coarse_tet = orient_tets(coarse_pos, np.concatenate(ctet_all)).astype(np.int32)
+    # orient_tets may swap pts[0]/pts[1]; remap the barycentric weights to match
+    raw = np.concatenate(ctet_all)
+    swapped = raw[:, 0] != coarse_tet[:, 0]
+    emb = cage_idx >= 0
+    sw = np.zeros(nv, bool)
+    sw[emb] = swapped[cage_idx[emb]]
+    # uvw are the weights of pts[1..3]; weight of pts[0] is 1-u-v-w; swapping pts 0/1
+    u_old = uvw[sw, 0].copy()
+    w0_old = 1.0 - uvw[sw].sum(1)
+    uvw[sw, 0] = w0_old
+    del u_old
+    blk_base, blk_dim, blk_matoff, flat = [], [], [], []
+    off = base = 0
+    for B in blocks:
+        n = B.shape[0]
+        blk_base += [base] * n
+        blk_dim += [n] * n
+        blk_matoff += [off] * n
+        flat.append(B.reshape(-1))
+        off += n * n
+        base += n
+    return Cage(coarse_pos=coarse_pos, coarse_tet=coarse_tet, cage_idx=cage_idx.astype(np.int32),
+                uvw=uvw.astype(np.float32), minv_flat=np.concatenate(flat).astype(np.float32),
+                blk_base=np.asarray(blk_base, np.int32), blk_dim=np.asarray(blk_dim, np.int32),
+                blk_matoff=np.asarray(blk_matoff, np.int32), mg_fine_nv=nv)

@@ -186,6 +186,12 @@ class MultiGridSim(MuscleSim):
                            quasi_static=self.quasi_static, omega=1.0, contraction_ratio=self.contraction_ratio,
                            fiber_stiffness_scale=self.fiber_stiffness_scale, tile_tets=cfg.get("tile_tets"))
         self._setup_kinematics()
+        self.mg = None
+        if self.use_multigrid:
+            if self.mg_mode != "hpbd":
+                raise NotImplementedError("mg_mode='projection' is not on the sm_100a path (use 'hpbd')")
+            from .multigrid import DeviceMultigrid
+            self.mg = DeviceMultigrid(self, spacing=float(cfg.get("mg_cage_spacing", 0.016)))
         self.collision_solvers = []
         self.collision_solvers_iter = []
         coll = (cfg.get("demo") or {}).get("collision") or {}
@@ -312,13 +318,16 @@ class MultiGridSim(MuscleSim):
             phase()
 
     def _multigrid_pre(self) -> None:
-        raise NotImplementedError("multigrid is enabled but the coarse cage is not built")
+        """_hpbd_vcycle (mg.py:1064-1079); the fine re-pin follows in pre_phase."""
+        self.mg.vcycle(pin_fine=False)
 
     def _kinematic_step(self, t: float) -> None:
         """mg.py:1396-1407: targets for frame t, hard pin (presubframe soft pin is 0)."""
         if self._frame_loaded != t:
             self.load_frame_targets(t)
         self._targets_kernel()
+        if self.mg is not None:
+            self.mg.refresh_target()
         if getattr(self, "bone_collider", None) is not None:
             self.bone_collider.bake()
         self.apply_pintotarget()
@@ -326,11 +335,13 @@ class MultiGridSim(MuscleSim):
     def _fusable(self) -> bool:
         cs = getattr(self, "collision_solvers", None) or []
         return (not getattr(self, "collision_solvers_iter", None) and not getattr(self, "constraint_solvers", None)
-                and all(isinstance(c, GridSdfCollider) for c in cs) and len(cs) <= 1 and not self.use_multigrid
+                and all(isinstance(c, GridSdfCollider) for c in cs) and len(cs) <= 1
                 and getattr(self, "program", None) is None)
 
     def _frame_fused(self) -> None:
         self._targets_kernel()
+        if self.mg is not None:
+            self.mg.refresh_target()
         sdf = self.collision_solvers[0] if self.collision_solvers else None
         if sdf is not None:
             sdf.bake()
@@ -341,8 +352,11 @@ class MultiGridSim(MuscleSim):
         vel = 0 if self.quasi_static else capi.OP_VELOCITY
         push = capi.OP_SDF if sdf is not None else 0
         for sub in range(self.nsubsteps):
-            ops = capi.OP_PREDICT | pin | ((push | vel) if sub > 0 else 0)
-            self._vstep(ops)
+            if self.mg is None:
+                self._vstep(capi.OP_PREDICT | pin | ((push | vel) if sub > 0 else 0))
+            else:
+                self._vstep(capi.OP_PREDICT | ((push | vel) if sub > 0 else 0))
+                self.mg.vcycle(pin_fine=bool(pin))
             for _ in range(self.fine_iters):
                 self._fused_iteration()
         if push | vel:

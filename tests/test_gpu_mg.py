@@ -115,9 +115,15 @@ def test_frames_fused_graph_vs_oracle():
               f"(1e-5 diag {1e-5 * bbox_diag(sc.verts):.3e}, ref atol {REF_ATOL})")
         assert e32 <= REF_ATOL and e64 <= REF_ATOL
     mt = sim.metrics()
-    r = o64.arap_residual()
-    rmax = r[o64.table.c["tetid"][o64.table.c["type"] == O.T_TETARAPSVD]].max()
-    assert abs(mt["resid_max"] - r.max()) <= 1e-3 * r.max() + 1e-6, (mt["resid_max"], r.max(), rmax)
+    r64, r32 = o64.arap_residual(), o32.arap_residual()
+    # the max residual sits on a few extreme tets that the count flips move:
+    # gate it at 1e-4 relative or three times the oracle's own FP32/FP64 spread
+    floor = abs(float(r32.max()) - float(r64.max()))
+    print(f"resid max gpu {mt['resid_max']:.6f} o32 {r32.max():.6f} o64 {r64.max():.6f}; "
+          f"rms gpu {np.sqrt(mt['resid_sq_sum'] / len(r64)):.6e} o64 {np.sqrt((r64 ** 2).mean()):.6e}")
+    assert abs(mt["resid_max"] - r64.max()) <= max(1e-4 * r64.max(), 3.0 * floor)
+    rms_gpu, rms64 = np.sqrt(mt["resid_sq_sum"] / len(r64)), np.sqrt((r64 ** 2).mean())
+    assert abs(rms_gpu - rms64) <= 1e-3 * rms64
     drift_gpu = (mt["vol_sum"] - sim.total_rest_volume) / sim.total_rest_volume
     drift_or = (o64.total_volume() - o64.total_rest_volume) / o64.total_rest_volume
     assert abs(drift_gpu - drift_or) <= 1e-4
