@@ -339,13 +339,14 @@ def run_ours(args):
 def run_profile_case(args):
     """Small deterministic workloads for ncu (no timing, no output line).
 
-    humanv2: ``--steps`` frames of the benchmark configuration through the
-    frame graph.  box3m: a 64x64x120-hex box (2.95M tets, ~150 MB of tet
+    humanv2: ``--steps`` frames of the benchmark configuration (the frame's
+    launches issued eagerly, without the graph).  box3m: a 64x64x120-hex box (2.95M tets, ~150 MB of tet
     streams, larger than L2) and ``--steps`` Jacobi iterations of its tet pass."""
     import torch
     if args.profile_case == "humanv2":
         from rlmusclev2_b200.mg import MultiGridSim, load_config
         sim = MultiGridSim(load_config(str(CONFIG)))
+        sim.use_graphs = False  # the same launches, issued eagerly so the profiler lists each kernel
         for f in range(sim.start_frame, sim.start_frame + args.steps):
             sim.set_fiber_activation(sim.scene.activation(f))
             sim.step_frame(f)

@@ -33,6 +33,13 @@ enum {
     XPBD_ERR_LIMIT = -4,  /* a size exceeds a documented maximum */
 };
 
+/* Device status word bits (OR-ed by kernels; the host reads and clears it). */
+enum {
+    XPBD_STATUS_PAIR_OVERFLOW = 1 << 0,    /* more candidate pairs than max_pairs (extra pairs dropped) */
+    XPBD_STATUS_CONTACT_OVERFLOW = 1 << 1, /* more contacts than max_contacts (extra contacts dropped) */
+    XPBD_STATUS_STACK_OVERFLOW = 1 << 2,   /* BVH traversal deeper than its stack (query cut short) */
+};
+
 #define XPBD_MAX_MATERIALS 64
 #define XPBD_MAX_ATTACH_MATERIALS 16
 #define XPBD_MAX_TILE_VERTS 4096
@@ -258,6 +265,61 @@ int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, f
  * XPBD_VF_PIN and pin_target.w != 0 (vflags/pin_target may be NULL). */
 int xpbd_mg_prolong_delta(const XpbdCage* cage, const float* coarse4, const float* coarse_prev4, float* fine4,
                           const int32_t* vflags, const float* pin_target, xpbd_stream_t stream);
+
+/* Triangle-triangle DCD between surface triangles (UdcfDcdCollider,
+ * collision/udcf/solver.py:146-457, BVH broadphase).  tris index vertices in
+ * the library order of the pos4 buffer the calls receive; inverse mass is
+ * read from pos4.w (0 = solid).  Scratch ws_* and the pair/contact buffers
+ * are caller-owned; sizes from xpbd_dcd_workspace_query. */
+typedef struct XpbdDcd {
+    int32_t n_tris, n_verts, max_pairs, max_contacts;
+    const int32_t* tris;      /* [n_tris][3] */
+    const int32_t* tri_group; /* [n_tris] 0 movable, 1 static; NULL = all movable */
+    int32_t allow_self;       /* movable-vs-movable pairs (UdcfParams.allow_self) */
+    int32_t jacobi_avg;       /* 1: dP/count (UdcfParams.jacobi_avg), 0: summed dP */
+    float thickness;          /* AABB padding (UdcfParams.thickness) */
+    float offset_eps;         /* contact accept threshold (UdcfParams.offset, 1e-6) */
+    float multiplier;         /* collisionConstraintMultiplier (1.01) */
+    float friction_static, friction_dynamic;
+    float max_push;           /* > 0: clamp contact depth (UdcfParams.max_push) */
+    float box_lo[3], box_hi[3]; /* Morton quantisation box (centres outside are clamped) */
+    int32_t* pairs;           /* [max_pairs][2] (i, j > i), deterministic order */
+    int32_t* n_pairs;         /* [1] candidate pairs found (may exceed max_pairs) */
+    int32_t* n_contacts;      /* [1] contacts found (may exceed max_contacts) */
+    int32_t* c_ids;           /* [max_contacts][8]: cur tri verts, pair index, closest tri verts, 0 */
+    float* c_data;            /* [max_contacts][12]: n.xyz, C, b1.xyz, C1, b2.xyz, C2 */
+    float* x_prev;            /* [n_verts][4] positions at the broadphase (friction reference) */
+    float* dP;                /* [n_verts][4] response accumulator, zero between calls */
+    int32_t* status;          /* [1] XPBD_STATUS_* bits */
+    float* ws_nodes;          /* workspace: BVH node boxes + leaf copy */
+    uint32_t* ws_keys;        /* [n_tris] Morton keys (sorted in place) */
+    int32_t* ws_vals;         /* [n_tris] triangle ids in Morton order */
+    uint32_t* ws_keys2;       /* [n_tris] sort ping-pong */
+    int32_t* ws_vals2;        /* [n_tris] */
+    int32_t* ws_hist;         /* radix histograms */
+    int32_t* ws_child;        /* [n_tris-1][2] */
+    int32_t* ws_parent;       /* [2 n_tris - 1] */
+    int32_t* ws_flags;        /* [n_tris-1] refit arrival counters */
+    int32_t* ws_count;        /* [n_tris] pairs per triangle, then their offsets */
+    int32_t* ws_total;        /* [1] */
+} XpbdDcd;
+
+/* Element counts of the DCD workspace arrays for n_tris triangles. */
+typedef struct XpbdDcdWorkspaceSizes {
+    int64_t nodes_floats, keys, hist, child, parent, flags, count;
+} XpbdDcdWorkspaceSizes;
+
+int xpbd_dcd_workspace_query(int32_t n_tris, XpbdDcdWorkspaceSizes* out);
+
+/* AABBs, LBVH rebuild (Morton sort + Karras hierarchy + refit) and the
+ * candidate pair list; snapshot_prev != 0 first copies pos4 to x_prev
+ * (UdcfDcdCollider.solve with i_iter == 0, udcf/solver.py:365-382). */
+int xpbd_dcd_broadphase(const XpbdDcd* dcd, const float* pos4, int32_t snapshot_prev, xpbd_stream_t stream);
+
+/* Narrowphase on the pair list, response and Jacobi apply onto pos4
+ * (narrow_kernel, respond_kernel, apply_kernel; udcf/kernel.py:316-474,
+ * 713-822). */
+int xpbd_dcd_narrow_respond(const XpbdDcd* dcd, float* pos4, xpbd_stream_t stream);
 
 /* Stream capture helpers (a captured substep replays as one graph launch). */
 int xpbd_graph_begin(xpbd_stream_t stream);

@@ -512,3 +512,53 @@ class OracleMultiGridSim(OracleSolver):
                          float(self.coll.get("contact_offset", 0.0)), float(self.coll.get("max_push", -1.0)),
                          self.P.name)
             self.update_velocities()
+
+
+# ---- DCD (collision/udcf/kernel.py) on the oracle, FP32 -------------------------
+def dcd_pairs(tris, pos4, thickness=0.0, allow_self=True, group=None):
+    L = lib()
+    tris = np.ascontiguousarray(tris, np.int32)
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    n = tris.shape[0]
+    boxes = np.zeros((n, 6), np.float32)
+    L.orc_dcd_aabb.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p]
+    L.orc_dcd_aabb(n, _p(tris), _p(pos4), C.c_float(thickness), _p(boxes))
+    cap = 1 << 16
+    while True:
+        pairs = np.zeros((cap, 2), np.int32)
+        L.orc_dcd_pairs.restype = C.c_long
+        L.orc_dcd_pairs.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_long]
+        g = None if group is None else np.ascontiguousarray(group, np.int32)
+        npairs = L.orc_dcd_pairs(n, _p(tris), _p(g), int(allow_self), _p(boxes), _p(pairs), cap)
+        if npairs <= cap:
+            return pairs[:npairs], boxes
+        cap = int(npairs)
+
+
+def dcd_narrow(pairs, tris, pos4, offset_eps=1e-6):
+    L = lib()
+    pairs = np.ascontiguousarray(pairs, np.int32)
+    cap = max(1, pairs.shape[0])
+    c_ids = np.zeros((cap, 8), np.int32)
+    c_data = np.zeros((cap, 12), np.float32)
+    L.orc_dcd_narrow.restype = C.c_long
+    L.orc_dcd_narrow.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
+                                 C.c_long]
+    nc = L.orc_dcd_narrow(pairs.shape[0], _p(pairs), _p(np.ascontiguousarray(tris, np.int32)),
+                          _p(np.ascontiguousarray(pos4, np.float32)), C.c_float(offset_eps), _p(c_ids), _p(c_data),
+                          cap)
+    return c_ids[:nc], c_data[:nc]
+
+
+def dcd_respond_apply(c_ids, c_data, pos4, xprev4, multiplier=1.01, mu_s=0.5, mu_d=0.4, max_push=0.0, jacobi_avg=True):
+    """Returns the new pos4 (input not modified)."""
+    L = lib()
+    out = np.ascontiguousarray(pos4, np.float32).copy()
+    dP = np.zeros_like(out)
+    L.orc_dcd_respond_apply.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
+                                        C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p]
+    L.orc_dcd_respond_apply(c_ids.shape[0], _p(np.ascontiguousarray(c_ids, np.int32)),
+                            _p(np.ascontiguousarray(c_data, np.float32)), _p(out),
+                            _p(np.ascontiguousarray(xprev4, np.float32)), out.shape[0], C.c_float(multiplier),
+                            C.c_float(mu_s), C.c_float(mu_d), C.c_float(max_push), int(jacobi_avg), _p(dP))
+    return out

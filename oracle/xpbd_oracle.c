@@ -28,3 +28,5 @@
 #include "xpbd_oracle_impl.h"
 #undef REAL
 #undef SFX
+
+#include "xpbd_oracle_dcd.h"

@@ -17,6 +17,7 @@ OK = 0
 MAT_ARAPSVD, MAT_VOLUME, MAT_ANISO, MAT_SNH, MAT_DAMPED = 1, 2, 4, 8, 16
 VF_ATTACH_MASK, VF_PIN = 0xFF, 1 << 8
 OP_SDF, OP_VELOCITY, OP_PREDICT, OP_PIN = 1, 2, 4, 8
+STATUS_PAIR_OVERFLOW, STATUS_CONTACT_OVERFLOW, STATUS_STACK_OVERFLOW = 1, 2, 4
 APPLY_ATTACH, APPLY_DIVIDE, APPLY_PIN, APPLY_CLEAR = 1, 2, 4, 8
 PROJECT_FUSED, PROJECT_ACCUMULATE, PROJECT_FUSED_LAST = 0, 1, 2
 
@@ -71,6 +72,25 @@ class XpbdCage(C.Structure):
                 ("p_w", C.c_void_p)]
 
 
+class XpbdDcd(C.Structure):
+    _fields_ = [("n_tris", C.c_int32), ("n_verts", C.c_int32), ("max_pairs", C.c_int32), ("max_contacts", C.c_int32),
+                ("tris", C.c_void_p), ("tri_group", C.c_void_p), ("allow_self", C.c_int32),
+                ("jacobi_avg", C.c_int32), ("thickness", C.c_float), ("offset_eps", C.c_float),
+                ("multiplier", C.c_float), ("friction_static", C.c_float), ("friction_dynamic", C.c_float),
+                ("max_push", C.c_float), ("box_lo", C.c_float * 3), ("box_hi", C.c_float * 3),
+                ("pairs", C.c_void_p), ("n_pairs", C.c_void_p), ("n_contacts", C.c_void_p), ("c_ids", C.c_void_p),
+                ("c_data", C.c_void_p), ("x_prev", C.c_void_p), ("dP", C.c_void_p), ("status", C.c_void_p),
+                ("ws_nodes", C.c_void_p), ("ws_keys", C.c_void_p), ("ws_vals", C.c_void_p),
+                ("ws_keys2", C.c_void_p), ("ws_vals2", C.c_void_p), ("ws_hist", C.c_void_p),
+                ("ws_child", C.c_void_p), ("ws_parent", C.c_void_p), ("ws_flags", C.c_void_p),
+                ("ws_count", C.c_void_p), ("ws_total", C.c_void_p)]
+
+
+class XpbdDcdWorkspaceSizes(C.Structure):
+    _fields_ = [("nodes_floats", C.c_int64), ("keys", C.c_int64), ("hist", C.c_int64), ("child", C.c_int64),
+                ("parent", C.c_int64), ("flags", C.c_int64), ("count", C.c_int64)]
+
+
 class XpbdMetrics(C.Structure):
     _fields_ = [("vol_sum", C.c_double), ("resid_sq_sum", C.c_double), ("resid_max", C.c_float),
                 ("n_inverted", C.c_int32), ("n_nonfinite", C.c_int32), ("reserved", C.c_int32)]
@@ -92,6 +112,9 @@ _SIGS = {
     "xpbd_gather": ([C.c_int32, C.c_int32, P, P, C.c_int32, P, C.c_int32, P], C.c_int),
     "xpbd_mg_restrict": ([C.POINTER(XpbdCage), P, P, P, P, P], C.c_int),
     "xpbd_mg_prolong_delta": ([C.POINTER(XpbdCage), P, P, P, P, P, P], C.c_int),
+    "xpbd_dcd_workspace_query": ([C.c_int32, C.POINTER(XpbdDcdWorkspaceSizes)], C.c_int),
+    "xpbd_dcd_broadphase": ([C.POINTER(XpbdDcd), P, C.c_int32, P], C.c_int),
+    "xpbd_dcd_narrow_respond": ([C.POINTER(XpbdDcd), P, P], C.c_int),
     "xpbd_graph_begin": ([P], C.c_int),
     "xpbd_graph_end": ([P, C.POINTER(C.c_void_p)], C.c_int),
     "xpbd_graph_launch": ([P, P], C.c_int),

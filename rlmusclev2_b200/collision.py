@@ -70,3 +70,131 @@ class GridSdfCollider:
     def __call__(self) -> None:
         """Push-out hook (collision_solvers entry, mg/mg.py:1366-1371)."""
         self.sim._vstep_sdf_only(self)
+
+
+# ----------------------------------------------------------------------------
+# Triangle-triangle DCD (UdcfDcdCollider, collision/udcf/solver.py:38-457)
+
+from dataclasses import dataclass  # noqa: E402
+
+
+@dataclass
+class UdcfParams:
+    """UdcfParams (udcf/solver.py:38-120); the BVH broadphase is the only one
+    (use_bvh=True), the serial Gauss-Seidel variant is not on this path."""
+    multiplier: float = 1.01
+    friction_static: float = 0.5
+    friction_dynamic: float = 0.4
+    offset: float = 1.0e-6
+    thickness: float = 0.0
+    max_pairs: int = 1 << 20
+    max_contacts: int = 1 << 18
+    allow_self: bool = False
+    jacobi_avg: bool = True
+    gauss_seidel: bool = False
+    max_push: float = 0.0
+    use_bvh: bool = True
+
+
+class DcdBuffers:
+    """Device buffers and the XpbdDcd descriptor for ``n_tris`` triangles over
+    a [n_verts][4] position buffer (library vertex ids)."""
+
+    def __init__(self, lib, device, tris_lib: np.ndarray, n_verts: int, params: UdcfParams, box_lo, box_hi,
+                 tri_group: np.ndarray | None = None):
+        self.lib = lib
+        self.p = params
+        n = int(tris_lib.shape[0])
+        sz = capi.XpbdDcdWorkspaceSizes()
+        capi.check(lib.xpbd_dcd_workspace_query(n, C.byref(sz)))
+        dev = device
+        i32 = torch.int32
+        self.t = dict(
+            tris=torch.from_numpy(np.ascontiguousarray(tris_lib, np.int32)).to(dev),
+            group=None if tri_group is None else torch.from_numpy(np.ascontiguousarray(tri_group, np.int32)).to(dev),
+            pairs=torch.zeros((params.max_pairs, 2), dtype=i32, device=dev),
+            counters=torch.zeros(8, dtype=i32, device=dev),  # n_pairs, n_contacts, status, total
+            c_ids=torch.zeros((params.max_contacts, 8), dtype=i32, device=dev),
+            c_data=torch.zeros((params.max_contacts, 12), dtype=torch.float32, device=dev),
+            x_prev=torch.zeros((n_verts, 4), dtype=torch.float32, device=dev),
+            dP=torch.zeros((n_verts, 4), dtype=torch.float32, device=dev),
+            nodes=torch.zeros(int(sz.nodes_floats), dtype=torch.float32, device=dev),
+            keys=torch.zeros(int(sz.keys), dtype=i32, device=dev), vals=torch.zeros(int(sz.keys), dtype=i32, device=dev),
+            keys2=torch.zeros(int(sz.keys), dtype=i32, device=dev), vals2=torch.zeros(int(sz.keys), dtype=i32, device=dev),
+            hist=torch.zeros(int(sz.hist), dtype=i32, device=dev), child=torch.zeros(int(sz.child), dtype=i32, device=dev),
+            parent=torch.zeros(int(sz.parent), dtype=i32, device=dev), flags=torch.zeros(int(sz.flags), dtype=i32, device=dev),
+            count=torch.zeros(int(sz.count), dtype=i32, device=dev))
+        t = self.t
+        d = capi.XpbdDcd()
+        d.n_tris, d.n_verts, d.max_pairs, d.max_contacts = n, int(n_verts), params.max_pairs, params.max_contacts
+        d.tris = t["tris"].data_ptr()
+        d.tri_group = None if t["group"] is None else t["group"].data_ptr()
+        d.allow_self, d.jacobi_avg = int(params.allow_self), int(params.jacobi_avg)
+        d.thickness, d.offset_eps, d.multiplier = params.thickness, params.offset, params.multiplier
+        d.friction_static, d.friction_dynamic, d.max_push = params.friction_static, params.friction_dynamic, params.max_push
+        d.box_lo[:] = [float(x) for x in box_lo]
+        d.box_hi[:] = [float(x) for x in box_hi]
+        cp = t["counters"].data_ptr()
+        d.pairs, d.n_pairs, d.n_contacts, d.status = t["pairs"].data_ptr(), cp, cp + 4, cp + 8
+        d.ws_total = cp + 12
+        d.c_ids, d.c_data, d.x_prev, d.dP = (t["c_ids"].data_ptr(), t["c_data"].data_ptr(), t["x_prev"].data_ptr(),
+                                             t["dP"].data_ptr())
+        d.ws_nodes, d.ws_keys, d.ws_vals = t["nodes"].data_ptr(), t["keys"].data_ptr(), t["vals"].data_ptr()
+        d.ws_keys2, d.ws_vals2, d.ws_hist = t["keys2"].data_ptr(), t["vals2"].data_ptr(), t["hist"].data_ptr()
+        d.ws_child, d.ws_parent, d.ws_flags = t["child"].data_ptr(), t["parent"].data_ptr(), t["flags"].data_ptr()
+        d.ws_count = t["count"].data_ptr()
+        self.d = d
+
+    def broadphase(self, pos4: torch.Tensor, snapshot_prev: bool, stream) -> None:
+        capi.check(self.lib.xpbd_dcd_broadphase(C.byref(self.d), C.c_void_p(pos4.data_ptr()), int(snapshot_prev),
+                                                stream))
+
+    def narrow_respond(self, pos4: torch.Tensor, stream) -> None:
+        capi.check(self.lib.xpbd_dcd_narrow_respond(C.byref(self.d), C.c_void_p(pos4.data_ptr()), stream))
+
+    def counters(self) -> dict:
+        c = self.t["counters"].cpu().numpy()
+        return {"n_pairs": int(c[0]), "n_contacts": int(c[1]), "status": int(c[2])}
+
+
+class UdcfDcdCollider:
+    """Self-collision DCD of a sim's surface triangles (movable vs movable with
+    allow_self, the configuration of the synthetic humanV2 scene).  Register
+    ``solve`` in ``sim.collision_solvers_iter``: it rebuilds the LBVH on the
+    first fine iteration of each substep and resolves contacts every
+    iteration (udcf/solver.py:365-440)."""
+
+    def __init__(self, sim, surface_tris: np.ndarray, params: UdcfParams | None = None, margin: float = 0.05):
+        self.params = params or UdcfParams(allow_self=True)
+        if self.params.gauss_seidel:
+            raise NotImplementedError("the serial Gauss-Seidel DCD variant is not on the sm_100a path")
+        if not self.params.allow_self:
+            raise ValueError("UdcfDcdCollider: no static body and allow_self=False -> nothing to collide")
+        self.sim = sim
+        tris = np.asarray(surface_tris, np.int64).reshape(-1, 3)
+        self.n_tris = tris.shape[0]
+        lo = sim.pos0_np.min(0) - margin
+        hi = sim.pos0_np.max(0) + margin
+        self.buf = DcdBuffers(sim._lib, sim.device, sim.layout.inv[tris], sim.n_verts, self.params, lo, hi)
+        self._peak = 0
+
+    def solve(self, i_iter: int = 0) -> None:
+        s = self.sim
+        if i_iter == 0:
+            self.buf.broadphase(s._pos4, True, s._sp)
+        self.buf.narrow_respond(s._pos4, s._sp)
+
+    __call__ = solve
+
+    def stats(self) -> dict:
+        """udcf/solver.py:442-457: counts of the last pass (one device sync)."""
+        self.sim.synchronize()
+        c = self.buf.counters()
+        p = self.params
+        if c["status"] & capi.STATUS_STACK_OVERFLOW:
+            print("[udcf_dcd] WARNING: BVH traversal stack overflow")
+        if c["n_pairs"] > p.max_pairs or c["n_contacts"] > p.max_contacts:
+            print(f"[udcf_dcd] WARNING: overflow pairs={c['n_pairs']}/{p.max_pairs} "
+                  f"contacts={c['n_contacts']}/{p.max_contacts} -- raise UdcfParams caps")
+        return {"n_pairs": min(c["n_pairs"], p.max_pairs), "n_contacts": min(c["n_contacts"], p.max_contacts),
+                "status": c["status"]}

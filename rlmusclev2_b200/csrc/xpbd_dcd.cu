@@ -1,0 +1,637 @@
+// Triangle-triangle discrete collision detection (DCD) for sm_100a.
+//
+// Broadphase: per-triangle AABBs padded by the thickness, 30-bit Morton codes
+// of their centres, a stable LSD radix sort (8-bit digits, per-warp ranking
+// with __match_any_sync), a linear BVH built with Karras' method ("Maximizing
+// Parallelism in the Construction of BVHs, Octrees, and k-d Trees", HPG 2012)
+// and refitted bottom-up with per-node arrival counters; then a two-pass
+// traversal (count, exclusive scan, fill) that lists the AABB-overlapping
+// pairs (i, j > i) of every triangle in a deterministic order.
+//
+// Narrowphase / response / apply restate the reference's UDCF kernels
+// (collision/udcf/kernel.py:164-474, 713-822): Moller interval rejection,
+// VF/FV/EE candidate depths C1/C2, smaller-positive wins (tie -> C2), equal
+// push of the three vertices of each movable face, friction on the
+// bary-weighted tangential displacement, Jacobi averaging.
+#include <cuda_runtime.h>
+
+#include "xpbd_common.cuh"
+#include "xpbd_device.cuh"
+
+using namespace xpbd;
+
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortChunk = 4096;  // keys per CTA per pass
+constexpr int kStack = 64;
+constexpr float kThresh = 1.0e-5f;  // udcf/kernel.py:40 THRESH
+
+struct Aabb {
+    float3 lo, hi;
+};
+
+__device__ __forceinline__ float4 ld4(const float* p, int i) { return reinterpret_cast<const float4*>(p)[i]; }
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// ---------------------------------------------------------------- AABBs
+__global__ void k_tri_aabb(XpbdDcd D, const float* __restrict__ pos4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n_tris) return;
+    const int a = D.tris[3 * i], b = D.tris[3 * i + 1], c = D.tris[3 * i + 2];
+    const float3 pa = f3(ld4(pos4, a)), pb = f3(ld4(pos4, b)), pc = f3(ld4(pos4, c));
+    const float t = D.thickness;
+    // tri_aabb_kernel (udcf/kernel.py:917-934)
+    const float3 lo = make_float3(fminf(fminf(pa.x, pb.x), pc.x) - t, fminf(fminf(pa.y, pb.y), pc.y) - t,
+                                  fminf(fminf(pa.z, pb.z), pc.z) - t);
+    const float3 hi = make_float3(fmaxf(fmaxf(pa.x, pb.x), pc.x) + t, fmaxf(fmaxf(pa.y, pb.y), pc.y) + t,
+                                  fmaxf(fmaxf(pa.z, pb.z), pc.z) + t);
+    float4* nodes = reinterpret_cast<float4*>(D.ws_nodes);
+    const int leaf = D.n_tris - 1 + i;
+    nodes[2 * leaf] = make_float4(lo.x, lo.y, lo.z, 0.f);
+    nodes[2 * leaf + 1] = make_float4(hi.x, hi.y, hi.z, 0.f);
+    const float3 cen = make_float3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
+    float q[3] = {cen.x, cen.y, cen.z};
+    uint32_t code = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float ext = fmaxf(D.box_hi[k] - D.box_lo[k], 1e-30f);
+        float u = (q[k] - D.box_lo[k]) / ext * 1023.f;
+        u = fminf(fmaxf(u, 0.f), 1023.f);
+        code |= spread10(uint32_t(u)) << k;
+    }
+    D.ws_keys[i] = code;
+    D.ws_vals[i] = i;
+}
+
+// ---------------------------------------------------------- radix sort
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint32_t* __restrict__ keys, int n, int shift,
+                                                            int* __restrict__ hist, int nblk) {
+    __shared__ int h[256];
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) h[d] = 0;
+    __syncthreads();
+    const int b = blockIdx.x;
+    const int beg = b * kSortChunk, end = min(n, beg + kSortChunk);
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) atomicAdd(&h[(keys[i] >> shift) & 255u], 1);
+    __syncthreads();
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[d * nblk + b] = h[d];  // digit-major
+}
+
+// exclusive scan of hist (256*nblk ints, digit-major) in place, one CTA
+__global__ void __launch_bounds__(1024) k_scan_excl(int* __restrict__ a, int n, int* __restrict__ total) {
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < n ? a[i] : 0;
+        int x = v;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sums[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int s = lane < (blockDim.x >> 5) ? warp_sums[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            warp_sums[lane] = s;
+        }
+        __syncthreads();
+        const int incl = x + (w > 0 ? warp_sums[w - 1] : 0) + carry;
+        if (i < n) a[i] = incl - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = incl;
+        __syncthreads();
+    }
+    if (total && threadIdx.x == 0) *total = carry;
+}
+
+// Stable scatter: keys of a chunk are ranked round by round (256 per round);
+// within a round, the rank of a key among equal digits is the count of equal
+// digits in earlier warps plus the lanes before it in its own warp.
+__global__ void __launch_bounds__(kSortThreads)
+    k_sort_scatter(const uint32_t* __restrict__ kin, const int32_t* __restrict__ vin, uint32_t* __restrict__ kout,
+                   int32_t* __restrict__ vout, int n, int shift, const int* __restrict__ offs, int nblk) {
+    __shared__ int run[256];
+    __shared__ int wcnt[kSortThreads / 32][256];
+    const int b = blockIdx.x;
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) run[d] = offs[d * nblk + b];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int beg = b * kSortChunk, end = min(n, beg + kSortChunk);
+    for (int r = beg; r < end; r += blockDim.x) {
+        for (int k = threadIdx.x; k < (kSortThreads / 32) * 256; k += blockDim.x) (&wcnt[0][0])[k] = 0;
+        __syncthreads();
+        const int i = r + threadIdx.x;
+        const bool valid = i < end;
+        const uint32_t key = valid ? kin[i] : 0u;
+        const int dig = valid ? int((key >> shift) & 255u) : 256;
+        const unsigned peers = __match_any_sync(0xffffffffu, dig);
+        const int lrank = __popc(peers & ((1u << lane) - 1u));
+        if (valid && lrank == 0) wcnt[w][dig] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            int before = 0;
+            for (int ww = 0; ww < w; ++ww) before += wcnt[ww][dig];
+            const int dst = run[dig] + before + lrank;
+            kout[dst] = key;
+            vout[dst] = vin[i];
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < 256; d += blockDim.x) {
+            int s = 0;
+            for (int ww = 0; ww < kSortThreads / 32; ++ww) s += wcnt[ww][d];
+            run[d] += s;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------- Karras build
+__device__ __forceinline__ int delta(const uint32_t* k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    const uint32_t a = k[i], b = k[j];
+    if (a == b) return 32 + __clz(uint32_t(i) ^ uint32_t(j));
+    return __clz(a ^ b);
+}
+
+__global__ void k_build(XpbdDcd D) {
+    const int n = D.n_tris;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const uint32_t* k = D.ws_keys;
+    const int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = delta(k, n, i, i - d);
+    int lmax = 2;
+    while (lmax < 2 * n && delta(k, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(k, n, i, i + (l + t) * d) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = delta(k, n, i, j);
+    int s = 0;
+    int t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (delta(k, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    const int g = i + s * d + min(d, 0);
+    const int lo = min(i, j), hi = max(i, j);
+    const int left = (lo == g) ? (n - 1 + g) : g;
+    const int right = (hi == g + 1) ? (n - 1 + g + 1) : g + 1;
+    D.ws_child[2 * i] = left;
+    D.ws_child[2 * i + 1] = right;
+    D.ws_parent[left] = i;
+    D.ws_parent[right] = i;
+    D.ws_flags[i] = 0;
+}
+
+// leaves were written in triangle order; the tree expects them in sorted order
+__global__ void k_permute_leaves(XpbdDcd D) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= D.n_tris) return;
+    const int tri = D.ws_vals[s];
+    const float4* src = reinterpret_cast<const float4*>(D.ws_nodes) + 2 * (2 * D.n_tris - 1);
+    float4* dst = reinterpret_cast<float4*>(D.ws_nodes);
+    const int leaf = D.n_tris - 1 + s;
+    dst[2 * leaf] = src[2 * tri];
+    dst[2 * leaf + 1] = src[2 * tri + 1];
+}
+
+__global__ void k_refit(XpbdDcd D) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = D.n_tris;
+    if (s >= n) return;
+    float4* nodes = reinterpret_cast<float4*>(D.ws_nodes);
+    int node = n - 1 + s;
+    if (n == 1) return;
+    for (int step = 0; step < n; ++step) {
+        const int p = D.ws_parent[node];
+        if (p < 0) break;
+        __threadfence();
+        if (atomicAdd(&D.ws_flags[p], 1) == 0) return;  // first arrival: the sibling finishes p
+        __threadfence();
+        const int a = D.ws_child[2 * p], b = D.ws_child[2 * p + 1];
+        const float4 alo = __ldcg(&nodes[2 * a]), ahi = __ldcg(&nodes[2 * a + 1]);
+        const float4 blo = __ldcg(&nodes[2 * b]), bhi = __ldcg(&nodes[2 * b + 1]);
+        nodes[2 * p] = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.f);
+        nodes[2 * p + 1] = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f);
+        node = p;
+    }
+}
+
+// ------------------------------------------------------------ traversal
+__device__ __forceinline__ bool overlap(float4 alo, float4 ahi, float4 blo, float4 bhi) {
+    return !(alo.x > bhi.x || blo.x > ahi.x || alo.y > bhi.y || blo.y > ahi.y || alo.z > bhi.z || blo.z > ahi.z);
+}
+
+// broadphase_find_pairs_bvh_kernel rules (udcf/kernel.py:937-981): j > i,
+// static-static never, movable-self only when allowed and sharing no vertex.
+__device__ __forceinline__ bool pair_ok(const XpbdDcd& D, int i, int j) {
+    if (j <= i) return false;
+    const int gi = D.tri_group ? D.tri_group[i] : 0, gj = D.tri_group ? D.tri_group[j] : 0;
+    if (gi == 1 && gj == 1) return false;
+    if (gi == 0 && gj == 0) {
+        if (!D.allow_self) return false;
+        const int a0 = D.tris[3 * i], a1 = D.tris[3 * i + 1], a2 = D.tris[3 * i + 2];
+        const int b0 = D.tris[3 * j], b1 = D.tris[3 * j + 1], b2 = D.tris[3 * j + 2];
+        if (a0 == b0 || a0 == b1 || a0 == b2 || a1 == b0 || a1 == b1 || a1 == b2 || a2 == b0 || a2 == b1 || a2 == b2)
+            return false;
+    }
+    return true;
+}
+
+template <bool FILL>
+__global__ void k_traverse(XpbdDcd D) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = D.n_tris;
+    if (i >= n) return;
+    const float4* nodes = reinterpret_cast<const float4*>(D.ws_nodes);
+    const float4* tri_box = nodes + 2 * (2 * n - 1);  // unsorted leaf copy, triangle order
+    const float4 qlo = tri_box[2 * i], qhi = tri_box[2 * i + 1];
+    int cnt = 0;
+    int out = FILL ? D.ws_count[i] : 0;
+    int stack[kStack];
+    int sp = 0;
+    stack[sp++] = (n == 1) ? 0 : 0;
+    bool single = (n == 1);
+    while (sp > 0) {
+        const int node = stack[--sp];
+        const int idx = single ? (n - 1) : node;
+        if (!overlap(qlo, qhi, nodes[2 * idx], nodes[2 * idx + 1])) continue;
+        if (idx >= n - 1) {  // leaf
+            const int j = D.ws_vals[idx - (n - 1)];
+            if (pair_ok(D, i, j)) {
+                if (FILL) {
+                    if (out < D.max_pairs) {
+                        D.pairs[2 * out] = i;
+                        D.pairs[2 * out + 1] = j;
+                    }
+                    ++out;
+                } else {
+                    ++cnt;
+                }
+            }
+            continue;
+        }
+        if (sp + 2 > kStack) {
+            atomicOr(D.status, XPBD_STATUS_STACK_OVERFLOW);
+            break;
+        }
+        stack[sp++] = D.ws_child[2 * idx];
+        stack[sp++] = D.ws_child[2 * idx + 1];
+    }
+    if (!FILL) D.ws_count[i] = cnt;
+}
+
+__global__ void k_pairs_total(XpbdDcd D) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const int tot = *D.ws_total;
+        *D.n_pairs = tot;
+        if (tot > D.max_pairs) atomicOr(D.status, XPBD_STATUS_PAIR_OVERFLOW);
+        *D.n_contacts = 0;
+    }
+}
+
+// ------------------------------------------------------------ narrowphase
+__device__ __forceinline__ float3 pick3(float3 a, float3 b, float3 c, int i) { return i == 0 ? a : (i == 1 ? b : c); }
+
+__device__ __forceinline__ bool inside_tri(float3 p1, float3 p2, float3 p3, float3 p) {
+    const float3 c1 = cross(p2 - p1, p - p2), c2 = cross(p3 - p2, p - p3), c3 = cross(p1 - p3, p - p1);
+    return dot(c1, c2) > 0.f && dot(c1, c3) > 0.f;
+}
+
+__device__ __forceinline__ float3 bary(float3 A, float3 B, float3 Cc, float3 P) {
+    const float3 v0 = B - A, v1 = Cc - A, v2 = P - A;
+    const float d00 = dot(v0, v0), d01 = dot(v0, v1), d11 = dot(v1, v1), d20 = dot(v2, v0), d21 = dot(v2, v1);
+    const float den = d00 * d11 - d01 * d01;
+    if (den == 0.f) return make_float3(1.f / 3.f, 1.f / 3.f, 1.f / 3.f);
+    const float v = (d11 * d20 - d01 * d21) / den, w = (d00 * d21 - d01 * d20) / den;
+    return make_float3(1.f - v - w, v, w);
+}
+
+__device__ __forceinline__ bool line_isect(float3 p1, float3 p2, float3 p3, float3 p4, float3 v1, float3 v2,
+                                           float3& out) {
+    const float3 d1 = p2 - p1, d2 = p4 - p3;
+    const float3 nrm = cross(d1, d2);
+    if (len(nrm) < 1.0e-6f) return false;
+    const float den = dot(nrm, nrm);
+    if (den < 1.0e-6f) return false;
+    const float3 v = p3 - p1;
+    const float t1 = dot(cross(v, d2), nrm) / den, t2 = dot(cross(v, d1), nrm) / den;
+    if (!(t2 >= 0.f && t2 <= 1.f && t1 >= 0.f && t1 <= 1.f)) return false;
+    out = v1 + t1 * (v2 - v1);
+    return true;
+}
+
+__device__ __forceinline__ bool gen_t(float3 N, float3 v0, float3 v1, float3 v2, float d, float3 D, float2& iv) {
+    const float d0 = dot(N, v0) + d, d1 = dot(N, v1) + d, d2 = dot(N, v2) + d;
+    if (d0 <= kThresh && d1 <= kThresh && d2 <= kThresh) return false;
+    if (d0 >= -kThresh && d1 >= -kThresh && d2 >= -kThresh) return false;
+    float3 s0 = v0, s1 = v1, s2 = v2;
+    float e0 = d0, e1 = d1, e2 = d2;
+    if ((d0 <= 0.f && d1 >= 0.f && d2 >= 0.f) || (d0 >= 0.f && d1 <= 0.f && d2 <= 0.f)) {
+        s0 = v1; s1 = v0; e0 = d1; e1 = d0;
+    } else if ((d0 >= 0.f && d1 >= 0.f && d2 <= 0.f) || (d0 <= 0.f && d1 <= 0.f && d2 >= 0.f)) {
+        s1 = v2; s2 = v1; e1 = d2; e2 = d1;
+    }
+    const float p0 = dot(D, s0), p1 = dot(D, s1), p2 = dot(D, s2);
+    const float tA = p0 + (p1 - p0) * fabsf(e0 / (e0 - e1));
+    const float tB = p2 + (p1 - p2) * fabsf(e2 / (e2 - e1));
+    iv = tA > tB ? make_float2(tB, tA) : make_float2(tA, tB);
+    return true;
+}
+
+__global__ void k_narrow(XpbdDcd D, const float* __restrict__ pos4) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int np = min(*D.n_pairs, D.max_pairs);
+    if (k >= np) return;
+    const int ta = D.pairs[2 * k], tb = D.pairs[2 * k + 1];
+    const float3 q00 = f3(ld4(pos4, D.tris[3 * ta])), q01 = f3(ld4(pos4, D.tris[3 * ta + 1])),
+                 q02 = f3(ld4(pos4, D.tris[3 * ta + 2]));
+    const float3 q10 = f3(ld4(pos4, D.tris[3 * tb])), q11 = f3(ld4(pos4, D.tris[3 * tb + 1])),
+                 q12 = f3(ld4(pos4, D.tris[3 * tb + 2]));
+    const float3 n1f = cross(q01 - q00, q02 - q00), n2f = cross(q11 - q10, q12 - q10);
+    const float l1 = len(n1f), l2 = len(n2f);
+    if (l1 == 0.f || l2 == 0.f) return;
+    const float3 N1 = n1f / l1, N2 = n2f / l2;
+    const float d1 = -dot(N1, q00), d2 = -dot(N2, q10);
+    const float3 cp = cross(N1, N2);
+    const float lcp = len(cp);
+    if (lcp < 1.0e-8f) return;
+    const float3 Dd = cp / lcp;
+    float2 iv1, iv2;
+    if (!gen_t(N2, q00, q01, q02, d2, Dd, iv1)) return;
+    if (!gen_t(N1, q10, q11, q12, d1, Dd, iv2)) return;
+    if (!(iv1.y >= iv2.x && iv2.y >= iv1.x)) return;
+    float C1 = 0.f, C2 = 0.f;
+    float3 b1 = make_float3(0.f, 0.f, 0.f), b2 = b1, b3 = b1, b4 = b1;
+    for (int j = 0; j < 3; ++j) {
+        const float3 q0j = pick3(q00, q01, q02, j), q1j = pick3(q10, q11, q12, j);
+        const float3 P0j = q0j - dot(N2, q0j - q10) * N2;
+        if (inside_tri(q10, q11, q12, P0j)) {
+            const float cand = dot(N2, q0j) + d2;
+            if (C1 < -cand) {
+                C1 = -cand;
+                b1 = bary(q00, q01, q02, q0j);
+                b2 = bary(q10, q11, q12, q0j - cand * N2);
+            }
+        }
+        {
+            const float den = dot(N1, N2);
+            if (den != 0.f) {
+                const float t = dot(N1, q00 - q1j) / den;
+                const float3 Q0j = q1j + t * N2;
+                if (inside_tri(q00, q01, q02, Q0j)) {
+                    const float cand = dot(N2, Q0j) + d2;
+                    if (C1 < -cand) {
+                        C1 = -cand;
+                        b1 = bary(q00, q01, q02, Q0j);
+                        b2 = bary(q10, q11, q12, Q0j - cand * N2);
+                    }
+                }
+            }
+        }
+        const float3 P1j = q1j - dot(N1, q1j - q00) * N1;
+        if (inside_tri(q00, q01, q02, P1j)) {
+            const float cand = dot(N1, q1j) + d1;
+            if (C2 < -cand) {
+                C2 = -cand;
+                b3 = bary(q10, q11, q12, q1j);
+                b4 = bary(q00, q01, q02, q1j - cand * N1);
+            }
+        }
+        {
+            const float den = dot(N2, N1);
+            if (den != 0.f) {
+                const float t = dot(N2, q10 - q0j) / den;
+                const float3 Q1j = q0j + t * N1;
+                if (inside_tri(q10, q11, q12, Q1j)) {
+                    const float cand = dot(N1, Q1j) + d1;
+                    if (C2 < -cand) {
+                        C2 = -cand;
+                        b3 = bary(q10, q11, q12, Q1j);
+                        b4 = bary(q00, q01, q02, Q1j - cand * N1);
+                    }
+                }
+            }
+        }
+        const int jn = (j + 1) % 3;
+        const float3 q0jn = pick3(q00, q01, q02, jn), q1jn = pick3(q10, q11, q12, jn);
+        const float3 P0jn = q0jn - dot(N2, q0jn - q10) * N2;
+        const float3 P1jn = q1jn - dot(N1, q1jn - q00) * N1;
+        for (int kk = 0; kk < 3; ++kk) {
+            const int kn = (kk + 1) % 3;
+            float3 o;
+            if (line_isect(P0j, P0jn, pick3(q10, q11, q12, kk), pick3(q10, q11, q12, kn), q0j, q0jn, o)) {
+                const float cand = dot(N2, o) + d2;
+                if (C1 < -cand) {
+                    C1 = -cand;
+                    b1 = bary(q00, q01, q02, o);
+                    b2 = bary(q10, q11, q12, o - cand * N2);
+                }
+            }
+            if (line_isect(P1j, P1jn, pick3(q00, q01, q02, kk), pick3(q00, q01, q02, kn), q1j, q1jn, o)) {
+                const float cand = dot(N1, o) + d1;
+                if (C2 < -cand) {
+                    C2 = -cand;
+                    b3 = bary(q10, q11, q12, o);
+                    b4 = bary(q00, q01, q02, o - cand * N1);
+                }
+            }
+        }
+    }
+    if (C1 <= D.offset_eps || C2 <= D.offset_eps) return;
+    const int slot = atomicAdd(D.n_contacts, 1);
+    if (slot >= D.max_contacts) {
+        atomicOr(D.status, XPBD_STATUS_CONTACT_OVERFLOW);
+        return;
+    }
+    const bool first = C1 < C2;  // tie -> C2 branch
+    const int tc = first ? ta : tb, tl = first ? tb : ta;
+    int4* cid = reinterpret_cast<int4*>(D.c_ids);
+    cid[2 * slot] = make_int4(D.tris[3 * tc], D.tris[3 * tc + 1], D.tris[3 * tc + 2], k);
+    cid[2 * slot + 1] = make_int4(D.tris[3 * tl], D.tris[3 * tl + 1], D.tris[3 * tl + 2], 0);
+    float4* cf = reinterpret_cast<float4*>(D.c_data);
+    const float3 n = first ? N2 : N1;
+    const float3 bb1 = first ? b1 : b3, bb2 = first ? b2 : b4;
+    cf[3 * slot] = make_float4(n.x, n.y, n.z, first ? C1 : C2);
+    cf[3 * slot + 1] = make_float4(bb1.x, bb1.y, bb1.z, C1);
+    cf[3 * slot + 2] = make_float4(bb2.x, bb2.y, bb2.z, C2);
+}
+
+// respond_kernel (udcf/kernel.py:713-806)
+__global__ void k_respond(XpbdDcd D, const float* __restrict__ pos4) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nc = min(*D.n_contacts, D.max_contacts);
+    if (k >= nc) return;
+    const int4 cu = reinterpret_cast<const int4*>(D.c_ids)[2 * k];
+    const int4 cl = reinterpret_cast<const int4*>(D.c_ids)[2 * k + 1];
+    const float4 f0 = reinterpret_cast<const float4*>(D.c_data)[3 * k];
+    const float4 f1 = reinterpret_cast<const float4*>(D.c_data)[3 * k + 1];
+    const float4 f2 = reinterpret_cast<const float4*>(D.c_data)[3 * k + 2];
+    float pen = f0.w;
+    if (D.max_push > 0.f && pen > D.max_push) pen = D.max_push;
+    float C = pen * D.multiplier;
+    if (C == 0.f) return;
+    const float3 nrm = make_float3(f0.x, f0.y, f0.z);
+    const float4 pu0 = ld4(pos4, cu.x), pu1 = ld4(pos4, cu.y), pu2 = ld4(pos4, cu.z);
+    const float4 pl0 = ld4(pos4, cl.x), pl1 = ld4(pos4, cl.y), pl2 = ld4(pos4, cl.z);
+    const bool solid_cur = pu0.w == 0.f || pu1.w == 0.f || pu2.w == 0.f;
+    const bool solid_clo = pl0.w == 0.f || pl1.w == 0.f || pl2.w == 0.f;
+    if (!solid_cur && !solid_clo) C = C * 0.5f;
+    const float3 push_clo = solid_clo ? make_float3(0.f, 0.f, 0.f) : (-C) * nrm;
+    const float3 push_cur = solid_cur ? make_float3(0.f, 0.f, 0.f) : C * nrm;
+    const float4* xp = reinterpret_cast<const float4*>(D.x_prev);
+    const float3 v0 = (f3(pl0) + push_clo) - f3(xp[cl.x]), v1 = (f3(pl1) + push_clo) - f3(xp[cl.y]),
+                 v2 = (f3(pl2) + push_clo) - f3(xp[cl.z]);
+    const float3 v3 = (f3(pu0) + push_cur) - f3(xp[cu.x]), v4 = (f3(pu1) + push_cur) - f3(xp[cu.y]),
+                 v5 = (f3(pu2) + push_cur) - f3(xp[cu.z]);
+    const float3 g = nrm / len(nrm);
+    const float3 b1 = make_float3(f1.x, f1.y, f1.z), b2 = make_float3(f2.x, f2.y, f2.z);
+    const float3 vclo = (b1.x * v0 + b1.y * v1) + b1.z * v2;
+    const float3 perp_clo = vclo - dot(vclo, g) * g;
+    const float3 vcur = (b2.x * v3 + b2.y * v4) + b2.z * v5;
+    const float3 perp_cur = vcur - dot(vcur, g) * g;
+    float3 diff = perp_cur - perp_clo;
+    const float dn = len(diff);
+    const float static_norm = pen * D.friction_static;
+    if (dn > static_norm && dn > 0.f) diff = (pen * D.friction_dynamic / dn) * diff;
+    const float3 diffV = 0.5f * diff;
+    const float3 diffT = diff - diffV;
+    float4* acc = reinterpret_cast<float4*>(D.dP);
+    const float3 mu = push_cur - diffV, ml = push_clo + diffT;
+    if (pu0.w > 0.f) atomicAdd(&acc[cu.x], make_float4(mu.x, mu.y, mu.z, 1.f));
+    if (pu1.w > 0.f) atomicAdd(&acc[cu.y], make_float4(mu.x, mu.y, mu.z, 1.f));
+    if (pu2.w > 0.f) atomicAdd(&acc[cu.z], make_float4(mu.x, mu.y, mu.z, 1.f));
+    if (pl0.w > 0.f) atomicAdd(&acc[cl.x], make_float4(ml.x, ml.y, ml.z, 1.f));
+    if (pl1.w > 0.f) atomicAdd(&acc[cl.y], make_float4(ml.x, ml.y, ml.z, 1.f));
+    if (pl2.w > 0.f) atomicAdd(&acc[cl.z], make_float4(ml.x, ml.y, ml.z, 1.f));
+}
+
+// apply_kernel (udcf/kernel.py:809-822), clearing the accumulator it reads
+__global__ void k_dcd_apply(XpbdDcd D, float* pos4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n_verts) return;
+    float4* acc = reinterpret_cast<float4*>(D.dP);
+    const float4 a = acc[i];
+    if (a.w > 0.f) {
+        float4 p = reinterpret_cast<float4*>(pos4)[i];
+        if (D.jacobi_avg) {
+            p.x += a.x / a.w;
+            p.y += a.y / a.w;
+            p.z += a.z / a.w;
+        } else {
+            p.x += a.x;
+            p.y += a.y;
+            p.z += a.z;
+        }
+        reinterpret_cast<float4*>(pos4)[i] = p;
+        acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+__global__ void k_copy4(const float4* __restrict__ src, float4* __restrict__ dst, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i];
+}
+
+int check_dcd(const XpbdDcd* D) {
+    if (!D || D->n_tris <= 0 || D->n_verts <= 0 || !D->tris || !D->pairs || !D->n_pairs || !D->n_contacts ||
+        !D->c_ids || !D->c_data || !D->x_prev || !D->dP || !D->status || !D->ws_nodes || !D->ws_keys || !D->ws_vals ||
+        !D->ws_keys2 || !D->ws_vals2 || !D->ws_hist || !D->ws_child || !D->ws_parent || !D->ws_flags || !D->ws_count ||
+        !D->ws_total)
+        return fail(XPBD_ERR_ARG, "XpbdDcd: null member or empty size");
+    if (D->max_pairs <= 0 || D->max_contacts <= 0) return fail(XPBD_ERR_ARG, "XpbdDcd: capacities must be > 0");
+    if (!aligned16(D->ws_nodes) || !aligned16(D->c_ids) || !aligned16(D->c_data) || !aligned16(D->x_prev) ||
+        !aligned16(D->dP))
+        return fail(XPBD_ERR_ALIGN, "XpbdDcd: 16-byte alignment");
+    return XPBD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int xpbd_dcd_workspace_query(int32_t n_tris, XpbdDcdWorkspaceSizes* out) {
+    if (n_tris <= 0 || !out) return fail(XPBD_ERR_ARG, "xpbd_dcd_workspace_query: bad arguments");
+    const int nblk = (n_tris + kSortChunk - 1) / kSortChunk;
+    out->nodes_floats = int64_t(2 * (2 * n_tris - 1)) * 4 * 2;  // sorted tree + unsorted leaf copy
+    out->keys = n_tris;
+    out->hist = int64_t(256) * nblk;
+    out->child = int64_t(2) * (n_tris > 1 ? n_tris - 1 : 1);
+    out->parent = int64_t(2) * n_tris - 1;
+    out->flags = n_tris > 1 ? n_tris - 1 : 1;
+    out->count = n_tris;
+    return XPBD_OK;
+}
+
+int xpbd_dcd_broadphase(const XpbdDcd* D, const float* pos4, int32_t snapshot_prev, xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_dcd(D))) return rc;
+    if (!pos4 || !aligned16(pos4)) return fail(XPBD_ERR_ARG, "xpbd_dcd_broadphase: pos4");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = D->n_tris;
+    if (snapshot_prev)
+        k_copy4<<<(D->n_verts + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float4*>(pos4),
+                                                          reinterpret_cast<float4*>(D->x_prev), D->n_verts);
+    // leaf boxes go to the unsorted copy region first
+    XpbdDcd Dl = *D;
+    Dl.ws_nodes = D->ws_nodes + int64_t(2 * (2 * n - 1)) * 4 - int64_t(2 * (n - 1)) * 4;
+    k_tri_aabb<<<(n + 255) / 256, 256, 0, s>>>(Dl, pos4);
+    // radix sort (keys, tri ids): 4 passes of 8 bits, ping-pong
+    const int nblk = (n + kSortChunk - 1) / kSortChunk;
+    uint32_t* ka = D->ws_keys;
+    int32_t* va = D->ws_vals;
+    uint32_t* kb = D->ws_keys2;
+    int32_t* vb = D->ws_vals2;
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 8 * pass;
+        k_sort_hist<<<nblk, kSortThreads, 0, s>>>(ka, n, shift, D->ws_hist, nblk);
+        k_scan_excl<<<1, 1024, 0, s>>>(D->ws_hist, 256 * nblk, nullptr);
+        k_sort_scatter<<<nblk, kSortThreads, 0, s>>>(ka, va, kb, vb, n, shift, D->ws_hist, nblk);
+        uint32_t* tk = ka; ka = kb; kb = tk;
+        int32_t* tv = va; va = vb; vb = tv;
+    }
+    // after an even number of passes the sorted data is back in ws_keys/ws_vals
+    if (n > 1) {
+        k_build<<<(n - 1 + 255) / 256, 256, 0, s>>>(*D);
+        cudaMemsetAsync(D->ws_parent, 0xff, sizeof(int32_t), s);  // root has no parent
+    } else {
+        cudaMemsetAsync(D->ws_parent, 0xff, sizeof(int32_t), s);
+    }
+    k_permute_leaves<<<(n + 255) / 256, 256, 0, s>>>(*D);
+    if (n > 1) k_refit<<<(n + 255) / 256, 256, 0, s>>>(*D);
+    k_traverse<false><<<(n + 127) / 128, 128, 0, s>>>(*D);
+    k_scan_excl<<<1, 1024, 0, s>>>(D->ws_count, n, D->ws_total);
+    k_traverse<true><<<(n + 127) / 128, 128, 0, s>>>(*D);
+    k_pairs_total<<<1, 32, 0, s>>>(*D);
+    return cuda_check("xpbd_dcd_broadphase");
+}
+
+int xpbd_dcd_narrow_respond(const XpbdDcd* D, float* pos4, xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_dcd(D))) return rc;
+    if (!pos4 || !aligned16(pos4)) return fail(XPBD_ERR_ARG, "xpbd_dcd_narrow_respond: pos4");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaMemsetAsync(D->n_contacts, 0, sizeof(int32_t), s);
+    k_narrow<<<(D->max_pairs + 255) / 256, 256, 0, s>>>(*D, pos4);
+    k_respond<<<(D->max_contacts + 255) / 256, 256, 0, s>>>(*D, pos4);
+    k_dcd_apply<<<(D->n_verts + 255) / 256, 256, 0, s>>>(*D, pos4);
+    return cuda_check("xpbd_dcd_narrow_respond");
+}
+
+}  // extern "C"

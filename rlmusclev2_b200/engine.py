@@ -36,9 +36,11 @@ def _ptr(t) -> int | None:
 class XpbdEngine:
     """State-independent substep primitives plus the program runner."""
 
-    #: fused Jacobi iteration: PROJECT_FUSED_LAST (one launch) or PROJECT_FUSED
-    #: (tile pass + boundary finish launch)
-    fused_mode = capi.PROJECT_FUSED_LAST
+    #: fused Jacobi iteration: PROJECT_FUSED (tile pass + boundary finish
+    #: launch; measured faster on B200) or PROJECT_FUSED_LAST (one launch)
+    fused_mode = capi.PROJECT_FUSED
+    #: replay frames as CUDA graphs (False: launch the same kernels eagerly)
+    use_graphs = True
 
     # subclasses fill these before calling _setup_device()
     pos0_np: np.ndarray
@@ -414,6 +416,9 @@ class XpbdEngine:
     def _graph(self, key, body) -> None:
         """Capture ``body`` (a sequence of library launches on the engine stream)
         once per key, then replay it."""
+        if not self.use_graphs:
+            body()
+            return
         g = self._graphs.get(key)
         if g is None:
             capi.check(self._lib.xpbd_graph_begin(self._sp))
