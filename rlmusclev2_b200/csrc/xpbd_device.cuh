@@ -164,22 +164,84 @@ struct Corr4 {
     float3 d[4];
 };
 
+// Rotation factor R of F = R S for det F > 0, by Higham's scaled Newton
+// iteration X <- (g X + (g X)^-T) / 2, g = |det X|^(-1/3) (N. J. Higham,
+// "Computing the polar decomposition with applications", SIAM J. Sci. Stat.
+// Comput. 7, 1986).  X^-T = cof(X)/det X with the cofactor columns as cross
+// products of X's columns.  Returns false (caller falls back to the SVD) for
+// det F <= tiny or when 10 steps do not converge.
+__device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
+    float3 x0 = make_float3(F.m[0][0], F.m[1][0], F.m[2][0]);
+    float3 x1 = make_float3(F.m[0][1], F.m[1][1], F.m[2][1]);
+    float3 x2 = make_float3(F.m[0][2], F.m[1][2], F.m[2][2]);
+    const float n2 = dot(x0, x0) + dot(x1, x1) + dot(x2, x2);
+    float3 c0 = cross(x1, x2);
+    float det = dot(x0, c0);
+    if (!(det > 1e-6f * n2 * sqrtf(n2))) return false;
+#pragma unroll 1
+    for (int it = 0; it < 10; ++it) {
+        const float3 c1 = cross(x2, x0), c2 = cross(x0, x1);
+        const float g = rcbrtf(det);          // |det X|^(-1/3), det > 0
+        const float h = 0.5f / (g * det);     // 1 / (2 g det)
+        const float a = 0.5f * g;
+        const float3 y0 = a * x0 + h * c0, y1 = a * x1 + h * c1, y2 = a * x2 + h * c2;
+        const float3 e0 = y0 - x0, e1 = y1 - x1, e2 = y2 - x2;
+        const float ch = dot(e0, e0) + dot(e1, e1) + dot(e2, e2);
+        x0 = y0;
+        x1 = y1;
+        x2 = y2;
+        if (ch <= 1e-12f) {  // step <= 1e-6: quadratic convergence leaves an error ~1e-12
+            R.m[0][0] = x0.x; R.m[1][0] = x0.y; R.m[2][0] = x0.z;
+            R.m[0][1] = x1.x; R.m[1][1] = x1.y; R.m[2][1] = x1.z;
+            R.m[0][2] = x2.x; R.m[1][2] = x2.y; R.m[2][2] = x2.z;
+            return true;
+        }
+        c0 = cross(x1, x2);
+        det = dot(x0, c0);
+        if (!(det > 0.f)) return false;
+    }
+    return false;
+}
+
 // solve_tetarap_svd_kernel, solve_kernels.py:1194-1307 (Jacobi branch).
+// With the sign-fixed SVD F = U diag(s) V^T (U, V rotations) the constraint is
+// C = ||s - 1|| = ||F - U V^T||_F and dC/dF = U diag((s-1)/C) V^T = (F - U V^T)/C,
+// U V^T being the rotation nearest F.  For det F > 0 that rotation is the polar
+// factor, obtained without the SVD; inverted or degenerate tets use the SVD.
 __device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float k, float dt, Corr4& out) {
-    const Svd3 s = svd3(F);
-    const float a = s.s0 - 1.f, b = s.s1 - 1.f, c = s.s2 - 1.f;
-    const float ssq = a * a + b * b + c * c;
-    if (ssq < 1.0e-12f) return false;
-    const float C = sqrtf(ssq);
-    const float invC = 1.f / C;
-    const float d0 = invC * a, d1 = invC * b, d2 = invC * c;
-    const float U[3][3] = {{s.u0.x, s.u1.x, s.u2.x}, {s.u0.y, s.u1.y, s.u2.y}, {s.u0.z, s.u1.z, s.u2.z}};
-    const float V[3][3] = {{s.v0.x, s.v1.x, s.v2.x}, {s.v0.y, s.v1.y, s.v2.y}, {s.v0.z, s.v1.z, s.v2.z}};
     M3 G;
+    M3 R;
+    float ssq;
+    if (polar_rotation(F, R)) {
+        ssq = 0.f;
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+        for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) G.m[i][j] = U[i][0] * V[j][0] * d0 + U[i][1] * V[j][1] * d1 + U[i][2] * V[j][2] * d2;
+            for (int j = 0; j < 3; ++j) {
+                G.m[i][j] = F.m[i][j] - R.m[i][j];
+                ssq += G.m[i][j] * G.m[i][j];
+            }
+        if (ssq < 1.0e-12f) return false;
+        const float invC = rsqrtf(ssq);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) G.m[i][j] *= invC;
+    } else {
+        const Svd3 s = svd3(F);
+        const float a = s.s0 - 1.f, b = s.s1 - 1.f, c = s.s2 - 1.f;
+        ssq = a * a + b * b + c * c;
+        if (ssq < 1.0e-12f) return false;
+        const float invC = 1.f / sqrtf(ssq);
+        const float d0 = invC * a, d1 = invC * b, d2 = invC * c;
+        const float U[3][3] = {{s.u0.x, s.u1.x, s.u2.x}, {s.u0.y, s.u1.y, s.u2.y}, {s.u0.z, s.u1.z, s.u2.z}};
+        const float V[3][3] = {{s.v0.x, s.v1.x, s.v2.x}, {s.v0.y, s.v1.y, s.v2.y}, {s.v0.z, s.v1.z, s.v2.z}};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) G.m[i][j] = U[i][0] * V[j][0] * d0 + U[i][1] * V[j][1] * d1 + U[i][2] * V[j][2] * d2;
+    }
+    const float C = sqrtf(ssq);
     float3 g[4];
     g[0] = grad_row(G, B, 0);
     g[1] = grad_row(G, B, 1);
