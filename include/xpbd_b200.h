@@ -321,6 +321,23 @@ int xpbd_dcd_broadphase(const XpbdDcd* dcd, const float* pos4, int32_t snapshot_
  * 713-822). */
 int xpbd_dcd_narrow_respond(const XpbdDcd* dcd, float* pos4, xpbd_stream_t stream);
 
+/* Allocation-free Jacobi iteration.  This entry point has no counterpart in
+ * the reference.  It is for callers that cannot allocate device memory or
+ * hand the library a scratch buffer: a step recorded inside another
+ * framework's CUDA graph capture (cudaMalloc is illegal during capture), a
+ * plugin in a process whose GPU memory is owned by another allocator, a
+ * real-time loop that forbids allocation after start-up.  It performs the
+ * same fused iteration as xpbd_project(XPBD_PROJECT_FUSED) followed by
+ * xpbd_apply_boundary(ATTACH | DIVIDE | PIN | CLEAR); v->accum is ignored and
+ * the accumulator is instead a fixed device array of XPBD_NOALLOC_MAX_VERTS
+ * float4 (4 MiB) that every GPU loading the library holds until process
+ * exit.  Meshes with more than XPBD_NOALLOC_MAX_VERTS vertices are rejected
+ * with XPBD_ERR_LIMIT.  The first call on a device looks up that array's
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
+#define XPBD_NOALLOC_MAX_VERTS 262144
+int xpbd_iterate_noalloc(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v, xpbd_stream_t stream);
+
 /* Stream capture helpers (a captured substep replays as one graph launch). */
 int xpbd_graph_begin(xpbd_stream_t stream);
 int xpbd_graph_end(xpbd_stream_t stream, void** exec_out);

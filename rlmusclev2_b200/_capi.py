@@ -12,6 +12,7 @@ from pathlib import Path
 MAX_MATERIALS = 64
 MAX_ATTACH_MATERIALS = 16
 MAX_TILE_VERTS = 4096
+NOALLOC_MAX_VERTS = 262144
 
 OK = 0
 MAT_ARAPSVD, MAT_VOLUME, MAT_ANISO, MAT_SNH, MAT_DAMPED = 1, 2, 4, 8, 16
@@ -115,6 +116,7 @@ _SIGS = {
     "xpbd_dcd_workspace_query": ([C.c_int32, C.POINTER(XpbdDcdWorkspaceSizes)], C.c_int),
     "xpbd_dcd_broadphase": ([C.POINTER(XpbdDcd), P, C.c_int32, P], C.c_int),
     "xpbd_dcd_narrow_respond": ([C.POINTER(XpbdDcd), P, P], C.c_int),
+    "xpbd_iterate_noalloc": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), P], C.c_int),
     "xpbd_graph_begin": ([P], C.c_int),
     "xpbd_graph_end": ([P, C.POINTER(C.c_void_p)], C.c_int),
     "xpbd_graph_launch": ([P, P], C.c_int),
