@@ -30,11 +30,18 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
-CONFIG = ROOT / "rlmusclev2_b200" / "configs" / "humanv2_synth.json"
+CONFIGS = {
+    "humanv2": (ROOT / "rlmusclev2_b200" / "configs" / "humanv2_synth.json",
+                "humanv2_synth_535k_tets (10 substeps x 20 Jacobi iterations, SDF push-out)"),
+    "humanv2_mg_dcd": (ROOT / "rlmusclev2_b200" / "configs" / "humanv2_synth_mg_dcd.json",
+                       "humanv2_synth_535k_tets + 2-level multigrid (2 coarse + 1 fine iterations) + tri-tri DCD "
+                       "with per-substep LBVH + SNH fascia"),
+}
+CONFIG = CONFIGS["humanv2"][0]
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC = ROOT / "profiles" / "ncu_traffic.json"
 FALLBACK_HBM_GBS = 6650.0
-WORKLOAD = "humanv2_synth_535k_tets (10 substeps x 20 Jacobi iterations, SDF push-out)"
+WORKLOAD = CONFIGS["humanv2"][1]
 
 
 def _peak_hbm():
@@ -284,13 +291,17 @@ def run_ours(args):
     sim._targets_kernel()
     sim.collision_solvers[0].bake() if sim.collision_solvers else None
     for sub in range(sim.nsubsteps):
-        sim._vstep(capi.OP_PREDICT | (capi.OP_PIN if sim._has_pins else 0))
-        for _ in range(sim.fine_iters):
+        sim._vstep(capi.OP_PREDICT | (capi.OP_PIN if sim._has_pins and sim.mg is None else 0))
+        if sim.mg is not None:
+            sim.mg.vcycle(pin_fine=sim._has_pins)
+        for it in range(sim.fine_iters):
             a, b = ev(), ev()
             a.record(stream)
             sim._fused_iteration()
             b.record(stream)
             iters.append((a, b))
+            for fn in sim.collision_solvers_iter:
+                fn(it)
     stream.synchronize()
     it_ms = float(np.mean([a.elapsed_time(b) for a, b in iters]))
     alg_bytes = L.n_tets * 56 + L.n_verts * 40
@@ -302,8 +313,11 @@ def run_ours(args):
         traffic = tr.get("bytes_per_iteration")
     except Exception:
         pass
-    launches_per_frame = 1 + (1 if sim.collision_solvers else 0) + (1 if sim._has_pins else 0) + sim.nsubsteps * (
-        1 + 2 * sim.fine_iters) + 1
+    per_iter = 2 + (3 if getattr(sim, "dcd", None) is not None else 0)
+    per_sub = 1 + sim.fine_iters * per_iter + (2 + 2 * sim.mg.iters if sim.mg is not None else 0)
+    per_sub += 21 if getattr(sim, "dcd", None) is not None else 0  # broadphase on the first iteration
+    launches_per_frame = 1 + (1 if sim.collision_solvers else 0) + (1 if sim._has_pins else 0) + (
+        1 if sim.mg is not None else 0) + sim.nsubsteps * per_sub + 1
     n_iter = sim.nsubsteps * sim.fine_iters
     line = {
         "metric": "ms/frame", "value": round(ms_frame, 4), "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
@@ -324,7 +338,7 @@ def run_ours(args):
         "clocks": clk.summary(),
         "gpu_launches": (launches_per_frame + 1) * args.steps,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config == "humanv2":
         cb = CpuBaseline(cfg, sc)
         line["cpu_baseline"] = cb.describe(cb.sample(2), 2)
     sim.release_graphs()
@@ -374,10 +388,14 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="humanv2",
+                    help="workload (default: the 535k-tet configuration the metric is quoted on)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", choices=["humanv2", "box3m"], default=None,
                     help="run a small fixed workload for ncu and exit")
     args = ap.parse_args()
+    global CONFIG, WORKLOAD
+    CONFIG, WORKLOAD = CONFIGS[args.config]
     if args.profile_case:
         return run_profile_case(args)
     if args.warmup < 3:

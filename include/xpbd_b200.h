@@ -78,7 +78,8 @@ typedef struct XpbdParams {
     float fiber_stiffness_scale; /* aniso_arap stiffness multiplier */
     int32_t n_materials;
     int32_t n_attach_materials;
-    int32_t tile_variant;        /* tile-pass build: 0 = 2 CTAs/SM (128 regs), 1 = 3 CTAs/SM (80 regs) */
+    int32_t tile_variant;        /* bit 0: tile pass with 3 CTAs/SM (80 regs) instead of 2 (128 regs);
+                                    bit 1: ARAP-SVD through the SVD even where the polar rotation applies */
     XpbdMaterial materials[XPBD_MAX_MATERIALS];
     XpbdAttachMaterial attach[XPBD_MAX_ATTACH_MATERIALS];
 } XpbdParams;
@@ -206,14 +207,18 @@ int xpbd_pin_overwrite_masked(int32_t n, const int32_t* pts, const float* target
 int xpbd_metrics(const XpbdTiles* tiles, const XpbdVerts* v, XpbdMetrics* out, xpbd_stream_t stream);
 
 /* Per-frame kinematic targets of bone-bound vertices.  transforms is
- * [n_bones][12] = row-major 3x4 [R | t]; vertex i (library order) has bone
- * vert_bone[i] and rest position rest4[i] (x,y,z,-); target = R x + t is
- * written to pin_target[i].xyz and attach_target[i].xyz (their .w lanes are
- * kept).  Replaces the per-frame target refresh of MultiGridSim
- * (load_frame_targets / _update_belly_attach_targets, mg/mg.py:1386-1407,
- * 725-734) without the reference's device->host->device round trip. */
+ * [n_bones][12] = row-major 3x4 [R | t]; vertex i (library order) rides bones
+ * vert_bone[i][0..1] with blend weight vert_w[i] (NULL = 0) from rest
+ * position rest4[i] (x,y,z,-): target = (1-w)(R_a x + t_a) + w (R_b x + t_b)
+ * (two-bone linear blend skinning, the reference's target_mode="lbs",
+ * mg/mg.py:1176-1209), written to pin_target[i].xyz and
+ * attach_target[i].xyz (their .w lanes are kept).  Replaces the per-frame
+ * target refresh of MultiGridSim (load_frame_targets /
+ * _update_belly_attach_targets, mg/mg.py:1386-1407, 725-734) without the
+ * reference's device->host->device round trip. */
 int xpbd_bone_targets(int32_t n, int32_t n_bones, const float* transforms, const int32_t* vert_bone,
-                      const float* rest4, float* pin_target, float* attach_target, xpbd_stream_t stream);
+                      const float* vert_w, const float* rest4, float* pin_target, float* attach_target,
+                      xpbd_stream_t stream);
 
 /* Capsule bone, rest pose: centre, unit axis, half segment length, radius. */
 typedef struct XpbdCapsule {

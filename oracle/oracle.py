@@ -402,6 +402,8 @@ class OracleMultiGridSim(OracleSolver):
         self.inv_mass = np.where(self.mass > 0, 1.0 / np.where(self.mass > 0, self.mass, 1), 0).astype(self.P.dt)
         self.target = None
         self.mg = None
+        scfg = (cfg.get("demo") or {}).get("self_collision") or {}
+        self.dcd = scfg if str(scfg.get("method", "none")).lower() == "udcf" else None
         if cfg.get("use_multigrid", False):
             self._init_mg(float(arap["stiffness"]))
 
@@ -476,14 +478,35 @@ class OracleMultiGridSim(OracleSolver):
             + w[:, 3:4] * d[self.mg_t[:, 3]]
 
     def targets(self, frame):
+        """Two-bone blended target (1-w)(R_a x + t_a) + w (R_b x + t_b), float32."""
         T = self.scene.bone_transforms(frame).astype(np.float32)
-        b = self.scene.vert_bone
         x = self.scene.verts.astype(np.float32)
-        Tb = T[b]
-        out = np.empty_like(x)
-        for r in range(3):
-            out[:, r] = ((Tb[:, r, 0] * x[:, 0] + Tb[:, r, 1] * x[:, 1]) + Tb[:, r, 2] * x[:, 2]) + Tb[:, r, 3]
-        return out, T.reshape(-1, 12)
+        outs = []
+        for k in range(2):
+            Tb = T[self.scene.vert_bone[:, k]]
+            o = np.empty_like(x)
+            for r in range(3):
+                o[:, r] = ((Tb[:, r, 0] * x[:, 0] + Tb[:, r, 1] * x[:, 1]) + Tb[:, r, 2] * x[:, 2]) + Tb[:, r, 3]
+            outs.append(o)
+        w = self.scene.vert_bw.astype(np.float32)[:, None]
+        return (outs[0] + w * (outs[1] - outs[0])).astype(np.float32), T.reshape(-1, 12)
+
+    def dcd_solve(self, it):
+        """UdcfDcdCollider.solve (udcf/solver.py:365-440) on the muscle surface, FP32."""
+        c = self.dcd
+        p4 = np.zeros((self.nv, 4), np.float32)
+        p4[:, :3] = self.pos
+        p4[:, 3] = self.inv_mass
+        tris = self.scene.surface_tris
+        if it == 0:
+            self.dcd_prev = p4.copy()
+            self.dcd_pairs, _ = dcd_pairs(tris, p4, float(c.get("thickness", 0.0)), bool(c.get("allow_self", True)))
+        ids, data = dcd_narrow(self.dcd_pairs, tris, p4, float(c.get("offset", 1e-6)))
+        out = dcd_respond_apply(ids, data, p4, self.dcd_prev, float(c.get("multiplier", 1.01)),
+                                float(c.get("friction_static", 0.5)), float(c.get("friction_dynamic", 0.4)),
+                                float(c.get("max_push", 0.0)))
+        self.pos[:] = out[:, :3]
+        self.dcd_last = (self.dcd_pairs.shape[0], ids.shape[0])
 
     def apply_pins(self):
         self.pos[self.active] = self.target[self.active]
@@ -503,10 +526,12 @@ class OracleMultiGridSim(OracleSolver):
             if self.mg is not None:
                 self.vcycle()
             self.apply_pins()
-            for _ in range(self.fine_iters):
+            for it in range(self.fine_iters):
                 self.project()
                 self.apply_dP()
                 self.apply_pins()
+                if self.dcd is not None:
+                    self.dcd_solve(it)
             if self.coll:
                 sdf_push(self.pos, self.inv_mass, self.phi, self.sdf_origin, self.sdf_h,
                          float(self.coll.get("contact_offset", 0.0)), float(self.coll.get("max_push", -1.0)),

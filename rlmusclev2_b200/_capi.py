@@ -108,7 +108,7 @@ _SIGS = {
     "xpbd_apply_all": ([C.POINTER(XpbdParams), C.POINTER(XpbdVerts), C.c_uint32, P], C.c_int),
     "xpbd_pin_overwrite_masked": ([C.c_int32, P, P, P, P, P, P], C.c_int),
     "xpbd_metrics": ([C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), P, P], C.c_int),
-    "xpbd_bone_targets": ([C.c_int32, C.c_int32, P, P, P, P, P, P], C.c_int),
+    "xpbd_bone_targets": ([C.c_int32, C.c_int32, P, P, P, P, P, P, P], C.c_int),
     "xpbd_sdf_bake_capsules": ([C.POINTER(XpbdSdf), C.c_int32, P, P, C.c_float, P], C.c_int),
     "xpbd_gather": ([C.c_int32, C.c_int32, P, P, C.c_int32, P, C.c_int32, P], C.c_int),
     "xpbd_mg_restrict": ([C.POINTER(XpbdCage), P, P, P, P, P], C.c_int),

@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
                           prm.fiber_stiffness_scale, prm.dt, c))
                 add(c);
         }
-        if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, m.arap_k, prm.dt, c)) add(c);
+        if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, m.arap_k, prm.dt, c, (prm.tile_variant & 2) != 0)) add(c);
         if (nact != 0.f) {
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
@@ -420,7 +420,7 @@ int check_params(const XpbdParams* p) {
         p->n_attach_materials > XPBD_MAX_ATTACH_MATERIALS)
         return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range");
     if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0");
-    if (p->tile_variant < 0 || p->tile_variant > 1) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be 0 or 1");
+    if (p->tile_variant < 0 || p->tile_variant > 3) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..3");
     return XPBD_OK;
 }
 int check_tiles(const XpbdTiles* t) {
@@ -464,7 +464,7 @@ int launch_project_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts*
 
 template <int MODE, bool DAMP>
 int launch_project(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
-    if (prm->tile_variant == 1) return launch_project_v<MODE, DAMP, 3>(prm, T, V, fops, s);
+    if (prm->tile_variant & 1) return launch_project_v<MODE, DAMP, 3>(prm, T, V, fops, s);
     return launch_project_v<MODE, DAMP, 2>(prm, T, V, fops, s);
 }
 

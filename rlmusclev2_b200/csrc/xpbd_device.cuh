@@ -208,11 +208,12 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
 // C = ||s - 1|| = ||F - U V^T||_F and dC/dF = U diag((s-1)/C) V^T = (F - U V^T)/C,
 // U V^T being the rotation nearest F.  For det F > 0 that rotation is the polar
 // factor, obtained without the SVD; inverted or degenerate tets use the SVD.
-__device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float k, float dt, Corr4& out) {
+__device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float k, float dt, Corr4& out,
+                                            bool force_svd = false) {
     M3 G;
     M3 R;
     float ssq;
-    if (polar_rotation(F, R)) {
+    if (!force_svd && polar_rotation(F, R)) {
         ssq = 0.f;
 #pragma unroll
         for (int i = 0; i < 3; ++i)

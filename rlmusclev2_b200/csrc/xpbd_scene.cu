@@ -11,25 +11,33 @@ using namespace xpbd;
 
 namespace {
 
-__global__ void k_bone_targets(int n, int nb, const float* __restrict__ tr, const int32_t* __restrict__ vb,
-                               const float4* __restrict__ rest4, float4* pin, float4* att) {
+__device__ __forceinline__ float3 xform(const float* T, float4 x) {
+    return make_float3(T[0] * x.x + T[1] * x.y + T[2] * x.z + T[3], T[4] * x.x + T[5] * x.y + T[6] * x.z + T[7],
+                       T[8] * x.x + T[9] * x.y + T[10] * x.z + T[11]);
+}
+
+__global__ void k_bone_targets(int n, int nb, const float* __restrict__ tr, const int2* __restrict__ vb,
+                               const float* __restrict__ vw, const float4* __restrict__ rest4, float4* pin, float4* att) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int b = vb[i];
-    if (b < 0 || b >= nb) return;
-    const float* T = tr + 12 * b;
+    const int2 b = vb[i];
+    if (b.x < 0 || b.x >= nb || b.y < 0 || b.y >= nb) return;
     const float4 x = rest4[i];
-    const float tx = T[0] * x.x + T[1] * x.y + T[2] * x.z + T[3];
-    const float ty = T[4] * x.x + T[5] * x.y + T[6] * x.z + T[7];
-    const float tz = T[8] * x.x + T[9] * x.y + T[10] * x.z + T[11];
+    const float3 ta = xform(tr + 12 * b.x, x);
+    float3 t = ta;
+    if (vw) {
+        const float w = vw[i];
+        const float3 tb = xform(tr + 12 * b.y, x);
+        t = make_float3(ta.x + w * (tb.x - ta.x), ta.y + w * (tb.y - ta.y), ta.z + w * (tb.z - ta.z));
+    }
     if (pin) {
         float4 p = pin[i];
-        p.x = tx; p.y = ty; p.z = tz;
+        p.x = t.x; p.y = t.y; p.z = t.z;
         pin[i] = p;
     }
     if (att) {
         float4 a = att[i];
-        a.x = tx; a.y = ty; a.z = tz;
+        a.x = t.x; a.y = t.y; a.z = t.z;
         att[i] = a;
     }
 }
@@ -109,14 +117,17 @@ __global__ void k_gather(int n, int width, const int32_t* __restrict__ idx, cons
 extern "C" {
 
 int xpbd_bone_targets(int32_t n, int32_t n_bones, const float* transforms, const int32_t* vert_bone,
-                      const float* rest4, float* pin_target, float* attach_target, xpbd_stream_t stream) {
+                      const float* vert_w, const float* rest4, float* pin_target, float* attach_target,
+                      xpbd_stream_t stream) {
     if (n < 0 || n_bones <= 0 || !transforms || !vert_bone || !rest4 || (!pin_target && !attach_target))
         return fail(XPBD_ERR_ARG, "xpbd_bone_targets: bad arguments");
-    if (!aligned16(rest4) || !aligned16(pin_target) || !aligned16(attach_target))
+    if (!aligned16(rest4) || !aligned16(pin_target) || !aligned16(attach_target) ||
+        (reinterpret_cast<uintptr_t>(vert_bone) & 7u))
         return fail(XPBD_ERR_ALIGN, "xpbd_bone_targets: [n][4] arrays must be 16-byte aligned");
     if (n == 0) return XPBD_OK;
     k_bone_targets<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
-        n, n_bones, transforms, vert_bone, reinterpret_cast<const float4*>(rest4), reinterpret_cast<float4*>(pin_target),
+        n, n_bones, transforms, reinterpret_cast<const int2*>(vert_bone), vert_w, reinterpret_cast<const float4*>(rest4),
+        reinterpret_cast<float4*>(pin_target),
         reinterpret_cast<float4*>(attach_target));
     return cuda_check("xpbd_bone_targets");
 }

@@ -184,7 +184,8 @@ class Scene:
     bone_axis: np.ndarray        # (NB,3) unit
     bone_half: np.ndarray        # (NB,) half segment length
     bone_radius: np.ndarray      # (NB,)
-    vert_bone: np.ndarray        # (NV,) nearest bone per vertex
+    vert_bone: np.ndarray        # (NV,2) bones at the two ends of the vertex's muscle
+    vert_bw: np.ndarray          # (NV,) blend weight of vert_bone[:,1] (axial coordinate 0..1)
     traj: dict                   # bone trajectory parameters
     aniso_muscle: int
     meta: dict = field(default_factory=dict)
@@ -211,6 +212,19 @@ class Scene:
             out[b, :, :3] = R
             out[b, :, 3] = c + d - R @ c
         return out
+
+    def targets(self, frame: float) -> np.ndarray:
+        """Bone-driven target of every vertex at ``frame`` (float32, the device's
+        operation order): (1-w) (R_a x + t_a) + w (R_b x + t_b)."""
+        T = self.bone_transforms(frame).astype(np.float32)
+        x = self.verts.astype(np.float32)
+        out = []
+        for k in range(2):
+            Tb = T[self.vert_bone[:, k]]
+            out.append(np.stack([((Tb[:, r, 0] * x[:, 0] + Tb[:, r, 1] * x[:, 1]) + Tb[:, r, 2] * x[:, 2]) + Tb[:, r, 3]
+                                 for r in range(3)], 1))
+        w = self.vert_bw.astype(np.float32)[:, None]
+        return (out[0] + w * (out[1] - out[0])).astype(np.float32)
 
     def activation(self, frame: int, start: int = 1, end: int = 50) -> np.ndarray:
         """RampActivationSource (util/activation.py:28-44) on the aniso muscle's tets."""
@@ -314,7 +328,7 @@ def humanv2_scene(seed: int = 0, n_muscles: int = 40, n_bones: int = 20, target_
         if acc >= fascia_tets * 0.95:
             break
     fsel = np.isin(face_part, chosen)
-    fverts, ftets, _ = extrude_shell(mverts, surf[fsel], fascia_thickness)
+    fverts, ftets, fsrc = extrude_shell(mverts, surf[fsel], fascia_thickness)
     nmv = mverts.shape[0]
     allv = np.concatenate([mverts, fverts]).astype(np.float32)
     ftets = orient_tets(allv, ftets + nmv)
@@ -332,9 +346,20 @@ def humanv2_scene(seed: int = 0, n_muscles: int = 40, n_bones: int = 20, target_
         ang = np.deg2rad(rng.normal(0.0, 10.0, sel.shape[0]))
         fib[sel] = np.cos(ang)[:, None] * ax + np.sin(ang)[:, None] * perp
     fib[vert_part < 0] = [1.0, 0.0, 0.0]
-    # nearest bone per vertex (surface distance of the capsule)
-    dist = np.stack([capsule_sdf(allv.astype(np.float64), bc[b], ba[b], bh[b], br[b]) for b in range(n_bones)], 1)
-    vert_bone = dist.argmin(1).astype(np.int32)
+    # two-bone binding: each muscle rides the bones nearest its two axial ends,
+    # blended linearly along the axis (smooth within a muscle); fascia vertices
+    # inherit the binding of the surface vertex they were extruded from
+    end_bone = np.zeros((n_muscles, 2), np.int64)
+    for i in range(n_muscles):
+        ax = rots[i][:, 0]
+        for k, sgn in enumerate((-1.0, 1.0)):
+            e = cents[i] + sgn * ax * L[i] / 2
+            end_bone[i, k] = int(np.argmin([capsule_sdf(e[None], bc[b], ba[b], bh[b], br[b])[0]
+                                            for b in range(n_bones)]))
+    mb = end_bone[vpart]
+    mw = np.clip(xr, 0.0, 1.0)
+    vert_bone = np.concatenate([mb, mb[np.concatenate([fsrc, fsrc])]]).astype(np.int32)
+    vert_bw = np.concatenate([mw, mw[np.concatenate([fsrc, fsrc])]]).astype(np.float32)
     aniso = int(np.argmax(L * R1 * R2))
     traj = dict(rot_axis=rng.normal(size=(n_bones, 3)), rot_amp=np.deg2rad(rng.uniform(10, 25, n_bones)),
                 rot_w=rng.uniform(0.05, 0.12, n_bones), rot_phase=rng.uniform(0, 2 * np.pi, n_bones),
@@ -344,7 +369,7 @@ def humanv2_scene(seed: int = 0, n_muscles: int = 40, n_bones: int = 20, target_
     traj["start_frame"] = 1
     return Scene(verts=allv, tets=alltets, tet_part=tet_part, vert_part=vert_part, v_tendon=v_tendon,
                  v_fiber=fib.astype(np.float32), surface_tris=surf.astype(np.int32), bone_center=bc, bone_axis=ba,
-                 bone_half=bh, bone_radius=br, vert_bone=vert_bone, traj=traj, aniso_muscle=aniso,
+                 bone_half=bh, bone_radius=br, vert_bone=vert_bone, vert_bw=vert_bw, traj=traj, aniso_muscle=aniso,
                  muscle_rot=np.stack(rots), muscle_center=np.stack(cents), muscle_len=L,
                  meta=dict(seed=seed, h=h, n_muscle_verts=nmv, n_muscle_tets=mtets.shape[0],
                            n_fascia_tets=ftets.shape[0], fascia_muscles=chosen))

@@ -19,7 +19,7 @@ import torch
 
 from . import _capi as capi
 from .builder import ConstraintTable, collect_raw_constraints, create_attach_constraints, lumped_mass, tet_rest_data
-from .collision import GridSdfCollider
+from .collision import GridSdfCollider, UdcfDcdCollider, UdcfParams
 from .meshgen import Scene, humanv2_scene
 from .musclesim import MuscleSim
 
@@ -186,6 +186,7 @@ class MultiGridSim(MuscleSim):
                            quasi_static=self.quasi_static, omega=1.0, contraction_ratio=self.contraction_ratio,
                            fiber_stiffness_scale=self.fiber_stiffness_scale, tile_tets=cfg.get("tile_tets"))
         self._setup_kinematics()
+        self.collision_solvers_iter = []
         self.mg = None
         if self.use_multigrid:
             if self.mg_mode != "hpbd":
@@ -193,7 +194,6 @@ class MultiGridSim(MuscleSim):
             from .multigrid import DeviceMultigrid
             self.mg = DeviceMultigrid(self, spacing=float(cfg.get("mg_cage_spacing", 0.016)))
         self.collision_solvers = []
-        self.collision_solvers_iter = []
         coll = (cfg.get("demo") or {}).get("collision") or {}
         if coll.get("enabled", False):
             self.bone_collider = GridSdfCollider(
@@ -201,14 +201,22 @@ class MultiGridSim(MuscleSim):
                 contact_offset=float(coll.get("contact_offset", 0.0)), max_push=float(coll.get("max_push", -1.0)))
             self.bone_collider.transforms = self._bone_tr
             self.collision_solvers.append(self.bone_collider)
+        sc_cfg = (cfg.get("demo") or {}).get("self_collision") or {}
+        if str(sc_cfg.get("method", "none")).lower() == "udcf":
+            prm = UdcfParams(multiplier=float(sc_cfg.get("multiplier", 1.01)),
+                             friction_static=float(sc_cfg.get("friction_static", 0.5)),
+                             friction_dynamic=float(sc_cfg.get("friction_dynamic", 0.4)),
+                             offset=float(sc_cfg.get("offset", 1e-6)), thickness=float(sc_cfg.get("thickness", 0.0)),
+                             max_pairs=int(sc_cfg.get("max_pairs", 1 << 22)),
+                             max_contacts=int(sc_cfg.get("max_contacts", 1 << 20)),
+                             allow_self=bool(sc_cfg.get("allow_self", True)), max_push=float(sc_cfg.get("max_push", 0.0)))
+            self.dcd = UdcfDcdCollider(self, sc.surface_tris, prm)
+            self.collision_solvers_iter.append(self.dcd.solve)
         self._frame_loaded = None
 
     # ----------------------------------------------------------- kinematics
     def _host_targets(self, frame: float) -> np.ndarray:
-        T = self.scene.bone_transforms(frame)
-        b = self.scene.vert_bone
-        x = self.pos0_np.astype(np.float64)
-        return (np.einsum("nij,nj->ni", T[b, :, :3], x) + T[b, :, 3]).astype(np.float32)
+        return self.scene.targets(frame)
 
     def _setup_kinematics(self) -> None:
         L = self.layout
@@ -216,7 +224,8 @@ class MultiGridSim(MuscleSim):
         nb = self.scene.n_bones
         self._bone_tr = torch.zeros((nb, 12), dtype=torch.float32, device=dev)
         self._bone_tr_host = torch.zeros((nb, 12), dtype=torch.float32).pin_memory()
-        self._vert_bone = torch.from_numpy(self.scene.vert_bone[L.perm].astype(np.int32)).to(dev)
+        self._vert_bone = torch.from_numpy(np.ascontiguousarray(self.scene.vert_bone[L.perm], np.int32)).to(dev)
+        self._vert_bw = torch.from_numpy(np.ascontiguousarray(self.scene.vert_bw[L.perm], np.float32)).to(dev)
         r4 = np.zeros((self.NV, 4), np.float32)
         r4[:, :3] = self.pos0_np
         self._rest4 = torch.from_numpy(r4[L.perm]).to(dev)
@@ -244,6 +253,7 @@ class MultiGridSim(MuscleSim):
         v = self._verts
         capi.check(self._lib.xpbd_bone_targets(self.NV, self.scene.n_bones, C.c_void_p(self._bone_tr.data_ptr()),
                                                C.c_void_p(self._vert_bone.data_ptr()),
+                                               C.c_void_p(self._vert_bw.data_ptr()),
                                                C.c_void_p(self._rest4.data_ptr()), v.pin_target, v.attach_target,
                                                self._sp))
 
@@ -334,7 +344,9 @@ class MultiGridSim(MuscleSim):
 
     def _fusable(self) -> bool:
         cs = getattr(self, "collision_solvers", None) or []
-        return (not getattr(self, "collision_solvers_iter", None) and not getattr(self, "constraint_solvers", None)
+        its = getattr(self, "collision_solvers_iter", None) or []
+        dcd = getattr(self, "dcd", None)
+        return (all(dcd is not None and fn == dcd.solve for fn in its) and not getattr(self, "constraint_solvers", None)
                 and all(isinstance(c, GridSdfCollider) for c in cs) and len(cs) <= 1
                 and getattr(self, "program", None) is None)
 
@@ -357,8 +369,10 @@ class MultiGridSim(MuscleSim):
             else:
                 self._vstep(capi.OP_PREDICT | ((push | vel) if sub > 0 else 0))
                 self.mg.vcycle(pin_fine=bool(pin))
-            for _ in range(self.fine_iters):
+            for it in range(self.fine_iters):
                 self._fused_iteration()
+                for fn in self.collision_solvers_iter:
+                    fn(it)
         if push | vel:
             self._vstep(push | vel)
 

@@ -161,8 +161,7 @@ def test_full_size_properties():
         sim.step_frame(frame)
     p = sim.positions_np()
     assert np.isfinite(p).all()
-    tgt, _ = (lambda T: (np.einsum("nij,nj->ni", T[sc.vert_bone, :, :3], sc.verts.astype(np.float64))
-                         + T[sc.vert_bone, :, 3], T))(sc.bone_transforms(3))
+    tgt = sc.targets(3)
     act = sim.pin_active_np != 0
     assert act.sum() > 1000
     # pinned verts end the frame at their targets unless the push-out moved them
@@ -176,3 +175,44 @@ def test_full_size_properties():
         sim._fused_iteration()
     r1 = sim.metrics()["resid_sq_sum"]
     assert r1 <= r0 * 1.0001
+
+
+CFG3 = "rlmusclev2_b200/configs/humanv2_synth_mg_dcd.json"
+
+
+def test_config3_small_vs_oracle():
+    """Multigrid + DCD + SNH fascia on the small scene, three frames."""
+    cfg = load_config(CFG3)
+    cfg["demo"]["collision"]["sdf_res"] = 96
+    sc = humanv2_scene(seed=1, n_muscles=5, n_bones=4, target_tets=20000, fascia_tets=3000, box=(0.35, 0.35, 0.35))
+    sim = MultiGridSim(cfg, scene=sc)
+    o32 = O.OracleMultiGridSim(cfg, sc, prec="f32")
+    o64 = O.OracleMultiGridSim(cfg, sc, prec="f64")
+    for frame in (1, 2, 3):
+        sim.set_fiber_activation(sc.activation(frame))
+        sim.step_frame(frame)
+        o32.step_frame(frame)
+        o64.step_frame(frame)
+        p = sim.positions_np()
+        e64 = np.abs(p - o64.pos).max()
+        spread = np.abs(o32.pos - o64.pos).max()
+        st = sim.dcd.stats()
+        print(f"config3 frame {frame}: |gpu-o64| {e64:.3e} oracle spread {spread:.3e} dcd gpu {st} oracle "
+              f"{o32.dcd_last}")
+        assert np.isfinite(p).all()
+        assert e64 <= max(REF_ATOL, 3.0 * spread)
+        assert st["status"] == 0
+
+
+def test_config3_full_size_runs():
+    cfg = load_config(CFG3)
+    sim = MultiGridSim(cfg)
+    for frame in (1, 2, 3):
+        sim.set_fiber_activation(sim.scene.activation(frame))
+        sim.step_frame(frame)
+    p = sim.positions_np()
+    st = sim.dcd.stats()
+    m = sim.metrics()
+    print(f"config3 full: dcd {st}, metrics {m}, coarse nv {sim.mg.coarse.n_verts}")
+    assert np.isfinite(p).all() and m["n_nonfinite"] == 0
+    assert st["status"] == 0 and st["n_pairs"] > 10000
