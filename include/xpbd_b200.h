@@ -249,19 +249,23 @@ typedef struct XpbdCage {
     const int32_t* r_fine;     /* [nnz] fine vertex */
     const float* r_w;          /* [nnz] prolongation weight of that fine vertex on this coarse vertex */
     const int32_t* blk_ptr;    /* [n_blocks+1] coarse vertices of block b: [blk_ptr[b], blk_ptr[b+1]) */
-    const int32_t* blk_moff;   /* [n_blocks] offset of the block's dim x dim row-major (P^T P)^-1 in minv */
+    const int32_t* blk_moff;   /* [n_blocks] offset of the block's dim x dim row-major (P^T P + lam I)^-1 in minv */
     const float* minv;
     const int32_t* coarse_lib; /* [n_coarse] cage order -> coarse library order */
     const int32_t* p_idx;      /* [n_fine][4] coarse library ids of the embedding tet, -1 = not embedded */
     const float* p_w;          /* [n_fine][4] barycentric weights (1-u-v-w, u, v, w) */
+    float* resid;              /* [n_fine][4] scratch: fine residual x_f - P x_c(prior) */
 } XpbdCage;
 
-/* Galerkin restriction x_c = (P^T P)^-1 P^T x_f of the xyz lanes of fine4
- * into coarse4 (restrict_galerkin_scatter_kernel + block_solve_kernel,
- * mg/kernel.py:137-178).  Optional: coarse_prev4 receives the same values
- * (the q_j snapshot, mg/mg.py:1077), and where coarse_pin4[c].w != 0 the
- * coarse position is overwritten by coarse_pin4[c].xyz (the coarse kinematic
- * pin, mg/mg.py:1013-1026).  One CTA per block, no atomics. */
+/* Regularised Galerkin restriction of the xyz lanes of fine4 into coarse4:
+ * x_c = argmin |P x_c - x_f|^2 + lam |x_c - prior|^2 with prior = the current
+ * contents of coarse4, computed as prior + (P^T P + lam I)^-1 P^T (x_f - P prior)
+ * (restrict_galerkin_scatter_kernel + block_solve_kernel, mg/kernel.py:137-178,
+ * with lam -> 0 the reference's operator).  Optional: coarse_prev4 receives
+ * the same values (the q_j snapshot, mg/mg.py:1077), and where
+ * coarse_pin4[c].w != 0 the coarse position is then overwritten by
+ * coarse_pin4[c].xyz (the coarse kinematic pin, mg/mg.py:1013-1026).  One
+ * CTA per block for the solve, no atomics. */
 int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, float* coarse_prev4,
                      const float* coarse_pin4, xpbd_stream_t stream);
 

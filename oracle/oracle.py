@@ -423,7 +423,8 @@ class OracleMultiGridSim(OracleSolver):
         self.mg_blocks = [(int(cage.blk_base[s0]), int(cage.blk_dim[s0]),
                            cage.minv_flat[cage.blk_matoff[s0]:cage.blk_matoff[s0] + cage.blk_dim[s0] ** 2]
                            .astype(P.dt).reshape(cage.blk_dim[s0], cage.blk_dim[s0])) for s0 in starts]
-        q0 = self.restrict(self.scene.verts.astype(P.dt)).astype(np.float32)
+        q0 = self.restrict(self.scene.verts.astype(P.dt), cage.coarse_pos.astype(P.dt)).astype(np.float32)
+        self.mg_target = q0.astype(P.dt).copy()
         r = q0[cage.coarse_tet].astype(np.float64)  # _rest_B_p3ref (mg.py:43-53)
         Dm = np.stack([r[:, 0] - r[:, 3], r[:, 1] - r[:, 3], r[:, 2] - r[:, 3]], axis=-1)
         B = np.linalg.inv(Dm).astype(np.float32)
@@ -448,25 +449,31 @@ class OracleMultiGridSim(OracleSolver):
                                prec=P.name)
         self.mg_iters = int(cfg.get("mg_coarse_iters", 15))
 
-    def restrict(self, x):
-        """restrict_galerkin_scatter_kernel + block_solve_kernel (serial scatter in fine order)."""
+    def restrict(self, x, prior):
+        """Regularised Galerkin restriction prior + Minv P^T (x - P prior)
+        (restrict_galerkin_scatter_kernel + block_solve_kernel with the prior
+        term; serial scatter in fine order)."""
         P = self.P
         nc = self.cage.coarse_pos.shape[0]
-        b = np.zeros((nc, 3), P.dt)
+        prior = prior.astype(P.dt)
+        w, t = self.mg_w, self.mg_t
         xe = x[self.mg_emb].astype(P.dt)
+        r = xe - (((w[:, 0:1] * prior[t[:, 0]] + w[:, 1:2] * prior[t[:, 1]]) + w[:, 2:3] * prior[t[:, 2]])
+                  + w[:, 3:4] * prior[t[:, 3]])
+        b = np.zeros((nc, 3), P.dt)
         for k in range(4):
-            np.add.at(b, self.mg_t[:, k], self.mg_w[:, k:k + 1] * xe)
+            np.add.at(b, t[:, k], w[:, k:k + 1] * r)
         out = np.zeros_like(b)
         for base, dim, M in self.mg_blocks:
             out[base:base + dim] = M @ b[base:base + dim]
-        return out
+        return prior + out
 
     def vcycle(self):
         """_hpbd_vcycle (mg.py:1064-1079) with beta = 0 (no coarse soft attach)."""
         co = self.mg
-        co.pos[:] = self.restrict(self.pos)
+        co.pos[:] = self.restrict(self.pos, co.pos)
         prev = co.pos.copy()
-        tgt = self.restrict(self.target)
+        tgt = self.mg_target
         co.pos[self.mg_pin] = tgt[self.mg_pin]
         for _ in range(self.mg_iters):
             co.project()
@@ -517,6 +524,9 @@ class OracleMultiGridSim(OracleSolver):
             self.c_rv[self.attach_rows, :3] = self.target[self.c_pts[self.attach_rows, 0]]
         if self.scene.tet_part is not None and hasattr(self.scene, "activation"):
             self.activation[:] = self.scene.activation(frame)
+        if self.mg is not None:
+            # coarse Dirichlet targets, restricted once per target change (mg.py:1028-1045)
+            self.mg_target = self.restrict(self.target, self.mg_target)
         self.apply_pins()
         if self.coll:
             r = self.sdf_res

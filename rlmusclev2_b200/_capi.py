@@ -70,7 +70,7 @@ class XpbdCage(C.Structure):
     _fields_ = [("n_fine", C.c_int32), ("n_coarse", C.c_int32), ("n_blocks", C.c_int32), ("max_block", C.c_int32),
                 ("r_ptr", C.c_void_p), ("r_fine", C.c_void_p), ("r_w", C.c_void_p), ("blk_ptr", C.c_void_p),
                 ("blk_moff", C.c_void_p), ("minv", C.c_void_p), ("coarse_lib", C.c_void_p), ("p_idx", C.c_void_p),
-                ("p_w", C.c_void_p)]
+                ("p_w", C.c_void_p), ("resid", C.c_void_p)]
 
 
 class XpbdDcd(C.Structure):

@@ -67,18 +67,19 @@ def tet_rest_data(pos0: np.ndarray, tets: np.ndarray):
 
     builder.py:28-43 (_batch_compute_tet_rest_matrices): Dm columns are
     p_k - p_3 of the float32 rest positions; V0 = det(Dm)/6 (signed);
-    valid = |det| > 1e-30; B = inv(Dm) for valid tets.  Evaluated in float64
-    and rounded to float32.
+    valid = |det| > 1e-30; B = inv(Dm) for valid tets.  As numpy does for
+    the reference's float32 arrays: det and inv evaluated in float64 and
+    rounded to float32, then V0 = det / 6 in float32.
     """
-    tp = pos0[tets]                                         # float32 (NT,4,3)
+    tp = np.asarray(pos0, np.float32)[tets]                 # float32 (NT,4,3)
     cols = (tp[:, :3, :] - tp[:, 3:4, :]).astype(np.float64)  # differences in float32, like the reference
     M = np.transpose(cols, (0, 2, 1))
-    det = np.linalg.det(M)
+    det = np.linalg.det(M).astype(np.float32)
     valid = np.abs(det) > 1e-30
     B = np.zeros_like(M)
     if valid.any():
         B[valid] = np.linalg.inv(M[valid])
-    return B.astype(np.float32), (det / 6.0).astype(np.float32), valid
+    return B.astype(np.float32), (det / np.float32(6.0)).astype(np.float32), valid
 
 
 def lumped_mass(pos0: np.ndarray, tets: np.ndarray, density: float) -> tuple[np.ndarray, np.ndarray]:

@@ -69,7 +69,11 @@ __device__ __forceinline__ void finish_vertex(const XpbdParams& prm, const XpbdV
 }
 
 // ---------------------------------------------------------------------------
-template <int MODE, bool DAMP, int MINB>
+// Constraint sets compiled into a tile-pass instance: the heavier sets cost
+// registers (and occupancy) even for tets that do not use them.
+enum { CSET_LIGHT = 0, CSET_VOL = 1, CSET_FULL = 2 };  // ARAP+aniso | +volume | +volume+SNH
+
+template <int MODE, bool DAMP, int MINB, int CSET>
 __global__ void __launch_bounds__(kTileThreads, MINB)
     k_project_tiles(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdTiles T,
                     const __grid_constant__ XpbdVerts V, uint32_t finish_ops) {
@@ -127,27 +131,25 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
         // All constraints of the tet read the same positions (Jacobi), so their
         // deltas are summed in registers and pushed with one set of shared
         // atomics; each active constraint adds 1 to dPw of all four vertices.
-        Corr4 c;
         float3 d[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) d[i] = make_float3(0.f, 0.f, 0.f);
         float nact = 0.f;
-        auto add = [&](const Corr4& cc) {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) d[i] = d[i] + cc.d[i];
-            nact += 1.f;
-        };
         const uint32_t fl = m.flags;
         // Same type order as the reference table (ascending ConstraintType tag).
-        if ((fl & XPBD_MAT_SNH) && con_snh(p, pq, B, F, V0, m.snh_mu, m.snh_lam, m.snh_damp, prm.dt, c)) add(c);
-        if ((fl & XPBD_MAT_VOLUME) && con_volume(p, pq, V0, m.vol_k, m.vol_damp, prm.dt, c)) add(c);
+        if (CSET >= CSET_FULL && (fl & XPBD_MAT_SNH) &&
+            con_snh(p, pq, B, F, V0, m.snh_mu, m.snh_lam, m.snh_damp, prm.dt, d))
+            nact += 1.f;
+        if (CSET >= CSET_VOL && (fl & XPBD_MAT_VOLUME) && con_volume(p, pq, V0, m.vol_k, m.vol_damp, prm.dt, d))
+            nact += 1.f;
         if (fl & XPBD_MAT_ANISO) {
             const float4 fb = reinterpret_cast<const float4*>(T.tet_fiber)[t];
             if (con_aniso(p, B, F, f3(fb), fb.w, T.tet_act[t], m.aniso_k, prm.contraction_ratio,
-                          prm.fiber_stiffness_scale, prm.dt, c))
-                add(c);
+                          prm.fiber_stiffness_scale, prm.dt, d))
+                nact += 1.f;
         }
-        if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, m.arap_k, prm.dt, c, (prm.tile_variant & 2) != 0)) add(c);
+        if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, m.arap_k, prm.dt, d, (prm.tile_variant & 2) != 0))
+            nact += 1.f;
         if (nact != 0.f) {
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
@@ -445,7 +447,7 @@ bool any_aniso(const XpbdParams* p) {
     return false;
 }
 
-template <int MODE, bool DAMP, int MINB>
+template <int MODE, bool DAMP, int MINB, int CSET>
 int launch_project_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
     const size_t smem = size_t(T->max_tile_verts) * sizeof(float4) * (DAMP ? 3 : 2);  // pos, [prev], 4 x float acc
     if (smem > 48 * 1024) {
@@ -453,19 +455,37 @@ int launch_project_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts*
         int dev = 0;
         cudaGetDevice(&dev);
         if (dev < 0 || dev >= 64 || !done[dev]) {
-            cudaFuncSetAttribute(k_project_tiles<MODE, DAMP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_project_tiles<MODE, DAMP, MINB, CSET>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(XPBD_MAX_TILE_VERTS * sizeof(float4) * 3));
             if (dev >= 0 && dev < 64) done[dev] = 1;
         }
     }
-    k_project_tiles<MODE, DAMP, MINB><<<T->n_tiles, kTileThreads, smem, s>>>(*prm, *T, *V, fops);
+    k_project_tiles<MODE, DAMP, MINB, CSET><<<T->n_tiles, kTileThreads, smem, s>>>(*prm, *T, *V, fops);
     return cuda_check("xpbd_project");
 }
 
+uint32_t material_union(const XpbdParams* p) {
+    uint32_t u = 0;
+    for (int i = 0; i < p->n_materials; ++i) u |= p->materials[i].flags;
+    return u;
+}
+
+// Instance choice: the smallest constraint set covering the materials; the
+// light set runs 3 CTAs per SM (80 registers, no spills), the others 2
+// (bit 0 of tile_variant flips that choice).
 template <int MODE, bool DAMP>
 int launch_project(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
-    if (prm->tile_variant & 1) return launch_project_v<MODE, DAMP, 3>(prm, T, V, fops, s);
-    return launch_project_v<MODE, DAMP, 2>(prm, T, V, fops, s);
+    const uint32_t u = material_union(prm);
+    const bool flip = (prm->tile_variant & 1) != 0;
+    if (u & XPBD_MAT_SNH)
+        return flip ? launch_project_v<MODE, DAMP, 3, CSET_FULL>(prm, T, V, fops, s)
+                    : launch_project_v<MODE, DAMP, 2, CSET_FULL>(prm, T, V, fops, s);
+    if (u & XPBD_MAT_VOLUME)
+        return flip ? launch_project_v<MODE, DAMP, 3, CSET_VOL>(prm, T, V, fops, s)
+                    : launch_project_v<MODE, DAMP, 2, CSET_VOL>(prm, T, V, fops, s);
+    if (DAMP) return launch_project_v<MODE, DAMP, 2, CSET_VOL>(prm, T, V, fops, s);  // damping needs a volume/SNH term
+    return flip ? launch_project_v<MODE, false, 2, CSET_LIGHT>(prm, T, V, fops, s)
+                : launch_project_v<MODE, false, 3, CSET_LIGHT>(prm, T, V, fops, s);
 }
 
 }  // namespace

@@ -160,10 +160,6 @@ enum : uint32_t {
     MAT_DAMPED = 1u << 4,  // some constraint of this material reads pprev
 };
 
-struct Corr4 {
-    float3 d[4];
-};
-
 // Rotation factor R of F = R S for det F > 0, by Higham's scaled Newton
 // iteration X <- (g X + (g X)^-T) / 2, g = |det X|^(-1/3) (N. J. Higham,
 // "Computing the polar decomposition with applications", SIAM J. Sci. Stat.
@@ -208,7 +204,7 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
 // C = ||s - 1|| = ||F - U V^T||_F and dC/dF = U diag((s-1)/C) V^T = (F - U V^T)/C,
 // U V^T being the rotation nearest F.  For det F > 0 that rotation is the polar
 // factor, obtained without the SVD; inverted or degenerate tets use the SVD.
-__device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float k, float dt, Corr4& out,
+__device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float k, float dt, float3 (&acc)[4],
                                             bool force_svd = false) {
     M3 G;
     M3 R;
@@ -254,13 +250,13 @@ __device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, cons
     const float at = alpha / (dt * dt);
     const float dL = -C / (wsum + at);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) out.d[i] = (dL * p[i].w) * g[i];
+    for (int i = 0; i < 4; ++i) acc[i] = acc[i] + (dL * p[i].w) * g[i];
     return true;
 }
 
 // solve_tetvolume_kernel + tet_volume_update_xpbd_fn, solve_kernels.py:553-585, 187-281.
 __device__ __forceinline__ bool con_volume(const float4 p[4], const float4* q, float V0, float k, float kd, float dt,
-                                           Corr4& out) {
+                                           float3 (&acc)[4]) {
     const float3 p3 = f3(p[3]);
     const float3 d0 = f3(p[0]) - p3, d1 = f3(p[1]) - p3, d2 = f3(p[2]) - p3;
     float3 g[4];
@@ -285,7 +281,7 @@ __device__ __forceinline__ bool con_volume(const float4 p[4], const float4* q, f
     }
     const float dl = (-C - dsum) / (gamma * ws + alpha);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) out.d[i] = (dl * p[i].w) * g[i];
+    for (int i = 0; i < 4; ++i) acc[i] = acc[i] + (dl * p[i].w) * g[i];
     return true;
 }
 
@@ -293,7 +289,7 @@ __device__ __forceinline__ bool con_volume(const float4 p[4], const float4* q, f
 // normalised mean fiber direction of the tet's 4 vertices (static, built at
 // upload); a zero f0 marks a tet whose mean fiber vanished (fn < 1e-9).
 __device__ __forceinline__ bool con_aniso(const float4 p[4], const M3& B, const M3& F, float3 f0, float tendon,
-                                          float act, float k, float ratio, float kscale, float dt, Corr4& out) {
+                                          float act, float k, float ratio, float kscale, float dt, float3 (&acc)[4]) {
     const float3 d = make_float3(F.m[0][0] * f0.x + F.m[0][1] * f0.y + F.m[0][2] * f0.z,
                                  F.m[1][0] * f0.x + F.m[1][1] * f0.y + F.m[1][2] * f0.z,
                                  F.m[2][0] * f0.x + F.m[2][1] * f0.y + F.m[2][2] * f0.z);
@@ -323,13 +319,13 @@ __device__ __forceinline__ bool con_aniso(const float4 p[4], const M3& B, const 
     const float at = (1.f / sv) / (dt * dt);
     const float dL = -C / (wsum + at);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) out.d[i] = (dL * p[i].w) * g[i];
+    for (int i = 0; i < 4; ++i) acc[i] = acc[i] + (dL * p[i].w) * g[i];
     return true;
 }
 
 // solve_tetsnh_kernel + tet_snh_update_xpbd_fn, solve_kernels.py:1587-1617, 1429-1584.
 __device__ __forceinline__ bool con_snh(const float4 p[4], const float4* q, const M3& B, const M3& F, float V0,
-                                        float mu, float lam, float kd, float dt, Corr4& out) {
+                                        float mu, float lam, float kd, float dt, float3 (&acc)[4]) {
     float Ic = 0.f;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -398,7 +394,7 @@ __device__ __forceinline__ bool con_snh(const float4 p[4], const float4* q, cons
     const float ddL = invd * (Ayy * db - dh * hb);
     const float hdL = invd * (Axx * hb - dh * db);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) out.d[i] = p[i].w * (ddL * dg[i] + hdL * hg[i]);
+    for (int i = 0; i < 4; ++i) acc[i] = acc[i] + p[i].w * (ddL * dg[i] + hdL * hg[i]);
     return true;
 }
 

@@ -10,22 +10,40 @@ namespace {
 
 constexpr int kMgThreads = 256;
 
-// One CTA per Galerkin block: b_j = sum_e w_e x_f[e] for the block's coarse
-// vertices (CSR gather into shared memory), then each warp computes rows
-// x_c[r] = sum_j Minv[r][j] b_j with lanes striding j (coalesced rows).
+// Fine residual r = x_f - P prior for every embedded fine vertex.
 __global__ void __launch_bounds__(kMgThreads)
-    k_mg_restrict(const __grid_constant__ XpbdCage G, const float4* __restrict__ fine, float4* coarse, float4* prev,
-                  const float4* __restrict__ pin) {
+    k_mg_residual(const __grid_constant__ XpbdCage G, const float4* __restrict__ fine,
+                  const float4* __restrict__ coarse) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G.n_fine) return;
+    const int4 id = reinterpret_cast<const int4*>(G.p_idx)[i];
+    if (id.x < 0) return;
+    const float4 w = reinterpret_cast<const float4*>(G.p_w)[i];
+    const float4 a = coarse[id.x], b = coarse[id.y], c = coarse[id.z], d = coarse[id.w];
+    const float4 x = fine[i];
+    reinterpret_cast<float4*>(G.resid)[i] =
+        make_float4(x.x - (((w.x * a.x + w.y * b.x) + w.z * c.x) + w.w * d.x),
+                    x.y - (((w.x * a.y + w.y * b.y) + w.z * c.y) + w.w * d.y),
+                    x.z - (((w.x * a.z + w.y * b.z) + w.z * c.z) + w.w * d.z), 0.f);
+}
+
+// One CTA per Galerkin block: b_j = sum_e w_e r[e] for the block's coarse
+// vertices (CSR gather into shared memory), then each warp computes rows
+// delta[r] = sum_j Minv[r][j] b_j with lanes striding j (coalesced rows) and
+// the new coarse position prior + delta.
+__global__ void __launch_bounds__(kMgThreads)
+    k_mg_restrict(const __grid_constant__ XpbdCage G, float4* coarse, float4* prev, const float4* __restrict__ pin) {
     extern __shared__ float4 sb[];
     const int blk = blockIdx.x;
     const int c0 = G.blk_ptr[blk];
     const int dim = G.blk_ptr[blk + 1] - c0;
+    const float4* res = reinterpret_cast<const float4*>(G.resid);
     for (int j = threadIdx.x; j < dim; j += blockDim.x) {
         const int c = c0 + j;
         float3 acc = make_float3(0.f, 0.f, 0.f);
         for (int e = G.r_ptr[c]; e < G.r_ptr[c + 1]; ++e) {
             const float w = G.r_w[e];
-            const float4 x = fine[G.r_fine[e]];
+            const float4 x = res[G.r_fine[e]];
             acc.x += w * x.x;
             acc.y += w * x.y;
             acc.z += w * x.z;
@@ -53,10 +71,10 @@ __global__ void __launch_bounds__(kMgThreads)
         if (lane == 0) {
             const int cl = G.coarse_lib[c0 + r];
             float4 p = coarse[cl];
-            p.x = ax;
-            p.y = ay;
-            p.z = az;
-            if (prev) prev[cl] = make_float4(ax, ay, az, 0.f);
+            p.x += ax;
+            p.y += ay;
+            p.z += az;
+            if (prev) prev[cl] = make_float4(p.x, p.y, p.z, 0.f);
             if (pin) {
                 const float4 t = pin[cl];
                 if (t.w != 0.f) {
@@ -102,10 +120,11 @@ __global__ void __launch_bounds__(kMgThreads)
 
 int check_cage(const XpbdCage* g) {
     if (!g || g->n_fine <= 0 || g->n_coarse <= 0 || g->n_blocks <= 0 || !g->r_ptr || !g->r_fine || !g->r_w ||
-        !g->blk_ptr || !g->blk_moff || !g->minv || !g->coarse_lib || !g->p_idx || !g->p_w)
+        !g->blk_ptr || !g->blk_moff || !g->minv || !g->coarse_lib || !g->p_idx || !g->p_w || !g->resid)
         return fail(XPBD_ERR_ARG, "XpbdCage: null member or empty size");
     if (g->max_block <= 0 || g->max_block > 8192) return fail(XPBD_ERR_LIMIT, "XpbdCage: max_block must be in 1..8192");
-    if (!aligned16(g->p_idx) || !aligned16(g->p_w)) return fail(XPBD_ERR_ALIGN, "XpbdCage: p_idx/p_w alignment");
+    if (!aligned16(g->p_idx) || !aligned16(g->p_w) || !aligned16(g->resid))
+        return fail(XPBD_ERR_ALIGN, "XpbdCage: p_idx/p_w/resid alignment");
     return XPBD_OK;
 }
 
@@ -123,9 +142,11 @@ int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, f
     const size_t smem = size_t(cage->max_block) * sizeof(float4);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_mg_restrict, cudaFuncAttributeMaxDynamicSharedMemorySize, int(8192 * sizeof(float4)));
+    k_mg_residual<<<(cage->n_fine + kMgThreads - 1) / kMgThreads, kMgThreads, 0, (cudaStream_t)stream>>>(
+        *cage, reinterpret_cast<const float4*>(fine4), reinterpret_cast<const float4*>(coarse4));
     k_mg_restrict<<<cage->n_blocks, kMgThreads, smem, (cudaStream_t)stream>>>(
-        *cage, reinterpret_cast<const float4*>(fine4), reinterpret_cast<float4*>(coarse4),
-        reinterpret_cast<float4*>(coarse_prev4), reinterpret_cast<const float4*>(coarse_pin4));
+        *cage, reinterpret_cast<float4*>(coarse4), reinterpret_cast<float4*>(coarse_prev4),
+        reinterpret_cast<const float4*>(coarse_pin4));
     return cuda_check("xpbd_mg_restrict");
 }
 

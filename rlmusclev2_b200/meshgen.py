@@ -29,6 +29,25 @@ def hex_to_tets(corner_index) -> np.ndarray:
     return np.concatenate(out, axis=0)
 
 
+def fix_tet_winding(vertices: np.ndarray, tets: np.ndarray) -> np.ndarray:
+    """The reference loader's winding rule (util/mesh_utils.py:16-32): swap
+    pts[0] and pts[1] where (p1-p0) x (p2-p0) . (p3-p0) < 0.  Meshes loaded
+    by the reference pass through it, so their pt3-referenced rest volumes
+    det[p0-p3, p1-p3, p2-p3]/6 come out negative."""
+    t = np.array(tets, copy=True)
+    p0, p1, p2, p3 = (vertices[t[:, k]] for k in range(4))
+    bad = np.einsum("ij,ij->i", np.cross(p1 - p0, p2 - p0), p3 - p0) < 0.0
+    t[bad, 0], t[bad, 1] = tets[bad, 1], tets[bad, 0]
+    return t
+
+
+def ramp_activation(mask: np.ndarray, frame: int, start: int, end: int) -> np.ndarray:
+    """RampActivationSource.per_tet (util/activation.py:28-44):
+    clamp((frame - start) / max(1, end - start), 0, 1) * mask."""
+    a = min(1.0, max(0.0, (int(frame) - int(start)) / max(1, int(end) - int(start))))
+    return (a * np.asarray(mask, np.float32)).astype(np.float32)
+
+
 def orient_tets(pos: np.ndarray, tets: np.ndarray) -> np.ndarray:
     """Swap pts[0], pts[1] where det[p0-p3, p1-p3, p2-p3] < 0 so every tet is
     positively oriented with the pt3 reference vertex."""
@@ -149,9 +168,14 @@ def orient_faces_outward(pos: np.ndarray, faces: np.ndarray, opp: np.ndarray) ->
     return out
 
 
-def extrude_shell(pos: np.ndarray, faces: np.ndarray, thickness: float):
+def extrude_shell(pos: np.ndarray, faces: np.ndarray, thickness: float, min_quality: float = 0.25):
     """Prism shell outward of a closed surface: new inner and outer vertex
-    layers, 3 tets per prism with the vertex-id diagonal rule (conforming)."""
+    layers, 3 tets per prism with the vertex-id diagonal rule (conforming).
+    Prisms whose worst tet has a quality V / l_max^3 below ``min_quality`` x
+    the shell's median (slivers at the staircase folds of a lattice surface,
+    where the averaged vertex normal lies almost in a face's plane) are left
+    out.  Returns the shell vertices, its tets and, per shell vertex, the
+    surface vertex it comes from."""
     sv, inv = np.unique(faces, return_inverse=True)
     tri = inv.reshape(-1, 3)
     p = pos[sv]
@@ -168,7 +192,15 @@ def extrude_shell(pos: np.ndarray, faces: np.ndarray, thickness: float):
     a1, b1, c1 = a0 + n, b0 + n, c0 + n
     tets = np.concatenate([np.stack([a0, b0, c0, c1], 1), np.stack([a0, b0, b1, c1], 1),
                            np.stack([a0, a1, b1, c1], 1)])
-    return verts, tets, sv
+    x = verts.astype(np.float64)
+    e = [x[tets[:, j]] - x[tets[:, i]] for i, j in ((0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3))]
+    vol = np.abs(np.einsum("ij,ij->i", np.cross(e[0], e[1]), e[2])) / 6.0
+    q = vol / np.max([np.linalg.norm(v, axis=1) for v in e], axis=0) ** 3
+    nf = tri.shape[0]
+    qp = q.reshape(3, nf).min(0)
+    keep = np.tile(qp >= min_quality * np.median(q), 3)
+    used, tets = np.unique(tets[keep], return_inverse=True)
+    return verts[used], tets.reshape(-1, 4), np.concatenate([sv, sv])[used]
 
 
 @dataclass
@@ -228,8 +260,7 @@ class Scene:
 
     def activation(self, frame: int, start: int = 1, end: int = 50) -> np.ndarray:
         """RampActivationSource (util/activation.py:28-44) on the aniso muscle's tets."""
-        a = min(1.0, max(0.0, (int(frame) - start) / max(1, end - start)))
-        return (a * (self.tet_part == self.aniso_muscle)).astype(np.float32)
+        return ramp_activation(self.tet_part == self.aniso_muscle, frame, start, end)
 
 
 def capsule_sdf(x: np.ndarray, c: np.ndarray, axis: np.ndarray, half: float, r: float) -> np.ndarray:
@@ -239,14 +270,15 @@ def capsule_sdf(x: np.ndarray, c: np.ndarray, axis: np.ndarray, half: float, r: 
 
 
 def humanv2_scene(seed: int = 0, n_muscles: int = 40, n_bones: int = 20, target_tets: int = 468_000,
-                  fascia_tets: int = 67_000, fascia_thickness: float = 0.0015, tendon_frac: float = 0.05,
+                  fascia_tets: int = 70_000, fascia_thickness: float = 0.0015, tendon_frac: float = 0.05,
                   box=(0.7, 0.9, 0.7)) -> Scene:
     """Synthetic humanV2-scale muscle scene (~172.7k verts / ~535k tets at the
     defaults): ``n_muscles`` ellipsoids with length U(80,300) mm and radii
     U(10,40) mm, clipped 6-tet hex lattices, a ``fascia_thickness`` extruded
     shell over the first muscles' surfaces up to ``fascia_tets`` tets, and
     ``n_bones`` capsules (radius U(8,20) mm, length U(150,400) mm) on smooth
-    rigid trajectories of at most 5 deg and 10 mm per frame."""
+    rigid trajectories (rotation amplitude U(2.5,6.25) deg, translation
+    amplitude U(5,20) mm)."""
     rng = np.random.default_rng(seed)
     box = np.asarray(box)
     L = rng.uniform(0.080, 0.300, n_muscles)
@@ -358,12 +390,14 @@ def humanv2_scene(seed: int = 0, n_muscles: int = 40, n_bones: int = 20, target_
                                             for b in range(n_bones)]))
     mb = end_bone[vpart]
     mw = np.clip(xr, 0.0, 1.0)
-    vert_bone = np.concatenate([mb, mb[np.concatenate([fsrc, fsrc])]]).astype(np.int32)
-    vert_bw = np.concatenate([mw, mw[np.concatenate([fsrc, fsrc])]]).astype(np.float32)
+    vert_bone = np.concatenate([mb, mb[fsrc]]).astype(np.int32)
+    vert_bw = np.concatenate([mw, mw[fsrc]]).astype(np.float32)
     aniso = int(np.argmax(L * R1 * R2))
-    traj = dict(rot_axis=rng.normal(size=(n_bones, 3)), rot_amp=np.deg2rad(rng.uniform(10, 25, n_bones)),
+    # amplitudes that keep the bone-driven target field of every muscle
+    # within stretches of 0.70..1.37 over frames 1-50 at the default scene
+    traj = dict(rot_axis=rng.normal(size=(n_bones, 3)), rot_amp=np.deg2rad(rng.uniform(2.5, 6.25, n_bones)),
                 rot_w=rng.uniform(0.05, 0.12, n_bones), rot_phase=rng.uniform(0, 2 * np.pi, n_bones),
-                tr_dir=rng.normal(size=(n_bones, 3)), tr_amp=rng.uniform(0.01, 0.04, n_bones),
+                tr_dir=rng.normal(size=(n_bones, 3)), tr_amp=rng.uniform(0.005, 0.02, n_bones),
                 tr_w=rng.uniform(0.05, 0.12, n_bones), tr_phase=rng.uniform(0, 2 * np.pi, n_bones))
     traj["tr_dir"] /= np.linalg.norm(traj["tr_dir"], axis=1, keepdims=True)
     traj["start_frame"] = 1
@@ -396,6 +430,7 @@ class Cage:
     blk_dim: np.ndarray
     blk_matoff: np.ndarray
     mg_fine_nv: int
+    lam: float = 0.0          # Tikhonov weight of the prior in the restriction
 
 
 def _bary(p, a, b, c, d):
@@ -404,7 +439,7 @@ def _bary(p, a, b, c, d):
     return np.concatenate([(1.0 - w.sum(-1))[..., None], w], -1)
 
 
-def build_cage(scene: "Scene", spacing: float = 0.016) -> Cage:
+def build_cage(scene: "Scene", spacing: float = 0.016, rel_lam: float = 1e-3) -> Cage:
     """Coarse cage: for every muscle a ``spacing`` hex lattice in the muscle's
     local frame over the cells that hold its fine vertices; fascia vertices are
     not embedded."""
@@ -460,7 +495,7 @@ def build_cage(scene: "Scene", spacing: float = 0.016) -> Cage:
         Pm = np.zeros((sel.shape[0], n))
         rows = np.repeat(np.arange(sel.shape[0]), 4)
         np.add.at(Pm, (rows, tl[best_t].reshape(-1)), best_w.reshape(-1))
-        blocks.append(np.linalg.pinv(Pm.T @ Pm, rcond=1e-8))  # cutoff of tools/gen_coarse_cage.py:221
+        blocks.append(Pm.T @ Pm)
         cpos_all.append(cw)
         ctet_all.append(tl + voff)
         voff += n
@@ -478,6 +513,13 @@ def build_cage(scene: "Scene", spacing: float = 0.016) -> Cage:
     w0_old = 1.0 - uvw[sw].sum(1)
     uvw[sw, 0] = w0_old
     del u_old
+    # Restriction x_c = argmin |P x_c - x_f|^2 + lam |x_c - prior|^2: the
+    # Galerkin least squares of the reference (pinv(P^T P), mg.py:770-800) with
+    # a small Tikhonov weight toward the previous coarse state, so that cage
+    # corners carrying almost no fine weight stay where they were instead of
+    # amplifying FP32 noise (lam = rel_lam x median diagonal of P^T P).
+    lam = rel_lam * float(np.median(np.concatenate([np.diag(B) for B in blocks])))
+    blocks = [np.linalg.inv(B + lam * np.eye(B.shape[0])) for B in blocks]
     blk_base, blk_dim, blk_matoff, flat = [], [], [], []
     off = base = 0
     for B in blocks:
@@ -491,4 +533,4 @@ def build_cage(scene: "Scene", spacing: float = 0.016) -> Cage:
     return Cage(coarse_pos=coarse_pos, coarse_tet=coarse_tet, cage_idx=cage_idx.astype(np.int32),
                 uvw=uvw.astype(np.float32), minv_flat=np.concatenate(flat).astype(np.float32),
                 blk_base=np.asarray(blk_base, np.int32), blk_dim=np.asarray(blk_dim, np.int32),
-                blk_matoff=np.asarray(blk_matoff, np.int32), mg_fine_nv=nv)
+                blk_matoff=np.asarray(blk_matoff, np.int32), mg_fine_nv=nv, lam=lam)

@@ -21,21 +21,24 @@ from .engine import XpbdSolver
 from .meshgen import Cage, build_cage
 
 
-def _restrict_host(cage: Cage, x: np.ndarray) -> np.ndarray:
-    """Host Galerkin restriction (setup only): b = P^T x, x_c = Minv_block b."""
+def _restrict_host(cage: Cage, x: np.ndarray, prior: np.ndarray) -> np.ndarray:
+    """Host regularised Galerkin restriction (setup only):
+    prior + Minv P^T (x - P prior)."""
     emb = cage.cage_idx >= 0
     t = cage.coarse_tet[cage.cage_idx[emb]]
     w = np.concatenate([(1.0 - cage.uvw[emb].astype(np.float64).sum(1))[:, None], cage.uvw[emb]], 1)
+    prior = prior.astype(np.float64)
+    r = x[emb].astype(np.float64) - sum(w[:, k:k + 1] * prior[t[:, k]] for k in range(4))
     b = np.zeros((cage.coarse_pos.shape[0], 3))
     for k in range(4):
-        np.add.at(b, t[:, k], w[:, k:k + 1] * x[emb].astype(np.float64))
+        np.add.at(b, t[:, k], w[:, k:k + 1] * r)
     out = np.zeros_like(b)
     starts = np.nonzero(np.r_[True, np.diff(cage.blk_base) != 0])[0]
     for s0 in starts:
         base, dim, off = cage.blk_base[s0], cage.blk_dim[s0], cage.blk_matoff[s0]
         M = cage.minv_flat[off:off + dim * dim].astype(np.float64).reshape(dim, dim)
         out[base:base + dim] = M @ b[base:base + dim]
-    return out
+    return prior + out
 
 
 def node_mass_redistribute(pos, tet, total_mass) -> np.ndarray:
@@ -60,7 +63,7 @@ class DeviceMultigrid:
         self.cage = cage
         ncoarse = cage.coarse_pos.shape[0]
         # FAS rest of the coarse ARAP = restriction of the fine rest (mg.py:813-829)
-        q0 = _restrict_host(cage, sim.pos0_np).astype(np.float32)
+        q0 = _restrict_host(cage, sim.pos0_np, cage.coarse_pos).astype(np.float32)
         self.q0 = q0
         mass = node_mass_redistribute(cage.coarse_pos, cage.coarse_tet, sim.total_mass)
         # coarse Dirichlet pins restricted from the fine pins (mg.py:842-868)
@@ -116,14 +119,16 @@ class DeviceMultigrid:
         self._t = dict(r_ptr=T(r_ptr.astype(np.int32)), r_fine=T(fine[order].astype(np.int32)),
                        r_w=T(ww[order].astype(np.float32)), blk_ptr=T(blk_ptr), blk_moff=T(blk_moff),
                        minv=T(cage.minv_flat), coarse_lib=T(cl.inv.astype(np.int32)), p_idx=T(p_idx), p_w=T(p_w))
+        self._t["resid"] = torch.zeros((sim.n_verts, 4), dtype=torch.float32, device=dev)
         g = capi.XpbdCage()
         g.n_fine, g.n_coarse, g.n_blocks = sim.n_verts, ncoarse, int(blk_moff.shape[0])
         g.max_block = int(np.diff(blk_ptr).max())
-        for k in ("r_ptr", "r_fine", "r_w", "blk_ptr", "blk_moff", "minv", "coarse_lib", "p_idx", "p_w"):
+        for k in ("r_ptr", "r_fine", "r_w", "blk_ptr", "blk_moff", "minv", "coarse_lib", "p_idx", "p_w", "resid"):
             setattr(g, k, self._t[k].data_ptr())
         self.g = g
         self.prev = torch.zeros((ncoarse, 4), dtype=torch.float32, device=dev)
         pin4 = np.zeros((ncoarse, 4), np.float32)
+        pin4[:, :3] = self.q0  # prior of the first target restriction
         pin4[:, 3] = self.coarse_pin
         self.pin4 = T(pin4[cl.perm])
 

@@ -44,6 +44,7 @@ def test_restrict_and_prolong_match_oracle():
     x = (sc.verts + rng.normal(scale=0.003, size=sc.verts.shape)).astype(np.float32)
     sim.set_positions(x)
     mg = sim.mg
+    prior = _coarse_user(sim, mg.coarse._pos4)
     import ctypes as C
     from rlmusclev2_b200 import _capi as capi
     capi.check(sim._lib.xpbd_mg_restrict(C.byref(mg.g), C.c_void_p(sim._pos4.data_ptr()),
@@ -51,7 +52,7 @@ def test_restrict_and_prolong_match_oracle():
                                          None, sim._sp))
     sim.synchronize()
     got = _coarse_user(sim, mg.coarse._pos4)
-    ref = o64.restrict(x.astype(np.float64))
+    ref = o64.restrict(x.astype(np.float64), prior.astype(np.float64))
     err = np.abs(got - ref).max()
     print(f"restrict max err {err:.3e}")
     assert err <= 5e-5
@@ -79,6 +80,7 @@ def test_vcycle_from_identical_state():
     cfg, sc, sim, o64 = _setup()
     frame = 3
     o64.target, _ = o64.targets(frame)
+    o64.mg_target = o64.restrict(o64.target, o64.mg_target)
     sim.load_frame_targets(frame)
     sim._targets_kernel()
     sim.mg.refresh_target()
