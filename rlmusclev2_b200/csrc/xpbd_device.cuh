@@ -177,8 +177,11 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
 #pragma unroll 1
     for (int it = 0; it < 10; ++it) {
         const float3 c1 = cross(x2, x0), c2 = cross(x0, x1);
-        const float g = rcbrtf(det);          // |det X|^(-1/3), det > 0
-        const float h = 0.5f / (g * det);     // 1 / (2 g det)
+        // Scaling g ~ det^(-1/3) only sets the convergence speed: at the fixed
+        // point det = 1, and a relative error e in g moves the iterate by
+        // O(e^2), so the fast approximate power and divide are enough.
+        const float g = __powf(det, -0.33333334f);
+        const float h = __fdividef(0.5f, g * det);  // 1 / (2 g det)
         const float a = 0.5f * g;
         const float3 y0 = a * x0 + h * c0, y1 = a * x1 + h * c1, y2 = a * x2 + h * c2;
         const float3 e0 = y0 - x0, e1 = y1 - x1, e2 = y2 - x2;

@@ -66,7 +66,8 @@ class XpbdEngine:
         self.n_cons = table.n
         self.cons_ranges = dict(table.cons_ranges)
         L = build_layout(self.pos0_np, self.tet_np, table, tile_tets=tile_tets, v_fiber=v_fiber,
-                         tet_tendonmask=tet_tendonmask)
+                         tet_tendonmask=tet_tendonmask,
+                         n_sm=torch.cuda.get_device_properties(self.device).multi_processor_count)
         self.layout: TileLayout = L
         dev = self.device
         f32 = torch.float32

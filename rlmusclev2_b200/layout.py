@@ -72,12 +72,24 @@ class TileLayout:
         return int(self.bnd_verts.shape[0])
 
 
-def default_tile_tets(n_tets: int, n_sm: int = 148, tiles_per_sm: float = 3.5) -> int:
-    """Tile size giving about 3.5 tiles per SM (measured best on B200 for the
-    535k-tet scene: 1024-tet tiles), clamped to [64, 2048]."""
-    t = int(np.ceil(n_tets / float(n_sm * tiles_per_sm)))
-    t = int(np.clip(t, 64, 2048))
-    return ((t + 31) // 32) * 32
+def ctas_per_sm(materials: list[dict]) -> int:
+    """Resident CTAs per SM of the tile pass the library launches for these
+    materials: 3 for the light constraint set (ARAP-SVD / aniso only, no
+    damping), 2 when any material has volume, SNH or damping."""
+    u = 0
+    for m in materials:
+        u |= int(m["flags"])
+    return 2 if u & (capi.MAT_VOLUME | capi.MAT_SNH | capi.MAT_DAMPED) else 3
+
+
+def default_tile_tets(n_tets: int, n_sm: int = 148, ctas: int = 3, max_tile: int = 2048) -> int:
+    """Tile size that fills whole waves: the tile count is a multiple of the
+    resident CTA slots (n_sm x ctas) with tiles of at most ``max_tile`` tets,
+    so no wave runs part-empty (at least 64 tets per tile)."""
+    slots = n_sm * ctas
+    waves = max(1, int(np.ceil(n_tets / float(slots * max_tile))))
+    t = int(np.ceil(n_tets / float(slots * waves)))
+    return int(np.clip(t, 64, max_tile))
 
 
 def tet_materials(n_tets: int, tets: np.ndarray, table: ConstraintTable):
@@ -143,14 +155,16 @@ def fiber_f0(v_fiber: np.ndarray, tets: np.ndarray) -> np.ndarray:
 
 
 def build_layout(pos0: np.ndarray, tets: np.ndarray, table: ConstraintTable, *, tile_tets: int | None = None,
-                 v_fiber: np.ndarray | None = None, tet_tendonmask: np.ndarray | None = None) -> TileLayout:
+                 v_fiber: np.ndarray | None = None, tet_tendonmask: np.ndarray | None = None,
+                 n_sm: int = 148) -> TileLayout:
     pos0 = np.asarray(pos0, np.float32)
     tets = np.asarray(tets, np.int64)
     nv, nt = pos0.shape[0], tets.shape[0]
     if nt == 0:
         raise ValueError("mesh has no tets")
+    mats, mat_of_user_tet, V0 = tet_materials(nt, tets, table)
     if tile_tets is None:
-        tile_tets = default_tile_tets(nt)
+        tile_tets = default_tile_tets(nt, n_sm, ctas_per_sm(mats))
     lo, hi = pos0.min(0), pos0.max(0)
     # 1. tets in Morton order of their centroid
     cent = pos0[tets].mean(axis=1)
@@ -216,7 +230,6 @@ def build_layout(pos0: np.ndarray, tets: np.ndarray, table: ConstraintTable, *, 
     max_tile_verts = int(counts.max())
     assert max_tile_verts <= capi.MAX_TILE_VERTS and local.max() < 65536
     # 6. materials, rest data, tet streams
-    mats, mat_of_user_tet, V0 = tet_materials(nt, tets, table)
     B, V0_geo, _ = tet_rest_data(pos0, tets)
     V0 = np.where(np.isnan(V0), V0_geo, V0).astype(np.float32)
     Bs = B[tet_perm].reshape(nt, 9)
