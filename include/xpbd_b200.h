@@ -38,6 +38,7 @@ enum {
     XPBD_STATUS_PAIR_OVERFLOW = 1 << 0,    /* more candidate pairs than max_pairs (extra pairs dropped) */
     XPBD_STATUS_CONTACT_OVERFLOW = 1 << 1, /* more contacts than max_contacts (extra contacts dropped) */
     XPBD_STATUS_STACK_OVERFLOW = 1 << 2,   /* BVH traversal deeper than its stack (query cut short) */
+    XPBD_STATUS_BARRIER_TIMEOUT = 1 << 3,  /* a grid-wide wait of the persistent pass gave up (results invalid) */
 };
 
 #define XPBD_MAX_MATERIALS 64
@@ -346,6 +347,32 @@ int xpbd_dcd_narrow_respond(const XpbdDcd* dcd, float* pos4, xpbd_stream_t strea
  * capture.  All calls share the array: calls that overlap on the GPU race. */
 #define XPBD_NOALLOC_MAX_VERTS 262144
 int xpbd_iterate_noalloc(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v, xpbd_stream_t stream);
+
+/* Persistent multi-iteration tet pass: state of xpbd_iterate_persistent. */
+typedef struct XpbdPersist {
+    const int32_t* tile_own; /* [n_tiles+1] tile k owns vertex ids [tile_own[k], tile_own[k+1]) (the vertices it
+                                touches first); ids from tile_own[n_tiles] up to n_verts are in no tet */
+    float* ring;             /* [3][n_verts][4] boundary accumulators; all zero before the first call */
+    uint32_t* sync;          /* [4] grid barrier count, generation, ring phase, reserved; zero before the first call */
+    int32_t* status;         /* [1] XPBD_STATUS_BARRIER_TIMEOUT; after it, zero ring and sync before the next call */
+} XpbdPersist;
+
+/* n_iters fused Jacobi iterations in ONE cooperative launch: the same
+ * per-iteration result as n_iters x (xpbd_project(XPBD_PROJECT_FUSED) +
+ * xpbd_apply_boundary(ATTACH | DIVIDE | PIN | CLEAR)), i.e. n_iters rounds of
+ * solve_constraints -> apply_dP -> apply_pintotarget of MultiGridSim's
+ * iteration phase (mg.py:1350-1360) with no hook in between.  Every tile's
+ * vertices stay in shared memory for all iterations; tile-boundary sums go
+ * through a ring of three global accumulators with one grid-wide barrier per
+ * iteration, and pos is written once at the end.  Needs all n_tiles CTAs
+ * resident at once (xpbd_persistent_fits); returns XPBD_ERR_LIMIT otherwise.
+ * Barrier waits are bounded (about a second); on timeout the status bit is
+ * set and the kernel runs to its end without waiting again. */
+int xpbd_iterate_persistent(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v,
+                            const XpbdPersist* ps, int32_t n_iters, xpbd_stream_t stream);
+/* *fits = 1 when the persistent pass of these materials can hold all tiles
+ * resident on the current device. */
+int xpbd_persistent_fits(const XpbdParams* prm, const XpbdTiles* tiles, int32_t* fits);
 
 /* Stream capture helpers (a captured substep replays as one graph launch). */
 int xpbd_graph_begin(xpbd_stream_t stream);

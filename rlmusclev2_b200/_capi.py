@@ -18,7 +18,7 @@ OK = 0
 MAT_ARAPSVD, MAT_VOLUME, MAT_ANISO, MAT_SNH, MAT_DAMPED = 1, 2, 4, 8, 16
 VF_ATTACH_MASK, VF_PIN = 0xFF, 1 << 8
 OP_SDF, OP_VELOCITY, OP_PREDICT, OP_PIN = 1, 2, 4, 8
-STATUS_PAIR_OVERFLOW, STATUS_CONTACT_OVERFLOW, STATUS_STACK_OVERFLOW = 1, 2, 4
+STATUS_PAIR_OVERFLOW, STATUS_CONTACT_OVERFLOW, STATUS_STACK_OVERFLOW, STATUS_BARRIER_TIMEOUT = 1, 2, 4, 8
 APPLY_ATTACH, APPLY_DIVIDE, APPLY_PIN, APPLY_CLEAR = 1, 2, 4, 8
 PROJECT_FUSED, PROJECT_ACCUMULATE, PROJECT_FUSED_LAST = 0, 1, 2
 
@@ -97,6 +97,10 @@ class XpbdMetrics(C.Structure):
                 ("n_inverted", C.c_int32), ("n_nonfinite", C.c_int32), ("reserved", C.c_int32)]
 
 
+class XpbdPersist(C.Structure):
+    _fields_ = [("tile_own", C.c_void_p), ("ring", C.c_void_p), ("sync", C.c_void_p), ("status", C.c_void_p)]
+
+
 P = C.c_void_p
 _SIGS = {
     "xpbd_abi_version": ([], C.c_int),
@@ -117,6 +121,9 @@ _SIGS = {
     "xpbd_dcd_broadphase": ([C.POINTER(XpbdDcd), P, C.c_int32, P], C.c_int),
     "xpbd_dcd_narrow_respond": ([C.POINTER(XpbdDcd), P, P], C.c_int),
     "xpbd_iterate_noalloc": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), P], C.c_int),
+    "xpbd_iterate_persistent": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(XpbdVerts),
+                                 C.POINTER(XpbdPersist), C.c_int32, P], C.c_int),
+    "xpbd_persistent_fits": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(C.c_int32)], C.c_int),
     "xpbd_graph_begin": ([P], C.c_int),
     "xpbd_graph_end": ([P, C.POINTER(C.c_void_p)], C.c_int),
     "xpbd_graph_launch": ([P, P], C.c_int),

@@ -1,0 +1,230 @@
+// Persistent multi-iteration tet pass (xpbd_iterate_persistent).
+//
+// One cooperative launch runs n_iters Jacobi iterations.  Each CTA keeps its
+// tile's vertices (positions, and previous positions for damped materials) in
+// shared memory for the whole launch.  Per iteration: project the tile's tets
+// into shared accumulators, finish the interior vertices in place, add the
+// tile-boundary partial sums to ring slot `cur` of a three-slot global
+// accumulator, one grid-wide barrier, then every tile touching a boundary
+// vertex finishes it from the complete sum (all of them compute the same
+// value from the same inputs).  The owner tile of each boundary vertex clears
+// slot `cur + 1`, which was last read two iterations earlier and is next
+// filled one iteration later, so one barrier per iteration suffices.  The
+// ring phase persists in sync[2] across launches; the slot the next launch
+// starts on is the one cleared in this launch's last iteration.
+#include <cuda/atomic>
+#include <cuda_runtime.h>
+
+#include "xpbd_common.cuh"
+#include "xpbd_tile.cuh"
+
+using namespace xpbd;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr unsigned kSpinLimit = 1u << 21;  // polls of ~0.5 us (L2 round trip + 32 ns sleep): about a second
+
+// Grid-wide barrier over gridDim.x co-resident CTAs (count, generation in
+// sync[0..1]).  Bounded: after kSpinLimit polls it sets the timeout bit, and
+// once that bit is set no CTA waits again.
+__device__ __forceinline__ void grid_barrier(uint32_t* sync, int32_t* status) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> cnt(sync[0]), gen(sync[1]);
+        cuda::atomic_ref<int32_t, cuda::thread_scope_device> st(*status);
+        if ((st.load(cuda::memory_order_relaxed) & XPBD_STATUS_BARRIER_TIMEOUT) == 0) {
+            const uint32_t g = gen.load(cuda::memory_order_acquire);
+            __threadfence();
+            const uint32_t arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+            if (arrived == gridDim.x - 1) {
+                cnt.store(0u, cuda::memory_order_relaxed);
+                gen.fetch_add(1u, cuda::memory_order_release);
+            } else {
+                uint32_t spins = 0;
+                while (gen.load(cuda::memory_order_acquire) == g) {
+                    if (++spins > kSpinLimit) {
+                        st.fetch_or(XPBD_STATUS_BARRIER_TIMEOUT, cuda::memory_order_relaxed);
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            __threadfence();
+        }
+    }
+    __syncthreads();
+}
+
+template <bool DAMP, int MINB, int CSET>
+__global__ void __launch_bounds__(kThreads, MINB)
+    k_iterate_persistent(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdTiles T,
+                         const __grid_constant__ XpbdVerts V, const __grid_constant__ XpbdPersist P, int n_iters) {
+    extern __shared__ float4 smem[];
+    const int tile = blockIdx.x;
+    const int vbeg = T.tile_vptr[tile];
+    const int nvt = T.tile_vptr[tile + 1] - vbeg;
+    const int nint = T.tile_nint[tile];
+    const int own_lo = P.tile_own[tile], own_hi = P.tile_own[tile + 1];
+    const int orph_lo = P.tile_own[T.n_tiles];
+    const int mtv = T.max_tile_verts;
+    float4* s_pos = smem;
+    float4* s_prev = smem + mtv;
+    float* s_ax = reinterpret_cast<float*>(smem + (DAMP ? 2 : 1) * mtv);
+    float* s_ay = s_ax + mtv;
+    float* s_az = s_ay + mtv;
+    float* s_aw = s_az + mtv;
+    const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
+    const float4* prev4 = reinterpret_cast<const float4*>(V.pprev);
+    float4* pos4w = reinterpret_cast<float4*>(V.pos);
+    float4* ring = reinterpret_cast<float4*>(P.ring);
+    const size_t nv = size_t(V.n);
+    const uint32_t phase0 = P.sync[2];
+    const uint32_t ops = XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_PIN;
+    for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
+        const int g = T.tile_verts[vbeg + i];
+        s_pos[i] = pos4[g];
+        if (DAMP) s_prev[i] = prev4[g];
+    }
+    for (int it = 0; it < n_iters; ++it) {
+        const uint32_t cur = (phase0 + uint32_t(it)) % 3u, nxt = (phase0 + uint32_t(it) + 1u) % 3u;
+        float4* rc = ring + cur * nv;
+        float4* rn = ring + nxt * nv;
+        for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
+            s_ax[i] = 0.f;
+            s_ay[i] = 0.f;
+            s_az[i] = 0.f;
+            s_aw[i] = 0.f;
+        }
+        __syncthreads();
+        project_tile_tets<DAMP, CSET>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_aw);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nint; i += blockDim.x) {
+            const int g = T.tile_verts[vbeg + i];
+            float4 pp = s_pos[i];
+            finish_vertex(prm, V, g, pp, make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]), ops);
+            s_pos[i] = pp;
+        }
+        for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
+            const int g = T.tile_verts[vbeg + i];
+            const float4 a = make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]);
+            if (a.w != 0.f) atomicAdd(&rc[g], a);
+            if (g >= own_lo && g < own_hi) rn[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        // vertices in no tet: attach and pin only, each handled by one thread
+        for (int g = orph_lo + int(blockIdx.x) * blockDim.x + threadIdx.x; g < V.n; g += gridDim.x * blockDim.x) {
+            float4 pp = pos4[g];
+            finish_vertex(prm, V, g, pp, make_float4(0.f, 0.f, 0.f, 0.f), ops);
+            pos4w[g] = pp;
+        }
+        grid_barrier(P.sync, P.status);
+        for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
+            const int g = T.tile_verts[vbeg + i];
+            float4 pp = s_pos[i];
+            finish_vertex(prm, V, g, pp, __ldcg(&rc[g]), ops);
+            s_pos[i] = pp;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
+        const int g = T.tile_verts[vbeg + i];
+        if (i < nint || (g >= own_lo && g < own_hi)) pos4w[g] = s_pos[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.sync[2] = (phase0 + uint32_t(n_iters)) % 3u;
+}
+
+uint32_t material_union(const XpbdParams* p) {
+    uint32_t u = 0;
+    for (int i = 0; i < p->n_materials; ++i) u |= p->materials[i].flags;
+    return u;
+}
+
+template <bool DAMP, int MINB, int CSET>
+int launch_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, const XpbdPersist* P, int n_iters,
+             cudaStream_t s, bool query_only, int* fits) {
+    auto kern = k_iterate_persistent<DAMP, MINB, CSET>;
+    const size_t smem = size_t(T->max_tile_verts) * sizeof(float4) * (DAMP ? 3 : 2);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        return cuda_check("xpbd_iterate_persistent: smem attribute");
+    int dev = 0, n_sm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem) != cudaSuccess)
+        return cuda_check("xpbd_iterate_persistent: occupancy");
+    const bool ok = int64_t(per_sm) * n_sm >= T->n_tiles;
+    if (query_only) {
+        *fits = ok ? 1 : 0;
+        return XPBD_OK;
+    }
+    if (!ok) return fail(XPBD_ERR_LIMIT, "xpbd_iterate_persistent: tiles exceed the resident CTA slots");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(T->n_tiles);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, kern, *prm, *T, *V, *P, n_iters) != cudaSuccess)
+        return cuda_check("xpbd_iterate_persistent: launch");
+    return cuda_check("xpbd_iterate_persistent");
+}
+
+// Same instance choice as the per-iteration pass.
+int dispatch(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, const XpbdPersist* P, int n_iters,
+             cudaStream_t s, bool query_only, int* fits) {
+    const uint32_t u = material_union(prm);
+    bool damp = false;
+    for (int i = 0; i < prm->n_materials; ++i)
+        if (prm->materials[i].flags & XPBD_MAT_DAMPED) damp = true;
+    const bool flip = (prm->tile_variant & 1) != 0;
+#define XPBD_LAUNCH(D, M, C) launch_v<D, M, C>(prm, T, V, P, n_iters, s, query_only, fits)
+    if (u & XPBD_MAT_SNH) {
+        if (damp) return flip ? XPBD_LAUNCH(true, 3, CSET_FULL) : XPBD_LAUNCH(true, 2, CSET_FULL);
+        return flip ? XPBD_LAUNCH(false, 3, CSET_FULL) : XPBD_LAUNCH(false, 2, CSET_FULL);
+    }
+    if (u & XPBD_MAT_VOLUME) {
+        if (damp) return flip ? XPBD_LAUNCH(true, 3, CSET_VOL) : XPBD_LAUNCH(true, 2, CSET_VOL);
+        return flip ? XPBD_LAUNCH(false, 3, CSET_VOL) : XPBD_LAUNCH(false, 2, CSET_VOL);
+    }
+    return flip ? XPBD_LAUNCH(false, 2, CSET_LIGHT) : XPBD_LAUNCH(false, 3, CSET_LIGHT);
+#undef XPBD_LAUNCH
+}
+
+}  // namespace
+
+extern "C" int xpbd_iterate_persistent(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v,
+                                       const XpbdPersist* ps, int32_t n_iters, xpbd_stream_t stream) {
+    if (!prm || !tiles || !v || !ps) return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: null argument");
+    if (n_iters < 0) return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: n_iters < 0");
+    if (n_iters == 0) return XPBD_OK;
+    if (!v->pos || v->n <= 0 || !tiles->tile_vptr || !tiles->tile_nint || !tiles->tile_tptr || !tiles->tile_verts ||
+        !tiles->tet_q || !tiles->tet_b0 || !tiles->tet_b1 || !tiles->tet_b2 || tiles->n_tiles <= 0)
+        return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: tiles/verts");
+    if (!ps->tile_own || !ps->ring || !ps->sync || !ps->status)
+        return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: XpbdPersist pointers");
+    if (!aligned16(v->pos) || !aligned16(ps->ring)) return fail(XPBD_ERR_ALIGN, "xpbd_iterate_persistent: alignment");
+    if (tiles->max_tile_verts > XPBD_MAX_TILE_VERTS) return fail(XPBD_ERR_LIMIT, "xpbd_iterate_persistent: tile size");
+    if (prm->n_materials < 1 || prm->n_materials > XPBD_MAX_MATERIALS)
+        return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: n_materials");
+    bool aniso = false, damp = false;
+    for (int i = 0; i < prm->n_materials; ++i) {
+        aniso |= (prm->materials[i].flags & XPBD_MAT_ANISO) != 0;
+        damp |= (prm->materials[i].flags & XPBD_MAT_DAMPED) != 0;
+    }
+    if (aniso && (!tiles->tet_fiber || !tiles->tet_act))
+        return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: aniso materials need tet_fiber and tet_act");
+    if (damp && !v->pprev) return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: damped materials need pprev");
+    return dispatch(prm, tiles, v, ps, n_iters, (cudaStream_t)stream, false, nullptr);
+}
+
+extern "C" int xpbd_persistent_fits(const XpbdParams* prm, const XpbdTiles* tiles, int32_t* fits) {
+    if (!prm || !tiles || !fits) return fail(XPBD_ERR_ARG, "xpbd_persistent_fits: null argument");
+    int f = 0;
+    const int rc = dispatch(prm, tiles, nullptr, nullptr, 0, nullptr, true, &f);
+    *fits = f;
+    return rc;
+}

@@ -1,0 +1,118 @@
+// Tile-pass building blocks shared by the per-iteration kernel
+// (k_project_tiles, xpbd_core.cu) and the persistent multi-iteration kernel
+// (xpbd_persist.cu): the per-vertex finish and the projection of one tile's
+// tets into shared-memory accumulators.
+#pragma once
+#include "xpbd_common.cuh"
+#include "xpbd_device.cuh"
+
+namespace xpbd {
+
+// ---------------------------------------------------------------------------
+// Per-vertex finish of a Jacobi iteration: ATTACH, divide, pin.
+__device__ __forceinline__ void finish_vertex(const XpbdParams& prm, const XpbdVerts& V, int g, float4& p, float4 a,
+                                              uint32_t ops) {
+    int f = 0;
+    if (V.vflags) f = V.vflags[g];
+    if ((ops & XPBD_APPLY_ATTACH) && (f & XPBD_VF_ATTACH_MASK) && (f & XPBD_VF_ATTACH_MASK) <= prm.n_attach_materials) {
+        const XpbdAttachMaterial& M = prm.attach[(f & XPBD_VF_ATTACH_MASK) - 1];
+        if (M.k > 0.f) {
+            const float4 at = reinterpret_cast<const float4*>(V.attach_target)[g];
+            float3 prev = make_float3(0.f, 0.f, 0.f);
+            if (M.damp > 0.f) prev = f3(reinterpret_cast<const float4*>(V.pprev)[g]);
+            float3 d;
+            if (con_attach(p, prev, f3(at), at.w, M.k, M.damp, prm.dt, d)) {
+                a.x += d.x;
+                a.y += d.y;
+                a.z += d.z;
+                a.w += 1.f;
+            }
+        }
+    }
+    if ((ops & XPBD_APPLY_DIVIDE) && a.w > 1e-9f) {
+        float3 d = make_float3(a.x / a.w, a.y / a.w, a.z / a.w);
+        if (prm.omega != 1.f) d = prm.omega * d;
+        p.x += d.x;
+        p.y += d.y;
+        p.z += d.z;
+    }
+    if ((ops & XPBD_APPLY_PIN) && (f & XPBD_VF_PIN)) {
+        const float4 t = reinterpret_cast<const float4*>(V.pin_target)[g];
+        if (t.w != 0.f) {
+            p.x = t.x;
+            p.y = t.y;
+            p.z = t.z;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Constraint sets compiled into a tile-pass instance: the heavier sets cost
+// registers (and occupancy) even for tets that do not use them.
+enum { CSET_LIGHT = 0, CSET_VOL = 1, CSET_FULL = 2 };  // ARAP+aniso | +volume | +volume+SNH
+
+// Projects every constraint of the tile's tets from the staged positions
+// (s_pos, s_prev) and adds the Jacobi deltas and counts to the shared
+// accumulators s_ax..s_aw (one thread per tet, strided over the CTA).
+template <bool DAMP, int CSET>
+__device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const XpbdTiles& T, int tile,
+                                                  const float4* s_pos, const float4* s_prev, float* s_ax, float* s_ay,
+                                                  float* s_az, float* s_aw) {
+    const int t1 = T.tile_tptr[tile + 1];
+    const uint4* tq = reinterpret_cast<const uint4*>(T.tet_q);
+    const float4* tb0 = reinterpret_cast<const float4*>(T.tet_b0);
+    const float4* tb1 = reinterpret_cast<const float4*>(T.tet_b1);
+    for (int t = T.tile_tptr[tile] + threadIdx.x; t < t1; t += blockDim.x) {
+        const uint4 q = tq[t];
+        const float4 b0 = tb0[t], b1 = tb1[t];
+        const float b2 = T.tet_b2[t];
+        const int l[4] = {int(q.x & 0xffffu), int(q.x >> 16), int(q.y & 0xffffu), int(q.y >> 16)};
+        const XpbdMaterial& m = prm.materials[min(int(q.z & 0xffu), XPBD_MAX_MATERIALS - 1)];
+        const float V0 = __uint_as_float(q.w);
+        M3 B;
+        B.m[0][0] = b0.x; B.m[0][1] = b0.y; B.m[0][2] = b0.z;
+        B.m[1][0] = b0.w; B.m[1][1] = b1.x; B.m[1][2] = b1.y;
+        B.m[2][0] = b1.z; B.m[2][1] = b1.w; B.m[2][2] = b2;
+        float4 p[4], pq[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            p[i] = s_pos[l[i]];
+            if (DAMP) pq[i] = s_prev[l[i]];
+        }
+        const float3 p3 = f3(p[3]);
+        const M3 F = deformation(f3(p[0]) - p3, f3(p[1]) - p3, f3(p[2]) - p3, B);
+        // All constraints of the tet read the same positions (Jacobi), so their
+        // deltas are summed in registers and pushed with one set of shared
+        // atomics; each active constraint adds 1 to dPw of all four vertices.
+        float3 d[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) d[i] = make_float3(0.f, 0.f, 0.f);
+        float nact = 0.f;
+        const uint32_t fl = m.flags;
+        // Same type order as the reference table (ascending ConstraintType tag).
+        if (CSET >= CSET_FULL && (fl & XPBD_MAT_SNH) &&
+            con_snh(p, pq, B, F, V0, m.snh_mu, m.snh_lam, m.snh_damp, prm.dt, d))
+            nact += 1.f;
+        if (CSET >= CSET_VOL && (fl & XPBD_MAT_VOLUME) && con_volume(p, pq, V0, m.vol_k, m.vol_damp, prm.dt, d))
+            nact += 1.f;
+        if (fl & XPBD_MAT_ANISO) {
+            const float4 fb = reinterpret_cast<const float4*>(T.tet_fiber)[t];
+            if (con_aniso(p, B, F, f3(fb), fb.w, T.tet_act[t], m.aniso_k, prm.contraction_ratio,
+                          prm.fiber_stiffness_scale, prm.dt, d))
+                nact += 1.f;
+        }
+        if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, m.arap_k, prm.dt, d, (prm.tile_variant & 2) != 0))
+            nact += 1.f;
+        if (nact != 0.f) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                atomicAdd(&s_ax[l[i]], d[i].x);
+                atomicAdd(&s_ay[l[i]], d[i].y);
+                atomicAdd(&s_az[l[i]], d[i].z);
+                atomicAdd(&s_aw[l[i]], nact);
+            }
+        }
+    }
+}
+
+}  // namespace xpbd

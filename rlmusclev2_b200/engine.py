@@ -90,6 +90,12 @@ class XpbdEngine:
         self._massd = T(self._mass_user[L.perm])
         self._accum = torch.zeros((nv, 4), dtype=f32, device=dev)
         self._accum_dirty = False
+        # persistent multi-iteration pass: boundary ring, grid barrier words, status
+        self._ring = torch.zeros((3, nv, 4), dtype=f32, device=dev)
+        self._psync = torch.zeros(4, dtype=torch.int32, device=dev)
+        self._pstatus = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._t_own = T(L.tile_own)
+        self.use_persistent = True
         self._metrics_buf = torch.zeros(8, dtype=torch.float64, device=dev)  # >= sizeof(XpbdMetrics)
         # tiles
         self._t_vptr = T(L.tile_vptr)
@@ -205,6 +211,13 @@ class XpbdEngine:
         else:
             to.n_boundary = 0
         self._tiles_orph = to
+        ps = capi.XpbdPersist()
+        ps.tile_own, ps.ring, ps.sync, ps.status = _ptr(self._t_own), _ptr(self._ring), _ptr(self._psync), _ptr(
+            self._pstatus)
+        self._persist = ps
+        fits = C.c_int32(0)
+        capi.check(self._lib.xpbd_persistent_fits(C.byref(self._prm), C.byref(t), C.byref(fits)))
+        self._persist_fits = bool(fits.value)
         for g in self._graphs.values():
             capi.check(self._lib.xpbd_graph_destroy(g))
         self._graphs = {}
@@ -244,6 +257,33 @@ class XpbdEngine:
             return
         self._project(capi.PROJECT_FUSED)
         self._apply_boundary(capi.APPLY_ATTACH | capi.APPLY_DIVIDE | capi.APPLY_PIN | capi.APPLY_CLEAR)
+
+    def _fused_iterations(self, n: int) -> None:
+        """n fused iterations: one persistent cooperative launch when all tiles
+        fit on the GPU at once, else n x _fused_iteration()."""
+        if n <= 0:
+            return
+        if self.use_persistent and self._persist_fits and self.fused_mode == capi.PROJECT_FUSED:
+            capi.check(self._lib.xpbd_iterate_persistent(C.byref(self._prm), C.byref(self._tiles),
+                                                         C.byref(self._verts), C.byref(self._persist), int(n),
+                                                         self._sp))
+            return
+        for _ in range(n):
+            self._fused_iteration()
+
+    def persistent_status(self, reset: bool = True) -> int:
+        """XPBD_STATUS_* bits of the persistent pass (synchronises).  After a
+        barrier timeout the ring and barrier words are cleared for the next
+        launch."""
+        self._stream.synchronize()
+        st = int(self._pstatus.item())
+        if st and reset:
+            with torch.cuda.stream(self._stream):
+                self._ring.zero_()
+                self._psync.zero_()
+                self._pstatus.zero_()
+            self._stream.synchronize()
+        return st
 
     def synchronize(self) -> None:
         self._stream.synchronize()

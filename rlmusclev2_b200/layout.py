@@ -62,6 +62,7 @@ class TileLayout:
     orphans: np.ndarray       # vertices in no tet (new order)
     materials: list           # list of dicts (XpbdMaterial fields)
     tet_material: np.ndarray  # (NT,) material id per new tet
+    tile_own: np.ndarray | None = None  # (n_tiles+1,) tile k owns new ids [tile_own[k], tile_own[k+1])
 
     @property
     def n_tiles(self) -> int:
@@ -256,4 +257,5 @@ def build_layout(pos0: np.ndarray, tets: np.ndarray, table: ConstraintTable, *, 
         bnd_verts=np.nonzero((ntile_of_v != 1)[perm])[0].astype(np.int32), max_tile_verts=max_tile_verts,
         tet_q=tet_q, tet_b0=tet_b0, tet_b1=tet_b1, tet_b2=tet_b2, tet_fiber=tet_fiber,
         vert_ntiles=ntile_of_v[perm].astype(np.int32), orphans=np.nonzero(ntile_of_v[perm] == 0)[0].astype(np.int32),
-        materials=mats, tet_material=mat_of_user_tet[tet_perm].astype(np.int32))
+        materials=mats, tet_material=mat_of_user_tet[tet_perm].astype(np.int32),
+        tile_own=np.searchsorted(first_tile[perm], np.arange(n_tiles + 1)).astype(np.int32))

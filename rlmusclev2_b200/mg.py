@@ -369,6 +369,9 @@ class MultiGridSim(MuscleSim):
             else:
                 self._vstep(capi.OP_PREDICT | ((push | vel) if sub > 0 else 0))
                 self.mg.vcycle(pin_fine=bool(pin))
+            if not self.collision_solvers_iter:
+                self._fused_iterations(self.fine_iters)
+                continue
             for it in range(self.fine_iters):
                 self._fused_iteration()
                 for fn in self.collision_solvers_iter:

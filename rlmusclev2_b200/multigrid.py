@@ -144,8 +144,7 @@ class DeviceMultigrid:
         capi.check(s._lib.xpbd_mg_restrict(C.byref(self.g), C.c_void_p(s._pos4.data_ptr()),
                                            C.c_void_p(co._pos4.data_ptr()), C.c_void_p(self.prev.data_ptr()),
                                            C.c_void_p(self.pin4.data_ptr()), s._sp))
-        for _ in range(self.iters):
-            co._fused_iteration()
+        co._fused_iterations(self.iters)
         vf = s._vflags.data_ptr() if (pin_fine and s._vflags is not None) else None
         pt = s._pin_tgt.data_ptr() if (pin_fine and s._pin_tgt is not None) else None
         capi.check(s._lib.xpbd_mg_prolong_delta(C.byref(self.g), C.c_void_p(co._pos4.data_ptr()),
