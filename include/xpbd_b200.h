@@ -79,8 +79,10 @@ typedef struct XpbdParams {
     float fiber_stiffness_scale; /* aniso_arap stiffness multiplier */
     int32_t n_materials;
     int32_t n_attach_materials;
-    int32_t tile_variant;        /* bit 0: tile pass with 3 CTAs/SM (80 regs) instead of 2 (128 regs);
-                                    bit 1: ARAP-SVD through the SVD even where the polar rotation applies */
+    int32_t tile_variant;        /* bit 0: flip the tile pass's CTAs/SM (default 3 at 80 regs for the
+                                    ARAP/aniso set, 2 at up to 128 regs with volume/SNH/damping);
+                                    bit 1: ARAP-SVD through the SVD even where the polar rotation applies;
+                                    bit 2: persistent pass loads the next tet's streams ahead (prefetch) */
     XpbdMaterial materials[XPBD_MAX_MATERIALS];
     XpbdAttachMaterial attach[XPBD_MAX_ATTACH_MATERIALS];
 } XpbdParams;

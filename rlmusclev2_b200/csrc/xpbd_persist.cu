@@ -23,21 +23,23 @@ using namespace xpbd;
 namespace {
 
 constexpr int kThreads = 256;
+constexpr size_t kSmemPerVert = 4 * sizeof(float4) + 4 * sizeof(float) + 2 * sizeof(int);  // 88 bytes
 constexpr unsigned kSpinLimit = 1u << 21;  // polls of ~0.5 us (L2 round trip + 32 ns sleep): about a second
 
 // Grid-wide barrier over gridDim.x co-resident CTAs (count, generation in
-// sync[0..1]).  Bounded: after kSpinLimit polls it sets the timeout bit, and
-// once that bit is set no CTA waits again.
+// sync[0..1]).  __syncthreads orders the CTA's writes before thread 0's
+// acquire-release arrival; the release of the new generation and the
+// acquiring polls carry them to the other CTAs, whose __syncthreads passes
+// them on to their threads.  Bounded: after kSpinLimit polls it sets the
+// timeout bit, and once that bit is set no CTA waits again.
 __device__ __forceinline__ void grid_barrier(uint32_t* sync, int32_t* status) {
     __syncthreads();
     if (threadIdx.x == 0) {
         cuda::atomic_ref<uint32_t, cuda::thread_scope_device> cnt(sync[0]), gen(sync[1]);
         cuda::atomic_ref<int32_t, cuda::thread_scope_device> st(*status);
         if ((st.load(cuda::memory_order_relaxed) & XPBD_STATUS_BARRIER_TIMEOUT) == 0) {
-            const uint32_t g = gen.load(cuda::memory_order_acquire);
-            __threadfence();
-            const uint32_t arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
-            if (arrived == gridDim.x - 1) {
+            const uint32_t g = gen.load(cuda::memory_order_relaxed);
+            if (cnt.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1) {
                 cnt.store(0u, cuda::memory_order_relaxed);
                 gen.fetch_add(1u, cuda::memory_order_release);
             } else {
@@ -50,13 +52,12 @@ __device__ __forceinline__ void grid_barrier(uint32_t* sync, int32_t* status) {
                     __nanosleep(32);
                 }
             }
-            __threadfence();
         }
     }
     __syncthreads();
 }
 
-template <bool DAMP, int MINB, int CSET>
+template <bool DAMP, int MINB, int CSET, bool PF>
 __global__ void __launch_bounds__(kThreads, MINB)
     k_iterate_persistent(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdTiles T,
                          const __grid_constant__ XpbdVerts V, const __grid_constant__ XpbdPersist P, int n_iters) {
@@ -67,13 +68,21 @@ __global__ void __launch_bounds__(kThreads, MINB)
     const int nint = T.tile_nint[tile];
     const int own_lo = P.tile_own[tile], own_hi = P.tile_own[tile + 1];
     const int orph_lo = P.tile_own[T.n_tiles];
+    // Shared layout per tile vertex: position, previous position, attach
+    // target, pin target (float4 each), the four accumulator floats, the
+    // global id and the vertex flags: 88 bytes.  Everything but the position
+    // and the accumulators is constant for the launch.
     const int mtv = T.max_tile_verts;
     float4* s_pos = smem;
     float4* s_prev = smem + mtv;
-    float* s_ax = reinterpret_cast<float*>(smem + (DAMP ? 2 : 1) * mtv);
+    float4* s_att = smem + 2 * mtv;
+    float4* s_pin = smem + 3 * mtv;
+    float* s_ax = reinterpret_cast<float*>(smem + 4 * mtv);
     float* s_ay = s_ax + mtv;
     float* s_az = s_ay + mtv;
     float* s_aw = s_az + mtv;
+    int* s_g = reinterpret_cast<int*>(s_aw + mtv);
+    int* s_f = s_g + mtv;
     const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
     const float4* prev4 = reinterpret_cast<const float4*>(V.pprev);
     float4* pos4w = reinterpret_cast<float4*>(V.pos);
@@ -81,10 +90,16 @@ __global__ void __launch_bounds__(kThreads, MINB)
     const size_t nv = size_t(V.n);
     const uint32_t phase0 = P.sync[2];
     const uint32_t ops = XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_PIN;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
         const int g = T.tile_verts[vbeg + i];
+        const int f = V.vflags ? V.vflags[g] : 0;
+        s_g[i] = g;
+        s_f[i] = f;
         s_pos[i] = pos4[g];
-        if (DAMP) s_prev[i] = prev4[g];
+        s_prev[i] = prev4 ? prev4[g] : z4;
+        s_att[i] = (f & XPBD_VF_ATTACH_MASK) ? reinterpret_cast<const float4*>(V.attach_target)[g] : z4;
+        s_pin[i] = (f & XPBD_VF_PIN) ? reinterpret_cast<const float4*>(V.pin_target)[g] : z4;
     }
     for (int it = 0; it < n_iters; ++it) {
         const uint32_t cur = (phase0 + uint32_t(it)) % 3u, nxt = (phase0 + uint32_t(it) + 1u) % 3u;
@@ -97,16 +112,16 @@ __global__ void __launch_bounds__(kThreads, MINB)
             s_aw[i] = 0.f;
         }
         __syncthreads();
-        project_tile_tets<DAMP, CSET>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_aw);
+        project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_aw);
         __syncthreads();
         for (int i = threadIdx.x; i < nint; i += blockDim.x) {
-            const int g = T.tile_verts[vbeg + i];
             float4 pp = s_pos[i];
-            finish_vertex(prm, V, g, pp, make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]), ops);
+            finish_core(prm, s_f[i], s_att[i], s_prev[i], s_pin[i], pp,
+                        make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]), ops);
             s_pos[i] = pp;
         }
         for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
-            const int g = T.tile_verts[vbeg + i];
+            const int g = s_g[i];
             const float4 a = make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]);
             if (a.w != 0.f) atomicAdd(&rc[g], a);
             if (g >= own_lo && g < own_hi) rn[g] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -119,15 +134,14 @@ __global__ void __launch_bounds__(kThreads, MINB)
         }
         grid_barrier(P.sync, P.status);
         for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
-            const int g = T.tile_verts[vbeg + i];
             float4 pp = s_pos[i];
-            finish_vertex(prm, V, g, pp, __ldcg(&rc[g]), ops);
+            finish_core(prm, s_f[i], s_att[i], s_prev[i], s_pin[i], pp, __ldcg(&rc[s_g[i]]), ops);
             s_pos[i] = pp;
         }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
-        const int g = T.tile_verts[vbeg + i];
+        const int g = s_g[i];
         if (i < nint || (g >= own_lo && g < own_hi)) pos4w[g] = s_pos[i];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) P.sync[2] = (phase0 + uint32_t(n_iters)) % 3u;
@@ -139,11 +153,11 @@ uint32_t material_union(const XpbdParams* p) {
     return u;
 }
 
-template <bool DAMP, int MINB, int CSET>
+template <bool DAMP, int MINB, int CSET, bool PF>
 int launch_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, const XpbdPersist* P, int n_iters,
              cudaStream_t s, bool query_only, int* fits) {
-    auto kern = k_iterate_persistent<DAMP, MINB, CSET>;
-    const size_t smem = size_t(T->max_tile_verts) * sizeof(float4) * (DAMP ? 3 : 2);
+    auto kern = k_iterate_persistent<DAMP, MINB, CSET, PF>;
+    const size_t smem = size_t(T->max_tile_verts) * kSmemPerVert;
     if (smem > 48 * 1024 &&
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return cuda_check("xpbd_iterate_persistent: smem attribute");
@@ -181,7 +195,10 @@ int dispatch(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, cons
     for (int i = 0; i < prm->n_materials; ++i)
         if (prm->materials[i].flags & XPBD_MAT_DAMPED) damp = true;
     const bool flip = (prm->tile_variant & 1) != 0;
-#define XPBD_LAUNCH(D, M, C) launch_v<D, M, C>(prm, T, V, P, n_iters, s, query_only, fits)
+    const bool pf = (prm->tile_variant & 4) != 0;
+#define XPBD_LAUNCH(D, M, C) \
+    (pf ? launch_v<D, M, C, true>(prm, T, V, P, n_iters, s, query_only, fits) \
+        : launch_v<D, M, C, false>(prm, T, V, P, n_iters, s, query_only, fits))
     if (u & XPBD_MAT_SNH) {
         if (damp) return flip ? XPBD_LAUNCH(true, 3, CSET_FULL) : XPBD_LAUNCH(true, 2, CSET_FULL);
         return flip ? XPBD_LAUNCH(false, 3, CSET_FULL) : XPBD_LAUNCH(false, 2, CSET_FULL);

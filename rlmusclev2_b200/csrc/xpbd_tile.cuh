@@ -9,17 +9,15 @@
 namespace xpbd {
 
 // ---------------------------------------------------------------------------
-// Per-vertex finish of a Jacobi iteration: ATTACH, divide, pin.
-__device__ __forceinline__ void finish_vertex(const XpbdParams& prm, const XpbdVerts& V, int g, float4& p, float4 a,
-                                              uint32_t ops) {
-    int f = 0;
-    if (V.vflags) f = V.vflags[g];
+// Per-vertex finish of a Jacobi iteration: ATTACH, divide, pin, from the
+// vertex's flags f, attach target at (xyz, restlength), previous position
+// (read only for damped attach) and pin target pin (w != 0: active).
+__device__ __forceinline__ void finish_core(const XpbdParams& prm, int f, float4 at, float4 prevp, float4 pin, float4& p,
+                                            float4 a, uint32_t ops) {
     if ((ops & XPBD_APPLY_ATTACH) && (f & XPBD_VF_ATTACH_MASK) && (f & XPBD_VF_ATTACH_MASK) <= prm.n_attach_materials) {
         const XpbdAttachMaterial& M = prm.attach[(f & XPBD_VF_ATTACH_MASK) - 1];
         if (M.k > 0.f) {
-            const float4 at = reinterpret_cast<const float4*>(V.attach_target)[g];
-            float3 prev = make_float3(0.f, 0.f, 0.f);
-            if (M.damp > 0.f) prev = f3(reinterpret_cast<const float4*>(V.pprev)[g]);
+            const float3 prev = M.damp > 0.f ? f3(prevp) : make_float3(0.f, 0.f, 0.f);
             float3 d;
             if (con_attach(p, prev, f3(at), at.w, M.k, M.damp, prm.dt, d)) {
                 a.x += d.x;
@@ -36,14 +34,25 @@ __device__ __forceinline__ void finish_vertex(const XpbdParams& prm, const XpbdV
         p.y += d.y;
         p.z += d.z;
     }
-    if ((ops & XPBD_APPLY_PIN) && (f & XPBD_VF_PIN)) {
-        const float4 t = reinterpret_cast<const float4*>(V.pin_target)[g];
-        if (t.w != 0.f) {
-            p.x = t.x;
-            p.y = t.y;
-            p.z = t.z;
-        }
+    if ((ops & XPBD_APPLY_PIN) && (f & XPBD_VF_PIN) && pin.w != 0.f) {
+        p.x = pin.x;
+        p.y = pin.y;
+        p.z = pin.z;
     }
+}
+
+// The finish with the vertex data read from global memory.
+__device__ __forceinline__ void finish_vertex(const XpbdParams& prm, const XpbdVerts& V, int g, float4& p, float4 a,
+                                              uint32_t ops) {
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int f = V.vflags ? V.vflags[g] : 0;
+    float4 at = z, prevp = z, pin = z;
+    if ((ops & XPBD_APPLY_ATTACH) && (f & XPBD_VF_ATTACH_MASK) && (f & XPBD_VF_ATTACH_MASK) <= prm.n_attach_materials) {
+        at = reinterpret_cast<const float4*>(V.attach_target)[g];
+        if (prm.attach[(f & XPBD_VF_ATTACH_MASK) - 1].damp > 0.f) prevp = reinterpret_cast<const float4*>(V.pprev)[g];
+    }
+    if ((ops & XPBD_APPLY_PIN) && (f & XPBD_VF_PIN)) pin = reinterpret_cast<const float4*>(V.pin_target)[g];
+    finish_core(prm, f, at, prevp, pin, p, a, ops);
 }
 
 // ---------------------------------------------------------------------------
@@ -54,7 +63,7 @@ enum { CSET_LIGHT = 0, CSET_VOL = 1, CSET_FULL = 2 };  // ARAP+aniso | +volume |
 // Projects every constraint of the tile's tets from the staged positions
 // (s_pos, s_prev) and adds the Jacobi deltas and counts to the shared
 // accumulators s_ax..s_aw (one thread per tet, strided over the CTA).
-template <bool DAMP, int CSET>
+template <bool DAMP, int CSET, bool PREFETCH = false>
 __device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const XpbdTiles& T, int tile,
                                                   const float4* s_pos, const float4* s_prev, float* s_ax, float* s_ay,
                                                   float* s_az, float* s_aw) {
@@ -62,10 +71,40 @@ __device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const X
     const uint4* tq = reinterpret_cast<const uint4*>(T.tet_q);
     const float4* tb0 = reinterpret_cast<const float4*>(T.tet_b0);
     const float4* tb1 = reinterpret_cast<const float4*>(T.tet_b1);
-    for (int t = T.tile_tptr[tile] + threadIdx.x; t < t1; t += blockDim.x) {
-        const uint4 q = tq[t];
-        const float4 b0 = tb0[t], b1 = tb1[t];
-        const float b2 = T.tet_b2[t];
+    // PREFETCH: the next tet's streams are loaded before this tet is
+    // projected, so their latency overlaps the math (costs registers).
+    int t = T.tile_tptr[tile] + threadIdx.x;
+    uint4 qn = make_uint4(0u, 0u, 0u, 0u);
+    float4 b0n = make_float4(0.f, 0.f, 0.f, 0.f), b1n = b0n;
+    float b2n = 0.f;
+    if (PREFETCH && t < t1) {
+        qn = tq[t];
+        b0n = tb0[t];
+        b1n = tb1[t];
+        b2n = T.tet_b2[t];
+    }
+    for (; t < t1; t += blockDim.x) {
+        uint4 q;
+        float4 b0, b1;
+        float b2;
+        if (PREFETCH) {
+            q = qn;
+            b0 = b0n;
+            b1 = b1n;
+            b2 = b2n;
+            const int tn = t + blockDim.x;
+            if (tn < t1) {
+                qn = tq[tn];
+                b0n = tb0[tn];
+                b1n = tb1[tn];
+                b2n = T.tet_b2[tn];
+            }
+        } else {
+            q = tq[t];
+            b0 = tb0[t];
+            b1 = tb1[t];
+            b2 = T.tet_b2[t];
+        }
         const int l[4] = {int(q.x & 0xffffu), int(q.x >> 16), int(q.y & 0xffffu), int(q.y >> 16)};
         const XpbdMaterial& m = prm.materials[min(int(q.z & 0xffu), XPBD_MAX_MATERIALS - 1)];
         const float V0 = __uint_as_float(q.w);
