@@ -37,6 +37,9 @@ CONFIGS = {
                        "humanv2_synth_535k_tets + 2-level multigrid (2 coarse + 1 fine iterations) + tri-tri DCD "
                        "with per-substep LBVH + SNH fascia"),
 }
+CONFIGS["batched"] = (ROOT / "rlmusclev2_b200" / "configs" / "batched_256.json",
+                      "batched_256_box_muscles_3.5M_tets (256 independent instances, per-instance 64^3 SDF and "
+                      "activation schedule, 10 substeps x 1 Jacobi iteration)")
 CONFIG = CONFIGS["humanv2"][0]
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC = ROOT / "profiles" / "ncu_traffic.json"
@@ -239,7 +242,21 @@ def run_ours(args):
     world, rank, local = _dist_setup()
     torch.cuda.set_device(local)
     cfg = load_config(str(CONFIG))
-    sim = MultiGridSim(cfg, device=f"cuda:{local}")
+    batched = args.config == "batched"
+    tuned = None
+    if batched:
+        # instances sharded over the ranks by tet count (no collective on the data path)
+        from rlmusclev2_b200.batch import BatchSim
+        sim = BatchSim(cfg, device=f"cuda:{local}", shard=(rank, world) if world > 1 else None)
+        sim.step_frame_inputs(sim.start_frame)
+        tuned = sim.autotune()
+        n_inst_total = int(sim.n_inst)
+        if world > 1:
+            t = torch.tensor([n_inst_total], device=sim.device)
+            torch.distributed.all_reduce(t)
+            n_inst_total = int(t.item())
+    else:
+        sim = MultiGridSim(cfg, device=f"cuda:{local}")
     sc = sim.scene
     nf = args.warmup + args.steps
     frames = [sim.start_frame + f for f in range(nf)]
@@ -249,14 +266,18 @@ def run_ours(args):
     # ---- device-resident inputs: all frames' bone poses and activations on the GPU
     trs = torch.from_numpy(np.stack([sc.bone_transforms(f).reshape(sc.n_bones, 12) for f in frames]).astype(
         np.float32)).to(sim.device)
-    acts_user = torch.from_numpy(np.stack([sc.activation(f) for f in frames])).to(sim.device)
-    perm_d = sim._tet_perm_d
+    if batched:
+        acts_src = torch.from_numpy(np.stack([sc.instance_activation(f) for f in frames])).to(sim.device)
+        act_idx, act_n = sim._tet_inst_lib, sim.NT
+    else:
+        acts_src = torch.from_numpy(np.stack([sc.activation(f) for f in frames])).to(sim.device)
+        act_idx, act_n = sim._tet_perm_d, sim.NT
 
     def frame_resident(i):
         with torch.cuda.stream(stream):
             sim._bone_tr.copy_(trs[i])
-        capi.check(sim._lib.xpbd_gather(sim.NT, 1, C.c_void_p(perm_d.data_ptr()),
-                                        C.c_void_p(acts_user[i].data_ptr()), 1, C.c_void_p(sim._t_act.data_ptr()), 1,
+        capi.check(sim._lib.xpbd_gather(act_n, 1, C.c_void_p(act_idx.data_ptr()),
+                                        C.c_void_p(acts_src[i].data_ptr()), 1, C.c_void_p(sim._t_act.data_ptr()), 1,
                                         sim._sp))
         sim._frame_loaded = frames[i]
         sim.step_frame(frames[i])
@@ -287,20 +308,26 @@ def run_ours(args):
         ms_frame = float(t.item())
 
     # ---- e2e through the public API: host inputs in, positions out, every frame
+    def set_act(f):
+        if batched:
+            sim.set_instance_activation(sc.instance_activation(f))
+        else:
+            sim.set_fiber_activation(sc.activation(f))
+
     for i in range(min(args.warmup, 3)):
-        sim.set_fiber_activation(sc.activation(frames[i]))
+        set_act(frames[i])
         sim.step_frame(frames[i])
         sim.positions_np()
     stream.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    h2d = sim.NT * 4 + sc.n_bones * 12 * 4
+    h2d = (sim.n_inst if batched else sim.NT) * 4 + sc.n_bones * 12 * 4
     d2h = sim.NV * 3 * 4
     evs2 = [(ev(), ev()) for _ in range(args.steps)]
     for k, i in enumerate(range(args.warmup, nf)):
         flush_l2()
         evs2[k][0].record(stream)
-        sim.set_fiber_activation(sc.activation(frames[i]))
+        set_act(frames[i])
         sim.step_frame(frames[i])
         _ = sim.positions_np()
         evs2[k][1].record(stream)
@@ -345,17 +372,20 @@ def run_ours(args):
     pstatus = sim.persistent_status()
     if pstatus:
         raise RuntimeError(f"persistent pass reported status {pstatus}")
-    alg_bytes = L.n_tets * 56 + L.n_verts * 40
+    flags = np.array([int(m["flags"]) for m in L.materials], np.int64)
+    n_aniso = int(((flags[L.tet_material] & capi.MAT_ANISO) != 0).sum())
+    alg_bytes = L.n_tets * 56 + n_aniso * 20 + L.n_verts * 40
     achieved = alg_bytes / (it_ms * 1e-3) / 1e9
     peak, peak_kind = _peak_hbm()
     traffic = None
     try:
         tr = json.loads(TRAFFIC.read_text())
-        traffic = tr.get("bytes_per_iteration")
+        if args.config in tr.get("configs", ["humanv2"]):
+            traffic = tr.get("bytes_per_iteration")
     except Exception:
         pass
     per_iter = 2 + (3 if getattr(sim, "dcd", None) is not None else 0)
-    fine = 1 if persistent else sim.fine_iters * per_iter
+    fine = len(sim._persist) if persistent else sim.fine_iters * per_iter
     coarse = 0
     if sim.mg is not None:
         co = sim.mg.coarse
@@ -367,11 +397,13 @@ def run_ours(args):
     n_iter = sim.nsubsteps * sim.fine_iters
     line = {
         "metric": "ms/frame", "value": round(ms_frame, 4), "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms_frame, 4), "higher_is_better": False, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": round(ms_frame, 4), "higher_is_better": False,
+        "scaling": "strong" if (batched and world > 1) else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD,
                    "n_verts": L.n_verts, "n_tets": L.n_tets, "n_tiles": L.n_tiles, "fine_iterations": sim.fine_iters,
-                   "nsubsteps": sim.nsubsteps, "parallelism": f"replicas x{world}",
+                   "nsubsteps": sim.nsubsteps,
+                   "parallelism": (f"instance shards x{world}" if batched else f"replicas x{world}"),
                    "l2": "flushed before every timed frame (256 MB write); inside a frame the ~37 MB "
                          "per-iteration working set stays in L2 (126 MB)"},
         "substeps_per_s": round(1e3 * sim.nsubsteps / ms_frame, 1),
@@ -385,6 +417,8 @@ def run_ours(args):
                      "algorithmic_bytes": alg_bytes, "iteration_us": round(it_ms * 1e3, 2),
                      "frame_roofline_ms": round(alg_bytes * n_iter / (peak * 1e9) * 1e3, 4)},
         "clocks": clk.summary(),
+        **({"instances": n_inst_total, "instance_substeps_per_s": round(n_inst_total * sim.nsubsteps / (ms_frame * 1e-3), 1),
+            "autotune": {k: v for k, v in tuned.items() if k != "tried"}} if batched else {}),
         "gpu_launches": (launches_per_frame + 1) * args.steps,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config == "humanv2":

@@ -238,6 +238,27 @@ typedef struct XpbdCapsule {
 int xpbd_sdf_bake_capsules(const XpbdSdf* sdf, int32_t n_caps, const XpbdCapsule* caps, const float* transforms,
                            float band, xpbd_stream_t stream);
 
+/* Batched instances (config of many independent meshes packed in one vertex
+ * set): one grid SDF per instance, all grids of nx*ny*nz nodes, grid i at
+ * phi + i*nx*ny*nz with its own origin and cell size. */
+typedef struct XpbdSdfBatch {
+    const float* phi;         /* [n_inst][nz][ny][nx] */
+    const float* frame;       /* [n_inst][4] origin xyz, cell size h */
+    const int32_t* vert_inst; /* [n_verts] instance of each vertex (library order), < 0: no push-out */
+    int32_t n_inst, nx, ny, nz;
+    float contact_offset, max_push;
+} XpbdSdfBatch;
+
+/* Bake every instance's grid from its own caps_per_inst capsules
+ * (caps[i*caps_per_inst ...], transforms [n_inst*caps_per_inst][12] or NULL),
+ * as xpbd_sdf_bake_capsules does for one grid; one launch for all grids. */
+int xpbd_sdf_bake_capsules_batched(const XpbdSdfBatch* sdf, int32_t caps_per_inst, const XpbdCapsule* caps,
+                                   const float* transforms, float band, xpbd_stream_t stream);
+
+/* xpbd_vertex_step with XPBD_OP_SDF reading each vertex's instance grid. */
+int xpbd_vertex_step_batched(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, const XpbdSdfBatch* sdf,
+                             xpbd_stream_t stream);
+
 /* dst[i] = src[idx[i]] for float lanes of width `width` (1..4). */
 int xpbd_gather(int32_t n, int32_t width, const int32_t* idx, const float* src, int32_t src_stride, float* dst,
                 int32_t dst_stride, xpbd_stream_t stream);
@@ -357,6 +378,10 @@ typedef struct XpbdPersist {
     float* ring;             /* [3][n_verts][4] boundary accumulators; all zero before the first call */
     uint32_t* sync;          /* [4] grid barrier count, generation, ring phase, reserved; zero before the first call */
     int32_t* status;         /* [1] XPBD_STATUS_BARRIER_TIMEOUT; after it, zero ring and sync before the next call */
+    int32_t tile_begin, tile_end; /* tiles [tile_begin, tile_end) in this launch (0, 0: all).  A sub-range must
+                                     be closed (no vertex shared with tiles outside it, e.g. whole instances of a
+                                     batch) and keeps its own sync words; vertices in no tet are finished by the
+                                     launch whose range ends at n_tiles */
 } XpbdPersist;
 
 /* n_iters fused Jacobi iterations in ONE cooperative launch: the same
@@ -373,8 +398,9 @@ typedef struct XpbdPersist {
 int xpbd_iterate_persistent(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v,
                             const XpbdPersist* ps, int32_t n_iters, xpbd_stream_t stream);
 /* *fits = 1 when the persistent pass of these materials can hold all tiles
- * resident on the current device. */
-int xpbd_persistent_fits(const XpbdParams* prm, const XpbdTiles* tiles, int32_t* fits);
+ * resident on the current device; *slots (optional) = how many CTAs of it
+ * can be resident at once (the largest tile range one launch can take). */
+int xpbd_persistent_fits(const XpbdParams* prm, const XpbdTiles* tiles, int32_t* fits, int32_t* slots);
 
 /* Stream capture helpers (a captured substep replays as one graph launch). */
 int xpbd_graph_begin(xpbd_stream_t stream);

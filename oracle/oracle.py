@@ -359,7 +359,10 @@ class OracleMultiGridSim(OracleSolver):
         self.contraction = float((fib or {}).get("contraction_ratio", 0.4))
         t = table_from_configs(verts, tets, cons, masks)
         V0, valid = signed_rest_volume(verts, tets)
-        rho = float(cfg["total_mass"]) / float(V0[valid].astype(np.float64).sum())
+        if cfg.get("density") is not None:
+            rho = float(cfg["density"])
+        else:
+            rho = float(cfg["total_mass"]) / float(V0[valid].astype(np.float64).sum())
         rv, B, mass, tot = precompute_rest(verts, tets, rho, prec)
         self.total_rest_volume = tot
         pin = _find(cfg, "muscleToBonePin")
@@ -529,8 +532,7 @@ class OracleMultiGridSim(OracleSolver):
             self.mg_target = self.restrict(self.target, self.mg_target)
         self.apply_pins()
         if self.coll:
-            r = self.sdf_res
-            self.phi = sdf_bake((r, r, r), self.sdf_origin, self.sdf_h, self.caps, T, self.band, self.P.name)
+            self._sdf_bake(T)
         for _ in range(self.nsub):
             self.integrate()
             if self.mg is not None:
@@ -543,10 +545,46 @@ class OracleMultiGridSim(OracleSolver):
                 if self.dcd is not None:
                     self.dcd_solve(it)
             if self.coll:
-                sdf_push(self.pos, self.inv_mass, self.phi, self.sdf_origin, self.sdf_h,
-                         float(self.coll.get("contact_offset", 0.0)), float(self.coll.get("max_push", -1.0)),
-                         self.P.name)
+                self._sdf_push()
             self.update_velocities()
+
+    def _sdf_bake(self, T):
+        r = self.sdf_res
+        self.phi = sdf_bake((r, r, r), self.sdf_origin, self.sdf_h, self.caps, T, self.band, self.P.name)
+
+    def _sdf_push(self):
+        sdf_push(self.pos, self.inv_mass, self.phi, self.sdf_origin, self.sdf_h,
+                 float(self.coll.get("contact_offset", 0.0)), float(self.coll.get("max_push", -1.0)), self.P.name)
+
+
+class OracleBatchSim(OracleMultiGridSim):
+    """The batched-instance program on the oracle: the same substep over a
+    BatchScene, each instance pushed out of its own capsule grid."""
+
+    def __init__(self, cfg, scene, prec="f32", band_cells=3.0):
+        super().__init__(cfg, scene, prec=prec)
+        if self.coll:
+            self.sdf_res = int(scene.sdf_res)
+            self.band = band_cells * float(scene.sdf_frame[:, 3].max())
+
+    def _sdf_bake(self, T):
+        sc, r = self.scene, self.sdf_res
+        self.phis = []
+        for i in range(sc.n_inst):
+            fr = sc.sdf_frame[i].astype(np.float64)
+            self.phis.append(sdf_bake((r, r, r), fr[:3], float(fr[3]), self.caps[2 * i:2 * i + 2],
+                                      T[2 * i:2 * i + 2], self.band, self.P.name))
+
+    def _sdf_push(self):
+        sc = self.scene
+        off, mp = float(self.coll.get("contact_offset", 0.0)), float(self.coll.get("max_push", -1.0))
+        for i in range(sc.n_inst):
+            v0, v1 = int(sc.inst_vptr[i]), int(sc.inst_vptr[i + 1])
+            fr = sc.sdf_frame[i].astype(np.float64)
+            sub = np.ascontiguousarray(self.pos[v0:v1])
+            sdf_push(sub, np.ascontiguousarray(self.inv_mass[v0:v1]), self.phis[i], fr[:3], float(fr[3]), off, mp,
+                     self.P.name)
+            self.pos[v0:v1] = sub
 
 
 # ---- DCD (collision/udcf/kernel.py) on the oracle, FP32 -------------------------

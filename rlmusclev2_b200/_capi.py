@@ -97,8 +97,15 @@ class XpbdMetrics(C.Structure):
                 ("n_inverted", C.c_int32), ("n_nonfinite", C.c_int32), ("reserved", C.c_int32)]
 
 
+class XpbdSdfBatch(C.Structure):
+    _fields_ = [("phi", C.c_void_p), ("frame", C.c_void_p), ("vert_inst", C.c_void_p), ("n_inst", C.c_int32),
+                ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("contact_offset", C.c_float),
+                ("max_push", C.c_float)]
+
+
 class XpbdPersist(C.Structure):
-    _fields_ = [("tile_own", C.c_void_p), ("ring", C.c_void_p), ("sync", C.c_void_p), ("status", C.c_void_p)]
+    _fields_ = [("tile_own", C.c_void_p), ("ring", C.c_void_p), ("sync", C.c_void_p), ("status", C.c_void_p),
+                ("tile_begin", C.c_int32), ("tile_end", C.c_int32)]
 
 
 P = C.c_void_p
@@ -114,6 +121,9 @@ _SIGS = {
     "xpbd_metrics": ([C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), P, P], C.c_int),
     "xpbd_bone_targets": ([C.c_int32, C.c_int32, P, P, P, P, P, P, P], C.c_int),
     "xpbd_sdf_bake_capsules": ([C.POINTER(XpbdSdf), C.c_int32, P, P, C.c_float, P], C.c_int),
+    "xpbd_sdf_bake_capsules_batched": ([C.POINTER(XpbdSdfBatch), C.c_int32, P, P, C.c_float, P], C.c_int),
+    "xpbd_vertex_step_batched": ([C.POINTER(XpbdParams), C.POINTER(XpbdVerts), C.c_uint32, C.POINTER(XpbdSdfBatch),
+                                  P], C.c_int),
     "xpbd_gather": ([C.c_int32, C.c_int32, P, P, C.c_int32, P, C.c_int32, P], C.c_int),
     "xpbd_mg_restrict": ([C.POINTER(XpbdCage), P, P, P, P, P], C.c_int),
     "xpbd_mg_prolong_delta": ([C.POINTER(XpbdCage), P, P, P, P, P, P], C.c_int),
@@ -123,7 +133,8 @@ _SIGS = {
     "xpbd_iterate_noalloc": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), P], C.c_int),
     "xpbd_iterate_persistent": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(XpbdVerts),
                                  C.POINTER(XpbdPersist), C.c_int32, P], C.c_int),
-    "xpbd_persistent_fits": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(C.c_int32)], C.c_int),
+    "xpbd_persistent_fits": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(C.c_int32),
+                              C.POINTER(C.c_int32)], C.c_int),
     "xpbd_graph_begin": ([P], C.c_int),
     "xpbd_graph_end": ([P, C.POINTER(C.c_void_p)], C.c_int),
     "xpbd_graph_launch": ([P, P], C.c_int),

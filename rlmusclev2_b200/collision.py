@@ -23,6 +23,8 @@ from . import _capi as capi
 class GridSdfCollider:
     """Per-frame capsule-bone SDF on a cubic grid plus the push-out hook."""
 
+    graph_safe = True  # bake + push are device launches only (the fused frame may capture them)
+
     def __init__(self, sim, centers, axes, halves, radii, *, res: int = 256, contact_offset: float = 0.0,
                  max_push: float = -1.0, band_cells: float = 3.0, margin: float = 0.02, bbox=None):
         self.sim = sim
@@ -70,6 +72,52 @@ class GridSdfCollider:
     def __call__(self) -> None:
         """Push-out hook (collision_solvers entry, mg/mg.py:1366-1371)."""
         self.sim._vstep_sdf_only(self)
+
+
+class BatchedSdfCollider:
+    """One capsule-bone SDF grid per instance of a batch (its two bones), all
+    baked in one launch; push-out reads each vertex's own grid."""
+
+    graph_safe = True
+
+    def __init__(self, sim, scene, *, contact_offset: float = 0.0, max_push: float = -1.0, band_cells: float = 3.0):
+        self.sim = sim
+        self.device = sim.device
+        n = scene.n_inst
+        self.caps_per_inst = 2
+        caps = (capi.XpbdCapsule * (2 * n))()
+        for i in range(2 * n):
+            caps[i].center[:] = [float(x) for x in scene.bone_center[i]]
+            caps[i].axis[:] = [float(x) for x in scene.bone_axis[i]]
+            caps[i].half = float(scene.bone_half[i])
+            caps[i].radius = float(scene.bone_radius[i])
+        self._caps = torch.frombuffer(bytearray(bytes(caps)), dtype=torch.uint8).to(self.device)
+        self.res = int(scene.sdf_res)
+        self.frame = torch.from_numpy(np.ascontiguousarray(scene.sdf_frame, np.float32)).to(self.device)
+        self.band = float(band_cells) * float(scene.sdf_frame[:, 3].max())
+        self.phi = torch.empty((n, self.res, self.res, self.res), dtype=torch.float32, device=self.device)
+        L = sim.layout
+        self.vert_inst = torch.from_numpy(np.ascontiguousarray(scene.vert_inst[L.perm], np.int32)).to(self.device)
+        s = capi.XpbdSdfBatch()
+        s.phi, s.frame, s.vert_inst = self.phi.data_ptr(), self.frame.data_ptr(), self.vert_inst.data_ptr()
+        s.n_inst, s.nx, s.ny, s.nz = n, self.res, self.res, self.res
+        s.contact_offset, s.max_push = float(contact_offset), float(max_push)
+        self._s = s
+        self.transforms = None  # device (2 n_inst, 12) or None = rest pose
+
+    def struct(self) -> capi.XpbdSdfBatch:
+        return self._s
+
+    def bake(self) -> None:
+        tr = None if self.transforms is None else C.c_void_p(self.transforms.data_ptr())
+        capi.check(self.sim._lib.xpbd_sdf_bake_capsules_batched(C.byref(self._s), self.caps_per_inst,
+                                                                C.c_void_p(self._caps.data_ptr()), tr,
+                                                                C.c_float(self.band), self.sim._sp))
+
+    def __call__(self) -> None:
+        """Push-out hook (collision_solvers entry)."""
+        self.sim._sdf = self
+        self.sim._vstep(capi.OP_SDF)
 
 
 # ----------------------------------------------------------------------------

@@ -184,11 +184,8 @@ __device__ __forceinline__ void sdf_push(const XpbdSdf& S, float4& p) {
     }
 }
 
-__global__ void __launch_bounds__(kVertThreads)
-    k_vertex_step(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdVerts V, uint32_t ops,
-                  const __grid_constant__ XpbdSdf S) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= V.n) return;
+__device__ __forceinline__ void vertex_step_at(const XpbdParams& prm, const XpbdVerts& V, uint32_t ops,
+                                               const XpbdSdf& S, int g) {
     float4* pos4 = reinterpret_cast<float4*>(V.pos);
     float4* prev4 = reinterpret_cast<float4*>(V.pprev);
     float4* vel4 = reinterpret_cast<float4*>(V.vel);
@@ -239,6 +236,44 @@ __global__ void __launch_bounds__(kVertThreads)
     }
     pos4[g] = p;
     if (ops & (XPBD_OP_VELOCITY | XPBD_OP_PREDICT)) vel4[g] = v;
+}
+
+__global__ void __launch_bounds__(kVertThreads)
+    k_vertex_step(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdVerts V, uint32_t ops,
+                  const __grid_constant__ XpbdSdf S) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= V.n) return;
+    vertex_step_at(prm, V, ops, S, g);
+}
+
+// Batched instances: each vertex is pushed out of its own instance's grid.
+__global__ void __launch_bounds__(kVertThreads)
+    k_vertex_step_batched(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdVerts V, uint32_t ops,
+                          const __grid_constant__ XpbdSdfBatch B) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= V.n) return;
+    XpbdSdf S;
+    S.nx = B.nx;
+    S.ny = B.ny;
+    S.nz = B.nz;
+    S.contact_offset = B.contact_offset;
+    S.max_push = B.max_push;
+    S.reserved = 0;
+    const int inst = (ops & XPBD_OP_SDF) ? B.vert_inst[g] : -1;
+    if (inst >= 0 && inst < B.n_inst) {
+        const float4 fr = reinterpret_cast<const float4*>(B.frame)[inst];
+        S.phi = B.phi + size_t(inst) * size_t(B.nx) * size_t(B.ny) * size_t(B.nz);
+        S.origin[0] = fr.x;
+        S.origin[1] = fr.y;
+        S.origin[2] = fr.z;
+        S.h = fr.w;
+    } else {
+        S.phi = nullptr;
+        S.origin[0] = S.origin[1] = S.origin[2] = 0.f;
+        S.h = 1.f;
+        ops &= ~uint32_t(XPBD_OP_SDF);
+    }
+    vertex_step_at(prm, V, ops, S, g);
 }
 
 __global__ void k_pin_masked(int n, const int32_t* pts, const float* target, const float* offset,
@@ -326,7 +361,7 @@ int check_params(const XpbdParams* p) {
         p->n_attach_materials > XPBD_MAX_ATTACH_MATERIALS)
         return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range");
     if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0");
-    if (p->tile_variant < 0 || p->tile_variant > 3) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..3");
+    if (p->tile_variant < 0 || p->tile_variant > 7) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..7");
     return XPBD_OK;
 }
 int check_tiles(const XpbdTiles* t) {
@@ -413,6 +448,25 @@ int xpbd_vertex_step(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, co
     if (sdf) S = *sdf;
     k_vertex_step<<<(v->n + kVertThreads - 1) / kVertThreads, kVertThreads, 0, (cudaStream_t)stream>>>(*prm, *v, ops, S);
     return cuda_check("xpbd_vertex_step");
+}
+
+int xpbd_vertex_step_batched(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, const XpbdSdfBatch* sdf,
+                             xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_params(prm)) || (rc = check_verts(v))) return rc;
+    if ((ops & XPBD_OP_SDF) && (!sdf || !sdf->phi || !sdf->frame || !sdf->vert_inst || sdf->n_inst < 1 ||
+                                sdf->nx < 2 || sdf->ny < 2 || sdf->nz < 2))
+        return fail(XPBD_ERR_ARG, "xpbd_vertex_step_batched: XPBD_OP_SDF needs a valid XpbdSdfBatch");
+    if ((ops & XPBD_OP_SDF) && !aligned16(sdf->frame)) return fail(XPBD_ERR_ALIGN, "xpbd_vertex_step_batched: frame");
+    if ((ops & (XPBD_OP_VELOCITY | XPBD_OP_PREDICT)) && (!v->pprev || !v->vel))
+        return fail(XPBD_ERR_ARG, "xpbd_vertex_step_batched: pprev/vel required");
+    if ((ops & XPBD_OP_PREDICT) && !v->mass) return fail(XPBD_ERR_ARG, "xpbd_vertex_step_batched: mass required");
+    XpbdSdfBatch B;
+    memset(&B, 0, sizeof(B));
+    if (sdf) B = *sdf;
+    k_vertex_step_batched<<<(v->n + kVertThreads - 1) / kVertThreads, kVertThreads, 0, (cudaStream_t)stream>>>(
+        *prm, *v, ops, B);
+    return cuda_check("xpbd_vertex_step_batched");
 }
 
 int xpbd_project(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v, int32_t mode,

@@ -62,12 +62,12 @@ __global__ void __launch_bounds__(kThreads, MINB)
     k_iterate_persistent(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdTiles T,
                          const __grid_constant__ XpbdVerts V, const __grid_constant__ XpbdPersist P, int n_iters) {
     extern __shared__ float4 smem[];
-    const int tile = blockIdx.x;
+    const int tile = P.tile_begin + int(blockIdx.x);
     const int vbeg = T.tile_vptr[tile];
     const int nvt = T.tile_vptr[tile + 1] - vbeg;
     const int nint = T.tile_nint[tile];
     const int own_lo = P.tile_own[tile], own_hi = P.tile_own[tile + 1];
-    const int orph_lo = P.tile_own[T.n_tiles];
+    const int orph_lo = P.tile_end == T.n_tiles ? P.tile_own[T.n_tiles] : V.n;  // last range only
     // Shared layout per tile vertex: position, previous position, attach
     // target, pin target (float4 each), the four accumulator floats, the
     // global id and the vertex flags: 88 bytes.  Everything but the position
@@ -166,14 +166,16 @@ int launch_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, cons
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem) != cudaSuccess)
         return cuda_check("xpbd_iterate_persistent: occupancy");
-    const bool ok = int64_t(per_sm) * n_sm >= T->n_tiles;
+    const int64_t slots = int64_t(per_sm) * n_sm;
     if (query_only) {
-        *fits = ok ? 1 : 0;
+        fits[0] = slots >= T->n_tiles ? 1 : 0;
+        fits[1] = int(slots);
         return XPBD_OK;
     }
-    if (!ok) return fail(XPBD_ERR_LIMIT, "xpbd_iterate_persistent: tiles exceed the resident CTA slots");
+    const int ntl = P->tile_end - P->tile_begin;
+    if (ntl > slots) return fail(XPBD_ERR_LIMIT, "xpbd_iterate_persistent: tiles exceed the resident CTA slots");
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(T->n_tiles);
+    cfg.gridDim = dim3(ntl);
     cfg.blockDim = dim3(kThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
@@ -223,6 +225,10 @@ extern "C" int xpbd_iterate_persistent(const XpbdParams* prm, const XpbdTiles* t
         return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: tiles/verts");
     if (!ps->tile_own || !ps->ring || !ps->sync || !ps->status)
         return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: XpbdPersist pointers");
+    XpbdPersist P = *ps;
+    if (P.tile_begin == 0 && P.tile_end == 0) P.tile_end = tiles->n_tiles;
+    if (P.tile_begin < 0 || P.tile_end > tiles->n_tiles || P.tile_begin >= P.tile_end)
+        return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: tile range");
     if (!aligned16(v->pos) || !aligned16(ps->ring)) return fail(XPBD_ERR_ALIGN, "xpbd_iterate_persistent: alignment");
     if (tiles->max_tile_verts > XPBD_MAX_TILE_VERTS) return fail(XPBD_ERR_LIMIT, "xpbd_iterate_persistent: tile size");
     if (prm->n_materials < 1 || prm->n_materials > XPBD_MAX_MATERIALS)
@@ -235,13 +241,16 @@ extern "C" int xpbd_iterate_persistent(const XpbdParams* prm, const XpbdTiles* t
     if (aniso && (!tiles->tet_fiber || !tiles->tet_act))
         return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: aniso materials need tet_fiber and tet_act");
     if (damp && !v->pprev) return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: damped materials need pprev");
-    return dispatch(prm, tiles, v, ps, n_iters, (cudaStream_t)stream, false, nullptr);
+    return dispatch(prm, tiles, v, &P, n_iters, (cudaStream_t)stream, false, nullptr);
 }
 
-extern "C" int xpbd_persistent_fits(const XpbdParams* prm, const XpbdTiles* tiles, int32_t* fits) {
+extern "C" int xpbd_persistent_fits(const XpbdParams* prm, const XpbdTiles* tiles, int32_t* fits, int32_t* slots) {
     if (!prm || !tiles || !fits) return fail(XPBD_ERR_ARG, "xpbd_persistent_fits: null argument");
-    int f = 0;
-    const int rc = dispatch(prm, tiles, nullptr, nullptr, 0, nullptr, true, &f);
-    *fits = f;
+    if (prm->n_materials < 1 || prm->n_materials > XPBD_MAX_MATERIALS)
+        return fail(XPBD_ERR_ARG, "xpbd_persistent_fits: n_materials");
+    int f[2] = {0, 0};
+    const int rc = dispatch(prm, tiles, nullptr, nullptr, 0, nullptr, true, f);
+    *fits = f[0];
+    if (slots) *slots = f[1];
     return rc;
 }

@@ -61,13 +61,10 @@ __device__ __forceinline__ float cap_phi(const CapW& c, float3 x) {
 // One CTA per 8x8x8 brick of grid nodes: the brick keeps only the capsules
 // whose distance to its centre is within band + the brick's half diagonal,
 // then every node takes the min over that short list (band elsewhere).
-__global__ void __launch_bounds__(512) k_sdf_bake(const __grid_constant__ XpbdSdf S, int nc,
-                                                  const XpbdCapsule* __restrict__ caps,
-                                                  const float* __restrict__ tr, float band) {
-    __shared__ CapW s_cap[kMaxCaps];
-    __shared__ int s_n;
-    const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
-    if (threadIdx.x == 0) s_n = 0;
+__device__ __forceinline__ void bake_brick(const XpbdSdf& S, int bx, int by, int bz, int nc,
+                                           const XpbdCapsule* __restrict__ caps, const float* __restrict__ tr,
+                                           float band, CapW* s_cap, int* s_n) {
+    if (threadIdx.x == 0) *s_n = 0;
     __syncthreads();
     const float hb = 0.5f * S.h * float(kBrick - 1);
     const float3 bc = make_float3(S.origin[0] + S.h * float(bx * kBrick) + hb, S.origin[1] + S.h * float(by * kBrick) + hb,
@@ -89,12 +86,12 @@ __global__ void __launch_bounds__(512) k_sdf_bake(const __grid_constant__ XpbdSd
         }
         CapW w{a, b, K.radius};
         if (cap_phi(w, bc) <= band + brad) {
-            const int k = atomicAdd(&s_n, 1);
+            const int k = atomicAdd(s_n, 1);
             if (k < kMaxCaps) s_cap[k] = w;
         }
     }
     __syncthreads();
-    const int ncand = min(s_n, kMaxCaps);
+    const int ncand = min(*s_n, kMaxCaps);
     const int lx = threadIdx.x & 7, ly = (threadIdx.x >> 3) & 7, lz = threadIdx.x >> 6;
     const int ix = bx * kBrick + lx, iy = by * kBrick + ly, iz = bz * kBrick + lz;
     if (ix >= S.nx || iy >= S.ny || iz >= S.nz) return;
@@ -102,6 +99,39 @@ __global__ void __launch_bounds__(512) k_sdf_bake(const __grid_constant__ XpbdSd
     float phi = band;
     for (int k = 0; k < ncand; ++k) phi = fminf(phi, cap_phi(s_cap[k], x));
     const_cast<float*>(S.phi)[(size_t(iz) * S.ny + iy) * S.nx + ix] = phi;
+}
+
+__global__ void __launch_bounds__(512) k_sdf_bake(const __grid_constant__ XpbdSdf S, int nc,
+                                                  const XpbdCapsule* __restrict__ caps,
+                                                  const float* __restrict__ tr, float band) {
+    __shared__ CapW s_cap[kMaxCaps];
+    __shared__ int s_n;
+    bake_brick(S, blockIdx.x, blockIdx.y, blockIdx.z, nc, caps, tr, band, s_cap, &s_n);
+}
+
+// Batched: blockIdx.z runs over (instance, brick z); instance i bakes its own
+// grid from its own capsules caps[i * cpi .. (i + 1) * cpi).
+__global__ void __launch_bounds__(512) k_sdf_bake_batched(const __grid_constant__ XpbdSdfBatch B, int cpi,
+                                                          const XpbdCapsule* __restrict__ caps,
+                                                          const float* __restrict__ tr, float band, int nbz) {
+    __shared__ CapW s_cap[kMaxCaps];
+    __shared__ int s_n;
+    const int inst = blockIdx.z / nbz, bz = blockIdx.z % nbz;
+    const float4 fr = reinterpret_cast<const float4*>(B.frame)[inst];
+    XpbdSdf S;
+    S.phi = B.phi + size_t(inst) * size_t(B.nx) * size_t(B.ny) * size_t(B.nz);
+    S.nx = B.nx;
+    S.ny = B.ny;
+    S.nz = B.nz;
+    S.origin[0] = fr.x;
+    S.origin[1] = fr.y;
+    S.origin[2] = fr.z;
+    S.h = fr.w;
+    S.contact_offset = B.contact_offset;
+    S.max_push = B.max_push;
+    S.reserved = 0;
+    bake_brick(S, blockIdx.x, blockIdx.y, bz, cpi, caps + size_t(inst) * cpi, tr ? tr + size_t(inst) * cpi * 12 : nullptr,
+               band, s_cap, &s_n);
 }
 
 __global__ void k_gather(int n, int width, const int32_t* __restrict__ idx, const float* __restrict__ src, int ss,
@@ -141,6 +171,22 @@ int xpbd_sdf_bake_capsules(const XpbdSdf* sdf, int32_t n_caps, const XpbdCapsule
     dim3 grid((sdf->nx + kBrick - 1) / kBrick, (sdf->ny + kBrick - 1) / kBrick, (sdf->nz + kBrick - 1) / kBrick);
     k_sdf_bake<<<grid, kBrick * kBrick * kBrick, 0, (cudaStream_t)stream>>>(*sdf, n_caps, caps, transforms, band);
     return cuda_check("xpbd_sdf_bake_capsules");
+}
+
+int xpbd_sdf_bake_capsules_batched(const XpbdSdfBatch* sdf, int32_t caps_per_inst, const XpbdCapsule* caps,
+                                   const float* transforms, float band, xpbd_stream_t stream) {
+    if (!sdf || !sdf->phi || !sdf->frame || sdf->n_inst < 1 || sdf->nx < 2 || sdf->ny < 2 || sdf->nz < 2 ||
+        !(band > 0.f))
+        return fail(XPBD_ERR_ARG, "xpbd_sdf_bake_capsules_batched: bad grid");
+    if (!aligned16(sdf->frame)) return fail(XPBD_ERR_ALIGN, "xpbd_sdf_bake_capsules_batched: frame alignment");
+    if (caps_per_inst < 0 || caps_per_inst > kMaxCaps || (caps_per_inst > 0 && !caps))
+        return fail(XPBD_ERR_LIMIT, "xpbd_sdf_bake_capsules_batched: 0 <= caps_per_inst <= 256 required");
+    const int nbz = (sdf->nz + kBrick - 1) / kBrick;
+    if (int64_t(nbz) * sdf->n_inst > 65535) return fail(XPBD_ERR_LIMIT, "xpbd_sdf_bake_capsules_batched: too many grids");
+    dim3 grid((sdf->nx + kBrick - 1) / kBrick, (sdf->ny + kBrick - 1) / kBrick, nbz * sdf->n_inst);
+    k_sdf_bake_batched<<<grid, kBrick * kBrick * kBrick, 0, (cudaStream_t)stream>>>(*sdf, caps_per_inst, caps,
+                                                                                   transforms, band, nbz);
+    return cuda_check("xpbd_sdf_bake_capsules_batched");
 }
 
 int xpbd_gather(int32_t n, int32_t width, const int32_t* idx, const float* src, int32_t src_stride, float* dst,

@@ -52,7 +52,7 @@ class XpbdEngine:
                       v_fiber: np.ndarray | None, tet_tendonmask: np.ndarray | None, dt: float,
                       gravity_vec, veldamping: float, quasi_static: bool, omega: float = 1.0,
                       contraction_ratio: float = 0.0, fiber_stiffness_scale: float = 1.0,
-                      tile_tets: int | None = None, stream=None) -> None:
+                      tile_tets: int | None = None, stream=None, vert_group: np.ndarray | None = None) -> None:
         self._lib = capi.load()
         self.device = torch.device(device)
         if self.device.type != "cuda":
@@ -67,7 +67,8 @@ class XpbdEngine:
         self.cons_ranges = dict(table.cons_ranges)
         L = build_layout(self.pos0_np, self.tet_np, table, tile_tets=tile_tets, v_fiber=v_fiber,
                          tet_tendonmask=tet_tendonmask,
-                         n_sm=torch.cuda.get_device_properties(self.device).multi_processor_count)
+                         n_sm=torch.cuda.get_device_properties(self.device).multi_processor_count,
+                         vert_group=vert_group)
         self.layout: TileLayout = L
         dev = self.device
         f32 = torch.float32
@@ -211,16 +212,33 @@ class XpbdEngine:
         else:
             to.n_boundary = 0
         self._tiles_orph = to
-        ps = capi.XpbdPersist()
-        ps.tile_own, ps.ring, ps.sync, ps.status = _ptr(self._t_own), _ptr(self._ring), _ptr(self._psync), _ptr(
-            self._pstatus)
-        self._persist = ps
-        fits = C.c_int32(0)
-        capi.check(self._lib.xpbd_persistent_fits(C.byref(self._prm), C.byref(t), C.byref(fits)))
-        self._persist_fits = bool(fits.value)
+        fits, slots = C.c_int32(0), C.c_int32(0)
+        capi.check(self._lib.xpbd_persistent_fits(C.byref(self._prm), C.byref(t), C.byref(fits), C.byref(slots)))
+        self._persist_slots = int(slots.value)
+        self._build_persist(self._persist_slots)
         for g in self._graphs.values():
             capi.check(self._lib.xpbd_graph_destroy(g))
         self._graphs = {}
+
+    def _build_persist(self, slots: int) -> None:
+        """Persistent-pass launch descriptors for tile ranges of at most
+        ``slots`` tiles (one set of barrier words per range)."""
+        ranges = self._persist_ranges(int(slots))
+        if 4 * len(ranges) > self._psync.numel():
+            self._psync = torch.zeros(4 * len(ranges), dtype=torch.int32, device=self.device)
+        # a vertex's ring slots follow its range's phase word: start all over
+        with torch.cuda.stream(self._stream):
+            self._ring.zero_()
+            self._psync.zero_()
+        self._stream.synchronize()
+        self._persist = []
+        for k, (b, e) in enumerate(ranges):
+            ps = capi.XpbdPersist()
+            ps.tile_own, ps.ring, ps.status = _ptr(self._t_own), _ptr(self._ring), _ptr(self._pstatus)
+            ps.sync = self._psync.data_ptr() + 16 * k
+            ps.tile_begin, ps.tile_end = b, e
+            self._persist.append(ps)
+        self._persist_fits = bool(ranges)
 
     # -------------------------------------------------------------- launches
     def _vstep(self, ops: int) -> None:
@@ -258,15 +276,37 @@ class XpbdEngine:
         self._project(capi.PROJECT_FUSED)
         self._apply_boundary(capi.APPLY_ATTACH | capi.APPLY_DIVIDE | capi.APPLY_PIN | capi.APPLY_CLEAR)
 
+    def _persist_ranges(self, slots: int) -> list[tuple[int, int]]:
+        """Tile ranges of the persistent pass: all tiles when they fit in the
+        resident CTA slots; for a layout of independent vertex groups, runs of
+        whole groups of at most ``slots`` tiles each; [] when neither works."""
+        L = self.layout
+        if slots <= 0:
+            return []
+        if L.n_tiles <= slots:
+            return [(0, L.n_tiles)]
+        if L.tile_group is None:
+            return []
+        starts = np.r_[0, np.nonzero(np.diff(L.tile_group))[0] + 1, L.n_tiles]
+        ranges, b = [], 0
+        for e0, e1 in zip(starts[:-1], starts[1:]):
+            if e1 - e0 > slots:
+                return []
+            if e1 - b > slots:
+                ranges.append((b, int(e0)))
+                b = int(e0)
+        ranges.append((b, L.n_tiles))
+        return ranges
+
     def _fused_iterations(self, n: int) -> None:
-        """n fused iterations: one persistent cooperative launch when all tiles
-        fit on the GPU at once, else n x _fused_iteration()."""
+        """n fused iterations: one persistent cooperative launch per tile range
+        when the tiles fit on the GPU at once, else n x _fused_iteration()."""
         if n <= 0:
             return
         if self.use_persistent and self._persist_fits and self.fused_mode == capi.PROJECT_FUSED:
-            capi.check(self._lib.xpbd_iterate_persistent(C.byref(self._prm), C.byref(self._tiles),
-                                                         C.byref(self._verts), C.byref(self._persist), int(n),
-                                                         self._sp))
+            for ps in self._persist:
+                capi.check(self._lib.xpbd_iterate_persistent(C.byref(self._prm), C.byref(self._tiles),
+                                                             C.byref(self._verts), C.byref(ps), int(n), self._sp))
             return
         for _ in range(n):
             self._fused_iteration()

@@ -63,6 +63,7 @@ class TileLayout:
     materials: list           # list of dicts (XpbdMaterial fields)
     tet_material: np.ndarray  # (NT,) material id per new tet
     tile_own: np.ndarray | None = None  # (n_tiles+1,) tile k owns new ids [tile_own[k], tile_own[k+1])
+    tile_group: np.ndarray | None = None  # (n_tiles,) group of each tile when built with vert_group
 
     @property
     def n_tiles(self) -> int:
@@ -155,9 +156,27 @@ def fiber_f0(v_fiber: np.ndarray, tets: np.ndarray) -> np.ndarray:
     return out
 
 
+def _grouped_codes(x: np.ndarray, group: np.ndarray | None, lo: np.ndarray, hi: np.ndarray) -> np.ndarray:
+    """Morton codes over the whole box, or with ``group``: (group, Morton
+    code over the group's own box), so each group stays contiguous."""
+    if group is None:
+        return morton_codes(x, lo, hi)
+    ng = int(group.max()) + 1
+    glo = np.full((ng, 3), np.inf, np.float64)
+    ghi = np.full((ng, 3), -np.inf, np.float64)
+    np.minimum.at(glo, group, x)
+    np.maximum.at(ghi, group, x)
+    codes = morton_codes(x.astype(np.float64), glo[group], ghi[group])
+    return (group.astype(np.uint64) << np.uint64(30)) | codes
+
+
 def build_layout(pos0: np.ndarray, tets: np.ndarray, table: ConstraintTable, *, tile_tets: int | None = None,
                  v_fiber: np.ndarray | None = None, tet_tendonmask: np.ndarray | None = None,
-                 n_sm: int = 148) -> TileLayout:
+                 n_sm: int = 148, vert_group: np.ndarray | None = None) -> TileLayout:
+    """``vert_group`` (optional, per vertex): independent meshes packed in one
+    vertex set (batched instances).  Tets are then ordered by group first and
+    no tile spans two groups, so any run of whole groups is a closed set of
+    tiles (no shared vertices with the other tiles)."""
     pos0 = np.asarray(pos0, np.float32)
     tets = np.asarray(tets, np.int64)
     nv, nt = pos0.shape[0], tets.shape[0]
@@ -167,14 +186,27 @@ def build_layout(pos0: np.ndarray, tets: np.ndarray, table: ConstraintTable, *, 
     if tile_tets is None:
         tile_tets = default_tile_tets(nt, n_sm, ctas_per_sm(mats))
     lo, hi = pos0.min(0), pos0.max(0)
-    # 1. tets in Morton order of their centroid
+    vgroup = None if vert_group is None else np.asarray(vert_group, np.int64)
+    tgroup = None if vgroup is None else vgroup[tets[:, 0]]
+    if tgroup is not None and not (vgroup[tets] == tgroup[:, None]).all():
+        raise ValueError("a tet spans two vertex groups")
+    # 1. tets in Morton order of their centroid (within their group)
     cent = pos0[tets].mean(axis=1)
-    tet_perm = np.argsort(morton_codes(cent, lo, hi), kind="stable")
+    tet_perm = np.argsort(_grouped_codes(cent, tgroup, lo, hi), kind="stable")
     tet_inv = np.empty(nt, np.int64)
     tet_inv[tet_perm] = np.arange(nt)
     tets_s = tets[tet_perm]
-    # 2. tiles of consecutive tets; split any tile whose vertex set would not fit
-    bounds = list(range(0, nt, tile_tets)) + [nt]
+    # 2. tiles of consecutive tets (cut at group starts, equal tiles within a
+    # group); split any tile whose vertex set would not fit
+    if tgroup is None:
+        bounds = list(range(0, nt, tile_tets)) + [nt]
+    else:
+        gs = tgroup[tet_perm]
+        starts = np.r_[0, np.nonzero(np.diff(gs))[0] + 1, nt]
+        bounds = [0]
+        for a, b in zip(starts[:-1], starts[1:]):
+            k = int(np.ceil((b - a) / tile_tets))
+            bounds += [int(a + (b - a) * j // k) for j in range(1, k + 1)]
     tptr = [0]
     for a, b in zip(bounds[:-1], bounds[1:]):
         s = a
@@ -212,7 +244,7 @@ def build_layout(pos0: np.ndarray, tets: np.ndarray, table: ConstraintTable, *, 
     np.minimum.at(first_tile, u_v, u_tile)
     bnd = ntile_of_v > 1
     # 4. vertex renumbering: (first tile, interior before boundary, Morton)
-    vm = morton_codes(pos0, lo, hi)
+    vm = _grouped_codes(pos0, vgroup, lo, hi)
     perm = np.lexsort((vm, bnd.astype(np.int64), first_tile))
     inv = np.empty(nv, np.int64)
     inv[perm] = np.arange(nv)
@@ -258,4 +290,5 @@ def build_layout(pos0: np.ndarray, tets: np.ndarray, table: ConstraintTable, *, 
         tet_q=tet_q, tet_b0=tet_b0, tet_b1=tet_b1, tet_b2=tet_b2, tet_fiber=tet_fiber,
         vert_ntiles=ntile_of_v[perm].astype(np.int32), orphans=np.nonzero(ntile_of_v[perm] == 0)[0].astype(np.int32),
         materials=mats, tet_material=mat_of_user_tet[tet_perm].astype(np.int32),
-        tile_own=np.searchsorted(first_tile[perm], np.arange(n_tiles + 1)).astype(np.int32))
+        tile_own=np.searchsorted(first_tile[perm], np.arange(n_tiles + 1)).astype(np.int32),
+        tile_group=None if tgroup is None else tgroup[tet_perm][tile_tptr[:-1]].astype(np.int32))

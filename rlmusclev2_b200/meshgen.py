@@ -234,15 +234,17 @@ class Scene:
         the identity at the start frame (targets bind to the rest pose there)."""
         tr = self.traj
         f = float(frame) - float(tr.get("start_frame", 1))
+        ang = tr["rot_amp"] * (np.sin(tr["rot_w"] * f + tr["rot_phase"]) - np.sin(tr["rot_phase"]))
+        a = tr["rot_axis"] / np.linalg.norm(tr["rot_axis"], axis=1, keepdims=True)
+        K = np.zeros((a.shape[0], 3, 3))
+        K[:, 0, 1], K[:, 0, 2], K[:, 1, 2] = -a[:, 2], a[:, 1], -a[:, 0]
+        K[:, 1, 0], K[:, 2, 0], K[:, 2, 1] = a[:, 2], -a[:, 1], a[:, 0]
+        R = np.eye(3) + np.sin(ang)[:, None, None] * K + (1.0 - np.cos(ang))[:, None, None] * (K @ K)
+        d = (tr["tr_amp"] * (np.sin(tr["tr_w"] * f + tr["tr_phase"]) - np.sin(tr["tr_phase"])))[:, None] * tr["tr_dir"]
+        c = np.asarray(self.bone_center, np.float64)
         out = np.zeros((self.n_bones, 3, 4))
-        for b in range(self.n_bones):
-            ang = tr["rot_amp"][b] * (np.sin(tr["rot_w"][b] * f + tr["rot_phase"][b]) - np.sin(tr["rot_phase"][b]))
-            R = axis_angle(tr["rot_axis"][b], ang)
-            d = tr["tr_amp"][b] * (np.sin(tr["tr_w"][b] * f + tr["tr_phase"][b]) - np.sin(tr["tr_phase"][b])) \
-                * tr["tr_dir"][b]
-            c = self.bone_center[b]
-            out[b, :, :3] = R
-            out[b, :, 3] = c + d - R @ c
+        out[:, :, :3] = R
+        out[:, :, 3] = c + d - np.einsum("bij,bj->bi", R, c)
         return out
 
     def targets(self, frame: float) -> np.ndarray:
@@ -534,3 +536,159 @@ def build_cage(scene: "Scene", spacing: float = 0.016, rel_lam: float = 1e-3) ->
                 uvw=uvw.astype(np.float32), minv_flat=np.concatenate(flat).astype(np.float32),
                 blk_base=np.asarray(blk_base, np.int32), blk_dim=np.asarray(blk_dim, np.int32),
                 blk_matoff=np.asarray(blk_matoff, np.int32), mg_fine_nv=nv, lam=lam)
+
+
+# --------------------------------------------------------------------------
+# Batched instances: many independent box muscles in one vertex set
+
+
+@dataclass
+class BatchScene(Scene):
+    """``n_inst`` independent box muscles packed back to back (CSR offsets
+    inst_vptr / inst_tptr into verts / tets), each placed in its own cell of
+    a square grid in x-z, with two capsule bones at its two ends (bones 2i and
+    2i+1), a 64^3-class SDF grid frame of its own (sdf_frame: origin xyz, h)
+    and a piecewise-linear activation schedule (act_knots[i, k] at frame
+    1 + k * knot_every)."""
+    inst_vptr: np.ndarray | None = None
+    inst_tptr: np.ndarray | None = None
+    vert_inst: np.ndarray | None = None
+    tet_inst: np.ndarray | None = None
+    act_knots: np.ndarray | None = None
+    knot_every: int = 8
+    sdf_frame: np.ndarray | None = None
+    sdf_res: int = 64
+
+    @property
+    def n_inst(self) -> int:
+        return int(self.inst_vptr.shape[0] - 1)
+
+    def instance_activation(self, frame: int) -> np.ndarray:
+        """(n_inst,) activation of every instance at ``frame``: linear between
+        knots, held at the last knot."""
+        f = (float(frame) - 1.0) / float(self.knot_every)
+        k = int(np.clip(np.floor(f), 0, self.act_knots.shape[1] - 2))
+        u = float(np.clip(f - k, 0.0, 1.0))
+        return ((1.0 - u) * self.act_knots[:, k] + u * self.act_knots[:, k + 1]).astype(np.float32)
+
+    def activation(self, frame: int, start: int = 1, end: int = 50) -> np.ndarray:
+        """Per-tet activation (user tet order) of the instance schedules."""
+        return self.instance_activation(frame)[self.tet_inst]
+
+
+def batched_box_scene(n_inst: int = 256, seed: int = 120, tets_lo: int = 2000, tets_hi: int = 60000,
+                      spacing: float = 0.0025, jitter: float = 0.0002, pin_frac: float = 0.05,
+                      n_knots: int = 8, knot_every: int = 8, sdf_res: int = 64) -> BatchScene:
+    """``n_inst`` box muscles with tet counts log-uniform in [tets_lo, tets_hi]
+    (square cross-section s x s hexes with s from an aspect a ~ U(3,5), length
+    set by the drawn count; the default seed draws 3.50M tets in total), 2.5 mm
+    spacing, U(-0.2, 0.2) mm jitter, fibers +z, the first/last ``pin_frac`` of
+    each box's z extent pinned to the bone at that end.  Bones: capsules
+    along x just beyond the end faces (radius 0.3 x the box width), on seeded
+    smooth rigid paths (rotation amplitude U(3,8) deg about the capsule centre,
+    translation amplitude U(2,6) mm), identity at frame 1."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(tets_lo), np.log(tets_hi), n_inst))
+    aspect = rng.uniform(3.0, 5.0, n_inst)
+    dims = []
+    for c, a in zip(counts, aspect):
+        s = max(2, int(round((c / (6.0 * a)) ** (1.0 / 3.0))))
+        dims.append((s, s, max(4, int(round(c / (6.0 * s * s))))))
+    ext = max(d[2] for d in dims) * spacing
+    pitch = ext + 0.06
+    side = int(np.ceil(np.sqrt(n_inst)))
+    verts, tets, vptr, tptr, vinst, tinst, tendon, vbone, vbw = [], [], [0], [0], [], [], [], [], []
+    bc, ba, bh, br, frames = [], [], [], [], []
+    for i, (nx, ny, nz) in enumerate(dims):
+        m = box_muscle(nx=nx, ny=ny, nz=nz, spacing=spacing, jitter=jitter, seed=seed * 100003 + i, pin_frac=pin_frac)
+        off = np.array([(i % side) * pitch, 0.0, (i // side) * pitch], np.float32)
+        v = m.verts + off
+        z = v[:, 2]
+        zr = (z - z.min()) / (z.max() - z.min())
+        verts.append(v)
+        tets.append(m.tets + vptr[-1])
+        vptr.append(vptr[-1] + v.shape[0])
+        tptr.append(tptr[-1] + m.tets.shape[0])
+        vinst.append(np.full(v.shape[0], i))
+        tinst.append(np.full(m.tets.shape[0], i))
+        tendon.append(m.stopped.astype(np.float32))
+        vbone.append(np.tile([2 * i, 2 * i + 1], (v.shape[0], 1)))
+        vbw.append(np.clip((zr - pin_frac) / (1.0 - 2.0 * pin_frac), 0.0, 1.0))
+        lo, hi = v.min(0).astype(np.float64), v.max(0).astype(np.float64)
+        w = hi[0] - lo[0]
+        r = 0.3 * w
+        for zend in (lo[2] - r - 0.001, hi[2] + r + 0.001):  # just beyond the end faces
+            bc.append([0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), zend])
+            ba.append([1.0, 0.0, 0.0])
+            bh.append(0.5 * w + r)
+            br.append(r)
+        margin = 3.0 * r + 0.012
+        glo = lo - margin
+        h = float((hi - lo + 2 * margin).max()) / (sdf_res - 1)
+        frames.append([glo[0], glo[1], glo[2], h])
+    verts = np.concatenate(verts).astype(np.float32)
+    nb = 2 * n_inst
+    traj = dict(rot_axis=rng.normal(size=(nb, 3)), rot_amp=np.deg2rad(rng.uniform(3.0, 8.0, nb)),
+                rot_w=rng.uniform(0.05, 0.12, nb), rot_phase=rng.uniform(0, 2 * np.pi, nb),
+                tr_dir=rng.normal(size=(nb, 3)), tr_amp=rng.uniform(0.002, 0.006, nb),
+                tr_w=rng.uniform(0.05, 0.12, nb), tr_phase=rng.uniform(0, 2 * np.pi, nb), start_frame=1)
+    traj["tr_dir"] /= np.linalg.norm(traj["tr_dir"], axis=1, keepdims=True)
+    knots = rng.uniform(0.0, 1.0, (n_inst, n_knots)).astype(np.float32)
+    knots[:, 0] = 0.0
+    vinst = np.concatenate(vinst).astype(np.int32)
+    tinst = np.concatenate(tinst).astype(np.int32)
+    return BatchScene(
+        verts=verts, tets=np.concatenate(tets).astype(np.int32), tet_part=tinst.copy(), vert_part=vinst.copy(),
+        v_tendon=np.concatenate(tendon).astype(np.float32),
+        v_fiber=np.tile(np.array([[0.0, 0.0, 1.0]], np.float32), (verts.shape[0], 1)),
+        surface_tris=np.zeros((0, 3), np.int32), bone_center=np.asarray(bc), bone_axis=np.asarray(ba),
+        bone_half=np.asarray(bh), bone_radius=np.asarray(br), vert_bone=np.concatenate(vbone).astype(np.int32),
+        vert_bw=np.concatenate(vbw).astype(np.float32), traj=traj, aniso_muscle=-1,
+        meta=dict(seed=seed, dims=dims, spacing=spacing),
+        inst_vptr=np.asarray(vptr, np.int64), inst_tptr=np.asarray(tptr, np.int64), vert_inst=vinst, tet_inst=tinst,
+        act_knots=knots, knot_every=knot_every, sdf_frame=np.asarray(frames, np.float32), sdf_res=sdf_res)
+
+
+def batch_subset(sc: BatchScene, idx) -> BatchScene:
+    """The instances ``idx`` of a batch as a batch of their own (CSR re-packed,
+    bones 2i, 2i+1 and schedules carried along)."""
+    idx = np.asarray(idx, np.int64)
+    verts, tets, vptr, tptr = [], [], [0], [0]
+    vsel_all, tsel_all, bones = [], [], []
+    for j, i in enumerate(idx):
+        v0, v1 = sc.inst_vptr[i], sc.inst_vptr[i + 1]
+        t0, t1 = sc.inst_tptr[i], sc.inst_tptr[i + 1]
+        vsel_all.append(np.arange(v0, v1))
+        tsel_all.append(np.arange(t0, t1))
+        tets.append(sc.tets[t0:t1] - v0 + vptr[-1])
+        vptr.append(vptr[-1] + (v1 - v0))
+        tptr.append(tptr[-1] + (t1 - t0))
+        bones += [2 * i, 2 * i + 1]
+    vs, ts, bones = np.concatenate(vsel_all), np.concatenate(tsel_all), np.asarray(bones)
+    remap = np.full(2 * sc.n_inst, -1, np.int64)
+    remap[bones] = np.arange(bones.shape[0])
+    vinst = np.repeat(np.arange(idx.shape[0]), np.diff(vptr)).astype(np.int32)
+    tinst = np.repeat(np.arange(idx.shape[0]), np.diff(tptr)).astype(np.int32)
+    traj = {k: (v[bones] if isinstance(v, np.ndarray) and v.shape[:1] == (2 * sc.n_inst,) else v)
+            for k, v in sc.traj.items()}
+    return BatchScene(
+        verts=sc.verts[vs], tets=np.concatenate(tets).astype(np.int32), tet_part=tinst.copy(), vert_part=vinst.copy(),
+        v_tendon=sc.v_tendon[vs], v_fiber=sc.v_fiber[vs], surface_tris=np.zeros((0, 3), np.int32),
+        bone_center=sc.bone_center[bones], bone_axis=sc.bone_axis[bones], bone_half=sc.bone_half[bones],
+        bone_radius=sc.bone_radius[bones], vert_bone=remap[sc.vert_bone[vs]].astype(np.int32),
+        vert_bw=sc.vert_bw[vs], traj=traj, aniso_muscle=-1, meta=dict(sc.meta, subset=idx.tolist()),
+        inst_vptr=np.asarray(vptr, np.int64), inst_tptr=np.asarray(tptr, np.int64), vert_inst=vinst, tet_inst=tinst,
+        act_knots=sc.act_knots[idx], knot_every=sc.knot_every, sdf_frame=sc.sdf_frame[idx], sdf_res=sc.sdf_res)
+
+
+def shard_instances(tet_counts, world: int) -> list[list[int]]:
+    """Greedy bin packing of instances over ``world`` ranks by tet count
+    (largest first onto the lightest rank); each rank's list sorted."""
+    order = np.argsort(-np.asarray(tet_counts), kind="stable")
+    load = np.zeros(world, np.int64)
+    out: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = int(np.argmin(load))
+        out[r].append(int(i))
+        load[r] += int(tet_counts[i])
+    return [sorted(x) for x in out]

@@ -44,9 +44,12 @@ def load_config(config_path: str) -> dict:
 def scene_from_cfg(cfg: dict) -> Scene:
     syn = dict(cfg.get("synthetic") or {})
     kind = syn.pop("kind", "humanv2")
-    if kind != "humanv2":
-        raise ValueError(f"unknown synthetic scene kind {kind!r}")
-    return humanv2_scene(**syn)
+    if kind == "humanv2":
+        return humanv2_scene(**syn)
+    if kind == "batched_boxes":
+        from .meshgen import batched_box_scene
+        return batched_box_scene(**syn)
+    raise ValueError(f"unknown synthetic scene kind {kind!r}")
 
 
 class MultiGridSim(MuscleSim):
@@ -76,7 +79,10 @@ class MultiGridSim(MuscleSim):
         if self.presubframe_pintotarget > 0.0:
             raise NotImplementedError("presubframe_pintotarget > 0 is not on the sm_100a path")
         self.fine_iters = int(cfg["fine_iterations"])
-        self.total_mass = float(cfg["total_mass"])
+        # density: total_mass spread over the signed rest volume (mg.py:736-740),
+        # or a fixed "density" (kg/m^3, the MuscleSim.from_procedural form)
+        self.total_mass = float(cfg.get("total_mass", 0.0))
+        self._fixed_density = cfg.get("density")
         self.dt = self.dt_frame / self.nsubsteps
         self.end_frame = int(cfg.get("end_frame", 90))
         self.start_frame = int(cfg.get("start_frame", 1))
@@ -142,7 +148,10 @@ class MultiGridSim(MuscleSim):
         table = collect_raw_constraints(self.pos0_np, self.tet_np, cons, tet_masks=masks)
         # density = total_mass / sum(signed V0) (mg.py:736-740), mass = |V| rho / 4
         _, V0, valid = tet_rest_data(self.pos0_np, self.tet_np)
-        self.density = self.total_mass / float(max(V0[valid].astype(np.float64).sum(), 1e-30))
+        if self._fixed_density is not None:
+            self.density = float(self._fixed_density)
+        else:
+            self.density = self.total_mass / float(max(V0[valid].astype(np.float64).sum(), 1e-30))
         mass, rest_volume = lumped_mass(self.pos0_np, self.tet_np, self.density)
         self.total_rest_volume = float(rest_volume.astype(np.float64).sum())
         # pins (muscleToBonePin, mg.py:486-535) and belly attach (mg.py:700-723)
@@ -184,7 +193,8 @@ class MultiGridSim(MuscleSim):
                            v_fiber=sc.v_fiber, tet_tendonmask=tendon_tet, dt=self.dt,
                            gravity_vec=self._gravity_vec, veldamping=float(cfg.get("veldamping", 0.0)),
                            quasi_static=self.quasi_static, omega=1.0, contraction_ratio=self.contraction_ratio,
-                           fiber_stiffness_scale=self.fiber_stiffness_scale, tile_tets=cfg.get("tile_tets"))
+                           fiber_stiffness_scale=self.fiber_stiffness_scale, tile_tets=cfg.get("tile_tets"),
+                           vert_group=getattr(sc, "vert_inst", None))
         self._setup_kinematics()
         self.collision_solvers_iter = []
         self.mg = None
@@ -347,7 +357,7 @@ class MultiGridSim(MuscleSim):
         its = getattr(self, "collision_solvers_iter", None) or []
         dcd = getattr(self, "dcd", None)
         return (all(dcd is not None and fn == dcd.solve for fn in its) and not getattr(self, "constraint_solvers", None)
-                and all(isinstance(c, GridSdfCollider) for c in cs) and len(cs) <= 1
+                and all(getattr(c, "graph_safe", False) for c in cs) and len(cs) <= 1
                 and getattr(self, "program", None) is None)
 
     def _frame_fused(self) -> None:
