@@ -39,6 +39,7 @@ enum {
     XPBD_STATUS_CONTACT_OVERFLOW = 1 << 1, /* more contacts than max_contacts (extra contacts dropped) */
     XPBD_STATUS_STACK_OVERFLOW = 1 << 2,   /* BVH traversal deeper than its stack (query cut short) */
     XPBD_STATUS_BARRIER_TIMEOUT = 1 << 3,  /* a grid-wide wait of the persistent pass gave up (results invalid) */
+    XPBD_STATUS_MMA_TIMEOUT = 1 << 4,      /* a tensor-core GEMM gave up waiting for its MMAs (results invalid) */
 };
 
 #define XPBD_MAX_MATERIALS 64
@@ -401,6 +402,52 @@ int xpbd_iterate_persistent(const XpbdParams* prm, const XpbdTiles* tiles, const
  * resident on the current device; *slots (optional) = how many CTAs of it
  * can be resident at once (the largest tile range one launch can take). */
 int xpbd_persistent_fits(const XpbdParams* prm, const XpbdTiles* tiles, int32_t* fits, int32_t* slots);
+
+/* ---- Learned coarse correction: the per-cage-vertex MLP's kernels.  These
+ * have no counterpart in the reference (its solver has no learned part); they
+ * serve the learned warm start of the cage (forward, backward, Adam). ---- */
+
+/* C[m][n] = sum_k A[m][k] B[n][k] on the tensor cores (tcgen05, BF16 operands,
+ * FP32 accumulation), then per element of C: z = C + bias[n] (bias optional);
+ * z *= gelu'(gelu_grad_of[m][n]) (optional, backward through a GELU whose
+ * pre-activation is stored there); out_pre = z; y = act ? gelu(z) : z
+ * (GELU tanh form of Hendrycks & Gimpel); out_f32 = y; out_bf16 = bf16(y);
+ * out_bf16_t[n][m] = bf16(y) (every output optional).  A and B are BF16
+ * row-major along k; k % 64 == 0; lda, ldb multiples of 8; rows of A beyond m
+ * and of B beyond n read as zero. */
+typedef struct XpbdGemm {
+    const uint16_t* a;
+    const uint16_t* b;
+    int32_t lda, ldb, m, n, k, act;
+    const float* bias;
+    const float* gelu_grad_of;
+    int32_t ld_g, ld_pre, ld_f32, ld_bf16, ld_bf16_t, reserved;
+    float* out_pre;
+    float* out_f32;
+    uint16_t* out_bf16;
+    uint16_t* out_bf16_t;
+    int32_t* status; /* XPBD_STATUS_MMA_TIMEOUT, optional */
+} XpbdGemm;
+
+/* One CTA per 128 x n_tile block of C (n_tile a multiple of 16, <= 256). */
+int xpbd_gemm_bf16(const XpbdGemm* g, int32_t n_tile, xpbd_stream_t stream);
+
+/* db[o] = sum_{s < m} dzt[o][s] for o < n_out (BF16 rows of length >= m). */
+int xpbd_colsum_bf16(int32_t n_out, int32_t m, const uint16_t* dzt, int32_t ld, float* db, xpbd_stream_t stream);
+
+/* Adam step (Kingma & Ba 2015) on FP32 weights w[rows][cols] with gradient
+ * g (row stride ld_g), moments m1, m2, bias correction of step `step`;
+ * refreshes the BF16 copy (optional) and the BF16 transposed copy
+ * w_bf16_t[cols][ld_t] (optional). */
+int xpbd_adam(int32_t rows, int32_t cols, float* w, const float* g, int32_t ld_g, float* m1, float* m2, float lr,
+              float beta1, float beta2, float eps, int32_t step, uint16_t* w_bf16, uint16_t* w_bf16_t, int32_t ld_t,
+              xpbd_stream_t stream);
+
+/* Mean-squared-error gradient 2 (y - t) / (m n_out) of the valid m x n_out
+ * block into the BF16 (m_pad x ld) buffer d (zero elsewhere) and optionally
+ * its transpose d_t[ld][ld_dt]; loss[0] += sum (y - t)^2. */
+int xpbd_mse_grad(int32_t m, int32_t m_pad, int32_t n_out, int32_t ld, const float* y, int32_t ld_y, const float* t,
+                  int32_t ld_t, uint16_t* d, uint16_t* d_t, int32_t ld_dt, float* loss, xpbd_stream_t stream);
 
 /* Stream capture helpers (a captured substep replays as one graph launch). */
 int xpbd_graph_begin(xpbd_stream_t stream);

@@ -19,6 +19,7 @@ MAT_ARAPSVD, MAT_VOLUME, MAT_ANISO, MAT_SNH, MAT_DAMPED = 1, 2, 4, 8, 16
 VF_ATTACH_MASK, VF_PIN = 0xFF, 1 << 8
 OP_SDF, OP_VELOCITY, OP_PREDICT, OP_PIN = 1, 2, 4, 8
 STATUS_PAIR_OVERFLOW, STATUS_CONTACT_OVERFLOW, STATUS_STACK_OVERFLOW, STATUS_BARRIER_TIMEOUT = 1, 2, 4, 8
+STATUS_MMA_TIMEOUT = 16
 APPLY_ATTACH, APPLY_DIVIDE, APPLY_PIN, APPLY_CLEAR = 1, 2, 4, 8
 PROJECT_FUSED, PROJECT_ACCUMULATE, PROJECT_FUSED_LAST = 0, 1, 2
 
@@ -103,6 +104,15 @@ class XpbdSdfBatch(C.Structure):
                 ("max_push", C.c_float)]
 
 
+class XpbdGemm(C.Structure):
+    _fields_ = [("a", C.c_void_p), ("b", C.c_void_p), ("lda", C.c_int32), ("ldb", C.c_int32), ("m", C.c_int32),
+                ("n", C.c_int32), ("k", C.c_int32), ("act", C.c_int32), ("bias", C.c_void_p),
+                ("gelu_grad_of", C.c_void_p), ("ld_g", C.c_int32), ("ld_pre", C.c_int32), ("ld_f32", C.c_int32),
+                ("ld_bf16", C.c_int32), ("ld_bf16_t", C.c_int32), ("reserved", C.c_int32), ("out_pre", C.c_void_p),
+                ("out_f32", C.c_void_p), ("out_bf16", C.c_void_p), ("out_bf16_t", C.c_void_p),
+                ("status", C.c_void_p)]
+
+
 class XpbdPersist(C.Structure):
     _fields_ = [("tile_own", C.c_void_p), ("ring", C.c_void_p), ("sync", C.c_void_p), ("status", C.c_void_p),
                 ("tile_begin", C.c_int32), ("tile_end", C.c_int32)]
@@ -135,6 +145,12 @@ _SIGS = {
                                  C.POINTER(XpbdPersist), C.c_int32, P], C.c_int),
     "xpbd_persistent_fits": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(C.c_int32),
                               C.POINTER(C.c_int32)], C.c_int),
+    "xpbd_gemm_bf16": ([C.POINTER(XpbdGemm), C.c_int32, P], C.c_int),
+    "xpbd_colsum_bf16": ([C.c_int32, C.c_int32, P, C.c_int32, P, P], C.c_int),
+    "xpbd_adam": ([C.c_int32, C.c_int32, P, P, C.c_int32, P, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32,
+                   P, P, C.c_int32, P], C.c_int),
+    "xpbd_mse_grad": ([C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, C.c_int32, P, C.c_int32, P, P, C.c_int32, P, P],
+                      C.c_int),
     "xpbd_graph_begin": ([P], C.c_int),
     "xpbd_graph_end": ([P, C.POINTER(C.c_void_p)], C.c_int),
     "xpbd_graph_launch": ([P, P], C.c_int),

@@ -1,0 +1,307 @@
+// Tensor-core GEMM and the small kernels of the learned coarse correction
+// (per-cage-vertex MLP: forward, backward and Adam, BF16 operands, FP32
+// accumulation).
+//
+// xpbd_gemm_bf16: C[m][n] = sum_k A[m][k] * B[n][k] on the 5th-generation
+// tensor cores (tcgen05.mma kind::f16, cta_group::1, accumulator in tensor
+// memory), one CTA per 128-row x n_tile block of C:
+//   * A and B are row-major along k (K-major), k a multiple of 64.  Each
+//     64-wide k block of A (128 x 64) and B (n_tile x 64) is copied from global
+//     memory into shared memory in the canonical no-swizzle K-major layout
+//     (8-row x 16-byte core matrices; leading byte offset 128 B between the two
+//     k halves of an MMA, stride byte offset 1024 B between 8-row groups);
+//   * two shared-memory stages: while the tensor core works on stage s (four
+//     128 x n_tile x 16 MMAs issued by one thread, completion tracked by an
+//     mbarrier through tcgen05.commit), the CTA loads stage s+1;
+//   * the epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
+//     lanes 32w..32w+31 = rows of the tile) and applies bias, the GELU
+//     derivative of a stored pre-activation (backward), GELU, and writes FP32
+//     and/or BF16 (row-major and/or transposed) outputs.
+// Every mbarrier wait is bounded; on timeout the status word gets
+// XPBD_STATUS_MMA_TIMEOUT, the CTA waits (bounded) once more for its MMAs and
+// frees its tensor memory before returning.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "xpbd_common.cuh"
+
+using namespace xpbd;
+
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kKB = 64;                 // k per stage
+constexpr uint32_t kLbo = 128;          // bytes between the two 8-wide k halves of a core-matrix pair
+constexpr uint32_t kSbo = 1024;         // bytes between 8-row groups (8 k-chunks x 128 B)
+constexpr long kWaitLimit = 1L << 22;   // try_wait polls (each suspends briefly): well over a second
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Byte offset of element (r, k) of a 64-wide k block in the canonical layout.
+__device__ __forceinline__ uint32_t kmajor_off(int r, int k) {
+    return uint32_t(r >> 3) * kSbo + uint32_t(k >> 3) * kLbo + uint32_t(r & 7) * 16u + uint32_t(k & 7) * 2u;
+}
+
+// Shared-memory matrix descriptor: start address, LBO, SBO (all >> 4),
+// version 1 (sm100), base offset 0, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((kLbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((kSbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 D, M = 128.
+__host__ __device__ constexpr uint32_t instr_desc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+    for (long i = 0; i < kWaitLimit; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ float gelu_f(float x) {
+    const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+    return 0.5f * x * (1.f + tanhf(u));
+}
+__device__ __forceinline__ float gelu_grad_f(float x) {
+    const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+    const float t = tanhf(u);
+    return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * 0.7978845608028654f * (1.f + 3.f * 0.044715f * x * x);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Copy a (rows x 64) k block (rows valid of nrows_valid, zero beyond) into
+// the canonical layout at smem byte address base.
+__device__ __forceinline__ void load_block(const uint16_t* __restrict__ g, int ld, int row0, int nrows_valid, int k0,
+                                           int rows, unsigned char* s) {
+    const int chunks = rows * 8;
+    for (int c = threadIdx.x; c < chunks; c += kThreads) {
+        const int r = c >> 3, kc = (c & 7) * 8;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (row0 + r < nrows_valid) v = *reinterpret_cast<const uint4*>(g + size_t(row0 + r) * ld + k0 + kc);
+        *reinterpret_cast<uint4*>(s + kmajor_off(r, kc)) = v;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(const __grid_constant__ XpbdGemm G, int n_tile, int tmem_cols) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint32_t s_tmem;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * n_tile;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const size_t a_bytes = size_t(128) * kKB * 2, b_bytes = size_t(n_tile) * kKB * 2;
+    unsigned char* sa[2] = {smem, smem + a_bytes + b_bytes};
+    unsigned char* sb[2] = {smem + a_bytes, smem + 2 * a_bytes + b_bytes};
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&s_tmem)),
+                     "r"(tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s_bar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s_bar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = instr_desc(n_tile);
+    const int nkb = G.k / kKB;
+    bool ok = true;
+    for (int kb = 0; kb < nkb && ok; ++kb) {
+        const int s = kb & 1;
+        if (kb >= 2) ok = mbar_wait(smem_u32(&s_bar[s]), uint32_t(((kb - 2) >> 1) & 1));
+        if (!ok) break;
+        load_block(G.a, G.lda, m0, G.m, kb * kKB, 128, sa[s]);
+        load_block(G.b, G.ldb, n0, G.n, kb * kKB, n_tile, sb[s]);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t a0 = smem_u32(sa[s]), b0 = smem_u32(sb[s]);
+#pragma unroll
+            for (int ks = 0; ks < kKB / 16; ++ks) {
+                const uint64_t ad = smem_desc(a0 + uint32_t(ks) * 2u * kLbo);
+                const uint64_t bd = smem_desc(b0 + uint32_t(ks) * 2u * kLbo);
+                const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&s_bar[s]))
+                         : "memory");
+        }
+    }
+    if (ok && nkb > 0) ok = mbar_wait(smem_u32(&s_bar[(nkb - 1) & 1]), uint32_t(((nkb - 1) >> 1) & 1));
+    if (!ok) {
+        if (threadIdx.x == 0 && G.status) atomicOr(G.status, XPBD_STATUS_MMA_TIMEOUT);
+        // bounded second wait for the MMAs this CTA issued, then release the tensor memory
+        if (nkb > 0) mbar_wait(smem_u32(&s_bar[(nkb - 1) & 1]), uint32_t(((nkb - 1) >> 1) & 1));
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (ok) {
+        const int row = m0 + warp * 32 + lane;
+        const bool rv = row < G.m;
+        for (int c0 = 0; c0 < n_tile; c0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), v);
+            if (!rv) continue;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int col = n0 + c0 + j;
+                if (col >= G.n) continue;
+                float z = v[j];
+                if (G.bias) z += G.bias[col];
+                if (G.gelu_grad_of) z *= gelu_grad_f(G.gelu_grad_of[size_t(row) * G.ld_g + col]);
+                if (G.out_pre) G.out_pre[size_t(row) * G.ld_pre + col] = z;
+                const float y = G.act == 1 ? gelu_f(z) : z;
+                if (G.out_f32) G.out_f32[size_t(row) * G.ld_f32 + col] = y;
+                const __nv_bfloat16 hb = __float2bfloat16_rn(y);
+                if (G.out_bf16) reinterpret_cast<__nv_bfloat16*>(G.out_bf16)[size_t(row) * G.ld_bf16 + col] = hb;
+                if (G.out_bf16_t) reinterpret_cast<__nv_bfloat16*>(G.out_bf16_t)[size_t(col) * G.ld_bf16_t + row] = hb;
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(tmem_cols));
+    }
+}
+
+// db[o] = sum over valid samples of dzt[o][s] (dzt: transposed BF16 deltas).
+__global__ void k_colsum_bf16(int n_out, int m, const uint16_t* __restrict__ dzt, int ld, float* __restrict__ db) {
+    const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (o >= n_out) return;
+    const __nv_bfloat16* r = reinterpret_cast<const __nv_bfloat16*>(dzt) + size_t(o) * ld;
+    float s = 0.f;
+    for (int i = lane; i < m; i += 32) s += __bfloat162float(r[i]);
+    for (int k = 16; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k);
+    if (lane == 0) db[o] = s;
+}
+
+// Adam on FP32 master weights (Kingma & Ba 2015), with the BF16 copy and the
+// BF16 transposed copy (rows x cols -> cols x ld_t) refreshed in place.
+__global__ void k_adam(int rows, int cols, float* __restrict__ w, const float* __restrict__ g, int ld_g,
+                       float* __restrict__ m1, float* __restrict__ m2, float lr, float b1, float b2, float eps,
+                       float c1, float c2, uint16_t* __restrict__ wb, uint16_t* __restrict__ wt, int ld_t) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows * cols) return;
+    const int r = i / cols, c = i % cols;
+    const float gi = g[size_t(r) * ld_g + c];
+    const float a = b1 * m1[i] + (1.f - b1) * gi;
+    const float b = b2 * m2[i] + (1.f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = b;
+    const float wi = w[i] - lr * (a / c1) / (sqrtf(b / c2) + eps);
+    w[i] = wi;
+    const __nv_bfloat16 h = __float2bfloat16_rn(wi);
+    if (wb) reinterpret_cast<__nv_bfloat16*>(wb)[i] = h;
+    if (wt) reinterpret_cast<__nv_bfloat16*>(wt)[size_t(c) * ld_t + r] = h;
+}
+
+// Loss gradient of the mean squared error over the valid rows:
+// d[r][c] = 2 (y - t) / (m * n_out) for r < m, c < n_out; 0 elsewhere in the
+// padded (m_pad x ld) BF16 output and its transpose.  loss[0] += sum (y-t)^2.
+__global__ void k_mse_grad(int m, int m_pad, int n_out, int ld, const float* __restrict__ y, int ld_y,
+                           const float* __restrict__ t, int ld_t, uint16_t* __restrict__ d, uint16_t* __restrict__ dt,
+                           int ld_dt, float* __restrict__ loss) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m_pad * ld) return;
+    const int r = i / ld, c = i % ld;
+    float gval = 0.f;
+    if (r < m && c < n_out) {
+        const float e = y[size_t(r) * ld_y + c] - t[size_t(r) * ld_t + c];
+        gval = 2.f * e / float(m * n_out);
+        atomicAdd(loss, e * e);
+    }
+    const __nv_bfloat16 h = __float2bfloat16_rn(gval);
+    reinterpret_cast<__nv_bfloat16*>(d)[i] = h;
+    if (dt) reinterpret_cast<__nv_bfloat16*>(dt)[size_t(c) * ld_dt + r] = h;
+}
+
+}  // namespace
+
+extern "C" {
+
+int xpbd_gemm_bf16(const XpbdGemm* g, int32_t n_tile, xpbd_stream_t stream) {
+    if (!g || !g->a || !g->b) return fail(XPBD_ERR_ARG, "xpbd_gemm_bf16: null operand");
+    if (g->m <= 0 || g->n <= 0 || g->k <= 0 || g->k % kKB) return fail(XPBD_ERR_ARG, "xpbd_gemm_bf16: m, n > 0, k % 64 == 0");
+    if (n_tile < 16 || n_tile > 256 || n_tile % 16) return fail(XPBD_ERR_ARG, "xpbd_gemm_bf16: n_tile in 16..256, % 16");
+    if (g->lda < g->k || g->ldb < g->k || g->lda % 8 || g->ldb % 8)
+        return fail(XPBD_ERR_ARG, "xpbd_gemm_bf16: lda/ldb >= k and multiples of 8");
+    if (!aligned16(g->a) || !aligned16(g->b)) return fail(XPBD_ERR_ALIGN, "xpbd_gemm_bf16: operands 16-byte aligned");
+    if (g->act != 0 && g->act != 1) return fail(XPBD_ERR_ARG, "xpbd_gemm_bf16: act");
+    int tmem_cols = 32;
+    while (tmem_cols < n_tile) tmem_cols <<= 1;
+    const size_t smem = size_t(2) * (128 + n_tile) * kKB * 2;
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        if (cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(size_t(2) * (128 + 256) * kKB * 2)) != cudaSuccess)
+            return cuda_check("xpbd_gemm_bf16: smem attribute");
+        attr_set[dev] = true;
+    }
+    dim3 grid((g->m + 127) / 128, (g->n + n_tile - 1) / n_tile);
+    k_gemm_bf16<<<grid, kThreads, smem, (cudaStream_t)stream>>>(*g, n_tile, tmem_cols);
+    return cuda_check("xpbd_gemm_bf16");
+}
+
+int xpbd_colsum_bf16(int32_t n_out, int32_t m, const uint16_t* dzt, int32_t ld, float* db, xpbd_stream_t stream) {
+    if (n_out <= 0 || m <= 0 || !dzt || !db || ld < m) return fail(XPBD_ERR_ARG, "xpbd_colsum_bf16: bad arguments");
+    k_colsum_bf16<<<(n_out + 7) / 8, 256, 0, (cudaStream_t)stream>>>(n_out, m, dzt, ld, db);
+    return cuda_check("xpbd_colsum_bf16");
+}
+
+int xpbd_adam(int32_t rows, int32_t cols, float* w, const float* g, int32_t ld_g, float* m1, float* m2, float lr,
+              float beta1, float beta2, float eps, int32_t step, uint16_t* w_bf16, uint16_t* w_bf16_t, int32_t ld_t,
+              xpbd_stream_t stream) {
+    if (rows <= 0 || cols <= 0 || !w || !g || !m1 || !m2 || step < 1 || ld_g < cols || (w_bf16_t && ld_t < rows))
+        return fail(XPBD_ERR_ARG, "xpbd_adam: bad arguments");
+    const float c1 = 1.f - powf(beta1, float(step)), c2 = 1.f - powf(beta2, float(step));
+    const int n = rows * cols;
+    k_adam<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(rows, cols, w, g, ld_g, m1, m2, lr, beta1, beta2, eps,
+                                                              c1, c2, w_bf16, w_bf16_t, ld_t);
+    return cuda_check("xpbd_adam");
+}
+
+int xpbd_mse_grad(int32_t m, int32_t m_pad, int32_t n_out, int32_t ld, const float* y, int32_t ld_y, const float* t,
+                  int32_t ld_t, uint16_t* d, uint16_t* d_t, int32_t ld_dt, float* loss, xpbd_stream_t stream) {
+    if (m <= 0 || m_pad < m || n_out <= 0 || ld < n_out || !y || !t || !d || !loss || (d_t && ld_dt < m_pad))
+        return fail(XPBD_ERR_ARG, "xpbd_mse_grad: bad arguments");
+    const int n = m_pad * ld;
+    k_mse_grad<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(m, m_pad, n_out, ld, y, ld_y, t, ld_t, d, d_t, ld_dt,
+                                                                  loss);
+    return cuda_check("xpbd_mse_grad");
+}
+
+}  // extern "C"
