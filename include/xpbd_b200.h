@@ -280,17 +280,20 @@ typedef struct XpbdCage {
     const int32_t* p_idx;      /* [n_fine][4] coarse library ids of the embedding tet, -1 = not embedded */
     const float* p_w;          /* [n_fine][4] barycentric weights (1-u-v-w, u, v, w) */
     float* resid;              /* [n_fine][4] scratch: fine residual x_f - P x_c(prior) */
+    float* rhs;                /* [n_coarse][4] scratch: P^T resid per coarse vertex (cage order) */
 } XpbdCage;
 
 /* Regularised Galerkin restriction of the xyz lanes of fine4 into coarse4:
  * x_c = argmin |P x_c - x_f|^2 + lam |x_c - prior|^2 with prior = the current
  * contents of coarse4, computed as prior + (P^T P + lam I)^-1 P^T (x_f - P prior)
  * (restrict_galerkin_scatter_kernel + block_solve_kernel, mg/kernel.py:137-178,
- * with lam -> 0 the reference's operator).  Optional: coarse_prev4 receives
+ * with lam -> 0 the reference's operator; the CSR gather runs one warp per
+ * coarse vertex, the block solve over row chunks of each block).  Optional: coarse_prev4 receives
  * the same values (the q_j snapshot, mg/mg.py:1077), and where
  * coarse_pin4[c].w != 0 the coarse position is then overwritten by
- * coarse_pin4[c].xyz (the coarse kinematic pin, mg/mg.py:1013-1026).  One
- * CTA per block for the solve, no atomics. */
+ * coarse_pin4[c].xyz (the coarse kinematic pin, mg/mg.py:1013-1026).  The
+ * CSR gather runs one warp per coarse vertex, the block solve over 64-row
+ * chunks of each block; no atomics. */
 int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, float* coarse_prev4,
                      const float* coarse_pin4, xpbd_stream_t stream);
 
@@ -448,6 +451,40 @@ int xpbd_adam(int32_t rows, int32_t cols, float* w, const float* g, int32_t ld_g
  * its transpose d_t[ld][ld_dt]; loss[0] += sum (y - t)^2. */
 int xpbd_mse_grad(int32_t m, int32_t m_pad, int32_t n_out, int32_t ld, const float* y, int32_t ld_y, const float* t,
                   int32_t ld_t, uint16_t* d, uint16_t* d_t, int32_t ld_dt, float* loss, xpbd_stream_t stream);
+
+/* Static description of the cage for the feature kernel (cage order j). */
+typedef struct XpbdCageFeatures {
+    int32_t n_cage, m_pad;     /* cage vertices; rows of the feature matrix (>= n_cage) */
+    const int32_t* coarse_lib; /* [n_cage] cage order -> coarse library order */
+    const int32_t* nbr;        /* [n_cage][6] lattice neighbours (+x,-x,+y,-y,+z,-z of the muscle frame), -1 = none */
+    const int32_t* owner;      /* [n_cage] owning muscle */
+    const float* act_muscle;   /* [n_muscles] activation of each muscle this frame */
+    const int32_t* cage_bone;  /* [n_cage][2] the owner's two end bones */
+    const float* cage_w;       /* [n_cage] axial blend weight of the second bone */
+    const float* bone_rel;     /* [n_bones][12] frame-to-frame bone motion [R | t], row-major */
+    const float* stat;         /* [n_cage][24] static features */
+    const float* c_rest4;      /* [n_coarse][4] rest cage (library order) */
+    const float* c_target4;    /* [n_coarse][4] restriction of the bone-driven fine targets (library order) */
+    const float* norm;         /* [64][2] (mean, 1/std) standardisation of each feature, or NULL */
+} XpbdCageFeatures;
+
+/* 64 features per cage vertex into X[m_pad][64] and its transpose Xt[64][m_pad]
+ * (BF16): predicted displacement c_pred - c_prev (mm), owner activation,
+ * blended bone motion, six neighbours' relative predicted displacement,
+ * offsets from the rest cage and to the restricted targets (mm), static rest
+ * features. */
+int xpbd_cage_features(const XpbdCageFeatures* cf, const float* c_pred4, const float* c_prev4, uint16_t* X,
+                       uint16_t* Xt, xpbd_stream_t stream);
+/* c_out4[lib j].xyz = c_pred4[lib j].xyz + scale * y[j][0..2]. */
+int xpbd_cage_apply(int32_t n_cage, const int32_t* coarse_lib, const float* c_pred4, const float* y, int32_t ldy,
+                    float scale, float* c_out4, xpbd_stream_t stream);
+/* t[j][0..2] = scale * (c_star4 - c_pred4)[lib j]: the training target. */
+int xpbd_cage_target(int32_t n_cage, const int32_t* coarse_lib, const float* c_star4, const float* c_pred4,
+                     float scale, float* t, xpbd_stream_t stream);
+/* If warm->resid_sq_sum > factor * plain->resid_sq_sum (or the warm state has
+ * a non-finite position), pos4 = saved4 and taken[0] += 1. */
+int xpbd_fallback_select(int32_t n, const XpbdMetrics* warm, const XpbdMetrics* plain, float factor,
+                         const float* saved4, float* pos4, int32_t* taken, xpbd_stream_t stream);
 
 /* Stream capture helpers (a captured substep replays as one graph launch). */
 int xpbd_graph_begin(xpbd_stream_t stream);

@@ -71,7 +71,7 @@ class XpbdCage(C.Structure):
     _fields_ = [("n_fine", C.c_int32), ("n_coarse", C.c_int32), ("n_blocks", C.c_int32), ("max_block", C.c_int32),
                 ("r_ptr", C.c_void_p), ("r_fine", C.c_void_p), ("r_w", C.c_void_p), ("blk_ptr", C.c_void_p),
                 ("blk_moff", C.c_void_p), ("minv", C.c_void_p), ("coarse_lib", C.c_void_p), ("p_idx", C.c_void_p),
-                ("p_w", C.c_void_p), ("resid", C.c_void_p)]
+                ("p_w", C.c_void_p), ("resid", C.c_void_p), ("rhs", C.c_void_p)]
 
 
 class XpbdDcd(C.Structure):
@@ -113,6 +113,13 @@ class XpbdGemm(C.Structure):
                 ("status", C.c_void_p)]
 
 
+class XpbdCageFeatures(C.Structure):
+    _fields_ = [("n_cage", C.c_int32), ("m_pad", C.c_int32), ("coarse_lib", C.c_void_p), ("nbr", C.c_void_p),
+                ("owner", C.c_void_p), ("act_muscle", C.c_void_p), ("cage_bone", C.c_void_p), ("cage_w", C.c_void_p),
+                ("bone_rel", C.c_void_p), ("stat", C.c_void_p), ("c_rest4", C.c_void_p), ("c_target4", C.c_void_p),
+                ("norm", C.c_void_p)]
+
+
 class XpbdPersist(C.Structure):
     _fields_ = [("tile_own", C.c_void_p), ("ring", C.c_void_p), ("sync", C.c_void_p), ("status", C.c_void_p),
                 ("tile_begin", C.c_int32), ("tile_end", C.c_int32)]
@@ -151,6 +158,10 @@ _SIGS = {
                    P, P, C.c_int32, P], C.c_int),
     "xpbd_mse_grad": ([C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, C.c_int32, P, C.c_int32, P, P, C.c_int32, P, P],
                       C.c_int),
+    "xpbd_cage_features": ([C.POINTER(XpbdCageFeatures), P, P, P, P, P], C.c_int),
+    "xpbd_cage_apply": ([C.c_int32, P, P, P, C.c_int32, C.c_float, P, P], C.c_int),
+    "xpbd_cage_target": ([C.c_int32, P, P, P, C.c_float, P, P], C.c_int),
+    "xpbd_fallback_select": ([C.c_int32, P, P, C.c_float, P, P, P, P], C.c_int),
     "xpbd_graph_begin": ([P], C.c_int),
     "xpbd_graph_end": ([P, C.POINTER(C.c_void_p)], C.c_int),
     "xpbd_graph_launch": ([P, P], C.c_int),

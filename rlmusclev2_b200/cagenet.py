@@ -125,14 +125,20 @@ class CageMLP:
         self.refresh_copies()
 
     # ------------------------------------------------------------ forward
-    def forward(self, m: int) -> torch.Tensor:
+    def forward(self, m: int, train: bool = True) -> torch.Tensor:
         """Forward of the first m rows of X (Xt must hold X's transpose when a
-        backward follows).  Returns Y[:m, :3] (a view)."""
+        backward follows).  train=False stores only what the next layer reads
+        (no pre-activations, no transposed copies) and splits each layer over
+        two 128-column tiles.  Returns Y[:m, :3] (a view)."""
         lib, sp = self.lib, self._sp
         H = [self.X] + self.H[1:]
         for l in range(4):
-            gemm(lib, sp, H[l], self.Wb[l], self.m_pad, 256, DIMS[l], bias=self.b[l], act=1, out_pre=self.Z[l],
-                 out_bf16=self.H[l + 1], out_bf16_t=self.Ht[l + 1], status=self.status)
+            if train:
+                gemm(lib, sp, H[l], self.Wb[l], self.m_pad, 256, DIMS[l], bias=self.b[l], act=1, out_pre=self.Z[l],
+                     out_bf16=self.H[l + 1], out_bf16_t=self.Ht[l + 1], status=self.status)
+            else:
+                gemm(lib, sp, H[l], self.Wb[l], self.m_pad, 256, DIMS[l], bias=self.b[l], act=1,
+                     out_bf16=self.H[l + 1], status=self.status, n_tile=128)
         gemm(lib, sp, self.H[4], self.Wb[4], self.m_pad, 3, 256, bias=self.bpad4, act=0, out_f32=self.Y,
              status=self.status, n_tile=16)
         return self.Y[:m, :3]

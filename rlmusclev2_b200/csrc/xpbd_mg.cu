@@ -27,35 +27,53 @@ __global__ void __launch_bounds__(kMgThreads)
                     x.z - (((w.x * a.z + w.y * b.z) + w.z * c.z) + w.w * d.z), 0.f);
 }
 
-// One CTA per Galerkin block: b_j = sum_e w_e r[e] for the block's coarse
-// vertices (CSR gather into shared memory), then each warp computes rows
+// b_c = sum_e w_e r[e] over the restriction CSR of coarse vertex c (cage
+// order): one warp per coarse vertex, lanes striding its entries.
+__global__ void __launch_bounds__(kMgThreads) k_mg_gather(const __grid_constant__ XpbdCage G) {
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (c >= G.n_coarse) return;
+    const float4* res = reinterpret_cast<const float4*>(G.resid);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (int e = G.r_ptr[c] + lane; e < G.r_ptr[c + 1]; e += 32) {
+        const float w = G.r_w[e];
+        const float4 x = res[G.r_fine[e]];
+        ax += w * x.x;
+        ay += w * x.y;
+        az += w * x.z;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    if (lane == 0) reinterpret_cast<float4*>(G.rhs)[c] = make_float4(ax, ay, az, 0.f);
+}
+
+// Galerkin block solve, kRestrictRows rows of one block per CTA
+// (blockIdx.x = block, blockIdx.y = row chunk): the block's right-hand side
+// is staged in shared memory, each warp computes rows
 // delta[r] = sum_j Minv[r][j] b_j with lanes striding j (coalesced rows) and
 // the new coarse position prior + delta.
+constexpr int kRestrictRows = 64;
 __global__ void __launch_bounds__(kMgThreads)
     k_mg_restrict(const __grid_constant__ XpbdCage G, float4* coarse, float4* prev, const float4* __restrict__ pin) {
     extern __shared__ float4 sb[];
     const int blk = blockIdx.x;
     const int c0 = G.blk_ptr[blk];
     const int dim = G.blk_ptr[blk + 1] - c0;
-    const float4* res = reinterpret_cast<const float4*>(G.resid);
-    for (int j = threadIdx.x; j < dim; j += blockDim.x) {
-        const int c = c0 + j;
-        float3 acc = make_float3(0.f, 0.f, 0.f);
-        for (int e = G.r_ptr[c]; e < G.r_ptr[c + 1]; ++e) {
-            const float w = G.r_w[e];
-            const float4 x = res[G.r_fine[e]];
-            acc.x += w * x.x;
-            acc.y += w * x.y;
-            acc.z += w * x.z;
-        }
-        sb[j] = make_float4(acc.x, acc.y, acc.z, 0.f);
-    }
+    const int r0 = blockIdx.y * kRestrictRows;
+    if (r0 >= dim) return;  // uniform over the CTA
+    const float4* rhs = reinterpret_cast<const float4*>(G.rhs);
+    for (int j = threadIdx.x; j < dim; j += blockDim.x) sb[j] = rhs[c0 + j];
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
     const float* M = G.minv + G.blk_moff[blk];
-    for (int r = warp; r < dim; r += nwarp) {
+    const int r1 = min(dim, r0 + kRestrictRows);
+    for (int r = r0 + warp; r < r1; r += nwarp) {
         const float* row = M + size_t(r) * dim;
         float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll 4
         for (int j = lane; j < dim; j += 32) {
             const float m = row[j];
             const float4 b = sb[j];
@@ -123,8 +141,9 @@ int check_cage(const XpbdCage* g) {
         !g->blk_ptr || !g->blk_moff || !g->minv || !g->coarse_lib || !g->p_idx || !g->p_w || !g->resid)
         return fail(XPBD_ERR_ARG, "XpbdCage: null member or empty size");
     if (g->max_block <= 0 || g->max_block > 8192) return fail(XPBD_ERR_LIMIT, "XpbdCage: max_block must be in 1..8192");
-    if (!aligned16(g->p_idx) || !aligned16(g->p_w) || !aligned16(g->resid))
-        return fail(XPBD_ERR_ALIGN, "XpbdCage: p_idx/p_w/resid alignment");
+    if (!g->rhs) return fail(XPBD_ERR_ARG, "XpbdCage: rhs scratch required");
+    if (!aligned16(g->p_idx) || !aligned16(g->p_w) || !aligned16(g->resid) || !aligned16(g->rhs))
+        return fail(XPBD_ERR_ALIGN, "XpbdCage: p_idx/p_w/resid/rhs alignment");
     return XPBD_OK;
 }
 
@@ -144,7 +163,9 @@ int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, f
         cudaFuncSetAttribute(k_mg_restrict, cudaFuncAttributeMaxDynamicSharedMemorySize, int(8192 * sizeof(float4)));
     k_mg_residual<<<(cage->n_fine + kMgThreads - 1) / kMgThreads, kMgThreads, 0, (cudaStream_t)stream>>>(
         *cage, reinterpret_cast<const float4*>(fine4), reinterpret_cast<const float4*>(coarse4));
-    k_mg_restrict<<<cage->n_blocks, kMgThreads, smem, (cudaStream_t)stream>>>(
+    k_mg_gather<<<(cage->n_coarse * 32 + kMgThreads - 1) / kMgThreads, kMgThreads, 0, (cudaStream_t)stream>>>(*cage);
+    const dim3 grid(cage->n_blocks, (cage->max_block + kRestrictRows - 1) / kRestrictRows);
+    k_mg_restrict<<<grid, kMgThreads, smem, (cudaStream_t)stream>>>(
         *cage, reinterpret_cast<float4*>(coarse4), reinterpret_cast<float4*>(coarse_prev4),
         reinterpret_cast<const float4*>(coarse_pin4));
     return cuda_check("xpbd_mg_restrict");

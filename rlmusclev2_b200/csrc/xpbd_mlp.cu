@@ -36,6 +36,8 @@ constexpr uint32_t kLbo = 128;          // bytes between the two 8-wide k halves
 constexpr uint32_t kSbo = 1024;         // bytes between 8-row groups (8 k-chunks x 128 B)
 constexpr long kWaitLimit = 1L << 22;   // try_wait polls (each suspends briefly): well over a second
 
+__device__ __forceinline__ bool aligned_ptr16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -70,13 +72,20 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
     return false;
 }
 
+// tanh(u) = 1 - 2 / (exp(2u) + 1) with the fast exponential (relative error
+// ~1e-6, far below the BF16 rounding of the activations it feeds); the
+// clamp keeps exp finite.
+__device__ __forceinline__ float tanh_fast(float u) {
+    const float e = __expf(2.f * fminf(fmaxf(u, -15.f), 15.f));
+    return 1.f - __fdividef(2.f, e + 1.f);
+}
 __device__ __forceinline__ float gelu_f(float x) {
     const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
-    return 0.5f * x * (1.f + tanhf(u));
+    return 0.5f * x * (1.f + tanh_fast(u));
 }
 __device__ __forceinline__ float gelu_grad_f(float x) {
     const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
-    const float t = tanhf(u);
+    const float t = tanh_fast(u);
     return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * 0.7978845608028654f * (1.f + 3.f * 0.044715f * x * x);
 }
 
@@ -94,14 +103,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 
 // Copy a (rows x 64) k block (rows valid of nrows_valid, zero beyond) into
 // the canonical layout at smem byte address base.
+// Loads are issued eight at a time before their stores, so their latencies
+// overlap instead of adding up.
 __device__ __forceinline__ void load_block(const uint16_t* __restrict__ g, int ld, int row0, int nrows_valid, int k0,
                                            int rows, unsigned char* s) {
     const int chunks = rows * 8;
-    for (int c = threadIdx.x; c < chunks; c += kThreads) {
-        const int r = c >> 3, kc = (c & 7) * 8;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (row0 + r < nrows_valid) v = *reinterpret_cast<const uint4*>(g + size_t(row0 + r) * ld + k0 + kc);
-        *reinterpret_cast<uint4*>(s + kmajor_off(r, kc)) = v;
+    for (int c0 = threadIdx.x; c0 < chunks; c0 += 8 * kThreads) {
+        uint4 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int c = c0 + q * kThreads, r = c >> 3, kc = (c & 7) * 8;
+            v[q] = make_uint4(0u, 0u, 0u, 0u);
+            if (c < chunks && row0 + r < nrows_valid)
+                v[q] = *reinterpret_cast<const uint4*>(g + size_t(row0 + r) * ld + k0 + kc);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int c = c0 + q * kThreads, r = c >> 3, kc = (c & 7) * 8;
+            if (c < chunks) *reinterpret_cast<uint4*>(s + kmajor_off(r, kc)) = v[q];
+        }
     }
 }
 
@@ -167,23 +187,70 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(const __grid_constant
     if (ok) {
         const int row = m0 + warp * 32 + lane;
         const bool rv = row < G.m;
+        // 16-byte vector stores of a row's 16 columns where the chunk is whole
+        // and the row strides keep them aligned
+        const bool vec_h = G.out_bf16 && (G.ld_bf16 % 8) == 0 && aligned_ptr16(G.out_bf16);
+        const bool vec_f = G.out_f32 && (G.ld_f32 % 4) == 0 && aligned_ptr16(G.out_f32);
+        const bool vec_p = G.out_pre && (G.ld_pre % 4) == 0 && aligned_ptr16(G.out_pre);
         for (int c0 = 0; c0 < n_tile; c0 += 16) {
             float v[16];
             tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), v);
             if (!rv) continue;
+            const bool whole = n0 + c0 + 16 <= G.n;
+            float y[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 const int col = n0 + c0 + j;
-                if (col >= G.n) continue;
                 float z = v[j];
-                if (G.bias) z += G.bias[col];
-                if (G.gelu_grad_of) z *= gelu_grad_f(G.gelu_grad_of[size_t(row) * G.ld_g + col]);
-                if (G.out_pre) G.out_pre[size_t(row) * G.ld_pre + col] = z;
-                const float y = G.act == 1 ? gelu_f(z) : z;
-                if (G.out_f32) G.out_f32[size_t(row) * G.ld_f32 + col] = y;
-                const __nv_bfloat16 hb = __float2bfloat16_rn(y);
-                if (G.out_bf16) reinterpret_cast<__nv_bfloat16*>(G.out_bf16)[size_t(row) * G.ld_bf16 + col] = hb;
-                if (G.out_bf16_t) reinterpret_cast<__nv_bfloat16*>(G.out_bf16_t)[size_t(col) * G.ld_bf16_t + row] = hb;
+                if (col < G.n) {
+                    if (G.bias) z += G.bias[col];
+                    if (G.gelu_grad_of) z *= gelu_grad_f(G.gelu_grad_of[size_t(row) * G.ld_g + col]);
+                }
+                v[j] = z;
+                y[j] = G.act == 1 ? gelu_f(z) : z;
+            }
+            const size_t cb = size_t(n0 + c0);
+            if (G.out_pre) {
+                if (whole && vec_p) {
+                    float4* d = reinterpret_cast<float4*>(G.out_pre + size_t(row) * G.ld_pre + cb);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                } else {
+                    for (int j = 0; j < 16; ++j)
+                        if (n0 + c0 + j < G.n) G.out_pre[size_t(row) * G.ld_pre + cb + j] = v[j];
+                }
+            }
+            if (G.out_f32) {
+                if (whole && vec_f) {
+                    float4* d = reinterpret_cast<float4*>(G.out_f32 + size_t(row) * G.ld_f32 + cb);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) d[q] = make_float4(y[4 * q], y[4 * q + 1], y[4 * q + 2], y[4 * q + 3]);
+                } else {
+                    for (int j = 0; j < 16; ++j)
+                        if (n0 + c0 + j < G.n) G.out_f32[size_t(row) * G.ld_f32 + cb + j] = y[j];
+                }
+            }
+            if (G.out_bf16) {
+                __nv_bfloat16* hb = reinterpret_cast<__nv_bfloat16*>(G.out_bf16) + size_t(row) * G.ld_bf16 + cb;
+                if (whole && vec_h) {
+                    uint4 pk[2];
+                    uint32_t* w = reinterpret_cast<uint32_t*>(pk);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const __nv_bfloat162 h2 = __floats2bfloat162_rn(y[2 * q], y[2 * q + 1]);
+                        w[q] = *reinterpret_cast<const uint32_t*>(&h2);
+                    }
+                    reinterpret_cast<uint4*>(hb)[0] = pk[0];
+                    reinterpret_cast<uint4*>(hb)[1] = pk[1];
+                } else {
+                    for (int j = 0; j < 16; ++j)
+                        if (n0 + c0 + j < G.n) hb[j] = __float2bfloat16_rn(y[j]);
+                }
+            }
+            if (G.out_bf16_t) {
+                __nv_bfloat16* ht = reinterpret_cast<__nv_bfloat16*>(G.out_bf16_t);
+                for (int j = 0; j < 16; ++j)
+                    if (n0 + c0 + j < G.n) ht[(cb + j) * G.ld_bf16_t + row] = __float2bfloat16_rn(y[j]);
             }
         }
     }

@@ -224,6 +224,7 @@ class Scene:
     muscle_rot: np.ndarray | None = None     # (M,3,3) local->world rotation (column 0 = long axis)
     muscle_center: np.ndarray | None = None  # (M,3)
     muscle_len: np.ndarray | None = None     # (M,)
+    act_sched: np.ndarray | None = None      # optional knots (every 8 frames from frame 1) of the fiber activation
 
     @property
     def n_bones(self) -> int:
@@ -261,8 +262,25 @@ class Scene:
         return (out[0] + w * (out[1] - out[0])).astype(np.float32)
 
     def activation(self, frame: int, start: int = 1, end: int = 50) -> np.ndarray:
-        """RampActivationSource (util/activation.py:28-44) on the aniso muscle's tets."""
+        """RampActivationSource (util/activation.py:28-44) on the aniso muscle's
+        tets, or the piecewise-linear schedule act_sched when one is set."""
+        if self.act_sched is not None:
+            return (self.muscle_activation(frame)[self.aniso_muscle] * (self.tet_part == self.aniso_muscle)).astype(
+                np.float32)
         return ramp_activation(self.tet_part == self.aniso_muscle, frame, start, end)
+
+    def muscle_activation(self, frame: int, start: int = 1, end: int = 50) -> np.ndarray:
+        """(n_muscles,) activation of every muscle (only the aniso muscle has a
+        fiber constraint; the others are 0)."""
+        out = np.zeros(self.muscle_rot.shape[0], np.float32)
+        if self.act_sched is not None:
+            f = (float(frame) - 1.0) / 8.0
+            k = int(np.clip(np.floor(f), 0, self.act_sched.shape[0] - 2))
+            u = float(np.clip(f - k, 0.0, 1.0))
+            out[self.aniso_muscle] = (1.0 - u) * self.act_sched[k] + u * self.act_sched[k + 1]
+        else:
+            out[self.aniso_muscle] = min(1.0, max(0.0, (int(frame) - start) / max(1, end - start)))
+        return out
 
 
 def capsule_sdf(x: np.ndarray, c: np.ndarray, axis: np.ndarray, half: float, r: float) -> np.ndarray:
@@ -692,3 +710,21 @@ def shard_instances(tet_counts, world: int) -> list[list[int]]:
         out[r].append(int(i))
         load[r] += int(tet_counts[i])
     return [sorted(x) for x in out]
+
+
+def reseed_motion(sc: Scene, seed: int, n_frames: int = 64) -> Scene:
+    """The same mesh with bone paths and a fiber activation schedule drawn
+    from ``seed`` (amplitudes and frequencies from the same distributions as
+    the scene's own; activation knots U(0,1) every 8 frames, 0 at frame 1)."""
+    import dataclasses
+    rng = np.random.default_rng(10_000 + int(seed))
+    nb = sc.n_bones
+    traj = dict(rot_axis=rng.normal(size=(nb, 3)), rot_amp=np.deg2rad(rng.uniform(2.5, 6.25, nb)),
+                rot_w=rng.uniform(0.05, 0.12, nb), rot_phase=rng.uniform(0, 2 * np.pi, nb),
+                tr_dir=rng.normal(size=(nb, 3)), tr_amp=rng.uniform(0.005, 0.02, nb),
+                tr_w=rng.uniform(0.05, 0.12, nb), tr_phase=rng.uniform(0, 2 * np.pi, nb),
+                start_frame=sc.traj.get("start_frame", 1))
+    traj["tr_dir"] /= np.linalg.norm(traj["tr_dir"], axis=1, keepdims=True)
+    knots = rng.uniform(0.0, 1.0, n_frames // 8 + 2).astype(np.float32)
+    knots[0] = 0.0
+    return dataclasses.replace(sc, traj=traj, act_sched=knots, meta=dict(sc.meta, motion_seed=int(seed)))

@@ -120,10 +120,11 @@ class DeviceMultigrid:
                        r_w=T(ww[order].astype(np.float32)), blk_ptr=T(blk_ptr), blk_moff=T(blk_moff),
                        minv=T(cage.minv_flat), coarse_lib=T(cl.inv.astype(np.int32)), p_idx=T(p_idx), p_w=T(p_w))
         self._t["resid"] = torch.zeros((sim.n_verts, 4), dtype=torch.float32, device=dev)
+        self._t["rhs"] = torch.zeros((ncoarse, 4), dtype=torch.float32, device=dev)
         g = capi.XpbdCage()
         g.n_fine, g.n_coarse, g.n_blocks = sim.n_verts, ncoarse, int(blk_moff.shape[0])
         g.max_block = int(np.diff(blk_ptr).max())
-        for k in ("r_ptr", "r_fine", "r_w", "blk_ptr", "blk_moff", "minv", "coarse_lib", "p_idx", "p_w", "resid"):
+        for k in ("r_ptr", "r_fine", "r_w", "blk_ptr", "blk_moff", "minv", "coarse_lib", "p_idx", "p_w", "resid", "rhs"):
             setattr(g, k, self._t[k].data_ptr())
         self.g = g
         self.prev = torch.zeros((ncoarse, 4), dtype=torch.float32, device=dev)

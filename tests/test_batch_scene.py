@@ -133,3 +133,21 @@ def test_sharded_oracle_matches_unsharded_gloo():
     for mine, pos in got:
         rows = np.concatenate([np.arange(sc.inst_vptr[i], sc.inst_vptr[i + 1]) for i in mine])
         np.testing.assert_array_equal(pos, full[rows])
+
+
+def test_cage_lattice_neighbours():
+    """The learned warm start's cage description: six axis neighbours found in
+    each muscle's lattice, symmetric (+x of j has j as -x), same owner."""
+    from rlmusclev2_b200.learned import cage_static
+    from rlmusclev2_b200.meshgen import build_cage, humanv2_scene
+    sc = humanv2_scene(seed=1, n_muscles=5, n_bones=4, target_tets=20000, fascia_tets=3000, box=(0.35, 0.35, 0.35))
+    cage = build_cage(sc)
+    st = cage_static(cage, sc)
+    nbr = st["nbr"]
+    assert (nbr >= 0).mean() > 0.5
+    for q in range(6):
+        j = np.nonzero(nbr[:, q] >= 0)[0]
+        k = nbr[j, q]
+        assert (nbr[k, q ^ 1] == j).all()
+        assert (st["owner"][k] == st["owner"][j]).all()
+    assert st["stat"].shape == (cage.coarse_pos.shape[0], 24)

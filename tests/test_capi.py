@@ -40,7 +40,7 @@ def test_ctypes_offsets_match_c_compiler(tmp_path):
     import subprocess
     structs = [capi.XpbdMaterial, capi.XpbdAttachMaterial, capi.XpbdParams, capi.XpbdVerts, capi.XpbdTiles,
                capi.XpbdSdf, capi.XpbdMetrics, capi.XpbdCage, capi.XpbdDcd, capi.XpbdDcdWorkspaceSizes,
-               capi.XpbdCapsule, capi.XpbdPersist, capi.XpbdSdfBatch, capi.XpbdGemm]
+               capi.XpbdCapsule, capi.XpbdPersist, capi.XpbdSdfBatch, capi.XpbdGemm, capi.XpbdCageFeatures]
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "xpbd_b200.h"', 'int main(void){']
     for s in structs:
         lines.append(f'printf("{s.__name__} %zu\\n", sizeof({s.__name__}));')
