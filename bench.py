@@ -40,6 +40,9 @@ CONFIGS = {
 CONFIGS["batched"] = (ROOT / "rlmusclev2_b200" / "configs" / "batched_256.json",
                       "batched_256_box_muscles_3.5M_tets (256 independent instances, per-instance 64^3 SDF and "
                       "activation schedule, 10 substeps x 1 Jacobi iteration)")
+CONFIGS["learned"] = (ROOT / "rlmusclev2_b200" / "configs" / "humanv2_synth_mg_dcd.json",
+                      "humanv2_synth_535k_tets, config-3 mesh and cage, learned coarse warm start + 10 Jacobi "
+                      "iterations per substep vs the plain solver at 20 (no DCD)")
 CONFIG = CONFIGS["humanv2"][0]
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC = ROOT / "profiles" / "ncu_traffic.json"
@@ -465,6 +468,76 @@ def run_profile_case(args):
     return 0
 
 
+def run_learned(args):
+    """The learned coarse warm start against the plain solver on config 3's
+    mesh and cage: ms/frame of each form (CUDA events, frames replayed on
+    held-out motion seed 41) and their error against the 200-iteration solve
+    from the same prediction, measured in this run."""
+    import torch
+
+    from rlmusclev2_b200 import learned as LW
+    from rlmusclev2_b200.meshgen import reseed_motion
+    from rlmusclev2_b200.mg import MultiGridSim
+
+    world, rank, local = _dist_setup()
+    torch.cuda.set_device(local)
+    sim = MultiGridSim(LW.learned_config(), device=f"cuda:{local}")
+    ws = LW.LearnedWarmStart(sim)
+    meta = LW.load_weights(ws)
+    n_l, n_p = 10, 20
+    err, rms = LW.evaluate(ws, [41], 4, [n_l, n_p])
+    base = sim.scene
+    ws.reset(reseed_motion(base, 41))
+    s = sim._stream
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def timed(n, learned):
+        for f in range(1, 1 + args.warmup):
+            ws.frame(f, n, learned)
+        times = []
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            for f in range(1 + args.warmup, 1 + args.warmup + args.steps):
+                ws.begin_frame(f)
+                a, b = ev(), ev()
+                a.record(s)
+                for sub in range(sim.nsubsteps):
+                    ws.substep(sub, n, learned)
+                b.record(s)
+                ws.end_frame()
+                b.synchronize()
+                times.append(a.elapsed_time(b))
+        return float(np.mean(times)), clk.summary()
+
+    ws.reset(reseed_motion(base, 41))
+    t_plain, _ = timed(n_p, False)
+    ws.reset(reseed_motion(base, 41))
+    t_learn, clocks = timed(n_l, True)
+    if world > 1:
+        t = torch.tensor([t_learn, t_plain], device=sim.device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_learn, t_plain = (float(x) for x in t.tolist())
+    summ = lambda e: dict(max_mm=round(float(e.max()), 4), p95_mm=round(float(np.percentile(e, 95)), 4))  # noqa: E731
+    line = {
+        "metric": "ms/frame (learned warm start)", "value": round(t_learn, 4), "unit": "ms/frame", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_learn, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network, f32 solver", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_verts": sim.NV, "n_tets": sim.NT, "cage_verts": ws.nc,
+                   "learned_iterations": n_l, "plain_iterations": n_p, "parallelism": f"replicas x{world}"},
+        "plain_ms_per_frame": round(t_plain, 4), "speedup_vs_plain": round(t_plain / t_learn, 3),
+        "error_vs_200_iteration_solve": {"learned": summ(err["learned"][n_l]), "plain": summ(err["plain"][n_p]),
+                                         "learned_rms_mm": round(float(rms["learned"][n_l].mean()), 5),
+                                         "plain_rms_mm": round(float(rms["plain"][n_p].mean()), 5),
+                                         "frames": "held-out seed 41, frames 1-4"},
+        "gate_0.1mm_max": bool(err["learned"][n_l].max() <= 0.1), "weights": meta, "clocks": clocks,
+    }
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -485,6 +558,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "learned":
+        return run_learned(args)
     return run_ours(args)
 
 

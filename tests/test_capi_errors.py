@@ -1,0 +1,63 @@
+"""Argument checks of the C ABI run before any launch, so they are testable
+without a GPU: every entry point rejects null pointers, bad sizes and
+misaligned buffers with a negative code and a message."""
+import ctypes as C
+
+import pytest
+
+from rlmusclev2_b200 import _capi as capi
+
+ERR_ARG, ERR_ALIGN, ERR_LIMIT = -1, -2, -4
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return capi.load()
+
+
+def _msg(lib):
+    m = lib.xpbd_error_string()
+    return m.decode() if m else ""
+
+
+def test_gemm_rejects_bad_shapes(lib):
+    g = capi.XpbdGemm()
+    assert lib.xpbd_gemm_bf16(C.byref(g), 256, None) == ERR_ARG          # null operands
+    g.a, g.b = 16, 16                                                  # aligned dummies, never dereferenced
+    g.m, g.n, g.k, g.lda, g.ldb = 128, 256, 100, 128, 128
+    assert lib.xpbd_gemm_bf16(C.byref(g), 256, None) == ERR_ARG          # k % 64 != 0
+    assert "k % 64" in _msg(lib)
+    g.k = 128
+    assert lib.xpbd_gemm_bf16(C.byref(g), 24, None) == ERR_ARG           # n_tile not a multiple of 16
+    g.lda = 130
+    assert lib.xpbd_gemm_bf16(C.byref(g), 256, None) == ERR_ARG          # lda not a multiple of 8
+    g.lda, g.a = 128, 8
+    assert lib.xpbd_gemm_bf16(C.byref(g), 256, None) == ERR_ALIGN        # misaligned operand
+
+
+def test_persistent_and_batched_checks(lib):
+    prm, tiles, verts, ps = capi.XpbdParams(), capi.XpbdTiles(), capi.XpbdVerts(), capi.XpbdPersist()
+    assert lib.xpbd_iterate_persistent(None, None, None, None, 1, None) == ERR_ARG
+    assert lib.xpbd_iterate_persistent(C.byref(prm), C.byref(tiles), C.byref(verts), C.byref(ps), -1, None) == ERR_ARG
+    assert lib.xpbd_iterate_persistent(C.byref(prm), C.byref(tiles), C.byref(verts), C.byref(ps), 0, None) == 0
+    assert lib.xpbd_iterate_persistent(C.byref(prm), C.byref(tiles), C.byref(verts), C.byref(ps), 2, None) == ERR_ARG
+    sb = capi.XpbdSdfBatch()
+    assert lib.xpbd_sdf_bake_capsules_batched(C.byref(sb), 2, None, None, C.c_float(0.01), None) == ERR_ARG
+    assert lib.xpbd_vertex_step_batched(C.byref(prm), C.byref(verts), capi.OP_SDF, None, None) < 0
+
+
+def test_learned_glue_checks(lib):
+    cf = capi.XpbdCageFeatures()
+    assert lib.xpbd_cage_features(C.byref(cf), None, None, None, None, None) == ERR_ARG
+    assert lib.xpbd_cage_apply(0, None, None, None, 16, C.c_float(1.0), None, None) == ERR_ARG
+    assert lib.xpbd_fallback_select(10, None, None, C.c_float(2.0), None, None, None, None) == ERR_ARG
+    assert lib.xpbd_adam(0, 0, None, None, 0, None, None, C.c_float(1e-3), C.c_float(0.9), C.c_float(0.999),
+                         C.c_float(1e-8), 1, None, None, 0, None) == ERR_ARG
+    assert lib.xpbd_mse_grad(0, 0, 3, 64, None, 16, None, 3, None, None, 0, None, None) == ERR_ARG
+
+
+def test_noalloc_rejects_oversized_meshes(lib):
+    prm, tiles, verts = capi.XpbdParams(), capi.XpbdTiles(), capi.XpbdVerts()
+    verts.n = capi.NOALLOC_MAX_VERTS + 1
+    assert lib.xpbd_iterate_noalloc(C.byref(prm), C.byref(tiles), C.byref(verts), None) == ERR_LIMIT
+    assert "XPBD_NOALLOC_MAX_VERTS" in _msg(lib)
