@@ -52,6 +52,8 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     float* s_aw = s_az + mtv;
     const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
     const float4* prev4 = reinterpret_cast<const float4*>(V.pprev);
+    __shared__ float s_arap_at[XPBD_MAX_MATERIALS];
+    fill_arap_at(prm, s_arap_at);
     for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
         const int g = T.tile_verts[vbeg + i];
         s_pos[i] = pos4[g];
@@ -63,7 +65,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     }
     __syncthreads();
 
-    project_tile_tets<DAMP, CSET>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_aw);
+    project_tile_tets<DAMP, CSET>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_aw, s_arap_at);
     __syncthreads();
 
     float4* pos4w = reinterpret_cast<float4*>(V.pos);

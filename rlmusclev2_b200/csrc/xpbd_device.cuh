@@ -189,7 +189,9 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
         x0 = y0;
         x1 = y1;
         x2 = y2;
-        if (ch <= 1e-12f) {  // step <= 1e-6: quadratic convergence leaves an error ~1e-12
+        // step <= 1e-4: Newton's quadratic convergence leaves an error ~|step|^2/2 = 5e-9
+        // after this update, below the FP32 resolution of R's entries
+        if (ch <= 1e-8f) {
             R.m[0][0] = x0.x; R.m[1][0] = x0.y; R.m[2][0] = x0.z;
             R.m[0][1] = x1.x; R.m[1][1] = x1.y; R.m[2][1] = x1.z;
             R.m[0][2] = x2.x; R.m[1][2] = x2.y; R.m[2][2] = x2.z;
@@ -207,7 +209,14 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
 // C = ||s - 1|| = ||F - U V^T||_F and dC/dF = U diag((s-1)/C) V^T = (F - U V^T)/C,
 // U V^T being the rotation nearest F.  For det F > 0 that rotation is the polar
 // factor, obtained without the SVD; inverted or degenerate tets use the SVD.
-__device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float k, float dt, float3 (&acc)[4],
+// at = alpha / dt^2 with alpha = 1 / stiffness, evaluated once per material
+// per launch (arap_alpha_tilde) in the reference's operation order.
+__device__ __forceinline__ float arap_alpha_tilde(float k, float dt) {
+    const float alpha = 1.f / k;
+    return alpha / (dt * dt);
+}
+
+__device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float at, float3 (&acc)[4],
                                             bool force_svd = false) {
     M3 G;
     M3 R;
@@ -249,8 +258,6 @@ __device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, cons
     g[3] = (-g[0] - g[1]) - g[2];
     const float wsum = p[0].w * dot(g[0], g[0]) + p[1].w * dot(g[1], g[1]) + p[2].w * dot(g[2], g[2]) + p[3].w * dot(g[3], g[3]);
     if (wsum == 0.f) return false;
-    const float alpha = 1.f / k;
-    const float at = alpha / (dt * dt);
     const float dL = -C / (wsum + at);
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[i] = acc[i] + (dL * p[i].w) * g[i];

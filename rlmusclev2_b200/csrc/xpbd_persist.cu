@@ -90,6 +90,8 @@ __global__ void __launch_bounds__(kThreads, MINB)
     const size_t nv = size_t(V.n);
     const uint32_t phase0 = P.sync[2];
     const uint32_t ops = XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_PIN;
+    __shared__ float s_arap_at[XPBD_MAX_MATERIALS];
+    fill_arap_at(prm, s_arap_at);
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
         const int g = T.tile_verts[vbeg + i];
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
             s_aw[i] = 0.f;
         }
         __syncthreads();
-        project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_aw);
+        project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_aw, s_arap_at);
         __syncthreads();
         for (int i = threadIdx.x; i < nint; i += blockDim.x) {
             float4 pp = s_pos[i];

@@ -56,6 +56,14 @@ __device__ __forceinline__ void finish_vertex(const XpbdParams& prm, const XpbdV
 }
 
 // ---------------------------------------------------------------------------
+// Per-material ARAP alpha tilde into shared memory (followed by the caller's
+// __syncthreads before the first projection).
+__device__ __forceinline__ void fill_arap_at(const XpbdParams& prm, float* s_at) {
+    for (int i = threadIdx.x; i < prm.n_materials && i < XPBD_MAX_MATERIALS; i += blockDim.x)
+        s_at[i] = arap_alpha_tilde(prm.materials[i].arap_k, prm.dt);
+}
+
+// ---------------------------------------------------------------------------
 // Constraint sets compiled into a tile-pass instance: the heavier sets cost
 // registers (and occupancy) even for tets that do not use them.
 enum { CSET_LIGHT = 0, CSET_VOL = 1, CSET_FULL = 2 };  // ARAP+aniso | +volume | +volume+SNH
@@ -66,7 +74,7 @@ enum { CSET_LIGHT = 0, CSET_VOL = 1, CSET_FULL = 2 };  // ARAP+aniso | +volume |
 template <bool DAMP, int CSET, bool PREFETCH = false>
 __device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const XpbdTiles& T, int tile,
                                                   const float4* s_pos, const float4* s_prev, float* s_ax, float* s_ay,
-                                                  float* s_az, float* s_aw) {
+                                                  float* s_az, float* s_aw, const float* s_arap_at) {
     const int t1 = T.tile_tptr[tile + 1];
     const uint4* tq = reinterpret_cast<const uint4*>(T.tet_q);
     const float4* tb0 = reinterpret_cast<const float4*>(T.tet_b0);
@@ -140,7 +148,8 @@ __device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const X
                           prm.fiber_stiffness_scale, prm.dt, d))
                 nact += 1.f;
         }
-        if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, m.arap_k, prm.dt, d, (prm.tile_variant & 2) != 0))
+        if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, s_arap_at[min(int(q.z & 0xffu), XPBD_MAX_MATERIALS - 1)], d,
+                                                   (prm.tile_variant & 2) != 0))
             nact += 1.f;
         if (nact != 0.f) {
 #pragma unroll
