@@ -443,9 +443,9 @@ def run_profile_case(args):
     launches issued eagerly, without the graph).  box3m: a 64x64x120-hex box (2.95M tets, ~150 MB of tet
     streams, larger than L2) and ``--steps`` Jacobi iterations of its tet pass."""
     import torch
-    if args.profile_case == "humanv2":
+    if args.profile_case in ("humanv2", "humanv2_mg_dcd"):
         from rlmusclev2_b200.mg import MultiGridSim, load_config
-        sim = MultiGridSim(load_config(str(CONFIG)))
+        sim = MultiGridSim(load_config(str(CONFIGS[args.profile_case][0])))
         sim.use_graphs = False  # the same launches, issued eagerly so the profiler lists each kernel
         for f in range(sim.start_frame, sim.start_frame + args.steps):
             sim.set_fiber_activation(sim.scene.activation(f))
@@ -547,7 +547,7 @@ def main():
     ap.add_argument("--config", choices=sorted(CONFIGS), default="humanv2",
                     help="workload (default: the 535k-tet configuration the metric is quoted on)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-case", choices=["humanv2", "box3m"], default=None,
+    ap.add_argument("--profile-case", choices=["humanv2", "humanv2_mg_dcd", "box3m"], default=None,
                     help="run a small fixed workload for ncu and exit")
     args = ap.parse_args()
     global CONFIG, WORKLOAD

@@ -15,6 +15,8 @@
 // bary-weighted tangential displacement, Jacobi averaging.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "xpbd_common.cuh"
 #include "xpbd_device.cuh"
 
@@ -23,7 +25,9 @@ using namespace xpbd;
 namespace {
 
 constexpr int kSortThreads = 256;
-constexpr int kSortChunk = 4096;  // keys per CTA per pass
+constexpr int kSortChunk = 1024;  // keys per CTA per pass (118 CTAs for 120k triangles)
+constexpr int kScanItems = 4;     // consecutive elements per thread in the block scan
+constexpr int kScanBlock = 1024 * kScanItems;
 constexpr int kStack = 64;
 constexpr float kThresh = 1.0e-5f;  // udcf/kernel.py:40 THRESH
 
@@ -85,39 +89,85 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint32_t* __re
     for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[d * nblk + b] = h[d];  // digit-major
 }
 
-// exclusive scan of hist (256*nblk ints, digit-major) in place, one CTA
-__global__ void __launch_bounds__(1024) k_scan_excl(int* __restrict__ a, int n, int* __restrict__ total) {
+// Exclusive scan in three launches: per-block scans of kScanBlock elements
+// (each thread a run of kScanItems, warp shuffles across threads) leaving
+// block totals in sums[], one CTA scanning sums[], and a launch adding each
+// block's offset.  total (optional) receives the sum of all elements.
+__device__ __forceinline__ int block_excl_scan(int v, int* warp_sums, int* block_total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int t = lane < int(blockDim.x >> 5) ? warp_sums[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        warp_sums[lane] = t;
+    }
+    __syncthreads();
+    const int incl = x + (w > 0 ? warp_sums[w - 1] : 0);
+    if (block_total && threadIdx.x == blockDim.x - 1) *block_total = incl;
+    return incl - v;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_blocks(int* __restrict__ a, int n, int* __restrict__ sums) {
+    __shared__ int warp_sums[32];
+    __shared__ int total;
+    const int base = blockIdx.x * kScanBlock + threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int run = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        v[q] = base + q < n ? a[base + q] : 0;
+        run += v[q];
+    }
+    int off = block_excl_scan(run, warp_sums, &total);
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        if (base + q < n) a[base + q] = off;
+        off += v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_sums(int* __restrict__ sums, int nb, int* __restrict__ total) {
     __shared__ int warp_sums[32];
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (int base = 0; base < n; base += blockDim.x) {
-        const int i = base + threadIdx.x;
-        const int v = i < n ? a[i] : 0;
-        int x = v;
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) warp_sums[w] = x;
+    for (int b0 = 0; b0 < nb; b0 += blockDim.x) {
+        const int i = b0 + threadIdx.x;
+        const int v = i < nb ? sums[i] : 0;
+        __shared__ int round_total;
+        const int e = block_excl_scan(v, warp_sums, &round_total) + carry;
+        if (i < nb) sums[i] = e;
         __syncthreads();
-        if (w == 0) {
-            int s = lane < (blockDim.x >> 5) ? warp_sums[lane] : 0;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, s, o);
-                if (lane >= o) s += y;
-            }
-            warp_sums[lane] = s;
-        }
-        __syncthreads();
-        const int incl = x + (w > 0 ? warp_sums[w - 1] : 0) + carry;
-        if (i < n) a[i] = incl - v;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry = incl;
+        if (threadIdx.x == 0) carry += round_total;
         __syncthreads();
     }
     if (total && threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_add(int* __restrict__ a, int n, const int* __restrict__ sums) {
+    const int add = sums[blockIdx.x];
+    const int base = blockIdx.x * kScanBlock + threadIdx.x * kScanItems;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q)
+        if (base + q < n) a[base + q] += add;
+}
+
+void scan_excl(int* a, int n, int* total, int* scratch, cudaStream_t s) {
+    const int nb = (n + kScanBlock - 1) / kScanBlock;
+    k_scan_blocks<<<nb, 1024, 0, s>>>(a, n, scratch);
+    k_scan_sums<<<1, 1024, 0, s>>>(scratch, nb, total);
+    if (nb > 1) k_scan_add<<<nb, 1024, 0, s>>>(a, n, scratch);
 }
 
 // Stable scatter: keys of a chunk are ranked round by round (256 per round);
@@ -254,11 +304,15 @@ __device__ __forceinline__ bool pair_ok(const XpbdDcd& D, int i, int j) {
     return true;
 }
 
+// Thread t queries the triangle at Morton position t, so a warp's queries
+// are spatially close and walk similar paths; outputs stay indexed by the
+// triangle id (the pair order is the same as with triangle-ordered threads).
 template <bool FILL>
 __global__ void k_traverse(XpbdDcd D) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = D.n_tris;
-    if (i >= n) return;
+    if (t >= n) return;
+    const int i = D.ws_vals[t];
     const float4* nodes = reinterpret_cast<const float4*>(D.ws_nodes);
     const float4* tri_box = nodes + 2 * (2 * n - 1);  // unsorted leaf copy, triangle order
     const float4 qlo = tri_box[2 * i], qhi = tri_box[2 * i + 1];
@@ -571,7 +625,8 @@ int xpbd_dcd_workspace_query(int32_t n_tris, XpbdDcdWorkspaceSizes* out) {
     const int nblk = (n_tris + kSortChunk - 1) / kSortChunk;
     out->nodes_floats = int64_t(2 * (2 * n_tris - 1)) * 4 * 2;  // sorted tree + unsorted leaf copy
     out->keys = n_tris;
-    out->hist = int64_t(256) * nblk;
+    const int64_t scan_blocks = (std::max<int64_t>(int64_t(256) * nblk, n_tris) + kScanBlock - 1) / kScanBlock;
+    out->hist = int64_t(256) * nblk + scan_blocks;  // radix histograms, then the scan's block sums
     out->child = int64_t(2) * (n_tris > 1 ? n_tris - 1 : 1);
     out->parent = int64_t(2) * n_tris - 1;
     out->flags = n_tris > 1 ? n_tris - 1 : 1;
@@ -594,6 +649,7 @@ int xpbd_dcd_broadphase(const XpbdDcd* D, const float* pos4, int32_t snapshot_pr
     k_tri_aabb<<<(n + 255) / 256, 256, 0, s>>>(Dl, pos4);
     // radix sort (keys, tri ids): 4 passes of 8 bits, ping-pong
     const int nblk = (n + kSortChunk - 1) / kSortChunk;
+    int* scan_scratch = D->ws_hist + int64_t(256) * nblk;
     uint32_t* ka = D->ws_keys;
     int32_t* va = D->ws_vals;
     uint32_t* kb = D->ws_keys2;
@@ -601,7 +657,7 @@ int xpbd_dcd_broadphase(const XpbdDcd* D, const float* pos4, int32_t snapshot_pr
     for (int pass = 0; pass < 4; ++pass) {
         const int shift = 8 * pass;
         k_sort_hist<<<nblk, kSortThreads, 0, s>>>(ka, n, shift, D->ws_hist, nblk);
-        k_scan_excl<<<1, 1024, 0, s>>>(D->ws_hist, 256 * nblk, nullptr);
+        scan_excl(D->ws_hist, 256 * nblk, nullptr, scan_scratch, s);
         k_sort_scatter<<<nblk, kSortThreads, 0, s>>>(ka, va, kb, vb, n, shift, D->ws_hist, nblk);
         uint32_t* tk = ka; ka = kb; kb = tk;
         int32_t* tv = va; va = vb; vb = tv;
@@ -616,7 +672,7 @@ int xpbd_dcd_broadphase(const XpbdDcd* D, const float* pos4, int32_t snapshot_pr
     k_permute_leaves<<<(n + 255) / 256, 256, 0, s>>>(*D);
     if (n > 1) k_refit<<<(n + 255) / 256, 256, 0, s>>>(*D);
     k_traverse<false><<<(n + 127) / 128, 128, 0, s>>>(*D);
-    k_scan_excl<<<1, 1024, 0, s>>>(D->ws_count, n, D->ws_total);
+    scan_excl(D->ws_count, n, D->ws_total, scan_scratch, s);
     k_traverse<true><<<(n + 127) / 128, 128, 0, s>>>(*D);
     k_pairs_total<<<1, 32, 0, s>>>(*D);
     return cuda_check("xpbd_dcd_broadphase");
