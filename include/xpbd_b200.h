@@ -320,7 +320,7 @@ typedef struct XpbdDcd {
     float friction_static, friction_dynamic;
     float max_push;           /* > 0: clamp contact depth (UdcfParams.max_push) */
     float box_lo[3], box_hi[3]; /* Morton quantisation box (centres outside are clamped) */
-    int32_t* pairs;           /* [max_pairs][2] (i, j > i), deterministic order */
+    int32_t* pairs;           /* [max_pairs][2] (i, j > i), deterministic order; 16-byte aligned */
     int32_t* n_pairs;         /* [1] candidate pairs found (may exceed max_pairs) */
     int32_t* n_contacts;      /* [1] contacts found (may exceed max_contacts) */
     int32_t* c_ids;           /* [max_contacts][8]: cur tri verts, pair index, closest tri verts, 0 */
@@ -337,13 +337,14 @@ typedef struct XpbdDcd {
     int32_t* ws_child;        /* [n_tris-1][2] */
     int32_t* ws_parent;       /* [2 n_tris - 1] */
     int32_t* ws_flags;        /* [n_tris-1] refit arrival counters */
-    int32_t* ws_count;        /* [n_tris] pairs per triangle, then their offsets */
+    int32_t* ws_count;        /* [n_tris] pairs per Morton position, then their offsets */
     int32_t* ws_total;        /* [1] */
+    int32_t* ws_slots;        /* [16][n_tris] first partners of each query (counting pass) */
 } XpbdDcd;
 
 /* Element counts of the DCD workspace arrays for n_tris triangles. */
 typedef struct XpbdDcdWorkspaceSizes {
-    int64_t nodes_floats, keys, hist, child, parent, flags, count;
+    int64_t nodes_floats, keys, hist, child, parent, flags, count, slots;
 } XpbdDcdWorkspaceSizes;
 
 int xpbd_dcd_workspace_query(int32_t n_tris, XpbdDcdWorkspaceSizes* out);

@@ -85,12 +85,12 @@ class XpbdDcd(C.Structure):
                 ("ws_nodes", C.c_void_p), ("ws_keys", C.c_void_p), ("ws_vals", C.c_void_p),
                 ("ws_keys2", C.c_void_p), ("ws_vals2", C.c_void_p), ("ws_hist", C.c_void_p),
                 ("ws_child", C.c_void_p), ("ws_parent", C.c_void_p), ("ws_flags", C.c_void_p),
-                ("ws_count", C.c_void_p), ("ws_total", C.c_void_p)]
+                ("ws_count", C.c_void_p), ("ws_total", C.c_void_p), ("ws_slots", C.c_void_p)]
 
 
 class XpbdDcdWorkspaceSizes(C.Structure):
     _fields_ = [("nodes_floats", C.c_int64), ("keys", C.c_int64), ("hist", C.c_int64), ("child", C.c_int64),
-                ("parent", C.c_int64), ("flags", C.c_int64), ("count", C.c_int64)]
+                ("parent", C.c_int64), ("flags", C.c_int64), ("count", C.c_int64), ("slots", C.c_int64)]
 
 
 class XpbdMetrics(C.Structure):

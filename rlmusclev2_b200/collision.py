@@ -171,7 +171,8 @@ class DcdBuffers:
             keys2=torch.zeros(int(sz.keys), dtype=i32, device=dev), vals2=torch.zeros(int(sz.keys), dtype=i32, device=dev),
             hist=torch.zeros(int(sz.hist), dtype=i32, device=dev), child=torch.zeros(int(sz.child), dtype=i32, device=dev),
             parent=torch.zeros(int(sz.parent), dtype=i32, device=dev), flags=torch.zeros(int(sz.flags), dtype=i32, device=dev),
-            count=torch.zeros(int(sz.count), dtype=i32, device=dev))
+            count=torch.zeros(int(sz.count), dtype=i32, device=dev),
+            slots=torch.zeros(int(sz.slots), dtype=i32, device=dev))
         t = self.t
         d = capi.XpbdDcd()
         d.n_tris, d.n_verts, d.max_pairs, d.max_contacts = n, int(n_verts), params.max_pairs, params.max_contacts
@@ -190,7 +191,7 @@ class DcdBuffers:
         d.ws_nodes, d.ws_keys, d.ws_vals = t["nodes"].data_ptr(), t["keys"].data_ptr(), t["vals"].data_ptr()
         d.ws_keys2, d.ws_vals2, d.ws_hist = t["keys2"].data_ptr(), t["vals2"].data_ptr(), t["hist"].data_ptr()
         d.ws_child, d.ws_parent, d.ws_flags = t["child"].data_ptr(), t["parent"].data_ptr(), t["flags"].data_ptr()
-        d.ws_count = t["count"].data_ptr()
+        d.ws_count, d.ws_slots = t["count"].data_ptr(), t["slots"].data_ptr()
         self.d = d
 
     def broadphase(self, pos4: torch.Tensor, snapshot_prev: bool, stream) -> None:

@@ -29,6 +29,7 @@ constexpr int kSortChunk = 1024;  // keys per CTA per pass (118 CTAs for 120k tr
 constexpr int kScanItems = 4;     // consecutive elements per thread in the block scan
 constexpr int kScanBlock = 1024 * kScanItems;
 constexpr int kStack = 64;
+constexpr int kSlots = 16;  // partners a query keeps from the counting pass
 constexpr float kThresh = 1.0e-5f;  // udcf/kernel.py:40 THRESH
 
 struct Aabb {
@@ -257,7 +258,9 @@ __global__ void k_permute_leaves(XpbdDcd D) {
     const float4* src = reinterpret_cast<const float4*>(D.ws_nodes) + 2 * (2 * D.n_tris - 1);
     float4* dst = reinterpret_cast<float4*>(D.ws_nodes);
     const int leaf = D.n_tris - 1 + s;
-    dst[2 * leaf] = src[2 * tri];
+    float4 lo = src[2 * tri];
+    lo.w = __int_as_float(s);  // last Morton position under the node (leaf: its own)
+    dst[2 * leaf] = lo;
     dst[2 * leaf + 1] = src[2 * tri + 1];
 }
 
@@ -271,13 +274,15 @@ __global__ void k_refit(XpbdDcd D) {
     for (int step = 0; step < n; ++step) {
         const int p = D.ws_parent[node];
         if (p < 0) break;
-        __threadfence();
-        if (atomicAdd(&D.ws_flags[p], 1) == 0) return;  // first arrival: the sibling finishes p
-        __threadfence();
+        // release this thread's box writes, acquire the sibling's (one acq_rel atomic)
+        int arrived;
+        asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(arrived) : "l"(&D.ws_flags[p]) : "memory");
+        if (arrived == 0) return;  // first arrival: the sibling finishes p
         const int a = D.ws_child[2 * p], b = D.ws_child[2 * p + 1];
         const float4 alo = __ldcg(&nodes[2 * a]), ahi = __ldcg(&nodes[2 * a + 1]);
         const float4 blo = __ldcg(&nodes[2 * b]), bhi = __ldcg(&nodes[2 * b + 1]);
-        nodes[2 * p] = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.f);
+        nodes[2 * p] = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z),
+                                   __int_as_float(max(__float_as_int(alo.w), __float_as_int(blo.w))));
         nodes[2 * p + 1] = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f);
         node = p;
     }
@@ -304,51 +309,83 @@ __device__ __forceinline__ bool pair_ok(const XpbdDcd& D, int i, int j) {
     return true;
 }
 
-// Thread t queries the triangle at Morton position t, so a warp's queries
-// are spatially close and walk similar paths; outputs stay indexed by the
-// triangle id (the pair order is the same as with triangle-ordered threads).
+// Thread t queries the triangle at Morton position t against the leaves at
+// later positions only: every unordered overlapping pair is met once, by the
+// query that comes first in Morton order, and subtrees whose last position
+// (kept in the node's lo.w) is <= t are skipped whole.  A warp's queries are
+// spatially close and walk similar paths.  Both children are tested before
+// descending; one stack entry per level with two live children.
+// The counting pass keeps the first kSlots partners in ws_slots; the fill
+// pass copies those and re-traverses only queries with more partners.
+// Pairs are written as (min, max) triangle id, grouped by query position.
+__device__ __forceinline__ bool live(const float4& qlo, const float4& qhi, const float4& lo, const float4& hi, int t) {
+    return __float_as_int(lo.w) > t && overlap(qlo, qhi, lo, hi);
+}
+
 template <bool FILL>
-__global__ void k_traverse(XpbdDcd D) {
+__device__ __forceinline__ void emit_leaf(const XpbdDcd& D, int i, int leaf_pos, int t, int& cnt, int& out) {
+    const int j = D.ws_vals[leaf_pos];
+    const int a = min(i, j), b = max(i, j);
+    if (!pair_ok(D, a, b)) return;
+    if (FILL) {
+        if (out < D.max_pairs) reinterpret_cast<int2*>(D.pairs)[out] = make_int2(a, b);
+        ++out;
+    } else {
+        if (cnt < kSlots) D.ws_slots[int64_t(cnt) * D.n_tris + t] = j;
+        ++cnt;
+    }
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(128) k_traverse(XpbdDcd D) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = D.n_tris;
     if (t >= n) return;
     const int i = D.ws_vals[t];
-    const float4* nodes = reinterpret_cast<const float4*>(D.ws_nodes);
-    const float4* tri_box = nodes + 2 * (2 * n - 1);  // unsorted leaf copy, triangle order
-    const float4 qlo = tri_box[2 * i], qhi = tri_box[2 * i + 1];
-    int cnt = 0;
-    int out = FILL ? D.ws_count[i] : 0;
-    int stack[kStack];
-    int sp = 0;
-    stack[sp++] = (n == 1) ? 0 : 0;
-    bool single = (n == 1);
-    while (sp > 0) {
-        const int node = stack[--sp];
-        const int idx = single ? (n - 1) : node;
-        if (!overlap(qlo, qhi, nodes[2 * idx], nodes[2 * idx + 1])) continue;
-        if (idx >= n - 1) {  // leaf
-            const int j = D.ws_vals[idx - (n - 1)];
-            if (pair_ok(D, i, j)) {
-                if (FILL) {
-                    if (out < D.max_pairs) {
-                        D.pairs[2 * out] = i;
-                        D.pairs[2 * out + 1] = j;
-                    }
-                    ++out;
-                } else {
-                    ++cnt;
-                }
+    int cnt = 0, out = 0;
+    if (FILL) {
+        out = D.ws_count[t];
+        const int end = t + 1 < n ? D.ws_count[t + 1] : *D.ws_total;
+        const int c = end - out;
+        if (c <= kSlots) {
+            for (int k = 0; k < c; ++k, ++out) {
+                if (out >= D.max_pairs) break;
+                const int j = D.ws_slots[int64_t(k) * n + t];
+                reinterpret_cast<int2*>(D.pairs)[out] = make_int2(min(i, j), max(i, j));
             }
-            continue;
+            return;
         }
-        if (sp + 2 > kStack) {
-            atomicOr(D.status, XPBD_STATUS_STACK_OVERFLOW);
-            break;
-        }
-        stack[sp++] = D.ws_child[2 * idx];
-        stack[sp++] = D.ws_child[2 * idx + 1];
     }
-    if (!FILL) D.ws_count[i] = cnt;
+    if (n > 1) {
+        const float4* nodes = reinterpret_cast<const float4*>(D.ws_nodes);
+        const float4* tri_box = nodes + 2 * (2 * n - 1);  // unsorted leaf copy, triangle order
+        const float4 qlo = tri_box[2 * i], qhi = tri_box[2 * i + 1];
+        int stack[kStack];
+        int sp = 0;
+        int node = 0;  // the root's box holds every query box
+        while (true) {
+            const int ca = D.ws_child[2 * node], cb = D.ws_child[2 * node + 1];
+            const bool la = live(qlo, qhi, nodes[2 * ca], nodes[2 * ca + 1], t);
+            const bool lb = live(qlo, qhi, nodes[2 * cb], nodes[2 * cb + 1], t);
+            const bool da = la && ca < n - 1, db = lb && cb < n - 1;  // internal children to descend
+            if (la && !da) emit_leaf<FILL>(D, i, ca - (n - 1), t, cnt, out);
+            if (lb && !db) emit_leaf<FILL>(D, i, cb - (n - 1), t, cnt, out);
+            if (da && db) {
+                if (sp >= kStack) {
+                    atomicOr(D.status, XPBD_STATUS_STACK_OVERFLOW);
+                    break;
+                }
+                stack[sp++] = cb;
+                node = ca;
+            } else if (da || db) {
+                node = da ? ca : cb;
+            } else {
+                if (sp == 0) break;
+                node = stack[--sp];
+            }
+        }
+    }
+    if (!FILL) D.ws_count[t] = cnt;
 }
 
 __global__ void k_pairs_total(XpbdDcd D) {
@@ -607,10 +644,10 @@ int check_dcd(const XpbdDcd* D) {
     if (!D || D->n_tris <= 0 || D->n_verts <= 0 || !D->tris || !D->pairs || !D->n_pairs || !D->n_contacts ||
         !D->c_ids || !D->c_data || !D->x_prev || !D->dP || !D->status || !D->ws_nodes || !D->ws_keys || !D->ws_vals ||
         !D->ws_keys2 || !D->ws_vals2 || !D->ws_hist || !D->ws_child || !D->ws_parent || !D->ws_flags || !D->ws_count ||
-        !D->ws_total)
+        !D->ws_total || !D->ws_slots)
         return fail(XPBD_ERR_ARG, "XpbdDcd: null member or empty size");
     if (D->max_pairs <= 0 || D->max_contacts <= 0) return fail(XPBD_ERR_ARG, "XpbdDcd: capacities must be > 0");
-    if (!aligned16(D->ws_nodes) || !aligned16(D->c_ids) || !aligned16(D->c_data) || !aligned16(D->x_prev) ||
+    if (!aligned16(D->ws_nodes) || !aligned16(D->pairs) || !aligned16(D->c_ids) || !aligned16(D->c_data) || !aligned16(D->x_prev) ||
         !aligned16(D->dP))
         return fail(XPBD_ERR_ALIGN, "XpbdDcd: 16-byte alignment");
     return XPBD_OK;
@@ -631,6 +668,7 @@ int xpbd_dcd_workspace_query(int32_t n_tris, XpbdDcdWorkspaceSizes* out) {
     out->parent = int64_t(2) * n_tris - 1;
     out->flags = n_tris > 1 ? n_tris - 1 : 1;
     out->count = n_tris;
+    out->slots = int64_t(kSlots) * n_tris;
     return XPBD_OK;
 }
 
