@@ -394,7 +394,8 @@ def run_ours(args):
         co = sim.mg.coarse
         coarse = 1 if (co.use_persistent and co._persist_fits) else 2 * sim.mg.iters
     per_sub = 1 + fine + (2 + coarse if sim.mg is not None else 0)
-    per_sub += 21 if getattr(sim, "dcd", None) is not None else 0  # broadphase on the first iteration
+    if getattr(sim, "dcd", None) is not None:  # broadphase on the first iteration
+        per_sub += sim.dcd.buf.broadphase_launches(True)
     launches_per_frame = 1 + (1 if sim.collision_solvers else 0) + (1 if sim._has_pins else 0) + (
         1 if sim.mg is not None else 0) + sim.nsubsteps * per_sub + 1
     n_iter = sim.nsubsteps * sim.fine_iters

@@ -198,6 +198,14 @@ class DcdBuffers:
         capi.check(self.lib.xpbd_dcd_broadphase(C.byref(self.d), C.c_void_p(pos4.data_ptr()), int(snapshot_prev),
                                                 stream))
 
+    def broadphase_launches(self, snapshot_prev: bool = True) -> int:
+        """Kernels one xpbd_dcd_broadphase call launches: snapshot copy, boxes,
+        cooperative sort, build, leaf permute, refit, counting traversal, the
+        count scan (2 launches, 3 above 4096 triangles), fill pass, total."""
+        n = int(self.d.n_tris)
+        scan = 2 + (1 if n > 4096 else 0)
+        return int(snapshot_prev) + 2 + (1 if n > 1 else 0) + 1 + (1 if n > 1 else 0) + 1 + scan + 2
+
     def narrow_respond(self, pos4: torch.Tensor, stream) -> None:
         capi.check(self.lib.xpbd_dcd_narrow_respond(C.byref(self.d), C.c_void_p(pos4.data_ptr()), stream))
 
@@ -240,6 +248,9 @@ class UdcfDcdCollider:
         self.sim.synchronize()
         c = self.buf.counters()
         p = self.params
+        if c["status"] & capi.STATUS_BARRIER_TIMEOUT:
+            raise RuntimeError("[udcf_dcd] the broadphase sort gave up waiting at a grid barrier; "
+                               "pairs are invalid (zero the workspace before the next call)")
         if c["status"] & capi.STATUS_STACK_OVERFLOW:
             print("[udcf_dcd] WARNING: BVH traversal stack overflow")
         if c["n_pairs"] > p.max_pairs or c["n_contacts"] > p.max_contacts:

@@ -19,13 +19,13 @@
 
 #include "xpbd_common.cuh"
 #include "xpbd_device.cuh"
+#include "xpbd_grid.cuh"
 
 using namespace xpbd;
 
 namespace {
 
-constexpr int kSortThreads = 256;
-constexpr int kSortChunk = 1024;  // keys per CTA per pass (118 CTAs for 120k triangles)
+constexpr int kSortThreads = 1024;  // keys per scatter round; the sort's CTA size
 constexpr int kScanItems = 4;     // consecutive elements per thread in the block scan
 constexpr int kScanBlock = 1024 * kScanItems;
 constexpr int kStack = 64;
@@ -78,18 +78,6 @@ __global__ void k_tri_aabb(XpbdDcd D, const float* __restrict__ pos4) {
 }
 
 // ---------------------------------------------------------- radix sort
-__global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint32_t* __restrict__ keys, int n, int shift,
-                                                            int* __restrict__ hist, int nblk) {
-    __shared__ int h[256];
-    for (int d = threadIdx.x; d < 256; d += blockDim.x) h[d] = 0;
-    __syncthreads();
-    const int b = blockIdx.x;
-    const int beg = b * kSortChunk, end = min(n, beg + kSortChunk);
-    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) atomicAdd(&h[(keys[i] >> shift) & 255u], 1);
-    __syncthreads();
-    for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[d * nblk + b] = h[d];  // digit-major
-}
-
 // Exclusive scan in three launches: per-block scans of kScanBlock elements
 // (each thread a run of kScanItems, warp shuffles across threads) leaving
 // block totals in sums[], one CTA scanning sums[], and a launch adding each
@@ -171,43 +159,98 @@ void scan_excl(int* a, int n, int* total, int* scratch, cudaStream_t s) {
     if (nb > 1) k_scan_add<<<nb, 1024, 0, s>>>(a, n, scratch);
 }
 
-// Stable scatter: keys of a chunk are ranked round by round (256 per round);
-// within a round, the rank of a key among equal digits is the count of equal
-// digits in earlier warps plus the lanes before it in its own warp.
-__global__ void __launch_bounds__(kSortThreads)
-    k_sort_scatter(const uint32_t* __restrict__ kin, const int32_t* __restrict__ vin, uint32_t* __restrict__ kout,
-                   int32_t* __restrict__ vout, int n, int shift, const int* __restrict__ offs, int nblk) {
-    __shared__ int run[256];
+// Radix sort of (Morton key, triangle id), 4 passes of 8 bits, in one
+// cooperative launch: CTA b owns the contiguous chunk [b C, (b+1) C) of the
+// pass input.  Per pass: (A) chunk histogram -> hist[b][256]; grid barrier;
+// (B) every CTA sums the histograms itself (digit totals, and the counts of
+// the chunks before its own) and scans the totals over digits, giving its
+// first output slot per digit; (C) stable scatter in rounds of kSortThreads
+// keys: warps rank equal digits with __match_any_sync, per-digit prefix over
+// the warps in shared memory; grid barrier before the next pass reads.
+// Even pass count: the sorted data ends in ws_keys/ws_vals.
+__device__ __forceinline__ int add_excl_over_warps(int (*wcnt)[256], int d, int run) {
+    for (int ww = 0; ww < kSortThreads / 32; ++ww) {
+        const int c = wcnt[ww][d];
+        wcnt[ww][d] = run;
+        run += c;
+    }
+    return run;
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_sort_coop(XpbdDcd D, int chunk, uint32_t* sync) {
     __shared__ int wcnt[kSortThreads / 32][256];
-    const int b = blockIdx.x;
-    for (int d = threadIdx.x; d < 256; d += blockDim.x) run[d] = offs[d * nblk + b];
+    __shared__ int run[256];
+    __shared__ int part[kSortThreads / 256][256];
+    __shared__ int warp_sums[32];
+    const int n = D.n_tris, G = gridDim.x, b = blockIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int beg = b * kSortChunk, end = min(n, beg + kSortChunk);
-    for (int r = beg; r < end; r += blockDim.x) {
-        for (int k = threadIdx.x; k < (kSortThreads / 32) * 256; k += blockDim.x) (&wcnt[0][0])[k] = 0;
+    const int beg = min(n, b * chunk), end = min(n, beg + chunk);
+    int* hist = D.ws_hist;  // [G][256]
+    uint32_t* ks = D.ws_keys;
+    int32_t* vs = D.ws_vals;
+    uint32_t* kd = D.ws_keys2;
+    int32_t* vd = D.ws_vals2;
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 8 * pass;
+        // (A) chunk histogram
+        if (threadIdx.x < 256) run[threadIdx.x] = 0;
         __syncthreads();
-        const int i = r + threadIdx.x;
-        const bool valid = i < end;
-        const uint32_t key = valid ? kin[i] : 0u;
-        const int dig = valid ? int((key >> shift) & 255u) : 256;
-        const unsigned peers = __match_any_sync(0xffffffffu, dig);
-        const int lrank = __popc(peers & ((1u << lane) - 1u));
-        if (valid && lrank == 0) wcnt[w][dig] = __popc(peers);
-        __syncthreads();
-        if (valid) {
-            int before = 0;
-            for (int ww = 0; ww < w; ++ww) before += wcnt[ww][dig];
-            const int dst = run[dig] + before + lrank;
-            kout[dst] = key;
-            vout[dst] = vin[i];
+        for (int i = beg + int(threadIdx.x); i < end; i += kSortThreads) {
+            const int dig = int((ks[i] >> shift) & 255u);
+            const unsigned peers = __match_any_sync(__activemask(), dig);
+            if ((peers & ((1u << lane) - 1u)) == 0) atomicAdd(&run[dig], __popc(peers));
         }
         __syncthreads();
-        for (int d = threadIdx.x; d < 256; d += blockDim.x) {
-            int s = 0;
-            for (int ww = 0; ww < kSortThreads / 32; ++ww) s += wcnt[ww][d];
-            run[d] += s;
+        if (threadIdx.x < 256) hist[b * 256 + threadIdx.x] = run[threadIdx.x];
+        grid_barrier(sync, D.status);
+        // (B) first output slot of each digit for this chunk
+        {
+            const int d = threadIdx.x & 255, q = threadIdx.x >> 8;
+            constexpr int kQ = kSortThreads / 256;
+            int tot = 0, pre = 0;
+            for (int bb = q; bb < G; bb += kQ) {
+                const int h = __ldcg(&hist[bb * 256 + d]);
+                tot += h;
+                if (bb < b) pre += h;
+            }
+            part[q][d] = tot;
+            wcnt[q][d] = pre;
+            __syncthreads();
+            int t_all = 0, p_all = 0;
+            if (q == 0) {
+                for (int k = 0; k < kQ; ++k) {
+                    t_all += part[k][d];
+                    p_all += wcnt[k][d];
+                }
+            }
+            const int base = block_excl_scan(q == 0 ? t_all : 0, warp_sums, nullptr);
+            if (q == 0) run[d] = base + p_all;
+            __syncthreads();
         }
-        __syncthreads();
+        // (C) stable scatter
+        for (int r = beg; r < end; r += kSortThreads) {
+            for (int k = threadIdx.x; k < (kSortThreads / 32) * 256; k += kSortThreads) (&wcnt[0][0])[k] = 0;
+            __syncthreads();
+            const int i = r + int(threadIdx.x);
+            const bool valid = i < end;
+            const uint32_t key = valid ? ks[i] : 0u;
+            const int dig = valid ? int((key >> shift) & 255u) : 256;
+            const unsigned peers = __match_any_sync(0xffffffffu, dig);
+            const int lrank = __popc(peers & ((1u << lane) - 1u));
+            if (valid && lrank == 0) wcnt[w][dig] = __popc(peers);
+            __syncthreads();
+            if (threadIdx.x < 256) run[threadIdx.x] = add_excl_over_warps(wcnt, threadIdx.x, run[threadIdx.x]);
+            __syncthreads();
+            const int dst = valid ? wcnt[w][dig] + lrank : -1;
+            if (dst >= 0 && dst < n) {  // always, unless a barrier gave up (status bit set)
+                kd[dst] = key;
+                vd[dst] = vs[i];
+            }
+            __syncthreads();
+        }
+        if (pass < 3) grid_barrier(sync, D.status);
+        uint32_t* tk = ks; ks = kd; kd = tk;
+        int32_t* tv = vs; vs = vd; vd = tv;
     }
 }
 
@@ -341,6 +384,7 @@ __global__ void __launch_bounds__(128) k_traverse(XpbdDcd D) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = D.n_tris;
     if (t >= n) return;
+    if (*D.status & XPBD_STATUS_BARRIER_TIMEOUT) return;  // the sort gave up: no valid tree
     const int i = D.ws_vals[t];
     int cnt = 0, out = 0;
     if (FILL) {
@@ -363,7 +407,11 @@ __global__ void __launch_bounds__(128) k_traverse(XpbdDcd D) {
         int stack[kStack];
         int sp = 0;
         int node = 0;  // the root's box holds every query box
-        while (true) {
+        for (int visits = 0;; ++visits) {
+            if (visits >= n) {  // more internal nodes than the tree has: not a tree
+                atomicOr(D.status, XPBD_STATUS_STACK_OVERFLOW);
+                break;
+            }
             const int ca = D.ws_child[2 * node], cb = D.ws_child[2 * node + 1];
             const bool la = live(qlo, qhi, nodes[2 * ca], nodes[2 * ca + 1], t);
             const bool lb = live(qlo, qhi, nodes[2 * cb], nodes[2 * cb + 1], t);
@@ -640,6 +688,40 @@ __global__ void k_copy4(const float4* __restrict__ src, float4* __restrict__ dst
     if (i < n) dst[i] = src[i];
 }
 
+// Sort CTAs: one per kSortThreads keys, at most the co-resident count.
+int64_t hist_words(int n) { return int64_t(256) * ((n + kSortThreads - 1) / kSortThreads); }
+int64_t scan_words(int n) { return (n + kScanBlock - 1) / kScanBlock; }
+
+int launch_sort(const XpbdDcd* D, uint32_t* sync, cudaStream_t s) {
+    static int slots[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cuda_check("xpbd_dcd_broadphase: device");
+    if (slots[dev] == 0) {
+        int n_sm = 0, per_sm = 0;
+        if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sort_coop, kSortThreads, 0) != cudaSuccess)
+            return cuda_check("xpbd_dcd_broadphase: sort occupancy");
+        if (per_sm < 1) return fail(XPBD_ERR_LIMIT, "xpbd_dcd_broadphase: sort kernel does not fit an SM");
+        slots[dev] = per_sm * n_sm;
+    }
+    const int n = D->n_tris;
+    const int need = (n + kSortThreads - 1) / kSortThreads;
+    const int G = std::min(need, slots[dev]);
+    const int chunk = ((n + G - 1) / G + kSortThreads - 1) / kSortThreads * kSortThreads;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(G);
+    cfg.blockDim = dim3(kSortThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k_sort_coop, *D, chunk, sync) != cudaSuccess)
+        return cuda_check("xpbd_dcd_broadphase: sort launch");
+    return XPBD_OK;
+}
+
 int check_dcd(const XpbdDcd* D) {
     if (!D || D->n_tris <= 0 || D->n_verts <= 0 || !D->tris || !D->pairs || !D->n_pairs || !D->n_contacts ||
         !D->c_ids || !D->c_data || !D->x_prev || !D->dP || !D->status || !D->ws_nodes || !D->ws_keys || !D->ws_vals ||
@@ -659,11 +741,10 @@ extern "C" {
 
 int xpbd_dcd_workspace_query(int32_t n_tris, XpbdDcdWorkspaceSizes* out) {
     if (n_tris <= 0 || !out) return fail(XPBD_ERR_ARG, "xpbd_dcd_workspace_query: bad arguments");
-    const int nblk = (n_tris + kSortChunk - 1) / kSortChunk;
     out->nodes_floats = int64_t(2 * (2 * n_tris - 1)) * 4 * 2;  // sorted tree + unsorted leaf copy
     out->keys = n_tris;
-    const int64_t scan_blocks = (std::max<int64_t>(int64_t(256) * nblk, n_tris) + kScanBlock - 1) / kScanBlock;
-    out->hist = int64_t(256) * nblk + scan_blocks;  // radix histograms, then the scan's block sums
+    // sort histograms [CTAs][256], the count scan's block sums, the sort's barrier words
+    out->hist = hist_words(n_tris) + scan_words(n_tris) + 4;
     out->child = int64_t(2) * (n_tris > 1 ? n_tris - 1 : 1);
     out->parent = int64_t(2) * n_tris - 1;
     out->flags = n_tris > 1 ? n_tris - 1 : 1;
@@ -685,22 +766,9 @@ int xpbd_dcd_broadphase(const XpbdDcd* D, const float* pos4, int32_t snapshot_pr
     XpbdDcd Dl = *D;
     Dl.ws_nodes = D->ws_nodes + int64_t(2 * (2 * n - 1)) * 4 - int64_t(2 * (n - 1)) * 4;
     k_tri_aabb<<<(n + 255) / 256, 256, 0, s>>>(Dl, pos4);
-    // radix sort (keys, tri ids): 4 passes of 8 bits, ping-pong
-    const int nblk = (n + kSortChunk - 1) / kSortChunk;
-    int* scan_scratch = D->ws_hist + int64_t(256) * nblk;
-    uint32_t* ka = D->ws_keys;
-    int32_t* va = D->ws_vals;
-    uint32_t* kb = D->ws_keys2;
-    int32_t* vb = D->ws_vals2;
-    for (int pass = 0; pass < 4; ++pass) {
-        const int shift = 8 * pass;
-        k_sort_hist<<<nblk, kSortThreads, 0, s>>>(ka, n, shift, D->ws_hist, nblk);
-        scan_excl(D->ws_hist, 256 * nblk, nullptr, scan_scratch, s);
-        k_sort_scatter<<<nblk, kSortThreads, 0, s>>>(ka, va, kb, vb, n, shift, D->ws_hist, nblk);
-        uint32_t* tk = ka; ka = kb; kb = tk;
-        int32_t* tv = va; va = vb; vb = tv;
-    }
-    // after an even number of passes the sorted data is back in ws_keys/ws_vals
+    int* scan_scratch = D->ws_hist + hist_words(n);
+    uint32_t* sort_sync = reinterpret_cast<uint32_t*>(scan_scratch + scan_words(n));
+    if ((rc = launch_sort(D, sort_sync, s))) return rc;
     if (n > 1) {
         k_build<<<(n - 1 + 255) / 256, 256, 0, s>>>(*D);
         cudaMemsetAsync(D->ws_parent, 0xff, sizeof(int32_t), s);  // root has no parent

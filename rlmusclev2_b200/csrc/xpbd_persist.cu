@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "xpbd_common.cuh"
+#include "xpbd_grid.cuh"
 #include "xpbd_tile.cuh"
 
 using namespace xpbd;
@@ -24,38 +25,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr size_t kSmemPerVert = 4 * sizeof(float4) + 4 * sizeof(float) + 2 * sizeof(int);  // 88 bytes
-constexpr unsigned kSpinLimit = 1u << 21;  // polls of ~0.5 us (L2 round trip + 32 ns sleep): about a second
-
-// Grid-wide barrier over gridDim.x co-resident CTAs (count, generation in
-// sync[0..1]).  __syncthreads orders the CTA's writes before thread 0's
-// acquire-release arrival; the release of the new generation and the
-// acquiring polls carry them to the other CTAs, whose __syncthreads passes
-// them on to their threads.  Bounded: after kSpinLimit polls it sets the
-// timeout bit, and once that bit is set no CTA waits again.
-__device__ __forceinline__ void grid_barrier(uint32_t* sync, int32_t* status) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> cnt(sync[0]), gen(sync[1]);
-        cuda::atomic_ref<int32_t, cuda::thread_scope_device> st(*status);
-        if ((st.load(cuda::memory_order_relaxed) & XPBD_STATUS_BARRIER_TIMEOUT) == 0) {
-            const uint32_t g = gen.load(cuda::memory_order_relaxed);
-            if (cnt.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1) {
-                cnt.store(0u, cuda::memory_order_relaxed);
-                gen.fetch_add(1u, cuda::memory_order_release);
-            } else {
-                uint32_t spins = 0;
-                while (gen.load(cuda::memory_order_acquire) == g) {
-                    if (++spins > kSpinLimit) {
-                        st.fetch_or(XPBD_STATUS_BARRIER_TIMEOUT, cuda::memory_order_relaxed);
-                        break;
-                    }
-                    __nanosleep(32);
-                }
-            }
-        }
-    }
-    __syncthreads();
-}
 
 template <bool DAMP, int MINB, int CSET, bool PF>
 __global__ void __launch_bounds__(kThreads, MINB)

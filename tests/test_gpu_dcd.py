@@ -57,6 +57,27 @@ def test_pairs_bit_exact_and_deterministic():
     np.testing.assert_array_equal(a["pairs"], b["pairs"])  # same order run to run
 
 
+def test_pairs_large_soup():
+    """350k disjoint triangles: more keys than one round of the cooperative sort
+    covers on every resident CTA (multi-round chunks), half of them static."""
+    rng = np.random.default_rng(11)
+    n = 350_000
+    cen = rng.random((n, 3), dtype=np.float32)
+    verts = (cen[:, None, :] + rng.normal(scale=0.003, size=(n, 3, 3)).astype(np.float32)).reshape(-1, 3)
+    p4 = np.ones((3 * n, 4), np.float32)
+    p4[:, :3] = verts
+    tris = np.arange(3 * n, dtype=np.int32).reshape(n, 3)
+    group = (rng.random(n) < 0.5).astype(np.int32)
+    prm = UdcfParams(allow_self=True, thickness=0.001, max_pairs=1 << 21, max_contacts=1 << 10)
+    a = _run(tris, p4, prm, group=group)
+    ref, _ = O.dcd_pairs(tris, p4, thickness=prm.thickness, allow_self=True, group=group)
+    print(f"tris {n} pairs {a['pairs'].shape[0]} oracle {ref.shape[0]}")
+    assert a["counters"]["status"] & ~capi.STATUS_CONTACT_OVERFLOW == 0
+    assert a["pairs"].shape[0] == ref.shape[0] > 10000
+    got = a["pairs"][np.lexsort((a["pairs"][:, 1], a["pairs"][:, 0]))]
+    np.testing.assert_array_equal(got, ref)
+
+
 def test_narrow_respond_match_oracle():
     tris, p4 = _scene_surface(seed=4, jitter=0.006)
     prm = UdcfParams(allow_self=True, thickness=0.0, max_pairs=1 << 21, max_contacts=1 << 19)
