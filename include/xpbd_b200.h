@@ -328,15 +328,13 @@ typedef struct XpbdDcd {
     float* x_prev;            /* [n_verts][4] positions at the broadphase (friction reference) */
     float* dP;                /* [n_verts][4] response accumulator, zero between calls */
     int32_t* status;          /* [1] XPBD_STATUS_* bits */
-    float* ws_nodes;          /* workspace: BVH node boxes + leaf copy */
+    float* ws_nodes;          /* workspace: BVH node records (children's boxes) + leaf boxes */
     uint32_t* ws_keys;        /* [n_tris] Morton keys (sorted in place) */
     int32_t* ws_vals;         /* [n_tris] triangle ids in Morton order */
     uint32_t* ws_keys2;       /* [n_tris] sort ping-pong */
     int32_t* ws_vals2;        /* [n_tris] */
     int32_t* ws_hist;         /* radix histograms */
-    int32_t* ws_child;        /* [n_tris-1][2] */
-    int32_t* ws_parent;       /* [2 n_tris - 1] */
-    int32_t* ws_flags;        /* [n_tris-1] refit arrival counters */
+    float* ws_bbox;           /* boxes of 32- and 1024-leaf Morton blocks (2 float4 each) */
     int32_t* ws_count;        /* [n_tris] pairs per Morton position, then their offsets */
     int32_t* ws_total;        /* [1] */
     int32_t* ws_slots;        /* [16][n_tris] first partners of each query (counting pass) */
@@ -344,7 +342,7 @@ typedef struct XpbdDcd {
 
 /* Element counts of the DCD workspace arrays for n_tris triangles. */
 typedef struct XpbdDcdWorkspaceSizes {
-    int64_t nodes_floats, keys, hist, child, parent, flags, count, slots;
+    int64_t nodes_floats, keys, hist, bbox_floats, count, slots;
 } XpbdDcdWorkspaceSizes;
 
 int xpbd_dcd_workspace_query(int32_t n_tris, XpbdDcdWorkspaceSizes* out);

@@ -84,13 +84,13 @@ class XpbdDcd(C.Structure):
                 ("c_data", C.c_void_p), ("x_prev", C.c_void_p), ("dP", C.c_void_p), ("status", C.c_void_p),
                 ("ws_nodes", C.c_void_p), ("ws_keys", C.c_void_p), ("ws_vals", C.c_void_p),
                 ("ws_keys2", C.c_void_p), ("ws_vals2", C.c_void_p), ("ws_hist", C.c_void_p),
-                ("ws_child", C.c_void_p), ("ws_parent", C.c_void_p), ("ws_flags", C.c_void_p),
+                ("ws_bbox", C.c_void_p),
                 ("ws_count", C.c_void_p), ("ws_total", C.c_void_p), ("ws_slots", C.c_void_p)]
 
 
 class XpbdDcdWorkspaceSizes(C.Structure):
-    _fields_ = [("nodes_floats", C.c_int64), ("keys", C.c_int64), ("hist", C.c_int64), ("child", C.c_int64),
-                ("parent", C.c_int64), ("flags", C.c_int64), ("count", C.c_int64), ("slots", C.c_int64)]
+    _fields_ = [("nodes_floats", C.c_int64), ("keys", C.c_int64), ("hist", C.c_int64),
+                ("bbox_floats", C.c_int64), ("count", C.c_int64), ("slots", C.c_int64)]
 
 
 class XpbdMetrics(C.Structure):

@@ -169,8 +169,8 @@ class DcdBuffers:
             nodes=torch.zeros(int(sz.nodes_floats), dtype=torch.float32, device=dev),
             keys=torch.zeros(int(sz.keys), dtype=i32, device=dev), vals=torch.zeros(int(sz.keys), dtype=i32, device=dev),
             keys2=torch.zeros(int(sz.keys), dtype=i32, device=dev), vals2=torch.zeros(int(sz.keys), dtype=i32, device=dev),
-            hist=torch.zeros(int(sz.hist), dtype=i32, device=dev), child=torch.zeros(int(sz.child), dtype=i32, device=dev),
-            parent=torch.zeros(int(sz.parent), dtype=i32, device=dev), flags=torch.zeros(int(sz.flags), dtype=i32, device=dev),
+            hist=torch.zeros(int(sz.hist), dtype=i32, device=dev),
+            bbox=torch.zeros(int(sz.bbox_floats), dtype=torch.float32, device=dev),
             count=torch.zeros(int(sz.count), dtype=i32, device=dev),
             slots=torch.zeros(int(sz.slots), dtype=i32, device=dev))
         t = self.t
@@ -190,7 +190,7 @@ class DcdBuffers:
                                              t["dP"].data_ptr())
         d.ws_nodes, d.ws_keys, d.ws_vals = t["nodes"].data_ptr(), t["keys"].data_ptr(), t["vals"].data_ptr()
         d.ws_keys2, d.ws_vals2, d.ws_hist = t["keys2"].data_ptr(), t["vals2"].data_ptr(), t["hist"].data_ptr()
-        d.ws_child, d.ws_parent, d.ws_flags = t["child"].data_ptr(), t["parent"].data_ptr(), t["flags"].data_ptr()
+        d.ws_bbox = t["bbox"].data_ptr()
         d.ws_count, d.ws_slots = t["count"].data_ptr(), t["slots"].data_ptr()
         self.d = d
 
@@ -200,11 +200,11 @@ class DcdBuffers:
 
     def broadphase_launches(self, snapshot_prev: bool = True) -> int:
         """Kernels one xpbd_dcd_broadphase call launches: snapshot copy, boxes,
-        cooperative sort, build, leaf permute, refit, counting traversal, the
-        count scan (2 launches, 3 above 4096 triangles), fill pass, total."""
+        cooperative sort, leaf permute, build, counting traversal, the count
+        scan (2 launches, 3 above 4096 triangles), fill pass, total."""
         n = int(self.d.n_tris)
         scan = 2 + (1 if n > 4096 else 0)
-        return int(snapshot_prev) + 2 + (1 if n > 1 else 0) + 1 + (1 if n > 1 else 0) + 1 + scan + 2
+        return int(snapshot_prev) + 3 + (1 if n > 1 else 0) + 1 + scan + 2
 
     def narrow_respond(self, pos4: torch.Tensor, stream) -> None:
         capi.check(self.lib.xpbd_dcd_narrow_respond(C.byref(self.d), C.c_void_p(pos4.data_ptr()), stream))

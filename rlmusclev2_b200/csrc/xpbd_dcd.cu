@@ -38,6 +38,14 @@ struct Aabb {
 
 __device__ __forceinline__ float4 ld4(const float* p, int i) { return reinterpret_cast<const float4*>(p)[i]; }
 
+// ws_nodes layout (float4 units): internal node records [4 (n-1)), then the
+// leaf boxes in Morton order [2 n), then the leaf boxes in triangle order
+// [2 n).  Record i holds its two children: lo_a (w: last Morton position
+// under a), hi_a (w: a's node id), lo_b, hi_b; node ids >= n-1 are leaves
+// (position id - (n-1)).  A visit is one 64-byte load.
+__host__ __device__ __forceinline__ int64_t sorted_leaf_base(int n) { return int64_t(4) * (n - 1); }
+__host__ __device__ __forceinline__ int64_t tri_leaf_base(int n) { return int64_t(4) * (n - 1) + 2 * int64_t(n); }
+
 __device__ __forceinline__ uint32_t spread10(uint32_t v) {
     v &= 0x3ffu;
     v = (v | (v << 16)) & 0x030000FFu;
@@ -59,10 +67,9 @@ __global__ void k_tri_aabb(XpbdDcd D, const float* __restrict__ pos4) {
                                   fminf(fminf(pa.z, pb.z), pc.z) - t);
     const float3 hi = make_float3(fmaxf(fmaxf(pa.x, pb.x), pc.x) + t, fmaxf(fmaxf(pa.y, pb.y), pc.y) + t,
                                   fmaxf(fmaxf(pa.z, pb.z), pc.z) + t);
-    float4* nodes = reinterpret_cast<float4*>(D.ws_nodes);
-    const int leaf = D.n_tris - 1 + i;
-    nodes[2 * leaf] = make_float4(lo.x, lo.y, lo.z, 0.f);
-    nodes[2 * leaf + 1] = make_float4(hi.x, hi.y, hi.z, 0.f);
+    float4* tri_box = reinterpret_cast<float4*>(D.ws_nodes) + tri_leaf_base(D.n_tris);
+    tri_box[2 * i] = make_float4(lo.x, lo.y, lo.z, 0.f);
+    tri_box[2 * i + 1] = make_float4(hi.x, hi.y, hi.z, 0.f);
     const float3 cen = make_float3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
     float q[3] = {cen.x, cen.y, cen.z};
     uint32_t code = 0;
@@ -262,6 +269,52 @@ __device__ __forceinline__ int delta(const uint32_t* k, int n, int i, int j) {
     return __clz(a ^ b);
 }
 
+// Box of the sorted leaves [a, b): leaf boxes at the ends, 32-leaf block boxes
+// (ws_bbox[0, nb32)) and 1024-leaf block boxes (ws_bbox[nb32, ...)) between.
+// Independent loads, no dependence on other internal nodes: the whole
+// hierarchy's boxes come out of the build launch without a bottom-up refit.
+struct Box {
+    float4 lo, hi;
+    __device__ __forceinline__ void add(const float4* p, int k) {
+        const float4 l = p[2 * k], h = p[2 * k + 1];
+        lo.x = fminf(lo.x, l.x), lo.y = fminf(lo.y, l.y), lo.z = fminf(lo.z, l.z);
+        hi.x = fmaxf(hi.x, h.x), hi.y = fmaxf(hi.y, h.y), hi.z = fmaxf(hi.z, h.z);
+    }
+};
+
+__device__ __forceinline__ void add_run(Box& bx, const float4* p, int a, int b) {
+#pragma unroll 4
+    for (int k = a; k < b; ++k) bx.add(p, k);
+}
+
+__device__ Box range_box(const XpbdDcd& D, int a, int b) {
+    const int n = D.n_tris;
+    const float4* leaves = reinterpret_cast<const float4*>(D.ws_nodes) + sorted_leaf_base(n);
+    const float4* b32 = reinterpret_cast<const float4*>(D.ws_bbox);
+    const float4* b1k = b32 + 2 * ((n + 31) / 32);
+    Box bx;
+    bx.lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+    bx.hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+    if (b - a <= 64) {
+        add_run(bx, leaves, a, b);
+        return bx;
+    }
+    const int a1 = (a + 31) >> 5, e1 = b >> 5;  // whole 32-leaf blocks [a1, e1)
+    add_run(bx, leaves, a, a1 << 5);
+    add_run(bx, leaves, e1 << 5, b);
+    if (e1 - a1 <= 64) {
+        add_run(bx, b32, a1, e1);
+        return bx;
+    }
+    const int a2 = (a1 + 31) >> 5, e2 = e1 >> 5;  // whole 1024-leaf blocks [a2, e2)
+    add_run(bx, b32, a1, a2 << 5);
+    add_run(bx, b32, e2 << 5, e1);
+    add_run(bx, b1k, a2, e2);
+    return bx;
+}
+
+// Karras (2012) hierarchy over the sorted keys; internal node i gets the
+// record of its two children, their boxes from their leaf ranges.
 __global__ void k_build(XpbdDcd D) {
     const int n = D.n_tris;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -286,48 +339,63 @@ __global__ void k_build(XpbdDcd D) {
     const int lo = min(i, j), hi = max(i, j);
     const int left = (lo == g) ? (n - 1 + g) : g;
     const int right = (hi == g + 1) ? (n - 1 + g + 1) : g + 1;
-    D.ws_child[2 * i] = left;
-    D.ws_child[2 * i + 1] = right;
-    D.ws_parent[left] = i;
-    D.ws_parent[right] = i;
-    D.ws_flags[i] = 0;
+    const Box ba = range_box(D, lo, g + 1), bb = range_box(D, g + 1, hi + 1);
+    float4* rec = reinterpret_cast<float4*>(D.ws_nodes) + 4 * int64_t(i);
+    rec[0] = make_float4(ba.lo.x, ba.lo.y, ba.lo.z, __int_as_float(g));
+    rec[1] = make_float4(ba.hi.x, ba.hi.y, ba.hi.z, __int_as_float(left));
+    rec[2] = make_float4(bb.lo.x, bb.lo.y, bb.lo.z, __int_as_float(hi));
+    rec[3] = make_float4(bb.hi.x, bb.hi.y, bb.hi.z, __int_as_float(right));
 }
 
-// leaves were written in triangle order; the tree expects them in sorted order
-__global__ void k_permute_leaves(XpbdDcd D) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= D.n_tris) return;
-    const int tri = D.ws_vals[s];
-    const float4* src = reinterpret_cast<const float4*>(D.ws_nodes) + 2 * (2 * D.n_tris - 1);
-    float4* dst = reinterpret_cast<float4*>(D.ws_nodes);
-    const int leaf = D.n_tris - 1 + s;
-    float4 lo = src[2 * tri];
-    lo.w = __int_as_float(s);  // last Morton position under the node (leaf: its own)
-    dst[2 * leaf] = lo;
-    dst[2 * leaf + 1] = src[2 * tri + 1];
+// Leaves were written in triangle order; the build wants them in Morton order.  A CTA of 1024 threads covers 1024
+// consecutive leaves and also writes their 32- and 1024-leaf block boxes.
+__device__ __forceinline__ void warp_box(float4& lo, float4& hi) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        lo.x = fminf(lo.x, __shfl_xor_sync(0xffffffffu, lo.x, o));
+        lo.y = fminf(lo.y, __shfl_xor_sync(0xffffffffu, lo.y, o));
+        lo.z = fminf(lo.z, __shfl_xor_sync(0xffffffffu, lo.z, o));
+        hi.x = fmaxf(hi.x, __shfl_xor_sync(0xffffffffu, hi.x, o));
+        hi.y = fmaxf(hi.y, __shfl_xor_sync(0xffffffffu, hi.y, o));
+        hi.z = fmaxf(hi.z, __shfl_xor_sync(0xffffffffu, hi.z, o));
+    }
 }
 
-__global__ void k_refit(XpbdDcd D) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(1024) k_permute_leaves(XpbdDcd D) {
+    __shared__ float4 s_box[32][2];
     const int n = D.n_tris;
-    if (s >= n) return;
-    float4* nodes = reinterpret_cast<float4*>(D.ws_nodes);
-    int node = n - 1 + s;
-    if (n == 1) return;
-    for (int step = 0; step < n; ++step) {
-        const int p = D.ws_parent[node];
-        if (p < 0) break;
-        // release this thread's box writes, acquire the sibling's (one acq_rel atomic)
-        int arrived;
-        asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(arrived) : "l"(&D.ws_flags[p]) : "memory");
-        if (arrived == 0) return;  // first arrival: the sibling finishes p
-        const int a = D.ws_child[2 * p], b = D.ws_child[2 * p + 1];
-        const float4 alo = __ldcg(&nodes[2 * a]), ahi = __ldcg(&nodes[2 * a + 1]);
-        const float4 blo = __ldcg(&nodes[2 * b]), bhi = __ldcg(&nodes[2 * b + 1]);
-        nodes[2 * p] = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z),
-                                   __int_as_float(max(__float_as_int(alo.w), __float_as_int(blo.w))));
-        nodes[2 * p + 1] = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f);
-        node = p;
+    const int s = blockIdx.x * 1024 + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+    if (s < n) {
+        const int tri = D.ws_vals[s];
+        const float4* src = reinterpret_cast<const float4*>(D.ws_nodes) + tri_leaf_base(n);
+        float4* dst = reinterpret_cast<float4*>(D.ws_nodes) + sorted_leaf_base(n);
+        lo = src[2 * tri];
+        hi = src[2 * tri + 1];
+        dst[2 * s] = lo;
+        dst[2 * s + 1] = hi;
+    }
+    warp_box(lo, hi);
+    float4* b32 = reinterpret_cast<float4*>(D.ws_bbox);
+    if (lane == 0 && s < n) {
+        b32[2 * (s >> 5)] = lo;
+        b32[2 * (s >> 5) + 1] = hi;
+    }
+    if (lane == 0) {
+        s_box[w][0] = lo;
+        s_box[w][1] = hi;
+    }
+    __syncthreads();
+    if (w == 0) {
+        lo = s_box[lane][0];
+        hi = s_box[lane][1];
+        warp_box(lo, hi);
+        if (lane == 0) {
+            float4* b1k = b32 + 2 * ((n + 31) / 32);
+            b1k[2 * blockIdx.x] = lo;
+            b1k[2 * blockIdx.x + 1] = hi;
+        }
     }
 }
 
@@ -401,20 +469,22 @@ __global__ void __launch_bounds__(128) k_traverse(XpbdDcd D) {
         }
     }
     if (n > 1) {
-        const float4* nodes = reinterpret_cast<const float4*>(D.ws_nodes);
-        const float4* tri_box = nodes + 2 * (2 * n - 1);  // unsorted leaf copy, triangle order
+        const float4* recs = reinterpret_cast<const float4*>(D.ws_nodes);
+        const float4* tri_box = recs + tri_leaf_base(n);
         const float4 qlo = tri_box[2 * i], qhi = tri_box[2 * i + 1];
         int stack[kStack];
         int sp = 0;
-        int node = 0;  // the root's box holds every query box
+        int node = 0;  // the root (its own box is never needed: its record tests both children)
         for (int visits = 0;; ++visits) {
             if (visits >= n) {  // more internal nodes than the tree has: not a tree
                 atomicOr(D.status, XPBD_STATUS_STACK_OVERFLOW);
                 break;
             }
-            const int ca = D.ws_child[2 * node], cb = D.ws_child[2 * node + 1];
-            const bool la = live(qlo, qhi, nodes[2 * ca], nodes[2 * ca + 1], t);
-            const bool lb = live(qlo, qhi, nodes[2 * cb], nodes[2 * cb + 1], t);
+            const float4* r = recs + 4 * int64_t(node);
+            const float4 alo = r[0], ahi = r[1], blo = r[2], bhi = r[3];
+            const int ca = __float_as_int(ahi.w), cb = __float_as_int(bhi.w);
+            const bool la = live(qlo, qhi, alo, ahi, t);
+            const bool lb = live(qlo, qhi, blo, bhi, t);
             const bool da = la && ca < n - 1, db = lb && cb < n - 1;  // internal children to descend
             if (la && !da) emit_leaf<FILL>(D, i, ca - (n - 1), t, cnt, out);
             if (lb && !db) emit_leaf<FILL>(D, i, cb - (n - 1), t, cnt, out);
@@ -725,11 +795,11 @@ int launch_sort(const XpbdDcd* D, uint32_t* sync, cudaStream_t s) {
 int check_dcd(const XpbdDcd* D) {
     if (!D || D->n_tris <= 0 || D->n_verts <= 0 || !D->tris || !D->pairs || !D->n_pairs || !D->n_contacts ||
         !D->c_ids || !D->c_data || !D->x_prev || !D->dP || !D->status || !D->ws_nodes || !D->ws_keys || !D->ws_vals ||
-        !D->ws_keys2 || !D->ws_vals2 || !D->ws_hist || !D->ws_child || !D->ws_parent || !D->ws_flags || !D->ws_count ||
+        !D->ws_keys2 || !D->ws_vals2 || !D->ws_hist || !D->ws_bbox || !D->ws_count ||
         !D->ws_total || !D->ws_slots)
         return fail(XPBD_ERR_ARG, "XpbdDcd: null member or empty size");
     if (D->max_pairs <= 0 || D->max_contacts <= 0) return fail(XPBD_ERR_ARG, "XpbdDcd: capacities must be > 0");
-    if (!aligned16(D->ws_nodes) || !aligned16(D->pairs) || !aligned16(D->c_ids) || !aligned16(D->c_data) || !aligned16(D->x_prev) ||
+    if (!aligned16(D->ws_nodes) || !aligned16(D->ws_bbox) || !aligned16(D->pairs) || !aligned16(D->c_ids) || !aligned16(D->c_data) || !aligned16(D->x_prev) ||
         !aligned16(D->dP))
         return fail(XPBD_ERR_ALIGN, "XpbdDcd: 16-byte alignment");
     return XPBD_OK;
@@ -741,13 +811,11 @@ extern "C" {
 
 int xpbd_dcd_workspace_query(int32_t n_tris, XpbdDcdWorkspaceSizes* out) {
     if (n_tris <= 0 || !out) return fail(XPBD_ERR_ARG, "xpbd_dcd_workspace_query: bad arguments");
-    out->nodes_floats = int64_t(2 * (2 * n_tris - 1)) * 4 * 2;  // sorted tree + unsorted leaf copy
+    out->nodes_floats = (tri_leaf_base(n_tris) + 2 * int64_t(n_tris)) * 4;  // records, leaves x2
     out->keys = n_tris;
     // sort histograms [CTAs][256], the count scan's block sums, the sort's barrier words
     out->hist = hist_words(n_tris) + scan_words(n_tris) + 4;
-    out->child = int64_t(2) * (n_tris > 1 ? n_tris - 1 : 1);
-    out->parent = int64_t(2) * n_tris - 1;
-    out->flags = n_tris > 1 ? n_tris - 1 : 1;
+    out->bbox_floats = int64_t(8) * ((n_tris + 31) / 32 + (n_tris + 1023) / 1024);  // 32- and 1024-leaf block boxes
     out->count = n_tris;
     out->slots = int64_t(kSlots) * n_tris;
     return XPBD_OK;
@@ -762,21 +830,12 @@ int xpbd_dcd_broadphase(const XpbdDcd* D, const float* pos4, int32_t snapshot_pr
     if (snapshot_prev)
         k_copy4<<<(D->n_verts + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float4*>(pos4),
                                                           reinterpret_cast<float4*>(D->x_prev), D->n_verts);
-    // leaf boxes go to the unsorted copy region first
-    XpbdDcd Dl = *D;
-    Dl.ws_nodes = D->ws_nodes + int64_t(2 * (2 * n - 1)) * 4 - int64_t(2 * (n - 1)) * 4;
-    k_tri_aabb<<<(n + 255) / 256, 256, 0, s>>>(Dl, pos4);
+    k_tri_aabb<<<(n + 255) / 256, 256, 0, s>>>(*D, pos4);
     int* scan_scratch = D->ws_hist + hist_words(n);
     uint32_t* sort_sync = reinterpret_cast<uint32_t*>(scan_scratch + scan_words(n));
     if ((rc = launch_sort(D, sort_sync, s))) return rc;
-    if (n > 1) {
-        k_build<<<(n - 1 + 255) / 256, 256, 0, s>>>(*D);
-        cudaMemsetAsync(D->ws_parent, 0xff, sizeof(int32_t), s);  // root has no parent
-    } else {
-        cudaMemsetAsync(D->ws_parent, 0xff, sizeof(int32_t), s);
-    }
-    k_permute_leaves<<<(n + 255) / 256, 256, 0, s>>>(*D);
-    if (n > 1) k_refit<<<(n + 255) / 256, 256, 0, s>>>(*D);
+    k_permute_leaves<<<(n + 1023) / 1024, 1024, 0, s>>>(*D);
+    if (n > 1) k_build<<<(n - 1 + 255) / 256, 256, 0, s>>>(*D);
     k_traverse<false><<<(n + 127) / 128, 128, 0, s>>>(*D);
     scan_excl(D->ws_count, n, D->ws_total, scan_scratch, s);
     k_traverse<true><<<(n + 127) / 128, 128, 0, s>>>(*D);
