@@ -313,11 +313,15 @@ __device__ Box range_box(const XpbdDcd& D, int a, int b) {
     return bx;
 }
 
-// Karras (2012) hierarchy over the sorted keys; internal node i gets the
-// record of its two children, their boxes from their leaf ranges.
+// Karras (2012) hierarchy over the sorted keys.  Two threads per internal
+// node i (adjacent lanes) both run its split search; thread `side` then
+// writes child `side`'s half of record i: box from the child's leaf range,
+// last Morton position, node id.  Two threads halve the range-box work per
+// thread and double the warps in flight: the launch is latency-bound.
 __global__ void k_build(XpbdDcd D) {
     const int n = D.n_tris;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gid >> 1, side = gid & 1;
     if (i >= n - 1) return;
     const uint32_t* k = D.ws_keys;
     const int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
@@ -337,14 +341,12 @@ __global__ void k_build(XpbdDcd D) {
     } while (t > 1);
     const int g = i + s * d + min(d, 0);
     const int lo = min(i, j), hi = max(i, j);
-    const int left = (lo == g) ? (n - 1 + g) : g;
-    const int right = (hi == g + 1) ? (n - 1 + g + 1) : g + 1;
-    const Box ba = range_box(D, lo, g + 1), bb = range_box(D, g + 1, hi + 1);
-    float4* rec = reinterpret_cast<float4*>(D.ws_nodes) + 4 * int64_t(i);
-    rec[0] = make_float4(ba.lo.x, ba.lo.y, ba.lo.z, __int_as_float(g));
-    rec[1] = make_float4(ba.hi.x, ba.hi.y, ba.hi.z, __int_as_float(left));
-    rec[2] = make_float4(bb.lo.x, bb.lo.y, bb.lo.z, __int_as_float(hi));
-    rec[3] = make_float4(bb.hi.x, bb.hi.y, bb.hi.z, __int_as_float(right));
+    const int first = side ? g + 1 : lo, last = side ? hi : g;  // the child's leaf range
+    const int id = (first == last) ? (n - 1 + first) : (side ? g + 1 : g);
+    const Box bx = range_box(D, first, last + 1);
+    float4* rec = reinterpret_cast<float4*>(D.ws_nodes) + 4 * int64_t(i) + 2 * side;
+    rec[0] = make_float4(bx.lo.x, bx.lo.y, bx.lo.z, __int_as_float(last));
+    rec[1] = make_float4(bx.hi.x, bx.hi.y, bx.hi.z, __int_as_float(id));
 }
 
 // Leaves were written in triangle order; the build wants them in Morton order.  A CTA of 1024 threads covers 1024
@@ -835,7 +837,7 @@ int xpbd_dcd_broadphase(const XpbdDcd* D, const float* pos4, int32_t snapshot_pr
     uint32_t* sort_sync = reinterpret_cast<uint32_t*>(scan_scratch + scan_words(n));
     if ((rc = launch_sort(D, sort_sync, s))) return rc;
     k_permute_leaves<<<(n + 1023) / 1024, 1024, 0, s>>>(*D);
-    if (n > 1) k_build<<<(n - 1 + 255) / 256, 256, 0, s>>>(*D);
+    if (n > 1) k_build<<<(2 * (n - 1) + 255) / 256, 256, 0, s>>>(*D);
     k_traverse<false><<<(n + 127) / 128, 128, 0, s>>>(*D);
     scan_excl(D->ws_count, n, D->ws_total, scan_scratch, s);
     k_traverse<true><<<(n + 127) / 128, 128, 0, s>>>(*D);
