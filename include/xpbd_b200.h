@@ -40,6 +40,7 @@ enum {
     XPBD_STATUS_STACK_OVERFLOW = 1 << 2,   /* BVH traversal deeper than its stack (query cut short) */
     XPBD_STATUS_BARRIER_TIMEOUT = 1 << 3,  /* a grid-wide wait of the persistent pass gave up (results invalid) */
     XPBD_STATUS_MMA_TIMEOUT = 1 << 4,      /* a tensor-core GEMM gave up waiting for its MMAs (results invalid) */
+    XPBD_STATUS_ACC_RANGE = 1 << 5,        /* a tet correction left the fixed-point accumulator's safe range */
 };
 
 #define XPBD_MAX_MATERIALS 64
@@ -84,6 +85,12 @@ typedef struct XpbdParams {
                                     ARAP/aniso set, 2 at up to 128 regs with volume/SNH/damping);
                                     bit 1: ARAP-SVD through the SVD even where the polar rotation applies;
                                     bit 2: persistent pass loads the next tet's streams ahead (prefetch) */
+    float acc_scale;             /* > 0: the tile passes sum each tet's corrections into shared memory as
+                                    32-bit integers round(d * acc_scale) (native integer atomics; shared
+                                    float atomics cost ~5x more) and read the sums back as float(sum) /
+                                    acc_scale; xpbd_acc_scale_for_extent gives the value for a mesh */
+    int32_t* status;             /* optional [1]: XPBD_STATUS_ACC_RANGE is or-ed in when a single tet's
+                                    correction exceeds 1/64 of the fixed-point range (sums may wrap) */
     XpbdMaterial materials[XPBD_MAX_MATERIALS];
     XpbdAttachMaterial attach[XPBD_MAX_ATTACH_MATERIALS];
 } XpbdParams;
@@ -176,6 +183,16 @@ enum {
 };
 
 int xpbd_abi_version(void);
+
+/* XpbdParams.acc_scale for positions whose coordinates stay below max_coord
+ * in magnitude: the largest power of two s with s x max_coord <= 2^26.  The
+ * quantum 1/s is then at most half an FP32 ulp of the largest coordinate (the
+ * position update cannot resolve finer steps there), a vertex's correction
+ * sum may reach 32 x max_coord before the 32-bit range ends, and one tet's
+ * correction above max_coord / 2 sets XPBD_STATUS_ACC_RANGE.
+ * Library-specific (the reference sums corrections with float atomics). */
+float xpbd_acc_scale_for_extent(float max_coord);
+
 const char* xpbd_error_string(void);
 
 /* Fused per-vertex substep boundary: [push-out] -> [velocity] -> [predict] -> [pin].

@@ -20,6 +20,7 @@ VF_ATTACH_MASK, VF_PIN = 0xFF, 1 << 8
 OP_SDF, OP_VELOCITY, OP_PREDICT, OP_PIN = 1, 2, 4, 8
 STATUS_PAIR_OVERFLOW, STATUS_CONTACT_OVERFLOW, STATUS_STACK_OVERFLOW, STATUS_BARRIER_TIMEOUT = 1, 2, 4, 8
 STATUS_MMA_TIMEOUT = 16
+STATUS_ACC_RANGE = 32
 APPLY_ATTACH, APPLY_DIVIDE, APPLY_PIN, APPLY_CLEAR = 1, 2, 4, 8
 PROJECT_FUSED, PROJECT_ACCUMULATE, PROJECT_FUSED_LAST = 0, 1, 2
 
@@ -37,7 +38,8 @@ class XpbdParams(C.Structure):
     _fields_ = [("dt", C.c_float), ("gravity", C.c_float * 3), ("veldamping", C.c_float),
                 ("quasi_static", C.c_int32), ("omega", C.c_float), ("contraction_ratio", C.c_float),
                 ("fiber_stiffness_scale", C.c_float), ("n_materials", C.c_int32),
-                ("n_attach_materials", C.c_int32), ("tile_variant", C.c_int32),
+                ("n_attach_materials", C.c_int32), ("tile_variant", C.c_int32), ("acc_scale", C.c_float),
+                ("status", C.c_void_p),
                 ("materials", XpbdMaterial * MAX_MATERIALS),
                 ("attach", XpbdAttachMaterial * MAX_ATTACH_MATERIALS)]
 
@@ -128,6 +130,7 @@ class XpbdPersist(C.Structure):
 P = C.c_void_p
 _SIGS = {
     "xpbd_abi_version": ([], C.c_int),
+    "xpbd_acc_scale_for_extent": ([C.c_float], C.c_float),
     "xpbd_error_string": ([], C.c_char_p),
     "xpbd_vertex_step": ([C.POINTER(XpbdParams), C.POINTER(XpbdVerts), C.c_uint32, C.POINTER(XpbdSdf), P], C.c_int),
     "xpbd_project": ([C.POINTER(XpbdParams), C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), C.c_int32, P], C.c_int),

@@ -10,6 +10,7 @@
 // pinning.
 #include <cuda_runtime.h>
 #include <stdio.h>
+#include <cmath>
 #include <string.h>
 
 #include "../../include/xpbd_b200.h"
@@ -41,15 +42,17 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     const int nvt = T.tile_vptr[tile + 1] - vbeg;
     const int nint = (MODE != XPBD_PROJECT_ACCUMULATE) ? T.tile_nint[tile] : 0;
     // Shared layout: positions (float4), previous positions (float4, damped
-    // materials only), and the accumulator as four separate float arrays so
-    // that atomics on random vertices spread over all 32 banks.
+    // materials only), and the accumulator as four separate 32-bit integer
+    // arrays (fixed-point sums, counts) so that atomics on random vertices
+    // spread over all 32 banks.
     const int mtv = T.max_tile_verts;
     float4* s_pos = smem;
     float4* s_prev = smem + mtv;
-    float* s_ax = reinterpret_cast<float*>(smem + (DAMP ? 2 : 1) * mtv);
-    float* s_ay = s_ax + mtv;
-    float* s_az = s_ay + mtv;
-    float* s_aw = s_az + mtv;
+    int* s_ax = reinterpret_cast<int*>(smem + (DAMP ? 2 : 1) * mtv);
+    int* s_ay = s_ax + mtv;
+    int* s_az = s_ay + mtv;
+    int* s_cnt = s_az + mtv;
+    const float inv_scale = 1.f / prm.acc_scale;
     const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
     const float4* prev4 = reinterpret_cast<const float4*>(V.pprev);
     __shared__ float s_arap_at[XPBD_MAX_MATERIALS];
@@ -57,15 +60,15 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
         const int g = T.tile_verts[vbeg + i];
         s_pos[i] = pos4[g];
-        s_ax[i] = 0.f;
-        s_ay[i] = 0.f;
-        s_az[i] = 0.f;
-        s_aw[i] = 0.f;
+        s_ax[i] = 0;
+        s_ay[i] = 0;
+        s_az[i] = 0;
+        s_cnt[i] = 0;
         if (DAMP) s_prev[i] = prev4[g];
     }
     __syncthreads();
 
-    project_tile_tets<DAMP, CSET>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_aw, s_arap_at);
+    project_tile_tets<DAMP, CSET>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at);
     __syncthreads();
 
     float4* pos4w = reinterpret_cast<float4*>(V.pos);
@@ -76,12 +79,12 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
         for (int i = threadIdx.x; i < nint; i += blockDim.x) {
             const int g = T.tile_verts[vbeg + i];
             float4 pp = s_pos[i];
-            finish_vertex(prm, V, g, pp, make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]), finish_ops);
+            finish_vertex(prm, V, g, pp, tile_acc(s_ax, s_ay, s_az, s_cnt, i, inv_scale), finish_ops);
             pos4w[g] = pp;
         }
     }
     for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
-        const float4 a = make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]);
+        const float4 a = tile_acc(s_ax, s_ay, s_az, s_cnt, i, inv_scale);
         const int g = T.tile_verts[vbeg + i];
         if (MODE != XPBD_PROJECT_FUSED_LAST) {
             if (a.w != 0.f) atomicAdd(&acc4[g], a);
@@ -364,6 +367,8 @@ int check_params(const XpbdParams* p) {
         return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range");
     if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0");
     if (p->tile_variant < 0 || p->tile_variant > 7) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..7");
+    if (!(p->acc_scale > 0.f) || !(p->acc_scale < 3.0e38f))
+        return fail(XPBD_ERR_ARG, "XpbdParams: acc_scale must be a finite value > 0 (xpbd_acc_scale_for_extent)");
     return XPBD_OK;
 }
 int check_tiles(const XpbdTiles* t) {
@@ -434,6 +439,14 @@ int launch_project(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V
 extern "C" {
 
 int xpbd_abi_version(void) { return 1; }
+
+float xpbd_acc_scale_for_extent(float max_coord) {
+    const double e = max_coord > 1e-9f ? double(max_coord) : 1e-9;
+    int k = 0;
+    while (k < 120 && e * std::ldexp(1.0, k + 1) <= 67108864.0) ++k;
+    while (k > -120 && e * std::ldexp(1.0, k) > 67108864.0) --k;
+    return float(std::ldexp(1.0, k));
+}
 const char* xpbd_error_string(void) { return err_buffer(); }
 
 int xpbd_vertex_step(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, const XpbdSdf* sdf,

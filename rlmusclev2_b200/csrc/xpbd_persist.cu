@@ -46,11 +46,12 @@ __global__ void __launch_bounds__(kThreads, MINB)
     float4* s_prev = smem + mtv;
     float4* s_att = smem + 2 * mtv;
     float4* s_pin = smem + 3 * mtv;
-    float* s_ax = reinterpret_cast<float*>(smem + 4 * mtv);
-    float* s_ay = s_ax + mtv;
-    float* s_az = s_ay + mtv;
-    float* s_aw = s_az + mtv;
-    int* s_g = reinterpret_cast<int*>(s_aw + mtv);
+    int* s_ax = reinterpret_cast<int*>(smem + 4 * mtv);
+    int* s_ay = s_ax + mtv;
+    int* s_az = s_ay + mtv;
+    int* s_cnt = s_az + mtv;
+    const float inv_scale = 1.f / prm.acc_scale;
+    int* s_g = s_cnt + mtv;
     int* s_f = s_g + mtv;
     const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
     const float4* prev4 = reinterpret_cast<const float4*>(V.pprev);
@@ -77,23 +78,23 @@ __global__ void __launch_bounds__(kThreads, MINB)
         float4* rc = ring + cur * nv;
         float4* rn = ring + nxt * nv;
         for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
-            s_ax[i] = 0.f;
-            s_ay[i] = 0.f;
-            s_az[i] = 0.f;
-            s_aw[i] = 0.f;
+            s_ax[i] = 0;
+            s_ay[i] = 0;
+            s_az[i] = 0;
+            s_cnt[i] = 0;
         }
         __syncthreads();
-        project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_aw, s_arap_at);
+        project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at);
         __syncthreads();
         for (int i = threadIdx.x; i < nint; i += blockDim.x) {
             float4 pp = s_pos[i];
             finish_core(prm, s_f[i], s_att[i], s_prev[i], s_pin[i], pp,
-                        make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]), ops);
+                        tile_acc(s_ax, s_ay, s_az, s_cnt, i, inv_scale), ops);
             s_pos[i] = pp;
         }
         for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
             const int g = s_g[i];
-            const float4 a = make_float4(s_ax[i], s_ay[i], s_az[i], s_aw[i]);
+            const float4 a = tile_acc(s_ax, s_ay, s_az, s_cnt, i, inv_scale);
             if (a.w != 0.f) atomicAdd(&rc[g], a);
             if (g >= own_lo && g < own_hi) rn[g] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
@@ -204,6 +205,8 @@ extern "C" int xpbd_iterate_persistent(const XpbdParams* prm, const XpbdTiles* t
     if (tiles->max_tile_verts > XPBD_MAX_TILE_VERTS) return fail(XPBD_ERR_LIMIT, "xpbd_iterate_persistent: tile size");
     if (prm->n_materials < 1 || prm->n_materials > XPBD_MAX_MATERIALS)
         return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: n_materials");
+    if (!(prm->acc_scale > 0.f) || !(prm->acc_scale < 3.0e38f))
+        return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: acc_scale must be a finite value > 0");
     bool aniso = false, damp = false;
     for (int i = 0; i < prm->n_materials; ++i) {
         aniso |= (prm->materials[i].flags & XPBD_MAT_ANISO) != 0;

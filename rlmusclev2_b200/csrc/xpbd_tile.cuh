@@ -70,11 +70,22 @@ enum { CSET_LIGHT = 0, CSET_VOL = 1, CSET_FULL = 2 };  // ARAP+aniso | +volume |
 
 // Projects every constraint of the tile's tets from the staged positions
 // (s_pos, s_prev) and adds the Jacobi deltas and counts to the shared
-// accumulators s_ax..s_aw (one thread per tet, strided over the CTA).
+// accumulators s_ax..s_az and the active-constraint counts s_cnt (one
+// thread per tet, strided over the CTA).  All four are 32-bit integers added
+// with native shared-memory integer atomics (shared float atomics cost about
+// five times more): the corrections in fixed point, round(d * acc_scale),
+// the counts exactly.  tile_acc reads a vertex's sums back as floats.
+__device__ __forceinline__ float4 tile_acc(const int* s_ax, const int* s_ay, const int* s_az, const int* s_cnt, int i,
+                                           float inv_scale) {
+    return make_float4(float(s_ax[i]) * inv_scale, float(s_ay[i]) * inv_scale, float(s_az[i]) * inv_scale,
+                       float(s_cnt[i]));
+}
+
 template <bool DAMP, int CSET, bool PREFETCH = false>
 __device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const XpbdTiles& T, int tile,
-                                                  const float4* s_pos, const float4* s_prev, float* s_ax, float* s_ay,
-                                                  float* s_az, float* s_aw, const float* s_arap_at) {
+                                                  const float4* s_pos, const float4* s_prev, int* s_ax, int* s_ay,
+                                                  int* s_az, int* s_cnt, const float* s_arap_at) {
+    const float acc_scale = prm.acc_scale;
     const int t1 = T.tile_tptr[tile + 1];
     const uint4* tq = reinterpret_cast<const uint4*>(T.tet_q);
     const float4* tb0 = reinterpret_cast<const float4*>(T.tet_b0);
@@ -134,30 +145,34 @@ __device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const X
         float3 d[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) d[i] = make_float3(0.f, 0.f, 0.f);
-        float nact = 0.f;
+        int nact = 0;
         const uint32_t fl = m.flags;
         // Same type order as the reference table (ascending ConstraintType tag).
         if (CSET >= CSET_FULL && (fl & XPBD_MAT_SNH) &&
             con_snh(p, pq, B, F, V0, m.snh_mu, m.snh_lam, m.snh_damp, prm.dt, d))
-            nact += 1.f;
+            nact += 1;
         if (CSET >= CSET_VOL && (fl & XPBD_MAT_VOLUME) && con_volume(p, pq, V0, m.vol_k, m.vol_damp, prm.dt, d))
-            nact += 1.f;
+            nact += 1;
         if (fl & XPBD_MAT_ANISO) {
             const float4 fb = reinterpret_cast<const float4*>(T.tet_fiber)[t];
             if (con_aniso(p, B, F, f3(fb), fb.w, T.tet_act[t], m.aniso_k, prm.contraction_ratio,
                           prm.fiber_stiffness_scale, prm.dt, d))
-                nact += 1.f;
+                nact += 1;
         }
         if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, s_arap_at[min(int(q.z & 0xffu), XPBD_MAX_MATERIALS - 1)], d,
                                                    (prm.tile_variant & 2) != 0))
-            nact += 1.f;
-        if (nact != 0.f) {
+            nact += 1;
+        if (nact != 0) {
+            float dmax = 0.f;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) dmax = fmaxf(dmax, fmaxf(fabsf(d[i].x), fmaxf(fabsf(d[i].y), fabsf(d[i].z))));
+            if (!(dmax * acc_scale <= 33554432.f) && prm.status) atomicOr(prm.status, XPBD_STATUS_ACC_RANGE);  // 2^31/64
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                atomicAdd(&s_ax[l[i]], d[i].x);
-                atomicAdd(&s_ay[l[i]], d[i].y);
-                atomicAdd(&s_az[l[i]], d[i].z);
-                atomicAdd(&s_aw[l[i]], nact);
+                atomicAdd(&s_ax[l[i]], __float2int_rn(d[i].x * acc_scale));
+                atomicAdd(&s_ay[l[i]], __float2int_rn(d[i].y * acc_scale));
+                atomicAdd(&s_az[l[i]], __float2int_rn(d[i].z * acc_scale));
+                atomicAdd(&s_cnt[l[i]], nact);
             }
         }
     }

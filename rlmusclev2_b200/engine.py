@@ -33,6 +33,7 @@ def _ptr(t) -> int | None:
     return None if t is None else int(t.data_ptr())
 
 
+
 class XpbdEngine:
     """State-independent substep primitives plus the program runner."""
 
@@ -132,6 +133,10 @@ class XpbdEngine:
         for i, m in enumerate(L.materials):
             for k, v in m.items():
                 setattr(prm.materials[i], k, v)
+        # fixed-point accumulation scale of the tile passes: quantum at most half an
+        # FP32 ulp of the largest rest coordinate
+        prm.acc_scale = float(self._lib.xpbd_acc_scale_for_extent(float(np.abs(self.pos0_np).max())))
+        prm.status = self._pstatus.data_ptr()
         prm.n_attach_materials = len(self._attach_mats)
         for i, (k, d) in enumerate(self._attach_mats):
             prm.attach[i].k = k
@@ -312,9 +317,9 @@ class XpbdEngine:
             self._fused_iteration()
 
     def persistent_status(self, reset: bool = True) -> int:
-        """XPBD_STATUS_* bits of the persistent pass (synchronises).  After a
-        barrier timeout the ring and barrier words are cleared for the next
-        launch."""
+        """XPBD_STATUS_* bits of the persistent pass and of the tile passes'
+        fixed-point range check (synchronises).  After a barrier timeout the
+        ring and barrier words are cleared for the next launch."""
         self._stream.synchronize()
         st = int(self._pstatus.item())
         if st and reset:

@@ -3,6 +3,8 @@ import ctypes
 import re
 from pathlib import Path
 
+import numpy as np
+
 from rlmusclev2_b200 import _capi as capi
 from rlmusclev2_b200.build import build, lib_path
 
@@ -14,7 +16,7 @@ def _declared():
     for h in HEADERS:
         txt = h.read_text()
         txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-        names |= set(re.findall(r"^\s*(?:int|const char\*|int32_t)\s+(xpbd_\w+)\s*\(", txt, flags=re.M))
+        names |= set(re.findall(r"^\s*(?:int|const char\*|int32_t|float)\s+(xpbd_\w+)\s*\(", txt, flags=re.M))
     return names
 
 
@@ -31,7 +33,7 @@ def test_library_loads_and_exports_declared_symbols():
 
 def test_struct_sizes_match_header_layout():
     assert ctypes.sizeof(capi.XpbdMaterial) == 32
-    assert ctypes.sizeof(capi.XpbdParams) == 48 + 32 * capi.MAX_MATERIALS + 8 * capi.MAX_ATTACH_MATERIALS
+    assert ctypes.sizeof(capi.XpbdParams) == 64 + 32 * capi.MAX_MATERIALS + 8 * capi.MAX_ATTACH_MATERIALS
     assert ctypes.sizeof(capi.XpbdMetrics) == 32
 
 
@@ -57,3 +59,14 @@ def test_ctypes_offsets_match_c_compiler(tmp_path):
         assert int(out[s.__name__]) == ctypes.sizeof(s), s.__name__
         for f, _ in s._fields_:
             assert int(out[f"{s.__name__}.{f}"]) == getattr(s, f).offset, (s.__name__, f)
+
+
+def test_acc_scale_for_extent_is_the_largest_safe_power_of_two():
+    lib = capi.load(build_if_missing=True)
+    for e in (1e-4, 0.0137, 0.5, 1.0, 3.17, 100.0, 2500.0):
+        s = float(lib.xpbd_acc_scale_for_extent(e))
+        k = np.log2(s)
+        assert k == round(k)
+        assert e * s <= 2.0 ** 26 < e * 2.0 * s
+        # quantum at most half an FP32 ulp of the largest coordinate
+        assert 1.0 / s <= np.spacing(np.float32(e)) / 2

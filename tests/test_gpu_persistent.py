@@ -85,3 +85,25 @@ def test_humanv2_small_matches_per_iteration_path():
     assert moved > 10 * tol
     assert err <= tol
     assert int(sim._psync[2].item()) == 20 % 3
+
+
+def test_fixed_point_range_check_flags_oversized_scale():
+    """The tile passes sum corrections as round(d x acc_scale) in 32-bit
+    integers.  With the library's scale for the mesh the range check stays
+    clean; with a scale 2^20 times too large every sizeable correction leaves
+    the safe range and the status word reports it (integer arithmetic only:
+    the sums wrap, nothing faults)."""
+    from rlmusclev2_b200 import _capi as capi
+    verts, tets, table, mass, vf, act, tendon, deformed, prev = _mixed_problem()
+    kw = dict(dt=1.0 / 240.0, contraction_ratio=0.4, fiber_stiffness_scale=3.0)
+    sim = XpbdSolver(verts, tets, table, mass=mass, v_fiber=vf, tet_tendonmask=tendon, device="cuda:0",
+                     tile_tets=64, **kw)
+    sim.set_activation(act)
+    sim.set_positions(prev, also_prev=True)
+    sim.set_positions(deformed)
+    sim._fused_iterations(2)
+    assert sim.persistent_status() == 0
+    sim._prm.acc_scale = sim._prm.acc_scale * 2.0 ** 20
+    sim.set_positions(deformed)
+    sim._fused_iterations(1)
+    assert sim.persistent_status() & capi.STATUS_ACC_RANGE
