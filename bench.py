@@ -399,7 +399,9 @@ def run_ours(args):
         coarse = 1 if (co.use_persistent and co._persist_fits) else 2 * sim.mg.iters
     per_sub = 1 + fine + (2 + coarse if sim.mg is not None else 0)
     if getattr(sim, "dcd", None) is not None:  # broadphase on the first iteration
-        per_sub += sim.dcd.buf.broadphase_launches(True)
+        every = max(1, int(sim.dcd.params.bvh_rebuild_every))
+        per_sub += sum(sim.dcd.buf.broadphase_launches(True, refit_only=(k % every) != 0)
+                       for k in range(sim.nsubsteps)) / sim.nsubsteps
     launches_per_frame = 1 + (1 if sim.collision_solvers else 0) + (1 if sim._has_pins else 0) + (
         1 if sim.mg is not None else 0) + sim.nsubsteps * per_sub + 1
     n_iter = sim.nsubsteps * sim.fine_iters
@@ -427,7 +429,7 @@ def run_ours(args):
         "clocks": clk.summary(),
         **({"instances": n_inst_total, "instance_substeps_per_s": round(n_inst_total * sim.nsubsteps / (ms_frame * 1e-3), 1),
             "autotune": {k: v for k, v in tuned.items() if k != "tried"}} if batched else {}),
-        "gpu_launches": (launches_per_frame + 1) * args.steps,
+        "gpu_launches": int(round((launches_per_frame + 1) * args.steps)),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config == "humanv2":
         cb = CpuBaseline(cfg, sc)

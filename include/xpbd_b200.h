@@ -355,11 +355,15 @@ typedef struct XpbdDcd {
     int32_t* ws_count;        /* [n_tris] pairs per Morton position, then their offsets */
     int32_t* ws_total;        /* [1] */
     int32_t* ws_slots;        /* [16][n_tris] first partners of each query (counting pass) */
+    int32_t* ws_split;        /* [n_tris-1][4] leaf range and split of each internal node */
+    int32_t refit_only;       /* 1: keep the Morton order and hierarchy of the last rebuild on this
+                                 workspace and recompute the boxes only (same pair set; no sort, no
+                                 split search).  Needs one earlier call with 0. */
 } XpbdDcd;
 
 /* Element counts of the DCD workspace arrays for n_tris triangles. */
 typedef struct XpbdDcdWorkspaceSizes {
-    int64_t nodes_floats, keys, hist, bbox_floats, count, slots;
+    int64_t nodes_floats, keys, hist, bbox_floats, count, slots, split;
 } XpbdDcdWorkspaceSizes;
 
 int xpbd_dcd_workspace_query(int32_t n_tris, XpbdDcdWorkspaceSizes* out);

@@ -87,12 +87,13 @@ class XpbdDcd(C.Structure):
                 ("ws_nodes", C.c_void_p), ("ws_keys", C.c_void_p), ("ws_vals", C.c_void_p),
                 ("ws_keys2", C.c_void_p), ("ws_vals2", C.c_void_p), ("ws_hist", C.c_void_p),
                 ("ws_bbox", C.c_void_p),
-                ("ws_count", C.c_void_p), ("ws_total", C.c_void_p), ("ws_slots", C.c_void_p)]
+                ("ws_count", C.c_void_p), ("ws_total", C.c_void_p), ("ws_slots", C.c_void_p),
+                ("ws_split", C.c_void_p), ("refit_only", C.c_int32)]
 
 
 class XpbdDcdWorkspaceSizes(C.Structure):
     _fields_ = [("nodes_floats", C.c_int64), ("keys", C.c_int64), ("hist", C.c_int64),
-                ("bbox_floats", C.c_int64), ("count", C.c_int64), ("slots", C.c_int64)]
+                ("bbox_floats", C.c_int64), ("count", C.c_int64), ("slots", C.c_int64), ("split", C.c_int64)]
 
 
 class XpbdMetrics(C.Structure):

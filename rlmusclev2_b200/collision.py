@@ -142,6 +142,10 @@ class UdcfParams:
     gauss_seidel: bool = False
     max_push: float = 0.0
     use_bvh: bool = True
+    # Library-specific: rebuild the LBVH (Morton sort + hierarchy) every n-th
+    # broadphase and refit the boxes in between.  1 = the reference's
+    # per-broadphase rebuild; the pair set is the same for any n.
+    bvh_rebuild_every: int = 1
 
 
 class DcdBuffers:
@@ -172,7 +176,8 @@ class DcdBuffers:
             hist=torch.zeros(int(sz.hist), dtype=i32, device=dev),
             bbox=torch.zeros(int(sz.bbox_floats), dtype=torch.float32, device=dev),
             count=torch.zeros(int(sz.count), dtype=i32, device=dev),
-            slots=torch.zeros(int(sz.slots), dtype=i32, device=dev))
+            slots=torch.zeros(int(sz.slots), dtype=i32, device=dev),
+            split=torch.zeros(int(sz.split), dtype=i32, device=dev))
         t = self.t
         d = capi.XpbdDcd()
         d.n_tris, d.n_verts, d.max_pairs, d.max_contacts = n, int(n_verts), params.max_pairs, params.max_contacts
@@ -192,19 +197,27 @@ class DcdBuffers:
         d.ws_keys2, d.ws_vals2, d.ws_hist = t["keys2"].data_ptr(), t["vals2"].data_ptr(), t["hist"].data_ptr()
         d.ws_bbox = t["bbox"].data_ptr()
         d.ws_count, d.ws_slots = t["count"].data_ptr(), t["slots"].data_ptr()
+        d.ws_split = t["split"].data_ptr()
+        self._built = False
         self.d = d
 
-    def broadphase(self, pos4: torch.Tensor, snapshot_prev: bool, stream) -> None:
+    def broadphase(self, pos4: torch.Tensor, snapshot_prev: bool, stream, refit_only: bool = False) -> None:
+        """Boxes, LBVH and pair list; ``refit_only`` keeps the last rebuild's
+        Morton order and hierarchy (the first call always rebuilds)."""
+        self.d.refit_only = int(bool(refit_only) and self._built)
         capi.check(self.lib.xpbd_dcd_broadphase(C.byref(self.d), C.c_void_p(pos4.data_ptr()), int(snapshot_prev),
                                                 stream))
+        self._built = True
 
-    def broadphase_launches(self, snapshot_prev: bool = True) -> int:
+    def broadphase_launches(self, snapshot_prev: bool = True, refit_only: bool = False) -> int:
         """Kernels one xpbd_dcd_broadphase call launches: snapshot copy, boxes,
-        cooperative sort, leaf permute, build, counting traversal, the count
-        scan (2 launches, 3 above 4096 triangles), fill pass, total."""
+        cooperative sort (not when refitting), leaf permute, build or refit,
+        counting traversal, the count scan (2 launches, 3 above 4096
+        triangles), fill pass, total."""
         n = int(self.d.n_tris)
         scan = 2 + (1 if n > 4096 else 0)
-        return int(snapshot_prev) + 3 + (1 if n > 1 else 0) + 1 + scan + 2
+        sort = 0 if refit_only else 1
+        return int(snapshot_prev) + 2 + sort + (1 if n > 1 else 0) + 1 + scan + 2
 
     def narrow_respond(self, pos4: torch.Tensor, stream) -> None:
         capi.check(self.lib.xpbd_dcd_narrow_respond(C.byref(self.d), C.c_void_p(pos4.data_ptr()), stream))
@@ -234,11 +247,14 @@ class UdcfDcdCollider:
         hi = sim.pos0_np.max(0) + margin
         self.buf = DcdBuffers(sim._lib, sim.device, sim.layout.inv[tris], sim.n_verts, self.params, lo, hi)
         self._peak = 0
+        self._n_broad = 0  # broadphase calls so far (rebuild cadence; a captured frame repeats its pattern)
 
     def solve(self, i_iter: int = 0) -> None:
         s = self.sim
         if i_iter == 0:
-            self.buf.broadphase(s._pos4, True, s._sp)
+            every = max(1, int(self.params.bvh_rebuild_every))
+            self.buf.broadphase(s._pos4, True, s._sp, refit_only=(self._n_broad % every) != 0)
+            self._n_broad += 1
         self.buf.narrow_respond(s._pos4, s._sp)
 
     __call__ = solve

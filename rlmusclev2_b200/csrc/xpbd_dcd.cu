@@ -56,6 +56,9 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
 }
 
 // ---------------------------------------------------------------- AABBs
+// KEYS = false (refit-only broadphase): boxes only; the Morton keys and the
+// sorted order of the last rebuild are kept.
+template <bool KEYS>
 __global__ void k_tri_aabb(XpbdDcd D, const float* __restrict__ pos4) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.n_tris) return;
@@ -70,6 +73,7 @@ __global__ void k_tri_aabb(XpbdDcd D, const float* __restrict__ pos4) {
     float4* tri_box = reinterpret_cast<float4*>(D.ws_nodes) + tri_leaf_base(D.n_tris);
     tri_box[2 * i] = make_float4(lo.x, lo.y, lo.z, 0.f);
     tri_box[2 * i + 1] = make_float4(hi.x, hi.y, hi.z, 0.f);
+    if (!KEYS) return;
     const float3 cen = make_float3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
     float q[3] = {cen.x, cen.y, cen.z};
     uint32_t code = 0;
@@ -313,6 +317,18 @@ __device__ Box range_box(const XpbdDcd& D, int a, int b) {
     return bx;
 }
 
+// Half `side` of internal node i's record: the box of the child covering
+// [lo, g] (side 0) or [g + 1, hi] (side 1), its last Morton position, its id.
+__device__ __forceinline__ void write_child(const XpbdDcd& D, int i, int side, int lo, int g, int hi) {
+    const int n = D.n_tris;
+    const int first = side ? g + 1 : lo, last = side ? hi : g;
+    const int id = (first == last) ? (n - 1 + first) : (side ? g + 1 : g);
+    const Box bx = range_box(D, first, last + 1);
+    float4* rec = reinterpret_cast<float4*>(D.ws_nodes) + 4 * int64_t(i) + 2 * side;
+    rec[0] = make_float4(bx.lo.x, bx.lo.y, bx.lo.z, __int_as_float(last));
+    rec[1] = make_float4(bx.hi.x, bx.hi.y, bx.hi.z, __int_as_float(id));
+}
+
 // Karras (2012) hierarchy over the sorted keys.  Two threads per internal
 // node i (adjacent lanes) both run its split search; thread `side` then
 // writes child `side`'s half of record i: box from the child's leaf range,
@@ -341,12 +357,21 @@ __global__ void k_build(XpbdDcd D) {
     } while (t > 1);
     const int g = i + s * d + min(d, 0);
     const int lo = min(i, j), hi = max(i, j);
-    const int first = side ? g + 1 : lo, last = side ? hi : g;  // the child's leaf range
-    const int id = (first == last) ? (n - 1 + first) : (side ? g + 1 : g);
-    const Box bx = range_box(D, first, last + 1);
-    float4* rec = reinterpret_cast<float4*>(D.ws_nodes) + 4 * int64_t(i) + 2 * side;
-    rec[0] = make_float4(bx.lo.x, bx.lo.y, bx.lo.z, __int_as_float(last));
-    rec[1] = make_float4(bx.hi.x, bx.hi.y, bx.hi.z, __int_as_float(id));
+    if (side == 0) reinterpret_cast<int4*>(D.ws_split)[i] = make_int4(lo, g, hi, 0);
+    write_child(D, i, side, lo, g, hi);
+}
+
+// Refit-only broadphase: the hierarchy of the last rebuild (leaf range and
+// split per internal node in ws_split) over the leaves in that rebuild's
+// Morton order, boxes recomputed from the current leaf boxes.  The pair set
+// does not depend on the hierarchy, only the traversal cost does.
+__global__ void k_refit_ranges(XpbdDcd D) {
+    const int n = D.n_tris;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gid >> 1, side = gid & 1;
+    if (i >= n - 1) return;
+    const int4 r = reinterpret_cast<const int4*>(D.ws_split)[i];
+    write_child(D, i, side, r.x, r.y, r.z);
 }
 
 // Leaves were written in triangle order; the build wants them in Morton order.  A CTA of 1024 threads covers 1024
@@ -797,11 +822,11 @@ int launch_sort(const XpbdDcd* D, uint32_t* sync, cudaStream_t s) {
 int check_dcd(const XpbdDcd* D) {
     if (!D || D->n_tris <= 0 || D->n_verts <= 0 || !D->tris || !D->pairs || !D->n_pairs || !D->n_contacts ||
         !D->c_ids || !D->c_data || !D->x_prev || !D->dP || !D->status || !D->ws_nodes || !D->ws_keys || !D->ws_vals ||
-        !D->ws_keys2 || !D->ws_vals2 || !D->ws_hist || !D->ws_bbox || !D->ws_count ||
+        !D->ws_keys2 || !D->ws_vals2 || !D->ws_hist || !D->ws_bbox || !D->ws_split || !D->ws_count ||
         !D->ws_total || !D->ws_slots)
         return fail(XPBD_ERR_ARG, "XpbdDcd: null member or empty size");
     if (D->max_pairs <= 0 || D->max_contacts <= 0) return fail(XPBD_ERR_ARG, "XpbdDcd: capacities must be > 0");
-    if (!aligned16(D->ws_nodes) || !aligned16(D->ws_bbox) || !aligned16(D->pairs) || !aligned16(D->c_ids) || !aligned16(D->c_data) || !aligned16(D->x_prev) ||
+    if (!aligned16(D->ws_nodes) || !aligned16(D->ws_bbox) || !aligned16(D->ws_split) || !aligned16(D->pairs) || !aligned16(D->c_ids) || !aligned16(D->c_data) || !aligned16(D->x_prev) ||
         !aligned16(D->dP))
         return fail(XPBD_ERR_ALIGN, "XpbdDcd: 16-byte alignment");
     return XPBD_OK;
@@ -820,6 +845,7 @@ int xpbd_dcd_workspace_query(int32_t n_tris, XpbdDcdWorkspaceSizes* out) {
     out->bbox_floats = int64_t(8) * ((n_tris + 31) / 32 + (n_tris + 1023) / 1024);  // 32- and 1024-leaf block boxes
     out->count = n_tris;
     out->slots = int64_t(kSlots) * n_tris;
+    out->split = int64_t(4) * (n_tris > 1 ? n_tris - 1 : 1);
     return XPBD_OK;
 }
 
@@ -832,12 +858,18 @@ int xpbd_dcd_broadphase(const XpbdDcd* D, const float* pos4, int32_t snapshot_pr
     if (snapshot_prev)
         k_copy4<<<(D->n_verts + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float4*>(pos4),
                                                           reinterpret_cast<float4*>(D->x_prev), D->n_verts);
-    k_tri_aabb<<<(n + 255) / 256, 256, 0, s>>>(*D, pos4);
     int* scan_scratch = D->ws_hist + hist_words(n);
-    uint32_t* sort_sync = reinterpret_cast<uint32_t*>(scan_scratch + scan_words(n));
-    if ((rc = launch_sort(D, sort_sync, s))) return rc;
-    k_permute_leaves<<<(n + 1023) / 1024, 1024, 0, s>>>(*D);
-    if (n > 1) k_build<<<(2 * (n - 1) + 255) / 256, 256, 0, s>>>(*D);
+    if (D->refit_only) {
+        k_tri_aabb<false><<<(n + 255) / 256, 256, 0, s>>>(*D, pos4);
+        k_permute_leaves<<<(n + 1023) / 1024, 1024, 0, s>>>(*D);
+        if (n > 1) k_refit_ranges<<<(2 * (n - 1) + 255) / 256, 256, 0, s>>>(*D);
+    } else {
+        k_tri_aabb<true><<<(n + 255) / 256, 256, 0, s>>>(*D, pos4);
+        uint32_t* sort_sync = reinterpret_cast<uint32_t*>(scan_scratch + scan_words(n));
+        if ((rc = launch_sort(D, sort_sync, s))) return rc;
+        k_permute_leaves<<<(n + 1023) / 1024, 1024, 0, s>>>(*D);
+        if (n > 1) k_build<<<(2 * (n - 1) + 255) / 256, 256, 0, s>>>(*D);
+    }
     k_traverse<false><<<(n + 127) / 128, 128, 0, s>>>(*D);
     scan_excl(D->ws_count, n, D->ws_total, scan_scratch, s);
     k_traverse<true><<<(n + 127) / 128, 128, 0, s>>>(*D);

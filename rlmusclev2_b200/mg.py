@@ -219,7 +219,8 @@ class MultiGridSim(MuscleSim):
                              offset=float(sc_cfg.get("offset", 1e-6)), thickness=float(sc_cfg.get("thickness", 0.0)),
                              max_pairs=int(sc_cfg.get("max_pairs", 1 << 22)),
                              max_contacts=int(sc_cfg.get("max_contacts", 1 << 20)),
-                             allow_self=bool(sc_cfg.get("allow_self", True)), max_push=float(sc_cfg.get("max_push", 0.0)))
+                             allow_self=bool(sc_cfg.get("allow_self", True)), max_push=float(sc_cfg.get("max_push", 0.0)),
+                             bvh_rebuild_every=int(sc_cfg.get("bvh_rebuild_every", 1)))
             self.dcd = UdcfDcdCollider(self, sc.surface_tris, prm)
             self.collision_solvers_iter.append(self.dcd.solve)
         self._frame_loaded = None

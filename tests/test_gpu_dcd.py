@@ -78,6 +78,34 @@ def test_pairs_large_soup():
     np.testing.assert_array_equal(got, ref)
 
 
+def test_refit_only_pairs_match_oracle():
+    """Refit-only broadphase (hierarchy of an earlier rebuild, boxes of the
+    moved mesh): the same pair set as the oracle on the new positions."""
+    import ctypes
+    tris, p4 = _scene_surface()
+    prm = UdcfParams(allow_self=True, thickness=0.0005, max_pairs=1 << 21, max_contacts=1 << 18)
+    lib = capi.load()
+    dev = torch.device("cuda:0")
+    s = torch.cuda.Stream(dev)
+    sp = ctypes.c_void_p(s.cuda_stream)
+    lo, hi = p4[:, :3].min(0) - 0.01, p4[:, :3].max(0) + 0.01
+    buf = DcdBuffers(lib, dev, tris, p4.shape[0], prm, lo, hi)
+    buf.broadphase(torch.from_numpy(p4).to(dev), True, sp)
+    rng = np.random.default_rng(9)
+    moved = p4.copy()
+    moved[:, :3] += rng.normal(scale=0.002, size=(p4.shape[0], 3)).astype(np.float32)
+    buf.broadphase(torch.from_numpy(moved).to(dev), True, sp, refit_only=True)
+    s.synchronize()
+    assert buf.d.refit_only == 1
+    cnt = buf.counters()
+    got = buf.t["pairs"][: cnt["n_pairs"]].cpu().numpy()
+    ref, _ = O.dcd_pairs(tris, moved, thickness=prm.thickness, allow_self=True)
+    print(f"refit-only: pairs {got.shape[0]} oracle {ref.shape[0]} status {cnt['status']}")
+    assert cnt["status"] == 0
+    assert got.shape[0] == ref.shape[0] > 1000
+    np.testing.assert_array_equal(got[np.lexsort((got[:, 1], got[:, 0]))], ref)
+
+
 def test_narrow_respond_match_oracle():
     tris, p4 = _scene_surface(seed=4, jitter=0.006)
     prm = UdcfParams(allow_self=True, thickness=0.0, max_pairs=1 << 21, max_contacts=1 << 19)
