@@ -241,6 +241,41 @@ int xpbd_bone_targets(int32_t n, int32_t n_bones, const float* transforms, const
                       const float* vert_w, const float* rest4, float* pin_target, float* attach_target,
                       xpbd_stream_t stream);
 
+/* Bone-surface binding, the reference's target_mode="mesh" driver.  A bone
+ * surface is a triangle mesh: bone4 [n_bverts][4] (x, y, z, -), btris
+ * [n_btris][3].  Barycentric (u, v) of face (A, B, C) weight A and B, C takes
+ * 1 - u - v (Warp's mesh_eval_position); the face frame is t1 = unit(A - C),
+ * n = unit((A - C) x (B - C)), t2 = n x t1 (_face_basis, mg/kernel.py:267-285).
+ * The closest-point queries are a brute force over all faces (ties keep the
+ * lowest face index), meant for bone surfaces of up to a few 10^4 faces.
+ *
+ * xpbd_bone_bind replaces bone_bind_kernel (mg/kernel.py:287-310): for each
+ * query4[i] the closest face within max_dist, its (u, v) and the offset
+ * R^T (query - closest point) in the face frame (face 0, zeros when none). */
+int xpbd_bone_bind(int32_t n, const float* query4, int32_t n_bverts, const float* bone4, int32_t n_btris,
+                   const int32_t* btris, float max_dist, int32_t* out_face, float* out_uv, float* out_local4,
+                   xpbd_stream_t stream);
+
+/* bone_slide_target_kernel (mg/kernel.py:313-347) on the current bone
+ * surface: with reproject != 0 each vertex re-binds to its closest face of
+ * muscle4 when that point lies within slide_range of its anchor (anchor_face,
+ * anchor_uv: the bind at the start frame), updating bind_face, bind_uv and
+ * local4; then target = closest point + R local, written to pin_target.xyz
+ * and/or attach_target.xyz (either may be NULL; .w lanes kept).  Faces must
+ * come from xpbd_bone_bind on a surface with the same triangles. */
+int xpbd_bone_slide_targets(int32_t n, const float* muscle4, const int32_t* anchor_face, const float* anchor_uv,
+                            int32_t* bind_face, float* bind_uv, float* local4, float slide_range, int32_t reproject,
+                            float max_dist, int32_t n_bverts, const float* bone4, int32_t n_btris,
+                            const int32_t* btris, float* pin_target, float* attach_target, xpbd_stream_t stream);
+
+/* Rigid pose of bone-surface vertices for a frame: out4[j] = R_b rest4[j] + t_b,
+ * b = vert_bone[j], transforms as for xpbd_bone_targets above ([n_bones][12]
+ * row-major [R | t]).  Stands in for the per-frame bone-mesh upload of
+ * MultiGridSim._update_slide_target (mg/mg.py:1160-1174) when the bones are
+ * rigid (the synthetic capsule skeleton). */
+int xpbd_bone_surface_pose(int32_t n_bverts, const float* rest4, const int32_t* vert_bone, int32_t n_bones,
+                           const float* transforms, float* out4, xpbd_stream_t stream);
+
 /* Capsule bone, rest pose: centre, unit axis, half segment length, radius. */
 typedef struct XpbdCapsule {
     float center[3];

@@ -635,3 +635,61 @@ def dcd_respond_apply(c_ids, c_data, pos4, xprev4, multiplier=1.01, mu_s=0.5, mu
                             _p(np.ascontiguousarray(xprev4, np.float32)), out.shape[0], C.c_float(multiplier),
                             C.c_float(mu_s), C.c_float(mu_d), C.c_float(max_push), int(jacobi_avg), _p(dP))
     return out
+
+
+# ------------------------------------------------ bone-surface binding (target_mode="mesh")
+def _v4(a):
+    a = np.asarray(a, np.float32)
+    if a.shape[1] == 4:
+        return np.ascontiguousarray(a)
+    out = np.zeros((a.shape[0], 4), np.float32)
+    out[:, :3] = a
+    return out
+
+
+def bone_bind(query, bone_verts, tris, max_dist):
+    """bone_bind_kernel (mg/kernel.py:287-310), brute force: (face, uv, local4)."""
+    L = lib()
+    q4, b4 = _v4(query), _v4(bone_verts)
+    tris = np.ascontiguousarray(tris, np.int32)
+    n = q4.shape[0]
+    face = np.zeros(n, np.int32)
+    uv = np.zeros((n, 2), np.float32)
+    loc = np.zeros((n, 4), np.float32)
+    L.orc_bone_bind.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_float, C.c_void_p,
+                                C.c_void_p, C.c_void_p]
+    L.orc_bone_bind(n, _p(q4), _p(b4), tris.shape[0], _p(tris), C.c_float(max_dist), _p(face), _p(uv), _p(loc))
+    return face, uv, loc
+
+
+def bone_slide_targets(muscle, anchor_face, anchor_uv, bind_face, bind_uv, local4, slide_range, reproject, max_dist,
+                       bone_verts, tris):
+    """bone_slide_target_kernel (mg/kernel.py:313-347): returns (targets [n,3],
+    bind_face, bind_uv, local4) with the binding updated by accepted slides."""
+    L = lib()
+    m4, b4 = _v4(muscle), _v4(bone_verts)
+    tris = np.ascontiguousarray(tris, np.int32)
+    bf = np.array(bind_face, np.int32)
+    buv = np.array(bind_uv, np.float32)
+    loc = np.array(local4, np.float32)
+    n = m4.shape[0]
+    tgt = np.zeros((n, 4), np.float32)
+    L.orc_bone_slide_targets.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_float, C.c_int, C.c_float, C.c_void_p, C.c_int, C.c_void_p,
+                                         C.c_void_p]
+    L.orc_bone_slide_targets(n, _p(m4), _p(np.ascontiguousarray(anchor_face, np.int32)),
+                             _p(np.ascontiguousarray(anchor_uv, np.float32)), _p(bf), _p(buv), _p(loc),
+                             C.c_float(slide_range), int(reproject), C.c_float(max_dist), _p(b4), tris.shape[0],
+                             _p(tris), _p(tgt))
+    return tgt[:, :3], bf, buv, loc
+
+
+def bone_pose(rest, vert_bone, transforms):
+    """Rigid pose of bone-surface vertices: R_b x + t_b per vertex (float32)."""
+    L = lib()
+    r4 = _v4(rest)
+    tr = np.ascontiguousarray(np.asarray(transforms, np.float32).reshape(-1, 12))
+    out = np.zeros_like(r4)
+    L.orc_bone_pose.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_bone_pose(r4.shape[0], _p(r4), _p(np.ascontiguousarray(vert_bone, np.int32)), _p(tr), _p(out))
+    return out[:, :3]

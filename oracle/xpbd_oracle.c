@@ -30,3 +30,4 @@
 #undef SFX
 
 #include "xpbd_oracle_dcd.h"
+#include "xpbd_oracle_bone.h"

@@ -230,6 +230,20 @@ class Scene:
     def n_bones(self) -> int:
         return int(self.bone_center.shape[0])
 
+    def bone_surface(self, n_around: int = 16, n_lat: int = 4):
+        """Rest triangle surfaces of all capsule bones, for the bone-surface
+        binding (target_mode="mesh"): (verts [NBV,3], tris [NBT,3], vert_bone
+        [NBV])."""
+        vs, ts, vb, off = [], [], [], 0
+        for b in range(self.n_bones):
+            v, t = capsule_surface(self.bone_center[b], self.bone_axis[b], float(self.bone_half[b]),
+                                   float(self.bone_radius[b]), n_around, n_lat)
+            vs.append(v)
+            ts.append(t + off)
+            vb.append(np.full(v.shape[0], b, np.int32))
+            off += v.shape[0]
+        return np.concatenate(vs), np.concatenate(ts).astype(np.int32), np.concatenate(vb)
+
     def bone_transforms(self, frame: float) -> np.ndarray:
         """(NB,3,4) rigid transforms [R | t] at ``frame``: x -> R (x - c) + c + d,
         the identity at the start frame (targets bind to the rest pose there)."""
@@ -281,6 +295,43 @@ class Scene:
         else:
             out[self.aniso_muscle] = min(1.0, max(0.0, (int(frame) - start) / max(1, end - start)))
         return out
+
+
+def capsule_surface(c, axis, half: float, r: float, n_around: int = 16, n_lat: int = 4):
+    """Closed triangle surface of a capsule (segment c +- half * axis, radius
+    r): two hemispheres of n_lat latitude rings each joined by the cylinder,
+    n_around vertices per ring plus the two poles.  Returns (verts, tris)."""
+    c = np.asarray(c, np.float64)
+    a = np.asarray(axis, np.float64)
+    a = a / np.linalg.norm(a)
+    e1 = np.cross(a, [1.0, 0.0, 0.0] if abs(a[0]) < 0.9 else [0.0, 1.0, 0.0])
+    e1 /= np.linalg.norm(e1)
+    e2 = np.cross(a, e1)
+    th = 2.0 * np.pi * np.arange(n_around) / n_around
+    rad = np.cos(th)[:, None] * e1 + np.sin(th)[:, None] * e2
+    rings = []
+    for k in range(1, n_lat + 1):  # bottom hemisphere, pole side first, ends at the equator
+        ph = -0.5 * np.pi + 0.5 * np.pi * k / n_lat
+        rings.append(c - half * a + r * (np.sin(ph) * a + np.cos(ph) * rad))
+    for k in range(n_lat):  # top hemisphere from its equator
+        ph = 0.5 * np.pi * k / n_lat
+        rings.append(c + half * a + r * (np.sin(ph) * a + np.cos(ph) * rad))
+    verts = [c - (half + r) * a[None]] + rings + [c + (half + r) * a[None]]
+    verts = np.concatenate(verts).astype(np.float32)
+    top = verts.shape[0] - 1
+    tris = []
+    for j in range(n_around):  # bottom fan (outward normals)
+        tris.append([0, 1 + (j + 1) % n_around, 1 + j])
+    for q in range(len(rings) - 1):
+        b0, b1 = 1 + q * n_around, 1 + (q + 1) * n_around
+        for j in range(n_around):
+            jn = (j + 1) % n_around
+            tris.append([b0 + j, b0 + jn, b1 + jn])
+            tris.append([b0 + j, b1 + jn, b1 + j])
+    last = 1 + (len(rings) - 1) * n_around
+    for j in range(n_around):
+        tris.append([last + j, last + (j + 1) % n_around, top])
+    return verts, np.asarray(tris, np.int32)
 
 
 def capsule_sdf(x: np.ndarray, c: np.ndarray, axis: np.ndarray, half: float, r: float) -> np.ndarray:

@@ -4,9 +4,13 @@ on the sm_100a engine.
 Same JSON schema (``constraints[]`` blocks looked up by name with ``enable``
 toggles, solver keys at the top level).  The rest mesh comes from a seeded
 synthetic generator (``cfg["synthetic"]``) because the reference's humanV2
-assets are not available; each vertex is bound to its nearest capsule bone and
-its target rides that bone rigidly (the reference's target_mode="mesh"
-binding with sliding off).
+assets are not available.  Kinematic targets (mg.py:436-446):
+target_mode="mesh" binds every vertex to the closest point of the bone
+surfaces at the start frame and rides (optionally slides along) them
+(mg.py:1117-1174; the synthetic bones are capsule surfaces posed rigidly);
+target_mode="lbs" gives every vertex a smooth target blended between the two
+bones at its muscle's ends, computed on the device from the bone poses (the
+synthetic counterpart of the reference's precomputed LBS target sequence).
 """
 from __future__ import annotations
 
@@ -110,6 +114,16 @@ class MultiGridSim(MuscleSim):
                                       "provide cfg['synthetic'] or a Scene")
         self.scene = scene if scene is not None else scene_from_cfg(cfg)
         sc = self.scene
+        # kinematic targets (mg.py:436-446)
+        self.target_mode = str(cfg.get("target_mode", "lbs"))
+        self.use_sliding = bool(cfg.get("use_sliding", False))
+        self.slide_range = float(cfg.get("slide_range", 0.005))
+        self.slide_interval = int(cfg.get("slide_interval", 1))
+        if self.target_mode not in ("mesh", "lbs"):
+            raise NotImplementedError(f"target_mode={self.target_mode!r} is not on the sm_100a path "
+                                      "(supported: 'mesh', 'lbs')")
+        if self.use_sliding and self.target_mode != "mesh":
+            raise ValueError("use_sliding=true requires target_mode='mesh' (mg.py:438-440)")
         self.pos0_np = sc.verts.astype(np.float32)
         self.tet_np = sc.tets.astype(np.int32)
         self.NV = self.n_verts = int(self.pos0_np.shape[0])
@@ -227,6 +241,10 @@ class MultiGridSim(MuscleSim):
 
     # ----------------------------------------------------------- kinematics
     def _host_targets(self, frame: float) -> np.ndarray:
+        if self.target_mode == "mesh":
+            if frame != self.start_frame:
+                raise ValueError("host targets of the surface binding exist for the start frame only")
+            return self.pos0_np.copy()  # the bind reconstructs the rest pose on the start-frame bones
         return self.scene.targets(frame)
 
     def _setup_kinematics(self) -> None:
@@ -248,6 +266,47 @@ class MultiGridSim(MuscleSim):
         self._pos_host = torch.zeros((self.NV, 3), dtype=torch.float32).pin_memory()
         self._h2d_event = torch.cuda.Event()
         self._h2d_event.record(self._stream)
+        if self.target_mode == "mesh":
+            self._setup_surface_binding()
+
+    def _setup_surface_binding(self) -> None:
+        """_build_bone_slide_binding (mg.py:1117-1158): the bone surfaces posed
+        at the start frame, every vertex's rest position bound to its closest
+        surface point (face, barycentric, offset in the face frame); the current
+        binding starts at that anchor."""
+        if not hasattr(self.scene, "bone_surface"):
+            raise NotImplementedError("target_mode='mesh' needs a scene with bone surfaces")
+        dev = self.device
+        bv, bt, bvb = self.scene.bone_surface()
+        r4 = np.zeros((bv.shape[0], 4), np.float32)
+        r4[:, :3] = bv
+        self._bs_rest4 = torch.from_numpy(r4).to(dev)
+        self._bs_pos4 = torch.zeros_like(self._bs_rest4)
+        self._bs_tris = torch.from_numpy(np.ascontiguousarray(bt, np.int32)).to(dev)
+        self._bs_vbone = torch.from_numpy(np.ascontiguousarray(bvb, np.int32)).to(dev)
+        self._slide_max_dist = float(self.slide_range + 1.0)  # mg.py:1131
+        nv = self.NV
+        self._anchor_face = torch.zeros(nv, dtype=torch.int32, device=dev)
+        self._anchor_uv = torch.zeros((nv, 2), dtype=torch.float32, device=dev)
+        self._local4 = torch.zeros((nv, 4), dtype=torch.float32, device=dev)
+        self.load_frame_targets(self.start_frame)
+        self._pose_bone_surface()
+        capi.check(self._lib.xpbd_bone_bind(nv, C.c_void_p(self._rest4.data_ptr()), int(bv.shape[0]),
+                                            C.c_void_p(self._bs_pos4.data_ptr()), int(bt.shape[0]),
+                                            C.c_void_p(self._bs_tris.data_ptr()), C.c_float(self._slide_max_dist),
+                                            C.c_void_p(self._anchor_face.data_ptr()),
+                                            C.c_void_p(self._anchor_uv.data_ptr()),
+                                            C.c_void_p(self._local4.data_ptr()), self._sp))
+        with torch.cuda.stream(self._stream):
+            self._bind_face = self._anchor_face.clone()
+            self._bind_uv = self._anchor_uv.clone()
+        self._reproject = False
+
+    def _pose_bone_surface(self) -> None:
+        capi.check(self._lib.xpbd_bone_surface_pose(int(self._bs_rest4.shape[0]), C.c_void_p(self._bs_rest4.data_ptr()),
+                                                    C.c_void_p(self._bs_vbone.data_ptr()), self.scene.n_bones,
+                                                    C.c_void_p(self._bone_tr.data_ptr()),
+                                                    C.c_void_p(self._bs_pos4.data_ptr()), self._sp))
 
     def load_frame_targets(self, frame: float) -> None:
         """Bone poses of ``frame`` -> device (one pinned H2D copy), then the
@@ -259,9 +318,22 @@ class MultiGridSim(MuscleSim):
             self._bone_tr.copy_(self._bone_tr_host, non_blocking=True)
         self._h2d_event.record(self._stream)
         self._frame_loaded = frame
+        # _update_slide_target (mg.py:1160-1174): re-project every slide_interval frames
+        self._reproject = bool(self.use_sliding and
+                               (int(frame) - int(self.start_frame)) % max(1, self.slide_interval) == 0)
 
     def _targets_kernel(self) -> None:
         v = self._verts
+        if self.target_mode == "mesh":
+            self._pose_bone_surface()
+            capi.check(self._lib.xpbd_bone_slide_targets(
+                self.NV, C.c_void_p(self._pos4.data_ptr()), C.c_void_p(self._anchor_face.data_ptr()),
+                C.c_void_p(self._anchor_uv.data_ptr()), C.c_void_p(self._bind_face.data_ptr()),
+                C.c_void_p(self._bind_uv.data_ptr()), C.c_void_p(self._local4.data_ptr()),
+                C.c_float(self.slide_range), int(self._reproject), C.c_float(self._slide_max_dist),
+                int(self._bs_rest4.shape[0]), C.c_void_p(self._bs_pos4.data_ptr()), int(self._bs_tris.shape[0]),
+                C.c_void_p(self._bs_tris.data_ptr()), v.pin_target, v.attach_target, self._sp))
+            return
         capi.check(self._lib.xpbd_bone_targets(self.NV, self.scene.n_bones, C.c_void_p(self._bone_tr.data_ptr()),
                                                C.c_void_p(self._vert_bone.data_ptr()),
                                                C.c_void_p(self._vert_bw.data_ptr()),
@@ -359,7 +431,7 @@ class MultiGridSim(MuscleSim):
         dcd = getattr(self, "dcd", None)
         return (all(dcd is not None and fn == dcd.solve for fn in its) and not getattr(self, "constraint_solvers", None)
                 and all(getattr(c, "graph_safe", False) for c in cs) and len(cs) <= 1
-                and getattr(self, "program", None) is None)
+                and getattr(self, "program", None) is None and not getattr(self, "use_sliding", False))
 
     def _frame_fused(self) -> None:
         self._targets_kernel()
