@@ -276,6 +276,16 @@ int xpbd_bone_slide_targets(int32_t n, const float* muscle4, const int32_t* anch
 int xpbd_bone_surface_pose(int32_t n_bverts, const float* rest4, const int32_t* vert_bone, int32_t n_bones,
                            const float* transforms, float* out4, xpbd_stream_t stream);
 
+/* Muscle-to-muscle glue (solve_m2m_glue_kernel, mg/kernel.py:350-394; run by
+ * MultiGridSim between apply_dP and apply_pintotarget, mg/mg.py:1346-1355):
+ * one XPBD distance step per pair (pair_a[c], pair_b[c]) toward restlen[c]
+ * with compliance[c] / dt^2 and a zero starting multiplier, scaled by omega,
+ * added to both endpoints of pos4 (library order) with atomics.  Inverse
+ * masses are pos4.w.  Pairs sharing a vertex update it concurrently, as the
+ * reference's atomic version does. */
+int xpbd_m2m_glue(int32_t n_pairs, const int32_t* pair_a, const int32_t* pair_b, const float* restlen,
+                  const float* compliance, float* pos4, float dt, float omega, xpbd_stream_t stream);
+
 /* Capsule bone, rest pose: centre, unit axis, half segment length, radius. */
 typedef struct XpbdCapsule {
     float center[3];

@@ -693,3 +693,15 @@ def bone_pose(rest, vert_bone, transforms):
     L.orc_bone_pose.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.orc_bone_pose(r4.shape[0], _p(r4), _p(np.ascontiguousarray(vert_bone, np.int32)), _p(tr), _p(out))
     return out[:, :3]
+
+
+def m2m_glue(pair_a, pair_b, restlen, compliance, pos4, dt, omega=1.0):
+    """solve_m2m_glue_kernel (mg/kernel.py:350-394), sequential over the pairs."""
+    L = lib()
+    out = np.array(pos4, np.float32)
+    L.orc_m2m_glue.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float,
+                               C.c_float]
+    L.orc_m2m_glue(len(pair_a), _p(np.ascontiguousarray(pair_a, np.int32)), _p(np.ascontiguousarray(pair_b, np.int32)),
+                   _p(np.ascontiguousarray(restlen, np.float32)), _p(np.ascontiguousarray(compliance, np.float32)),
+                   _p(out), C.c_float(dt), C.c_float(omega))
+    return out

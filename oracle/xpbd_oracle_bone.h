@@ -190,4 +190,28 @@ void orc_bone_pose(int nbv, const float* rest4, const int* vert_bone, const floa
     }
 }
 
+/* solve_m2m_glue_kernel (mg/kernel.py:350-394), pairs in index order, each
+ * seeing the corrections of the pairs before it; pos4.w = inverse mass. */
+void orc_m2m_glue(int n, const int* pa, const int* pb, const float* restlen, const float* compliance, float* pos4,
+                  float dt, float omega) {
+    for (int c = 0; c < n; ++c) {
+        float* xa = pos4 + 4 * pa[c];
+        float* xb = pos4 + 4 * pb[c];
+        const float d[3] = {xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2]};
+        const float len = sqrtf(ob_dot(d, d));
+        if (len < 1.0e-9f) continue;
+        const float dir[3] = {d[0] / len, d[1] / len, d[2] / len};
+        const float C = len - restlen[c];
+        const float wa = xa[3], wb = xb[3];
+        const float at = compliance[c] / (dt * dt);
+        const float den = (wa + wb) + at;
+        if (den < 1.0e-12f) continue;
+        const float f = omega * (-C / den);
+        for (int k = 0; k < 3; ++k) {
+            xa[k] += (f * wa) * dir[k];
+            xb[k] += (-f * wb) * dir[k];
+        }
+    }
+}
+
 #endif

@@ -1,7 +1,8 @@
 // Bone-surface binding of muscle vertices: the reference's target_mode="mesh"
 // kinematic driver (bone_bind_kernel / bone_slide_target_kernel,
-// mg/kernel.py:267-347, driven from mg/mg.py:1117-1174) and the per-frame
-// rigid pose of capsule bone surfaces.
+// mg/kernel.py:267-347, driven from mg/mg.py:1117-1174), the per-frame rigid
+// pose of capsule bone surfaces, and the muscle-to-muscle glue springs
+// (solve_m2m_glue_kernel, mg/kernel.py:350-394).
 //
 // The reference queries a Warp BVH mesh; here the closest-point query is a
 // brute force over the bone faces, staged through shared memory in chunks of
@@ -213,6 +214,38 @@ __global__ void k_bone_surface_pose(int nbv, const float4* __restrict__ rest4, c
     out4[j] = make_float4(o[0], o[1], o[2], 0.f);
 }
 
+// solve_m2m_glue_kernel (mg/kernel.py:350-394): one XPBD distance step per
+// cross-muscle pair with a fresh multiplier (the reference zeroes L before
+// every call), the correction added to both endpoints at once (atomics, as
+// the reference's wp.atomic_add).  Inverse masses come from pos4.w (0 for a
+// stopped or massless vertex, which then stays put).
+__global__ void k_m2m_glue(int n, const int* __restrict__ pa, const int* __restrict__ pb,
+                           const float* __restrict__ restlen, const float* __restrict__ compliance, float4* pos4,
+                           float dt, float omega) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int a = pa[c], b = pb[c];
+    const float4 xa = pos4[a], xb = pos4[b];
+    const float3 d = make_float3(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
+    const float len = sqrtf(dot(d, d));
+    if (len < 1.0e-9f) return;
+    const float3 dir = make_float3(d.x / len, d.y / len, d.z / len);
+    const float C = len - restlen[c];
+    const float wa = xa.w, wb = xb.w;
+    const float at = compliance[c] / (dt * dt);
+    const float den = (wa + wb) + at;
+    if (den < 1.0e-12f) return;
+    const float dl = -C / den;
+    const float f = omega * dl;
+    float* pf = reinterpret_cast<float*>(pos4);
+    atomicAdd(pf + 4 * a + 0, (f * wa) * dir.x);
+    atomicAdd(pf + 4 * a + 1, (f * wa) * dir.y);
+    atomicAdd(pf + 4 * a + 2, (f * wa) * dir.z);
+    atomicAdd(pf + 4 * b + 0, (-f * wb) * dir.x);
+    atomicAdd(pf + 4 * b + 1, (-f * wb) * dir.y);
+    atomicAdd(pf + 4 * b + 2, (-f * wb) * dir.z);
+}
+
 bool a16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 bool a8(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0; }
 
@@ -271,6 +304,17 @@ int xpbd_bone_surface_pose(int32_t n_bverts, const float* rest4, const int32_t* 
     k_bone_surface_pose<<<(n_bverts + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
         n_bverts, reinterpret_cast<const float4*>(rest4), vert_bone, transforms, reinterpret_cast<float4*>(out4));
     return cuda_check("xpbd_bone_surface_pose");
+}
+
+int xpbd_m2m_glue(int32_t n_pairs, const int32_t* pair_a, const int32_t* pair_b, const float* restlen,
+                  const float* compliance, float* pos4, float dt, float omega, xpbd_stream_t stream) {
+    if (n_pairs < 0 || (n_pairs > 0 && (!pair_a || !pair_b || !restlen || !compliance || !pos4)) || !(dt > 0.f))
+        return fail(XPBD_ERR_ARG, "xpbd_m2m_glue: bad arguments");
+    if (!a16(pos4)) return fail(XPBD_ERR_ALIGN, "xpbd_m2m_glue: pos4 must be 16-byte aligned");
+    if (n_pairs == 0) return XPBD_OK;
+    k_m2m_glue<<<(n_pairs + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n_pairs, pair_a, pair_b, restlen, compliance,
+                                                                        reinterpret_cast<float4*>(pos4), dt, omega);
+    return cuda_check("xpbd_m2m_glue");
 }
 
 }  // extern "C"

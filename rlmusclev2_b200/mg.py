@@ -210,6 +210,7 @@ class MultiGridSim(MuscleSim):
                            fiber_stiffness_scale=self.fiber_stiffness_scale, tile_tets=cfg.get("tile_tets"),
                            vert_group=getattr(sc, "vert_inst", None))
         self._setup_kinematics()
+        self._setup_m2m_glue()
         self.collision_solvers_iter = []
         self.mg = None
         if self.use_multigrid:
@@ -302,6 +303,80 @@ class MultiGridSim(MuscleSim):
             self._bind_uv = self._anchor_uv.clone()
         self._reproject = False
 
+    def _setup_m2m_glue(self) -> None:
+        """_build_m2m_glue (mg.py:581-660) when the config has a
+        muscleToMuscleGlue block.  The per-vertex muscle id comes from the
+        scene (``vert_muscle``, else the part of the vertex's tets); the enable
+        mask from the scene's ``m2m_mask`` or, for the synthetic scenes, the
+        block's ``region``: "all" muscle vertices, their "surface" ones, or the
+        "interface" ones (a vertex of another muscle within ``distance``), the
+        stand-in for the authored muscletomuscleglue mask."""
+        from .glue import build_m2m_pairs
+        self.n_m2m = 0
+        g = find_constraint(self.cfg, "muscleToMuscleGlue")
+        if g is None:
+            return
+        sc = self.scene
+        vm = getattr(sc, "vert_muscle", None)
+        if vm is None:
+            vm = np.full(self.NV, -1, np.int64)
+            part = np.asarray(sc.tet_part)
+            keep = part >= 0
+            vm[self.tet_np[keep].reshape(-1)] = np.repeat(part[keep], 4)
+        dist = float(g.get("distance", -1.0))
+        radius = dist if dist > 0.0 else 0.01
+        mask = getattr(sc, "m2m_mask", None)
+        if mask is None:
+            region = str(g.get("region", "all"))
+            mask = (vm >= 0).astype(np.float32)
+            if region == "surface":
+                on = np.zeros(self.NV, np.float32)
+                on[np.unique(sc.surface_tris)] = 1.0
+                mask = mask * on
+            elif region == "interface":
+                from scipy.spatial import cKDTree
+                on = np.zeros(self.NV, np.float32)
+                for m in np.unique(vm[vm >= 0]):
+                    mine, other = np.nonzero(vm == m)[0], np.nonzero((vm >= 0) & (vm != m))[0]
+                    if other.size:
+                        d, _ = cKDTree(self.pos0_np[other]).query(self.pos0_np[mine])
+                        on[mine[d <= radius]] = 1.0
+                mask = on
+            elif region != "all":
+                raise ValueError(f"muscleToMuscleGlue 'region' must be 'all', 'surface' or 'interface', "
+                                 f"got {region!r}")
+        a, b, rest = build_m2m_pairs(self.pos0_np, vm, mask, float(g.get("mask_threshold", 0.5)), radius,
+                                     int(g.get("knn", 8)))
+        if a.size == 0:
+            return
+        stiff = max(float(g.get("stiffness", 1.0e4)) * float(g.get("stiffness_scale", 1.0)), 1.0e-30)
+        inv = self.layout.inv
+        dev = self.device
+        self.m2m_pairs_user = (a, b)
+        self._m2m_a = torch.from_numpy(inv[a].astype(np.int32)).to(dev)
+        self._m2m_b = torch.from_numpy(inv[b].astype(np.int32)).to(dev)
+        self._m2m_rest = torch.from_numpy(rest).to(dev)
+        self._m2m_comp = torch.full((a.size,), 1.0 / stiff, dtype=torch.float32, device=dev)
+        self.n_m2m = int(a.size)
+
+    def _solve_m2m_glue(self) -> None:
+        """_solve_m2m_glue (mg.py:662-670): one glue step with the config's omega."""
+        if not self.n_m2m:
+            return
+        capi.check(self._lib.xpbd_m2m_glue(self.n_m2m, C.c_void_p(self._m2m_a.data_ptr()),
+                                           C.c_void_p(self._m2m_b.data_ptr()), C.c_void_p(self._m2m_rest.data_ptr()),
+                                           C.c_void_p(self._m2m_comp.data_ptr()), C.c_void_p(self._pos4.data_ptr()),
+                                           C.c_float(self.dt), C.c_float(self.omega), self._sp))
+
+    def _m2m_iteration(self) -> None:
+        """One fine iteration in the reference's order with the glue between the
+        averaged correction and the re-pin (mg.py:1346-1355)."""
+        self.clear()
+        self.solve_constraints(run_extras=False)
+        self.apply_dP()
+        self._solve_m2m_glue()
+        self.apply_pintotarget()
+
     def _pose_bone_surface(self) -> None:
         capi.check(self._lib.xpbd_bone_surface_pose(int(self._bs_rest4.shape[0]), C.c_void_p(self._bs_rest4.data_ptr()),
                                                     C.c_void_p(self._bs_vbone.data_ptr()), self.scene.n_bones,
@@ -393,6 +468,7 @@ class MultiGridSim(MuscleSim):
                 s.clear()
                 s.solve_constraints(run_extras=False)
                 s.apply_dP()
+                s._solve_m2m_glue()
                 s.apply_pintotarget()
                 for fn in getattr(s, "collision_solvers_iter", None) or []:
                     fn(it)
@@ -452,6 +528,12 @@ class MultiGridSim(MuscleSim):
             else:
                 self._vstep(capi.OP_PREDICT | ((push | vel) if sub > 0 else 0))
                 self.mg.vcycle(pin_fine=bool(pin))
+            if self.n_m2m:
+                for it in range(self.fine_iters):
+                    self._m2m_iteration()
+                    for fn in self.collision_solvers_iter:
+                        fn(it)
+                continue
             if not self.collision_solvers_iter:
                 self._fused_iterations(self.fine_iters)
                 continue
