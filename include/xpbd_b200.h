@@ -276,6 +276,21 @@ int xpbd_bone_slide_targets(int32_t n, const float* muscle4, const int32_t* anch
 int xpbd_bone_surface_pose(int32_t n_bverts, const float* rest4, const int32_t* vert_bone, int32_t n_bones,
                            const float* transforms, float* out4, xpbd_stream_t stream);
 
+/* Fascia ride coupling (Fascia ride mode, fascia/fascia.py:442-522).
+ * xpbd_surface_bind replaces fascia_bind_kernel (fascia.py:130-157): for each
+ * query4[i] (fascia rest position) the closest face of the muscle surface
+ * (surf4 [n_sverts][4], stris [n_stris][3]) within max_dist, its (u, v), the
+ * signed normal gap (query - closest point) . n and ok = 1 (face 0, zeros and
+ * ok = 0 when none); same barycentric convention, face normal and tie rule as
+ * xpbd_bone_bind.  xpbd_surface_ride replaces fascia_ride_kernel
+ * (fascia.py:160-176): fascia4[bound[i]].xyz <- position(face[i], uv[i]) on
+ * the current surface + n * gap[i] (.w kept). */
+int xpbd_surface_bind(int32_t n, const float* query4, int32_t n_sverts, const float* surf4, int32_t n_stris,
+                      const int32_t* stris, float max_dist, int32_t* out_face, float* out_uv, float* out_gap,
+                      int32_t* out_ok, xpbd_stream_t stream);
+int xpbd_surface_ride(int32_t n_bound, const int32_t* bound, const int32_t* face, const float* uv, const float* gap,
+                      const float* surf4, const int32_t* stris, float* fascia4, xpbd_stream_t stream);
+
 /* Muscle-to-muscle glue (solve_m2m_glue_kernel, mg/kernel.py:350-394; run by
  * MultiGridSim between apply_dP and apply_pintotarget, mg/mg.py:1346-1355):
  * one XPBD distance step per pair (pair_a[c], pair_b[c]) toward restlen[c]

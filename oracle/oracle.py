@@ -705,3 +705,30 @@ def m2m_glue(pair_a, pair_b, restlen, compliance, pos4, dt, omega=1.0):
                    _p(np.ascontiguousarray(restlen, np.float32)), _p(np.ascontiguousarray(compliance, np.float32)),
                    _p(out), C.c_float(dt), C.c_float(omega))
     return out
+
+
+def surface_bind(query, surf_verts, tris, max_dist):
+    """fascia_bind_kernel (fascia/fascia.py:130-157): (face, uv, gap, ok)."""
+    L = lib()
+    q4, s4 = _v4(query), _v4(surf_verts)
+    tris = np.ascontiguousarray(tris, np.int32)
+    n = q4.shape[0]
+    face, ok = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    uv, gap = np.zeros((n, 2), np.float32), np.zeros(n, np.float32)
+    L.orc_surface_bind.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_float, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_surface_bind(n, _p(q4), _p(s4), tris.shape[0], _p(tris), C.c_float(max_dist), _p(face), _p(uv), _p(gap),
+                       _p(ok))
+    return face, uv, gap, ok
+
+
+def surface_ride(bound, face, uv, gap, surf_verts, tris, fascia_pos):
+    """fascia_ride_kernel (fascia/fascia.py:160-176) on a copy of fascia_pos."""
+    L = lib()
+    f4 = _v4(fascia_pos).copy()
+    L.orc_surface_ride.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]
+    L.orc_surface_ride(len(bound), _p(np.ascontiguousarray(bound, np.int32)), _p(np.ascontiguousarray(face, np.int32)),
+                       _p(np.ascontiguousarray(uv, np.float32)), _p(np.ascontiguousarray(gap, np.float32)),
+                       _p(_v4(surf_verts)), _p(np.ascontiguousarray(tris, np.int32)), _p(f4))
+    return f4[:, :3]

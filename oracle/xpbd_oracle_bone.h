@@ -214,4 +214,42 @@ void orc_m2m_glue(int n, const int* pa, const int* pb, const float* restlen, con
     }
 }
 
+/* fascia_bind_kernel (fascia/fascia.py:130-157): face, uv, signed normal gap
+ * (q - cp) . n of the closest surface face within max_dist; ok 0 when none. */
+void orc_surface_bind(int n, const float* q4, const float* surf4, int nt, const int* tris, float max_dist, int* out_face,
+                      float* out_uv, float* out_gap, int* out_ok) {
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int i = 0; i < n; ++i) {
+        float u = 0.f, v = 0.f;
+        const int f = ob_query(q4 + 4 * i, surf4, nt, tris, max_dist, &u, &v);
+        if (f < 0) {
+            out_face[i] = 0;
+            out_uv[2 * i] = out_uv[2 * i + 1] = 0.f;
+            out_gap[i] = 0.f;
+            out_ok[i] = 0;
+            continue;
+        }
+        float cp[3], R[3][3], d[3];
+        ob_eval(surf4, tris, f, u, v, cp);
+        ob_basis(surf4, tris, f, R);
+        for (int k = 0; k < 3; ++k) d[k] = q4[4 * i + k] - cp[k];
+        out_face[i] = f;
+        out_uv[2 * i] = u;
+        out_uv[2 * i + 1] = v;
+        out_gap[i] = R[0][2] * d[0] + R[1][2] * d[1] + R[2][2] * d[2];
+        out_ok[i] = 1;
+    }
+}
+
+/* fascia_ride_kernel (fascia/fascia.py:160-176) */
+void orc_surface_ride(int n, const int* bound, const int* face, const float* uv, const float* gap, const float* surf4,
+                      const int* tris, float* fascia4) {
+    for (int i = 0; i < n; ++i) {
+        float cp[3], R[3][3];
+        ob_eval(surf4, tris, face[i], uv[2 * i], uv[2 * i + 1], cp);
+        ob_basis(surf4, tris, face[i], R);
+        for (int k = 0; k < 3; ++k) fascia4[4 * bound[i] + k] = cp[k] + R[k][2] * gap[i];
+    }
+}
+
 #endif

@@ -136,6 +136,8 @@ _SIGS = {
                                  C.c_int32, P, P, P, P], C.c_int),
     "xpbd_bone_surface_pose": ([C.c_int32, P, P, C.c_int32, P, P, P], C.c_int),
     "xpbd_m2m_glue": ([C.c_int32, P, P, P, P, P, C.c_float, C.c_float, P], C.c_int),
+    "xpbd_surface_bind": ([C.c_int32, P, C.c_int32, P, C.c_int32, P, C.c_float, P, P, P, P, P], C.c_int),
+    "xpbd_surface_ride": ([C.c_int32, P, P, P, P, P, P, P, P], C.c_int),
     "xpbd_acc_scale_for_extent": ([C.c_float], C.c_float),
     "xpbd_error_string": ([], C.c_char_p),
     "xpbd_vertex_step": ([C.POINTER(XpbdParams), C.POINTER(XpbdVerts), C.c_uint32, C.POINTER(XpbdSdf), P], C.c_int),

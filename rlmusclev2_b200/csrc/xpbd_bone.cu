@@ -1,8 +1,10 @@
 // Bone-surface binding of muscle vertices: the reference's target_mode="mesh"
 // kinematic driver (bone_bind_kernel / bone_slide_target_kernel,
 // mg/kernel.py:267-347, driven from mg/mg.py:1117-1174), the per-frame rigid
-// pose of capsule bone surfaces, and the muscle-to-muscle glue springs
-// (solve_m2m_glue_kernel, mg/kernel.py:350-394).
+// pose of capsule bone surfaces, the muscle-to-muscle glue springs
+// (solve_m2m_glue_kernel, mg/kernel.py:350-394), and the fascia shell's
+// ride coupling to the muscle surface (fascia_bind_kernel /
+// fascia_ride_kernel, fascia/fascia.py:130-176).
 //
 // The reference queries a Warp BVH mesh; here the closest-point query is a
 // brute force over the bone faces, staged through shared memory in chunks of
@@ -246,6 +248,54 @@ __global__ void k_m2m_glue(int n, const int* __restrict__ pa, const int* __restr
     atomicAdd(pf + 4 * b + 2, (-f * wb) * dir.z);
 }
 
+// fascia_bind_kernel (fascia/fascia.py:130-157): closest muscle-surface face
+// of each fascia rest vertex, its (u, v) and the signed normal gap
+// (rest - closest point) . n; ok = 0 when nothing lies within max_dist.
+__global__ void __launch_bounds__(kBoneThreads)
+    k_surface_bind(int n, const float4* __restrict__ q4, const float4* __restrict__ surf, int nt,
+                   const int* __restrict__ tris, float max_dist, int* __restrict__ out_face, float2* __restrict__ out_uv,
+                   float* __restrict__ out_gap, int* __restrict__ out_ok) {
+    __shared__ float3 s_tri[kFaceChunk][3];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < n;
+    const float3 p = active ? f3(q4[i]) : make_float3(0.f, 0.f, 0.f);
+    float u = 0.f, v = 0.f;
+    const int f = closest_face(p, active, surf, nt, tris, max_dist, u, v, s_tri);
+    if (!active) return;
+    if (f < 0) {
+        out_face[i] = 0;
+        out_uv[i] = make_float2(0.f, 0.f);
+        out_gap[i] = 0.f;
+        out_ok[i] = 0;
+        return;
+    }
+    float3 A, B, C;
+    face_corners(surf, tris, f, A, B, C);
+    const float3 cp = face_eval(A, B, C, u, v);
+    out_face[i] = f;
+    out_uv[i] = make_float2(u, v);
+    out_gap[i] = dot(p - cp, face_frame(A, B, C).n);
+    out_ok[i] = 1;
+}
+
+// fascia_ride_kernel (fascia/fascia.py:160-176): bound fascia vertex
+// bound[i] <- its barycentric point on the current muscle surface + n * gap.
+__global__ void k_surface_ride(int n, const int* __restrict__ bound, const int* __restrict__ face,
+                               const float2* __restrict__ uv, const float* __restrict__ gap,
+                               const float4* __restrict__ surf, const int* __restrict__ tris, float4* fascia4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 A, B, C;
+    face_corners(surf, tris, face[i], A, B, C);
+    const float2 w = uv[i];
+    const float3 cp = face_eval(A, B, C, w.x, w.y);
+    const float3 nn = face_frame(A, B, C).n;
+    const float g = gap[i];
+    const int k = bound[i];
+    const float4 o = fascia4[k];
+    fascia4[k] = make_float4(cp.x + nn.x * g, cp.y + nn.y * g, cp.z + nn.z * g, o.w);
+}
+
 bool a16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 bool a8(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0; }
 
@@ -304,6 +354,34 @@ int xpbd_bone_surface_pose(int32_t n_bverts, const float* rest4, const int32_t* 
     k_bone_surface_pose<<<(n_bverts + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
         n_bverts, reinterpret_cast<const float4*>(rest4), vert_bone, transforms, reinterpret_cast<float4*>(out4));
     return cuda_check("xpbd_bone_surface_pose");
+}
+
+int xpbd_surface_bind(int32_t n, const float* query4, int32_t n_sverts, const float* surf4, int32_t n_stris,
+                      const int32_t* stris, float max_dist, int32_t* out_face, float* out_uv, float* out_gap,
+                      int32_t* out_ok, xpbd_stream_t stream) {
+    if (n < 0 || n_sverts <= 0 || n_stris <= 0 || !surf4 || !stris ||
+        (n > 0 && (!query4 || !out_face || !out_uv || !out_gap || !out_ok)))
+        return fail(XPBD_ERR_ARG, "xpbd_surface_bind: bad arguments");
+    if (!a16(query4) || !a16(surf4) || !a8(out_uv))
+        return fail(XPBD_ERR_ALIGN, "xpbd_surface_bind: [n][4] arrays 16-byte, uv 8-byte aligned");
+    if (n == 0) return XPBD_OK;
+    k_surface_bind<<<(n + kBoneThreads - 1) / kBoneThreads, kBoneThreads, 0, (cudaStream_t)stream>>>(
+        n, reinterpret_cast<const float4*>(query4), reinterpret_cast<const float4*>(surf4), n_stris, stris, max_dist,
+        out_face, reinterpret_cast<float2*>(out_uv), out_gap, out_ok);
+    return cuda_check("xpbd_surface_bind");
+}
+
+int xpbd_surface_ride(int32_t n_bound, const int32_t* bound, const int32_t* face, const float* uv, const float* gap,
+                      const float* surf4, const int32_t* stris, float* fascia4, xpbd_stream_t stream) {
+    if (n_bound < 0 || (n_bound > 0 && (!bound || !face || !uv || !gap || !surf4 || !stris || !fascia4)))
+        return fail(XPBD_ERR_ARG, "xpbd_surface_ride: bad arguments");
+    if (!a16(surf4) || !a16(fascia4) || !a8(uv))
+        return fail(XPBD_ERR_ALIGN, "xpbd_surface_ride: [n][4] arrays 16-byte, uv 8-byte aligned");
+    if (n_bound == 0) return XPBD_OK;
+    k_surface_ride<<<(n_bound + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        n_bound, bound, face, reinterpret_cast<const float2*>(uv), gap, reinterpret_cast<const float4*>(surf4), stris,
+        reinterpret_cast<float4*>(fascia4));
+    return cuda_check("xpbd_surface_ride");
 }
 
 int xpbd_m2m_glue(int32_t n_pairs, const int32_t* pair_a, const int32_t* pair_b, const float* restlen,

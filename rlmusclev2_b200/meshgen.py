@@ -334,6 +334,24 @@ def capsule_surface(c, axis, half: float, r: float, n_around: int = 16, n_lat: i
     return verts, np.asarray(tris, np.int32)
 
 
+def fascia_shell(verts: np.ndarray, surface_tris: np.ndarray, gap: float = 0.001, thickness: float = 0.003):
+    """A separate tet shell over an outward-oriented surface (the stand-in for an
+    authored fascia asset of the ride mode): the surface vertices moved out by
+    ``gap`` along their area-weighted normals, then extruded by ``thickness``
+    as extrude_shell does (prisms of 3 tets, slivers dropped).  Shares no
+    vertex with the muscle.  Returns (verts, tets)."""
+    v = np.asarray(verts, np.float64)
+    t = np.asarray(surface_tris, np.int64).reshape(-1, 3)
+    fn = np.cross(v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 0]])
+    vn = np.zeros_like(v)
+    for k in range(3):
+        np.add.at(vn, t[:, k], fn)
+    vn /= np.maximum(np.linalg.norm(vn, axis=1, keepdims=True), 1e-30)
+    moved = (v + gap * vn).astype(np.float32)
+    shell, tets, _ = extrude_shell(moved, t, thickness)
+    return shell.astype(np.float32), np.asarray(orient_tets(shell, tets), np.int32)
+
+
 def capsule_sdf(x: np.ndarray, c: np.ndarray, axis: np.ndarray, half: float, r: float) -> np.ndarray:
     d = x - c
     t = np.clip(d @ axis, -half, half)
@@ -422,7 +440,7 @@ def humanv2_scene(seed: int = 0, n_muscles: int = 40, n_bones: int = 20, target_
     # fascia shell over the first muscles' surfaces, up to the tet budget
     face_part = vpart[surf[:, 0]]
     chosen, acc = [], 0
-    for i in range(n_muscles):
+    for i in range(n_muscles if fascia_tets > 0 else 0):  # fascia_tets <= 0: no shell
         nf = int((face_part == i).sum())
         if acc + 3 * nf > fascia_tets * 1.05 and chosen:
             continue
@@ -431,7 +449,10 @@ def humanv2_scene(seed: int = 0, n_muscles: int = 40, n_bones: int = 20, target_
         if acc >= fascia_tets * 0.95:
             break
     fsel = np.isin(face_part, chosen)
-    fverts, ftets, fsrc = extrude_shell(mverts, surf[fsel], fascia_thickness)
+    if fsel.any():
+        fverts, ftets, fsrc = extrude_shell(mverts, surf[fsel], fascia_thickness)
+    else:
+        fverts, ftets, fsrc = np.zeros((0, 3), np.float32), np.zeros((0, 4), np.int64), np.zeros(0, np.int64)
     nmv = mverts.shape[0]
     allv = np.concatenate([mverts, fverts]).astype(np.float32)
     ftets = orient_tets(allv, ftets + nmv)

@@ -211,6 +211,7 @@ class MultiGridSim(MuscleSim):
                            vert_group=getattr(sc, "vert_inst", None))
         self._setup_kinematics()
         self._setup_m2m_glue()
+        self._setup_fascia()
         self.collision_solvers_iter = []
         self.mg = None
         if self.use_multigrid:
@@ -359,6 +360,36 @@ class MultiGridSim(MuscleSim):
         self._m2m_comp = torch.full((a.size,), 1.0 / stiff, dtype=torch.float32, device=dev)
         self.n_m2m = int(a.size)
 
+    def _setup_fascia(self) -> None:
+        """The fascia shell sub-solver (mg.py:556-566), ride mode only: the shell
+        from ``fascia_path`` (a .geo read by geo.GeoFile) or, for the synthetic
+        scenes, a shell offset from the muscle surface (meshgen.fascia_shell)."""
+        self.fascia = None
+        if not bool(self.cfg.get("use_fascia", False)):
+            return
+        mode = str(self.cfg.get("fascia_mode", "squeeze"))
+        if mode != "ride":
+            raise NotImplementedError(f"fascia_mode={mode!r} is not on the sm_100a path (supported: 'ride')")
+        if (np.asarray(self.scene.tet_part) < 0).any():
+            raise ValueError("use_fascia needs a scene without merged fascia tets (fascia_tets=0)")
+        from .fascia import FasciaRide
+        from .meshgen import fascia_shell
+        path = self.cfg.get("fascia_path")
+        if path and Path(path).exists():
+            from .geo import GeoFile
+            g = GeoFile(path)
+            fv, ft = g.positions, np.asarray(g.tet_indices, np.int32)
+        else:
+            fv, ft = fascia_shell(self.pos0_np, self.scene.surface_tris,
+                                  float(self.cfg.get("fascia_gap", 0.001)), float(self.cfg.get("fascia_thickness", 0.003)))
+        snh = find_constraint(self.cfg, "fascia_snh") or {}
+        glue = find_constraint(self.cfg, "fascia_glue") or {}
+        self.fascia = FasciaRide(self, fv, ft, snh_mu=float(snh.get("mu", 1.0e3)), snh_lam=float(snh.get("lam", 1.0e8)),
+                                 snh_damp=float(snh.get("dampingratio", 0.0)),
+                                 total_mass=float(self.cfg.get("fascia_total_mass", self.total_mass)),
+                                 iterations=int(glue.get("iterations", self.fine_iters)),
+                                 bind_max_dist=float(self.cfg.get("fascia_bind_max_dist", 0.05)))
+
     def _solve_m2m_glue(self) -> None:
         """_solve_m2m_glue (mg.py:662-670): one glue step with the config's omega."""
         if not self.n_m2m:
@@ -474,6 +505,8 @@ class MultiGridSim(MuscleSim):
                     fn(it)
 
         def post_phase():
+            if s.fascia is not None:
+                s.fascia.substep()
             for fn in getattr(s, "collision_solvers", None) or []:
                 fn()
             s.update_velocities()
@@ -528,21 +561,29 @@ class MultiGridSim(MuscleSim):
             else:
                 self._vstep(capi.OP_PREDICT | ((push | vel) if sub > 0 else 0))
                 self.mg.vcycle(pin_fine=bool(pin))
-            if self.n_m2m:
-                for it in range(self.fine_iters):
-                    self._m2m_iteration()
-                    for fn in self.collision_solvers_iter:
-                        fn(it)
-                continue
-            if not self.collision_solvers_iter:
-                self._fused_iterations(self.fine_iters)
-                continue
-            for it in range(self.fine_iters):
-                self._fused_iteration()
-                for fn in self.collision_solvers_iter:
-                    fn(it)
+            self._substep_iterations()
+            if self.fascia is not None:  # post_phase (mg.py:1361-1364), before the push-out and velocity
+                self.fascia.substep()
         if push | vel:
             self._vstep(push | vel)
+
+    def _substep_iterations(self) -> None:
+        """The fine iterations of one substep in the fused frame: the persistent
+        pass when no hook runs between iterations, else one iteration at a time
+        (the primitive order when the muscle-to-muscle glue is on)."""
+        if self.n_m2m:
+            for it in range(self.fine_iters):
+                self._m2m_iteration()
+                for fn in self.collision_solvers_iter:
+                    fn(it)
+            return
+        if not self.collision_solvers_iter:
+            self._fused_iterations(self.fine_iters)
+            return
+        for it in range(self.fine_iters):
+            self._fused_iteration()
+            for fn in self.collision_solvers_iter:
+                fn(it)
 
     def step_frame(self, frame: int) -> None:
         """mg.py:1409-1418: kinematic step then nsubsteps substeps at that pose."""
