@@ -279,3 +279,35 @@ class GeoWriter:
 def read_cons_frame(cons_dir: str | Path, frame: int) -> np.ndarray:
     """``target_pos`` of ``cons_<frame>.geo`` (geo_io.py:336-338)."""
     return GeoFile(Path(cons_dir) / f"cons_{frame}.geo").target_pos
+
+
+def scene_from_geo(rest_path: str | Path):
+    """A Scene from a ``restpos.geo`` asset, as MultiGridSim reads one
+    (mg/mg.py:300-350): points and tets, the fiber field ``materialW`` (+x when absent), the
+    ``tendonmask`` (0 when absent), the muscle of each tet from the
+    ``muscle_id`` primitive attribute (0 when absent), the outward surface from
+    the tets.  The asset carries no capsule skeleton: the scene has no bones,
+    so the targets come from ``cons_<frame>.geo`` frames (target_mode="points")."""
+    from .meshgen import Scene, boundary_faces, orient_faces_outward, orient_tets
+    g = GeoFile(rest_path)
+    verts = g.positions.astype(np.float32)
+    nv = verts.shape[0]
+    # every tet positive with the pt3 reference vertex (the reference loader's
+    # fix_tet_winding makes them all negative that way; the constraints see the
+    # same shapes either way, and the synthetic scenes use this orientation)
+    tets = orient_tets(verts, np.asarray(g.tet_indices, np.int64)).astype(np.int32)
+    fib = (g.point_attr("materialW").astype(np.float32).reshape(nv, 3) if g.has_point_attr("materialW")
+           else np.tile(np.array([1.0, 0.0, 0.0], np.float32), (nv, 1)))
+    tendon = (g.point_attr("tendonmask").astype(np.float32).reshape(nv) if g.has_point_attr("tendonmask")
+              else np.zeros(nv, np.float32))
+    tpart = (g.prim_attr("muscle_id").astype(np.int32).reshape(-1) if g.has_prim_attr("muscle_id")
+             else np.zeros(tets.shape[0], np.int32))
+    vpart = np.zeros(nv, np.int32)
+    vpart[tets.reshape(-1)] = np.repeat(tpart, 4)
+    faces, opp = boundary_faces(tets)
+    surf = orient_faces_outward(verts, faces, opp).astype(np.int32)
+    z3, z1 = np.zeros((0, 3), np.float32), np.zeros(0, np.float32)
+    return Scene(verts=verts, tets=tets, tet_part=tpart, vert_part=vpart, v_tendon=tendon, v_fiber=fib,
+                 surface_tris=surf, bone_center=z3, bone_axis=z3, bone_half=z1, bone_radius=z1,
+                 vert_bone=np.zeros((nv, 2), np.int32), vert_bw=np.zeros(nv, np.float32), traj={}, aniso_muscle=-1,
+                 meta=dict(source=str(rest_path)))

@@ -109,9 +109,14 @@ class MultiGridSim(MuscleSim):
         if self.use_fiber and self.fiber_model != "aniso_arap":
             raise NotImplementedError(f"fiber_model={self.fiber_model!r} is not on the sm_100a path "
                                       "(supported: 'aniso_arap')")
-        if cfg.get("rest_path") and Path(cfg["rest_path"]).exists() and scene is None and "synthetic" not in cfg:
-            raise NotImplementedError("loading .geo/.usd rest meshes is not part of this project; "
-                                      "provide cfg['synthetic'] or a Scene")
+        if scene is None and "synthetic" not in cfg and cfg.get("rest_path"):
+            rp = Path(cfg["rest_path"])
+            if rp.suffix.lower() != ".geo":
+                raise NotImplementedError(f"rest mesh {rp.name}: only Houdini .geo assets are read (no USD)")
+            if not rp.exists():
+                raise FileNotFoundError(f"rest_path {rp} does not exist")
+            from .geo import scene_from_geo
+            scene = scene_from_geo(rp)
         self.scene = scene if scene is not None else scene_from_cfg(cfg)
         sc = self.scene
         # kinematic targets (mg.py:436-446)
@@ -119,9 +124,12 @@ class MultiGridSim(MuscleSim):
         self.use_sliding = bool(cfg.get("use_sliding", False))
         self.slide_range = float(cfg.get("slide_range", 0.005))
         self.slide_interval = int(cfg.get("slide_interval", 1))
-        if self.target_mode not in ("mesh", "lbs"):
+        if self.target_mode not in ("mesh", "lbs", "points"):
             raise NotImplementedError(f"target_mode={self.target_mode!r} is not on the sm_100a path "
-                                      "(supported: 'mesh', 'lbs')")
+                                      "(supported: 'mesh', 'lbs', 'points')")
+        self.cons_dir = cfg.get("cons_dir")
+        if self.target_mode == "points" and not self.cons_dir:
+            raise ValueError("target_mode='points' reads cons_<frame>.geo frames: set cons_dir")
         if self.use_sliding and self.target_mode != "mesh":
             raise ValueError("use_sliding=true requires target_mode='mesh' (mg.py:438-440)")
         self.pos0_np = sc.verts.astype(np.float32)
@@ -186,16 +194,30 @@ class MultiGridSim(MuscleSim):
                 active[:] = 0  # the synthetic rest carries no authored pinmask
             else:
                 raise ValueError(f"muscleToBonePin 'region' must be 'full', 'tendonmask' or 'pinmask', got {region!r}")
+        if self.target_mode == "points":
+            # pin-to-target topology from the start frame's cons file (mg.py:448-458):
+            # only its points are pinned or attached, offset by rest - target_pos
+            from .geo import GeoFile
+            cons0 = GeoFile(Path(self.cons_dir) / f"cons_{self.start_frame}.geo")
+            self._cons_pts = cons0.pts.astype(np.int64)
+            self._cons_cache = {}
+            in_cons = np.zeros(self.NV, bool)
+            in_cons[self._cons_pts] = True
+            active = (active.astype(bool) & in_cons).astype(np.int32)
         self.pin_active_np = active
         _belly = find_constraint(cfg, "belly_attach")
         self._belly_enabled = _belly is not None
         self.pin_attach_stiffness = float(_belly["stiffness"]) if _belly else 0.0
         self.pin_attach_damp = float(_belly.get("dampingratio", 0.0)) if _belly else 0.0
         self.rest_offset_np = np.zeros((self.NV, 3), np.float32)
+        if self.target_mode == "points":
+            self.rest_offset_np[self._cons_pts] = (self.pos0_np[self._cons_pts] - cons0.target_pos).astype(np.float32)
         target0 = self._host_targets(self.start_frame)
         parts = [table]
         if self._belly_enabled:
             belly = np.nonzero(active == 0)[0]
+            if self.target_mode == "points":
+                belly = belly[in_cons[belly]]
             parts.append(create_attach_constraints(belly, target0[belly] + self.rest_offset_np[belly], 0.0,
                                                    self.pin_attach_stiffness, self.pin_attach_damp))
         table = ConstraintTable.concat(parts).sorted_by_type()
@@ -221,6 +243,8 @@ class MultiGridSim(MuscleSim):
             self.mg = DeviceMultigrid(self, spacing=float(cfg.get("mg_cage_spacing", 0.016)))
         self.collision_solvers = []
         coll = (cfg.get("demo") or {}).get("collision") or {}
+        if coll.get("enabled", False) and sc.n_bones == 0:
+            raise ValueError("demo.collision needs capsule bones; this scene has none (disable it)")
         if coll.get("enabled", False):
             self.bone_collider = GridSdfCollider(
                 self, sc.bone_center, sc.bone_axis, sc.bone_half, sc.bone_radius, res=int(coll.get("sdf_res", 256)),
@@ -242,7 +266,21 @@ class MultiGridSim(MuscleSim):
         self._frame_loaded = None
 
     # ----------------------------------------------------------- kinematics
+    def _cons_targets(self, frame: int) -> np.ndarray:
+        """Targets of ``frame`` in user order: the cons file's target_pos on its
+        points, the rest position elsewhere (load_frame_targets, mg.py:1238-1250;
+        frames are read once and kept).  The pins and attachments add the rest
+        offset."""
+        if frame not in self._cons_cache:
+            from .geo import read_cons_frame
+            self._cons_cache[frame] = read_cons_frame(self.cons_dir, int(frame)).astype(np.float32)
+        tgt = self.pos0_np.copy()
+        tgt[self._cons_pts] = self._cons_cache[frame]
+        return tgt
+
     def _host_targets(self, frame: float) -> np.ndarray:
+        if self.target_mode == "points":
+            return self._cons_targets(int(frame))
         if self.target_mode == "mesh":
             if frame != self.start_frame:
                 raise ValueError("host targets of the surface binding exist for the start frame only")
@@ -268,6 +306,9 @@ class MultiGridSim(MuscleSim):
         self._pos_host = torch.zeros((self.NV, 3), dtype=torch.float32).pin_memory()
         self._h2d_event = torch.cuda.Event()
         self._h2d_event.record(self._stream)
+        if self.target_mode == "points":
+            self._pts_tgt = torch.zeros((self.NV, 3), dtype=torch.float32, device=dev)
+            self._pts_host = torch.zeros((self.NV, 3), dtype=torch.float32).pin_memory()
         if self.target_mode == "mesh":
             self._setup_surface_binding()
 
@@ -416,7 +457,18 @@ class MultiGridSim(MuscleSim):
 
     def load_frame_targets(self, frame: float) -> None:
         """Bone poses of ``frame`` -> device (one pinned H2D copy), then the
-        per-vertex pin/attach targets on the device (mg.py:1386-1407)."""
+        per-vertex pin/attach targets on the device (mg.py:1386-1407); with
+        target_mode="points" the frame's cons targets instead."""
+        if self.target_mode == "points":
+            tgt = (self._cons_targets(int(frame)) + self.rest_offset_np)[self.layout.perm]
+            self._h2d_event.synchronize()
+            self._pts_host.numpy()[:] = tgt
+            with torch.cuda.stream(self._stream):
+                self._pts_tgt.copy_(self._pts_host, non_blocking=True)
+            self._h2d_event.record(self._stream)
+            self._frame_loaded = frame
+            self._reproject = False
+            return
         T = self.scene.bone_transforms(frame).reshape(self.scene.n_bones, 12).astype(np.float32)
         self._h2d_event.synchronize()  # the previous copy has consumed the pinned buffer
         self._bone_tr_host.numpy()[:] = T
@@ -430,6 +482,12 @@ class MultiGridSim(MuscleSim):
 
     def _targets_kernel(self) -> None:
         v = self._verts
+        if self.target_mode == "points":
+            with torch.cuda.stream(self._stream):
+                for t in (self._pin_tgt, self._attach_tgt):
+                    if t is not None:
+                        t[:, :3].copy_(self._pts_tgt)
+            return
         if self.target_mode == "mesh":
             self._pose_bone_surface()
             capi.check(self._lib.xpbd_bone_slide_targets(

@@ -66,3 +66,16 @@ def test_run_length_groups_and_cons_frames(tmp_path):
     np.testing.assert_array_equal(read_cons_frame(tmp_path, 5), pos)
     assert GeoFile(tmp_path / "cons_5.geo").point_group("g").tolist() == [0, 1, 5, 11]
     assert GeoFile(tmp_path / "cons_5.geo").tet_indices.shape == (0, 0)
+
+
+def test_scene_from_geo_asset():
+    from rlmusclev2_b200.geo import scene_from_geo
+    sc = scene_from_geo(G / "geo_small.geo")
+    g = GeoFile(G / "geo_small.geo")
+    assert sc.verts.shape == g.positions.shape and sc.tets.shape == g.tet_indices.shape
+    q = sc.verts[sc.tets].astype(np.float64)
+    assert (np.linalg.det(np.stack([q[:, 0] - q[:, 3], q[:, 1] - q[:, 3], q[:, 2] - q[:, 3]], 1)) > 0).all()
+    np.testing.assert_array_equal(np.sort(sc.tets, 1), np.sort(g.tet_indices, 1))
+    np.testing.assert_array_equal(sc.tet_part, g.prim_attr("muscle_id"))
+    np.testing.assert_array_equal(sc.v_tendon, g.point_attr("tendonmask").astype(np.float32))
+    assert sc.n_bones == 0 and sc.surface_tris.shape[1] == 3 and sc.surface_tris.shape[0] > 0

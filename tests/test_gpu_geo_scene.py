@@ -1,0 +1,63 @@
+"""A rest mesh read from a .geo asset with pin-to-target frames from
+cons_<frame>.geo (the reference's default target_mode="points",
+mg/mg.py:300-350, 448-458, 1238-1250).  The asset is the synthetic scene
+written out (positions, tets, tendonmask, materialW, muscle_id), and its cons
+frames carry, bit for bit, the targets the synthetic run with
+target_mode="lbs" computes on the device for every vertex; the two runs must
+then agree (to the order of the float atomics of the boundary sums)."""
+import numpy as np
+import pytest
+
+from rlmusclev2_b200.geo import write_geo
+from rlmusclev2_b200.meshgen import humanv2_scene
+from rlmusclev2_b200.mg import MultiGridSim, load_config
+
+pytestmark = pytest.mark.gpu
+
+
+def test_geo_asset_with_cons_frames_matches_the_synthetic_run(tmp_path):
+    sc = humanv2_scene(seed=1, n_muscles=5, n_bones=4, target_tets=20000, fascia_tets=0, box=(0.35, 0.35, 0.35))
+    write_geo(tmp_path / "restpos.geo", sc.verts, sc.tets,
+              point_attrs={"tendonmask": sc.v_tendon, "materialW": sc.v_fiber},
+              prim_string_attrs={"muscle_id": ([f"m{i}" for i in range(5)], sc.tet_part)})
+    base = load_config("rlmusclev2_b200/configs/humanv2_synth.json")
+    base["demo"]["collision"]["enabled"] = False
+    for c in base["constraints"]:
+        if c.get("name") == "fiber":
+            c["region"] = "all"
+    ref_cfg = dict(base, target_mode="lbs")
+    ref = MultiGridSim(ref_cfg, scene=sc)
+    # cons frames carry the synthetic run's own device targets, bit for bit
+    cons = tmp_path / "cons"
+    cons.mkdir()
+    pts = np.arange(sc.verts.shape[0], dtype=np.int32)
+    tg = {}
+    for f in range(1, 5):
+        ref.load_frame_targets(f)
+        ref._targets_kernel()
+        ref.synchronize()
+        t = np.empty((ref.NV, 3), np.float32)
+        t[ref.layout.perm] = ref._pin_tgt[:, :3].cpu().numpy()
+        tg[f] = t
+        write_geo(cons / f"cons_{f}.geo", t, None, point_attrs={"pts": pts, "target_pos": t})
+    geo_cfg = {k: v for k, v in base.items() if k != "synthetic"}
+    geo_cfg.update(rest_path=str(tmp_path / "restpos.geo"), cons_dir=str(cons), target_mode="points")
+    sim = MultiGridSim(geo_cfg)
+    assert sim.NV == ref.NV and sim.NT == ref.NT and sim.scene.n_bones == 0
+    assert np.array_equal(sim.pin_active_np, ref.pin_active_np)
+    sim.load_frame_targets(3)
+    sim._targets_kernel()
+    sim.synchronize()
+    got = np.empty((sim.NV, 3), np.float32)
+    got[sim.layout.perm] = sim._pin_tgt[:, :3].cpu().numpy()
+    np.testing.assert_array_equal(got, tg[3])
+    for f in range(1, 5):
+        a = sc.activation(f)
+        for s in (ref, sim):
+            s.set_fiber_activation(a)
+            s.step_frame(f)
+    pr, pg = ref.positions_np(), sim.positions_np()
+    err = np.abs(pr - pg).max()
+    print(f"geo asset run vs synthetic run: max |diff| {err:.2e} m")
+    assert np.isfinite(pg).all()
+    assert err < 1e-6
