@@ -191,15 +191,21 @@ def _rle(indices: np.ndarray, n: int) -> list:
 def write_geo(path: str | Path, positions: np.ndarray, tets: np.ndarray | None = None,
               point_attrs: dict | None = None, prim_attrs: dict | None = None,
               prim_string_attrs: dict | None = None, groups: dict | None = None,
-              unordered_groups: dict | None = None) -> None:
+              unordered_groups: dict | None = None, tris: np.ndarray | None = None) -> None:
     """Write a ``.geo`` pair list that GeoFile (and the reference's reader)
     parses: ``P`` as fpreal32 tuples, tets as one ``Tetrahedron_run``,
     ``point_attrs`` (name -> (N,) or (N,k)), numeric ``prim_attrs``,
     ``prim_string_attrs`` (name -> (strings, per-tet index)), point groups as
-    ordered lists (``groups``) or boolean run-length codes (``unordered_groups``)."""
+    ordered lists (``groups``) or boolean run-length codes (``unordered_groups``).
+    ``tris`` instead of ``tets`` writes a triangle surface (one polygon run, the
+    layout of the reference's bone_<frame>.geo files)."""
     pos = np.asarray(positions, np.float32)
     n = int(pos.shape[0])
-    t = np.zeros((0, 4), np.int64) if tets is None else np.asarray(tets, np.int64)
+    if tris is not None and tets is not None:
+        raise ValueError("write_geo: tets or tris, not both")
+    t = (np.asarray(tris, np.int64).reshape(-1, 3) if tris is not None else
+         np.zeros((0, 4), np.int64) if tets is None else np.asarray(tets, np.int64))
+    run = "Polygon_run" if tris is not None else "Tetrahedron_run"
     pattrs = [_point_attr("P", pos)] + [_point_attr(k, v) for k, v in (point_attrs or {}).items()]
     prattrs = []
     for k, v in (prim_attrs or {}).items():
@@ -214,7 +220,7 @@ def write_geo(path: str | Path, positions: np.ndarray, tets: np.ndarray | None =
     root = ["fileversion", "19.5", "pointcount", n, "vertexcount", int(t.size), "primitivecount", int(t.shape[0]),
             "topology", ["pointref", ["indices", [int(x) for x in t.reshape(-1)]]],
             "attributes", ["pointattributes", pattrs, "primitiveattributes", prattrs],
-            "primitives", [[["type", "Tetrahedron_run"], ["startvertex", 0, "nprimitives", int(t.shape[0])]]]
+            "primitives", [[["type", run], ["startvertex", 0, "nprimitives", int(t.shape[0])]]]
             if t.shape[0] else [],
             "pointgroups", pgroups]
     with open(path, "w") as fp:
@@ -274,6 +280,13 @@ class GeoWriter:
             self._scalar("pen_depth", pen_depth, False)
         with open(out_path, "w") as fp:
             json.dump(self._root, fp)
+
+
+def read_geo_attr(path: str | Path, attr: str) -> np.ndarray:
+    """One attribute of a .geo: "P" (float32 positions) or "target_pos"
+    (read_geo_attr_cached, geo_io.py:312-333, without the on-disk cache)."""
+    g = GeoFile(path)
+    return g.positions if attr == "P" else getattr(g, attr)
 
 
 def read_cons_frame(cons_dir: str | Path, frame: int) -> np.ndarray:

@@ -317,10 +317,25 @@ class MultiGridSim(MuscleSim):
         at the start frame, every vertex's rest position bound to its closest
         surface point (face, barycentric, offset in the face frame); the current
         binding starts at that anchor."""
-        if not hasattr(self.scene, "bone_surface"):
-            raise NotImplementedError("target_mode='mesh' needs a scene with bone surfaces")
         dev = self.device
-        bv, bt, bvb = self.scene.bone_surface()
+        self._bone_dir = self.cfg.get("bone_dir")
+        if self._bone_dir and not Path(self._bone_dir).is_dir():
+            self._bone_dir = None
+        if self._bone_dir:
+            # GeoBoneSource (util/bone_source.py:84-116): triangles of bone_<start>.geo,
+            # positions of bone_<frame>.geo uploaded every frame
+            from .geo import GeoFile
+            g0 = GeoFile(Path(self._bone_dir) / f"bone_{self.start_frame}.geo")
+            bv = g0.positions
+            bt = np.asarray(g0.tet_indices, np.int32).reshape(-1, 3)
+            bvb = np.zeros(bv.shape[0], np.int32)
+            self._bone_frames = {}
+            self._bs_host = torch.zeros((bv.shape[0], 4), dtype=torch.float32).pin_memory()
+        elif hasattr(self.scene, "bone_surface") and self.scene.n_bones > 0:
+            bv, bt, bvb = self.scene.bone_surface()
+        else:
+            raise NotImplementedError("target_mode='mesh' needs bone surfaces: a bone_dir of bone_<frame>.geo "
+                                      "files or a scene with capsule bones")
         r4 = np.zeros((bv.shape[0], 4), np.float32)
         r4[:, :3] = bv
         self._bs_rest4 = torch.from_numpy(r4).to(dev)
@@ -449,7 +464,20 @@ class MultiGridSim(MuscleSim):
         self._solve_m2m_glue()
         self.apply_pintotarget()
 
+    def _upload_bone_frame(self, frame: int) -> None:
+        """bone_<frame>.geo positions into the bone-surface buffer (one pinned H2D copy)."""
+        from .geo import read_geo_attr
+        if frame not in self._bone_frames:
+            self._bone_frames[frame] = read_geo_attr(Path(self._bone_dir) / f"bone_{int(frame)}.geo", "P")
+        self._h2d_event.synchronize()
+        self._bs_host.numpy()[:, :3] = self._bone_frames[frame]
+        with torch.cuda.stream(self._stream):
+            self._bs_pos4.copy_(self._bs_host, non_blocking=True)
+        self._h2d_event.record(self._stream)
+
     def _pose_bone_surface(self) -> None:
+        if self._bone_dir:
+            return  # the frame's bone positions were uploaded by load_frame_targets
         capi.check(self._lib.xpbd_bone_surface_pose(int(self._bs_rest4.shape[0]), C.c_void_p(self._bs_rest4.data_ptr()),
                                                     C.c_void_p(self._bs_vbone.data_ptr()), self.scene.n_bones,
                                                     C.c_void_p(self._bone_tr.data_ptr()),
@@ -469,12 +497,15 @@ class MultiGridSim(MuscleSim):
             self._frame_loaded = frame
             self._reproject = False
             return
-        T = self.scene.bone_transforms(frame).reshape(self.scene.n_bones, 12).astype(np.float32)
-        self._h2d_event.synchronize()  # the previous copy has consumed the pinned buffer
-        self._bone_tr_host.numpy()[:] = T
-        with torch.cuda.stream(self._stream):
-            self._bone_tr.copy_(self._bone_tr_host, non_blocking=True)
-        self._h2d_event.record(self._stream)
+        if self.target_mode == "mesh" and getattr(self, "_bone_dir", None):
+            self._upload_bone_frame(int(frame))
+        else:
+            T = self.scene.bone_transforms(frame).reshape(self.scene.n_bones, 12).astype(np.float32)
+            self._h2d_event.synchronize()  # the previous copy has consumed the pinned buffer
+            self._bone_tr_host.numpy()[:] = T
+            with torch.cuda.stream(self._stream):
+                self._bone_tr.copy_(self._bone_tr_host, non_blocking=True)
+            self._h2d_event.record(self._stream)
         self._frame_loaded = frame
         # _update_slide_target (mg.py:1160-1174): re-project every slide_interval frames
         self._reproject = bool(self.use_sliding and

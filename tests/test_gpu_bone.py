@@ -167,3 +167,33 @@ def test_multigrid_mesh_sliding_steps():
         sim.step_frame(frame)
     assert np.isfinite(sim.positions_np()).all()
     assert np.isfinite(sim._pin_tgt.cpu().numpy()).all()
+
+
+def test_multigrid_mesh_from_bone_dir_matches_capsule_pose(tmp_path):
+    """target_mode="mesh" with a bone_dir of bone_<frame>.geo files (the
+    reference's GeoBoneSource): files holding, bit for bit, the capsule
+    surfaces the device posed give the same run as the device pose."""
+    from rlmusclev2_b200.geo import write_geo
+    sim, sc = _mesh_sim()
+    bdir = tmp_path / "bone"
+    bdir.mkdir()
+    tris = sim._bs_tris.cpu().numpy()
+    for f in range(1, 5):
+        sim.load_frame_targets(f)
+        sim._pose_bone_surface()
+        sim.synchronize()
+        write_geo(bdir / f"bone_{f}.geo", sim._bs_pos4[:, :3].cpu().numpy(), tris=tris)
+    sim2, _ = _mesh_sim()
+    cfg2 = dict(sim2.cfg, bone_dir=str(bdir))
+    from rlmusclev2_b200.mg import MultiGridSim
+    sim2 = MultiGridSim(cfg2, scene=sc)
+    sim, _ = _mesh_sim()
+    assert sim2._bone_dir
+    for frame in range(1, 5):
+        a = sc.activation(frame)
+        for s in (sim, sim2):
+            s.set_fiber_activation(a)
+            s.step_frame(frame)
+    err = np.abs(sim.positions_np() - sim2.positions_np()).max()
+    print(f"bone_dir run vs capsule-pose run: max |diff| {err:.2e} m")
+    assert err < 1e-6
