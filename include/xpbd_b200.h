@@ -291,6 +291,24 @@ int xpbd_surface_bind(int32_t n, const float* query4, int32_t n_sverts, const fl
 int xpbd_surface_ride(int32_t n_bound, const int32_t* bound, const int32_t* face, const float* uv, const float* gap,
                       const float* surf4, const int32_t* stris, float* fascia4, xpbd_stream_t stream);
 
+/* Fascia squeeze mode (fascia/fascia.py:45-125, 524-566).  target4 is the
+ * muscle's per-vertex bone target (the pin target: target + rest offset), in
+ * the muscle library order.  xpbd_fascia_advect (fascia_advect_bone_kernel):
+ * fascia4[i] += target4[follow[i]] - prev_world4[i], then prev_world4[i] =
+ * target4[follow[i]] (once per frame).  xpbd_fascia_anchor
+ * (fascia_anchor_bone_kernel): fascia4[local[i]].xyz = target4[cons[i]] +
+ * offset4[i].  xpbd_fascia_glue (solve_glue_kernel): one-way XPBD distance
+ * step per pair holding restlen[c], compliance[c] / dt^2, zero starting
+ * multiplier, scaled by omega: only the muscle vertex moves (atomics), by its
+ * inverse mass muscle4.w. */
+int xpbd_fascia_advect(int32_t n, const int32_t* follow, const float* target4, float* prev_world4, float* fascia4,
+                       xpbd_stream_t stream);
+int xpbd_fascia_anchor(int32_t n, const int32_t* local, const int32_t* cons, const float* offset4,
+                       const float* target4, float* fascia4, xpbd_stream_t stream);
+int xpbd_fascia_glue(int32_t n, const int32_t* pair_fascia, const int32_t* pair_muscle, const float* restlen,
+                     const float* compliance, const float* fascia4, float* muscle4, float dt, float omega,
+                     xpbd_stream_t stream);
+
 /* Muscle-to-muscle glue (solve_m2m_glue_kernel, mg/kernel.py:350-394; run by
  * MultiGridSim between apply_dP and apply_pintotarget, mg/mg.py:1346-1355):
  * one XPBD distance step per pair (pair_a[c], pair_b[c]) toward restlen[c]

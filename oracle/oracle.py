@@ -732,3 +732,36 @@ def surface_ride(bound, face, uv, gap, surf_verts, tris, fascia_pos):
                        _p(np.ascontiguousarray(uv, np.float32)), _p(np.ascontiguousarray(gap, np.float32)),
                        _p(_v4(surf_verts)), _p(np.ascontiguousarray(tris, np.int32)), _p(f4))
     return f4[:, :3]
+
+
+def fascia_advect(follow, target4, prev4, fascia4):
+    """fascia_advect_bone_kernel (fascia/fascia.py:45-62): (fascia4, prev4) updated copies."""
+    L = lib()
+    f4, p4 = np.array(fascia4, np.float32), np.array(prev4, np.float32)
+    L.orc_fascia_advect.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_fascia_advect(len(follow), _p(np.ascontiguousarray(follow, np.int32)),
+                        _p(np.ascontiguousarray(target4, np.float32)), _p(p4), _p(f4))
+    return f4, p4
+
+
+def fascia_anchor(local, cons, offset4, target4, fascia4):
+    """fascia_anchor_bone_kernel (fascia/fascia.py:65-80) on a copy."""
+    L = lib()
+    f4 = np.array(fascia4, np.float32)
+    L.orc_fascia_anchor.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_fascia_anchor(len(local), _p(np.ascontiguousarray(local, np.int32)), _p(np.ascontiguousarray(cons, np.int32)),
+                        _p(np.ascontiguousarray(offset4, np.float32)), _p(np.ascontiguousarray(target4, np.float32)),
+                        _p(f4))
+    return f4
+
+
+def fascia_glue(pf, pm, restlen, compliance, fascia4, muscle4, dt, omega=1.0):
+    """solve_glue_kernel (fascia/fascia.py:83-125), sequential, on a copy of muscle4."""
+    L = lib()
+    m4 = np.array(muscle4, np.float32)
+    L.orc_fascia_glue.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_float, C.c_float]
+    L.orc_fascia_glue(len(pf), _p(np.ascontiguousarray(pf, np.int32)), _p(np.ascontiguousarray(pm, np.int32)),
+                      _p(np.ascontiguousarray(restlen, np.float32)), _p(np.ascontiguousarray(compliance, np.float32)),
+                      _p(np.ascontiguousarray(fascia4, np.float32)), _p(m4), C.c_float(dt), C.c_float(omega))
+    return m4

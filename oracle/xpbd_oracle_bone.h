@@ -252,4 +252,42 @@ void orc_surface_ride(int n, const int* bound, const int* face, const float* uv,
     }
 }
 
+/* fascia_advect_bone_kernel (fascia/fascia.py:45-62) */
+void orc_fascia_advect(int n, const int* follow, const float* target4, float* prev4, float* fascia4) {
+    for (int i = 0; i < n; ++i) {
+        const float* cur = target4 + 4 * follow[i];
+        for (int k = 0; k < 3; ++k) {
+            fascia4[4 * i + k] = fascia4[4 * i + k] + (cur[k] - prev4[4 * i + k]);
+            prev4[4 * i + k] = cur[k];
+        }
+    }
+}
+
+/* fascia_anchor_bone_kernel (fascia/fascia.py:65-80) */
+void orc_fascia_anchor(int n, const int* local, const int* cons, const float* offset4, const float* target4,
+                       float* fascia4) {
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) fascia4[4 * local[i] + k] = target4[4 * cons[i] + k] + offset4[4 * i + k];
+}
+
+/* solve_glue_kernel (fascia/fascia.py:83-125), pairs in index order */
+void orc_fascia_glue(int n, const int* pf, const int* pm, const float* restlen, const float* compliance,
+                     const float* fascia4, float* muscle4, float dt, float omega) {
+    for (int c = 0; c < n; ++c) {
+        const float* xf = fascia4 + 4 * pf[c];
+        float* xm = muscle4 + 4 * pm[c];
+        const float d[3] = {xf[0] - xm[0], xf[1] - xm[1], xf[2] - xm[2]};
+        const float len = sqrtf(ob_dot(d, d));
+        if (len < 1.0e-9f) continue;
+        const float dir[3] = {d[0] / len, d[1] / len, d[2] / len};
+        const float C = len - restlen[c];
+        const float wj = xm[3];
+        const float at = compliance[c] / (dt * dt);
+        const float den = wj + at;
+        if (den < 1.0e-12f) continue;
+        const float f = omega * (-C / den);
+        for (int k = 0; k < 3; ++k) xm[k] += (-f * wj) * dir[k];
+    }
+}
+
 #endif

@@ -138,6 +138,9 @@ _SIGS = {
     "xpbd_m2m_glue": ([C.c_int32, P, P, P, P, P, C.c_float, C.c_float, P], C.c_int),
     "xpbd_surface_bind": ([C.c_int32, P, C.c_int32, P, C.c_int32, P, C.c_float, P, P, P, P, P], C.c_int),
     "xpbd_surface_ride": ([C.c_int32, P, P, P, P, P, P, P, P], C.c_int),
+    "xpbd_fascia_advect": ([C.c_int32, P, P, P, P, P], C.c_int),
+    "xpbd_fascia_anchor": ([C.c_int32, P, P, P, P, P, P], C.c_int),
+    "xpbd_fascia_glue": ([C.c_int32, P, P, P, P, P, P, C.c_float, C.c_float, P], C.c_int),
     "xpbd_acc_scale_for_extent": ([C.c_float], C.c_float),
     "xpbd_error_string": ([], C.c_char_p),
     "xpbd_vertex_step": ([C.POINTER(XpbdParams), C.POINTER(XpbdVerts), C.c_uint32, C.POINTER(XpbdSdf), P], C.c_int),

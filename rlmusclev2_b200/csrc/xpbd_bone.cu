@@ -296,6 +296,64 @@ __global__ void k_surface_ride(int n, const int* __restrict__ bound, const int* 
     fascia4[k] = make_float4(cp.x + nn.x * g, cp.y + nn.y * g, cp.z + nn.z * g, o.w);
 }
 
+// Fascia squeeze mode (fascia/fascia.py:45-125).  The bone-driven target of
+// a muscle vertex is target4[v].xyz (the pin target, target + rest offset).
+// fascia_advect_bone_kernel: every shell vertex moves by the frame's change of
+// the target of its nearest muscle vertex follow[i].
+__global__ void k_fascia_advect(int n, const int* __restrict__ follow, const float4* __restrict__ target4,
+                                float4* __restrict__ prev_world, float4* __restrict__ fascia4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 cur = target4[follow[i]];
+    const float4 pw = prev_world[i];
+    float4 p = fascia4[i];
+    p.x = p.x + (cur.x - pw.x);
+    p.y = p.y + (cur.y - pw.y);
+    p.z = p.z + (cur.z - pw.z);
+    fascia4[i] = p;
+    prev_world[i] = make_float4(cur.x, cur.y, cur.z, 0.f);
+}
+
+// fascia_anchor_bone_kernel: anchor shell vertices snapped to their muscle
+// vertex's bone target plus the rest offset between them.
+__global__ void k_fascia_anchor(int n, const int* __restrict__ local, const int* __restrict__ cons,
+                                const float4* __restrict__ offset4, const float4* __restrict__ target4,
+                                float4* __restrict__ fascia4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 t = target4[cons[i]], o = offset4[i];
+    const int k = local[i];
+    const float w = fascia4[k].w;
+    fascia4[k] = make_float4(t.x + o.x, t.y + o.y, t.z + o.z, w);
+}
+
+// solve_glue_kernel: one-way XPBD distance step from a kinematic shell vertex
+// to a muscle vertex (only the muscle moves; fresh multiplier every call),
+// atomics on the muscle positions.
+__global__ void k_fascia_glue(int n, const int* __restrict__ pf, const int* __restrict__ pm,
+                              const float* __restrict__ restlen, const float* __restrict__ compliance,
+                              const float4* __restrict__ fascia4, float4* muscle4, float dt, float omega) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const float4 xf = fascia4[pf[c]];
+    const int mi = pm[c];
+    const float4 xm = muscle4[mi];
+    const float3 d = make_float3(xf.x - xm.x, xf.y - xm.y, xf.z - xm.z);
+    const float len = sqrtf(dot(d, d));
+    if (len < 1.0e-9f) return;
+    const float3 dir = make_float3(d.x / len, d.y / len, d.z / len);
+    const float C = len - restlen[c];
+    const float wj = xm.w;
+    const float at = compliance[c] / (dt * dt);
+    const float den = wj + at;
+    if (den < 1.0e-12f) return;
+    const float f = omega * (-C / den);
+    float* pm4 = reinterpret_cast<float*>(muscle4) + 4 * mi;
+    atomicAdd(pm4 + 0, (-f * wj) * dir.x);
+    atomicAdd(pm4 + 1, (-f * wj) * dir.y);
+    atomicAdd(pm4 + 2, (-f * wj) * dir.z);
+}
+
 bool a16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 bool a8(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0; }
 
@@ -382,6 +440,47 @@ int xpbd_surface_ride(int32_t n_bound, const int32_t* bound, const int32_t* face
         n_bound, bound, face, reinterpret_cast<const float2*>(uv), gap, reinterpret_cast<const float4*>(surf4), stris,
         reinterpret_cast<float4*>(fascia4));
     return cuda_check("xpbd_surface_ride");
+}
+
+int xpbd_fascia_advect(int32_t n, const int32_t* follow, const float* target4, float* prev_world4, float* fascia4,
+                       xpbd_stream_t stream) {
+    if (n < 0 || (n > 0 && (!follow || !target4 || !prev_world4 || !fascia4)))
+        return fail(XPBD_ERR_ARG, "xpbd_fascia_advect: bad arguments");
+    if (!a16(target4) || !a16(prev_world4) || !a16(fascia4))
+        return fail(XPBD_ERR_ALIGN, "xpbd_fascia_advect: [n][4] arrays must be 16-byte aligned");
+    if (n == 0) return XPBD_OK;
+    k_fascia_advect<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        n, follow, reinterpret_cast<const float4*>(target4), reinterpret_cast<float4*>(prev_world4),
+        reinterpret_cast<float4*>(fascia4));
+    return cuda_check("xpbd_fascia_advect");
+}
+
+int xpbd_fascia_anchor(int32_t n, const int32_t* local, const int32_t* cons, const float* offset4,
+                       const float* target4, float* fascia4, xpbd_stream_t stream) {
+    if (n < 0 || (n > 0 && (!local || !cons || !offset4 || !target4 || !fascia4)))
+        return fail(XPBD_ERR_ARG, "xpbd_fascia_anchor: bad arguments");
+    if (!a16(offset4) || !a16(target4) || !a16(fascia4))
+        return fail(XPBD_ERR_ALIGN, "xpbd_fascia_anchor: [n][4] arrays must be 16-byte aligned");
+    if (n == 0) return XPBD_OK;
+    k_fascia_anchor<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        n, local, cons, reinterpret_cast<const float4*>(offset4), reinterpret_cast<const float4*>(target4),
+        reinterpret_cast<float4*>(fascia4));
+    return cuda_check("xpbd_fascia_anchor");
+}
+
+int xpbd_fascia_glue(int32_t n, const int32_t* pair_fascia, const int32_t* pair_muscle, const float* restlen,
+                     const float* compliance, const float* fascia4, float* muscle4, float dt, float omega,
+                     xpbd_stream_t stream) {
+    if (n < 0 || (n > 0 && (!pair_fascia || !pair_muscle || !restlen || !compliance || !fascia4 || !muscle4)) ||
+        !(dt > 0.f))
+        return fail(XPBD_ERR_ARG, "xpbd_fascia_glue: bad arguments");
+    if (!a16(fascia4) || !a16(muscle4))
+        return fail(XPBD_ERR_ALIGN, "xpbd_fascia_glue: [n][4] arrays must be 16-byte aligned");
+    if (n == 0) return XPBD_OK;
+    k_fascia_glue<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        n, pair_fascia, pair_muscle, restlen, compliance, reinterpret_cast<const float4*>(fascia4),
+        reinterpret_cast<float4*>(muscle4), dt, omega);
+    return cuda_check("xpbd_fascia_glue");
 }
 
 int xpbd_m2m_glue(int32_t n_pairs, const int32_t* pair_a, const int32_t* pair_b, const float* restlen,

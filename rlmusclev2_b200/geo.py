@@ -139,6 +139,9 @@ class GeoFile:
     def has_point_attr(self, name: str) -> bool:
         return name in self._attrs
 
+    def has_point_group(self, name: str) -> bool:
+        return name in self._groups
+
     def point_group(self, name: str) -> np.ndarray:
         if name not in self._groups:
             raise KeyError(f"point group '{name}' not in {sorted(self._groups)}")

@@ -417,29 +417,59 @@ class MultiGridSim(MuscleSim):
         self.n_m2m = int(a.size)
 
     def _setup_fascia(self) -> None:
-        """The fascia shell sub-solver (mg.py:556-566), ride mode only: the shell
-        from ``fascia_path`` (a .geo read by geo.GeoFile) or, for the synthetic
-        scenes, a shell offset from the muscle surface (meshgen.fascia_shell)."""
+        """The fascia shell sub-solver (mg.py:556-566) in "ride" or "squeeze"
+        mode: the shell from ``fascia_path`` (a .geo read by geo.GeoFile) or,
+        for the synthetic scenes, a shell offset from the muscle surface
+        (meshgen.fascia_shell)."""
         self.fascia = None
         if not bool(self.cfg.get("use_fascia", False)):
             return
         mode = str(self.cfg.get("fascia_mode", "squeeze"))
-        if mode != "ride":
-            raise NotImplementedError(f"fascia_mode={mode!r} is not on the sm_100a path (supported: 'ride')")
+        if mode not in ("ride", "squeeze"):
+            raise NotImplementedError(f"fascia_mode={mode!r} is not on the sm_100a path (supported: 'ride', "
+                                      "'squeeze')")
         if (np.asarray(self.scene.tet_part) < 0).any():
             raise ValueError("use_fascia needs a scene without merged fascia tets (fascia_tets=0)")
         from .fascia import FasciaRide
         from .meshgen import fascia_shell
         path = self.cfg.get("fascia_path")
+        g = None
         if path and Path(path).exists():
             from .geo import GeoFile
+            from .meshgen import orient_tets
             g = GeoFile(path)
-            fv, ft = g.positions, np.asarray(g.tet_indices, np.int32)
+            fv = g.positions
+            ft = orient_tets(fv, np.asarray(g.tet_indices, np.int64)).astype(np.int32)
         else:
             fv, ft = fascia_shell(self.pos0_np, self.scene.surface_tris,
                                   float(self.cfg.get("fascia_gap", 0.001)), float(self.cfg.get("fascia_thickness", 0.003)))
         snh = find_constraint(self.cfg, "fascia_snh") or {}
         glue = find_constraint(self.cfg, "fascia_glue") or {}
+        if mode == "squeeze":
+            from .fascia import FasciaSqueeze
+            arap = find_constraint(self.cfg, "fascia_arap") or {}
+            vol = find_constraint(self.cfg, "fascia_volume") or {}
+            anchor = find_constraint(self.cfg, "fascia_anchor") or {}
+            ak = float(arap.get("stiffness", -1.0))
+            if ak < 0.0:  # the asset's solidshapestiffness (fascia.py:244-248)
+                if g is None or not g.has_point_attr("solidshapestiffness"):
+                    raise ValueError("fascia_arap.stiffness is required without a 'solidshapestiffness' attribute")
+                ak = float(g.point_attr("solidshapestiffness").mean())
+            gk = glue.get("stiffness")
+            if gk is None:  # the asset's tissuetomusclestiffness (fascia.py:433-438)
+                if g is None or not g.has_point_attr("tissuetomusclestiffness"):
+                    raise ValueError("fascia_glue.stiffness is required without a 'tissuetomusclestiffness' attribute")
+                gk = float(g.point_attr("tissuetomusclestiffness").mean())
+            rigid = g.point_group("rigid") if (g is not None and g.has_point_group("rigid")) else None
+            self.fascia = FasciaSqueeze(
+                self, fv, ft, rest_scale=float(arap.get("rest_scale", 0.95)), arap_k=ak,
+                arap_damp=float(arap.get("dampingratio", 0.0)), vol_k=float(vol.get("stiffness", 1.0e10)),
+                vol_damp=float(vol.get("dampingratio", 0.0)),
+                glue_k=float(gk) * float(glue.get("stiffness_scale", 0.001)),
+                total_mass=float(self.cfg.get("fascia_total_mass", self.total_mass)),
+                iterations=int(glue.get("iterations", self.fine_iters)), anchor_count=int(anchor.get("count", 256)),
+                rigid=rigid)
+            return
         self.fascia = FasciaRide(self, fv, ft, snh_mu=float(snh.get("mu", 1.0e3)), snh_lam=float(snh.get("lam", 1.0e8)),
                                  snh_damp=float(snh.get("dampingratio", 0.0)),
                                  total_mass=float(self.cfg.get("fascia_total_mass", self.total_mass)),
@@ -633,6 +663,8 @@ class MultiGridSim(MuscleSim):
 
     def _frame_fused(self) -> None:
         self._targets_kernel()
+        if self.fascia is not None:
+            self.fascia.advect()  # step_frame (mg.py:1413-1416): once per frame, before the substeps
         if self.mg is not None:
             self.mg.refresh_target()
         sdf = self.collision_solvers[0] if self.collision_solvers else None
@@ -682,6 +714,8 @@ class MultiGridSim(MuscleSim):
             self._graph("frame", self._frame_fused)
         else:
             self._kinematic_step(frame)
+            if self.fascia is not None:
+                self.fascia.advect()
             for _ in range(self.nsubsteps):
                 self.substep()
         self.step_cnt += 1

@@ -39,3 +39,31 @@ def test_bind_then_ride_on_the_rest_surface():
     sel = bound[inner[bound]]
     assert sel.size > 0
     assert np.abs(back[sel] - fv[sel]).max() < 1e-6
+
+
+def test_squeeze_coupling_steps():
+    """fascia_advect_bone / fascia_anchor_bone / solve_glue (fascia.py:45-125)."""
+    rng = np.random.default_rng(4)
+    nf, nm = 50, 80
+    f4 = np.zeros((nf, 4), np.float32)
+    f4[:, :3] = rng.random((nf, 3))
+    t4 = np.zeros((nm, 4), np.float32)
+    t4[:, :3] = rng.random((nm, 3))
+    follow = rng.integers(0, nm, nf)
+    prev = np.zeros((nf, 4), np.float32)
+    prev[:, :3] = t4[follow, :3] - 0.01
+    out, p2 = O.fascia_advect(follow, t4, prev, f4)
+    np.testing.assert_allclose(out[:, :3], f4[:, :3] + 0.01, atol=1e-6)
+    np.testing.assert_array_equal(p2[:, :3], t4[follow, :3])
+    local, cons = np.arange(0, nf, 5), rng.integers(0, nm, 10)
+    off = np.zeros((10, 4), np.float32)
+    off[:, :3] = rng.normal(scale=0.01, size=(10, 3))
+    snapped = O.fascia_anchor(local, cons, off, t4, f4)
+    np.testing.assert_allclose(snapped[local, :3], t4[cons, :3] + off[:, :3], atol=1e-7)
+    m4 = np.zeros((nm, 4), np.float32)
+    m4[:, :3] = rng.random((nm, 3))
+    m4[:, 3] = 1.0
+    pf, pm = rng.integers(0, nf, 30), rng.permutation(nm)[:30]
+    rest = (np.linalg.norm(f4[pf, :3] - m4[pm, :3], axis=1) * 0.7).astype(np.float32)
+    moved = O.fascia_glue(pf, pm, rest, np.zeros(30, np.float32), f4, m4, 1.0 / 240.0, 1.0)
+    np.testing.assert_allclose(np.linalg.norm(f4[pf, :3] - moved[pm, :3], axis=1), rest, rtol=1e-5)
