@@ -81,11 +81,11 @@ class BatchSim(MultiGridSim):
         a = np.asarray(a_inst, np.float32).reshape(-1)
         if a.shape[0] != self.n_inst:
             raise ValueError(f"{a.shape[0]} activations for {self.n_inst} instances")
-        self._h2d_event.synchronize()
+        self._act_event.synchronize()
         self._inst_act_host.numpy()[:] = a
         with torch.cuda.stream(self._stream):
             self._inst_act.copy_(self._inst_act_host, non_blocking=True)
-        self._h2d_event.record(self._stream)
+        self._act_event.record(self._stream)
         capi.check(self._lib.xpbd_gather(self.NT, 1, C.c_void_p(self._tet_inst_lib.data_ptr()),
                                          C.c_void_p(self._inst_act.data_ptr()), 1,
                                          C.c_void_p(self._t_act.data_ptr()), 1, self._sp))

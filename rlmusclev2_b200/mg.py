@@ -304,6 +304,11 @@ class MultiGridSim(MuscleSim):
         self._act_host = torch.zeros(self.NT, dtype=torch.float32).pin_memory()
         self._pos_user = torch.zeros((self.NV, 3), dtype=torch.float32, device=dev)
         self._pos_host = torch.zeros((self.NV, 3), dtype=torch.float32).pin_memory()
+        # One event per pinned staging buffer: a buffer is refilled only after
+        # its own previous copy has been consumed, so the activation upload and
+        # the target upload of one frame do not wait on each other.
+        self._act_event = torch.cuda.Event()
+        self._act_event.record(self._stream)
         self._h2d_event = torch.cuda.Event()
         self._h2d_event.record(self._stream)
         if self.target_mode == "points":
@@ -520,7 +525,7 @@ class MultiGridSim(MuscleSim):
         if self.target_mode == "points":
             tgt = (self._cons_targets(int(frame)) + self.rest_offset_np)[self.layout.perm]
             self._h2d_event.synchronize()
-            self._pts_host.numpy()[:] = tgt
+            self._pts_host.copy_(torch.from_numpy(np.ascontiguousarray(tgt, np.float32)))
             with torch.cuda.stream(self._stream):
                 self._pts_tgt.copy_(self._pts_host, non_blocking=True)
             self._h2d_event.record(self._stream)
@@ -573,11 +578,11 @@ class MultiGridSim(MuscleSim):
         a = np.asarray(acti_np, np.float32).reshape(-1)
         if a.shape[0] != self.NT:
             raise ValueError(f"activation has {a.shape[0]} entries, expected NT={self.NT}")
-        self._h2d_event.synchronize()
-        self._act_host.numpy()[:] = a
+        self._act_event.synchronize()
+        self._act_host.copy_(torch.from_numpy(a))  # multi-threaded host copy
         with torch.cuda.stream(self._stream):
             self._act_user.copy_(self._act_host, non_blocking=True)
-        self._h2d_event.record(self._stream)
+        self._act_event.record(self._stream)
         capi.check(self._lib.xpbd_gather(self.NT, 1, C.c_void_p(self._tet_perm_d.data_ptr()),
                                          C.c_void_p(self._act_user.data_ptr()), 1, C.c_void_p(self._t_act.data_ptr()),
                                          1, self._sp))
@@ -590,7 +595,9 @@ class MultiGridSim(MuscleSim):
         with torch.cuda.stream(self._stream):
             self._pos_host.copy_(self._pos_user, non_blocking=True)
         self._stream.synchronize()
-        return self._pos_host.numpy().copy()
+        out = torch.empty((self.NV, 3), dtype=torch.float32)
+        out.copy_(self._pos_host)  # multi-threaded host copy out of the pinned buffer
+        return out.numpy()
 
     # -------------------------------------------------------------- program
     def apply_pintotarget(self) -> None:
