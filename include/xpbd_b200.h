@@ -428,7 +428,8 @@ typedef struct XpbdDcd {
     int32_t* ws_vals;         /* [n_tris] triangle ids in Morton order */
     uint32_t* ws_keys2;       /* [n_tris] sort ping-pong */
     int32_t* ws_vals2;        /* [n_tris] */
-    int32_t* ws_hist;         /* radix histograms */
+    int32_t* ws_hist;         /* radix histograms, scan scratch and the sort's four grid barrier words (its last
+                                 four entries); zero before the first call */
     float* ws_bbox;           /* boxes of 32- and 1024-leaf Morton blocks (2 float4 each) */
     int32_t* ws_count;        /* [n_tris] pairs per Morton position, then their offsets */
     int32_t* ws_total;        /* [1] */
@@ -478,7 +479,7 @@ typedef struct XpbdPersist {
     const int32_t* tile_own; /* [n_tiles+1] tile k owns vertex ids [tile_own[k], tile_own[k+1]) (the vertices it
                                 touches first); ids from tile_own[n_tiles] up to n_verts are in no tet */
     float* ring;             /* [3][n_verts][4] boundary accumulators; all zero before the first call */
-    uint32_t* sync;          /* [4] grid barrier count, generation, ring phase, reserved; zero before the first call */
+    uint32_t* sync;          /* [4] two grid barrier counters, ring phase, counter parity; zero before the first call */
     int32_t* status;         /* [1] XPBD_STATUS_BARRIER_TIMEOUT; after it, zero ring and sync before the next call */
     int32_t tile_begin, tile_end; /* tiles [tile_begin, tile_end) in this launch (0, 0: all).  A sub-range must
                                      be closed (no vertex shared with tiles outside it, e.g. whole instances of a
@@ -496,7 +497,8 @@ typedef struct XpbdPersist {
  * iteration, and pos is written once at the end.  Needs all n_tiles CTAs
  * resident at once (xpbd_persistent_fits); returns XPBD_ERR_LIMIT otherwise.
  * Barrier waits are bounded (about a second); on timeout the status bit is
- * set and the kernel runs to its end without waiting again. */
+ * set and the kernel runs to its end, every later barrier giving up within
+ * 64 polls.  At most 2^20 iterations per call. */
 int xpbd_iterate_persistent(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v,
                             const XpbdPersist* ps, int32_t n_iters, xpbd_stream_t stream);
 /* *fits = 1 when the persistent pass of these materials can hold all tiles

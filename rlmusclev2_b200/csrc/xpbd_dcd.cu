@@ -201,6 +201,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_coop(XpbdDcd D, int chunk
     int32_t* vs = D.ws_vals;
     uint32_t* kd = D.ws_keys2;
     int32_t* vd = D.ws_vals2;
+    GridBarrier bar = grid_barrier_begin(sync);
     for (int pass = 0; pass < 4; ++pass) {
         const int shift = 8 * pass;
         // (A) chunk histogram
@@ -213,7 +214,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_coop(XpbdDcd D, int chunk
         }
         __syncthreads();
         if (threadIdx.x < 256) hist[b * 256 + threadIdx.x] = run[threadIdx.x];
-        grid_barrier(sync, D.status);
+        grid_barrier(bar, D.status);
         // (B) first output slot of each digit for this chunk
         {
             const int d = threadIdx.x & 255, q = threadIdx.x >> 8;
@@ -259,10 +260,11 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_coop(XpbdDcd D, int chunk
             }
             __syncthreads();
         }
-        if (pass < 3) grid_barrier(sync, D.status);
+        if (pass < 3) grid_barrier(bar, D.status);
         uint32_t* tk = ks; ks = kd; kd = tk;
         int32_t* tv = vs; vs = vd; vd = tv;
     }
+    grid_barrier_end(sync, bar);
 }
 
 // ---------------------------------------------------------- Karras build

@@ -59,6 +59,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
     float4* ring = reinterpret_cast<float4*>(P.ring);
     const size_t nv = size_t(V.n);
     const uint32_t phase0 = P.sync[2];
+    GridBarrier bar = grid_barrier_begin(P.sync);
     const uint32_t ops = XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_PIN;
     __shared__ float s_arap_at[XPBD_MAX_MATERIALS];
     fill_arap_at(prm, s_arap_at);
@@ -104,7 +105,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
             finish_vertex(prm, V, g, pp, make_float4(0.f, 0.f, 0.f, 0.f), ops);
             pos4w[g] = pp;
         }
-        grid_barrier(P.sync, P.status);
+        grid_barrier(bar, P.status);
         for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
             float4 pp = s_pos[i];
             finish_core(prm, s_f[i], s_att[i], s_prev[i], s_pin[i], pp, __ldcg(&rc[s_g[i]]), ops);
@@ -117,6 +118,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
         if (i < nint || (g >= own_lo && g < own_hi)) pos4w[g] = s_pos[i];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) P.sync[2] = (phase0 + uint32_t(n_iters)) % 3u;
+    grid_barrier_end(P.sync, bar);
 }
 
 uint32_t material_union(const XpbdParams* p) {
@@ -192,6 +194,8 @@ extern "C" int xpbd_iterate_persistent(const XpbdParams* prm, const XpbdTiles* t
     if (!prm || !tiles || !v || !ps) return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: null argument");
     if (n_iters < 0) return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: n_iters < 0");
     if (n_iters == 0) return XPBD_OK;
+    // barrier counters reach n_iters x grid size within one launch
+    if (n_iters > (1 << 20)) return fail(XPBD_ERR_LIMIT, "xpbd_iterate_persistent: n_iters > 2^20");
     if (!v->pos || v->n <= 0 || !tiles->tile_vptr || !tiles->tile_nint || !tiles->tile_tptr || !tiles->tile_verts ||
         !tiles->tet_q || !tiles->tet_b0 || !tiles->tet_b1 || !tiles->tet_b2 || tiles->n_tiles <= 0)
         return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: tiles/verts");
