@@ -8,6 +8,12 @@
 
 namespace xpbd {
 
+// Dynamic shared memory above this asks for the opt-in attribute.  The default
+// per-block limit (48 KB) counts static shared memory too, so opting in only
+// above 48 KB of dynamic memory would leave kernels with a little static
+// memory unlaunchable just below it.
+constexpr size_t kSmemOptIn = 40 * 1024;
+
 // Last error of the calling host thread (returned by xpbd_error_string()).
 char* err_buffer();
 

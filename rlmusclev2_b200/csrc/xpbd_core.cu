@@ -396,7 +396,7 @@ bool any_aniso(const XpbdParams* p) {
 template <int MODE, bool DAMP, int MINB, int CSET>
 int launch_project_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
     const size_t smem = size_t(T->max_tile_verts) * sizeof(float4) * (DAMP ? 3 : 2);  // pos, [prev], 4 x float acc
-    if (smem > 48 * 1024) {
+    if (smem > kSmemOptIn) {
         static unsigned char done[64];
         int dev = 0;
         cudaGetDevice(&dev);
@@ -550,7 +550,7 @@ int xpbd_metrics(const XpbdTiles* tiles, const XpbdVerts* v, XpbdMetrics* out, x
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(out, 0, sizeof(XpbdMetrics), s) != cudaSuccess) return cuda_check("xpbd_metrics memset");
     const size_t smem = size_t(tiles->max_tile_verts) * sizeof(float4);
-    if (smem > 48 * 1024)
+    if (smem > kSmemOptIn)
         cudaFuncSetAttribute(k_metrics, cudaFuncAttributeMaxDynamicSharedMemorySize, int(XPBD_MAX_TILE_VERTS * sizeof(float4)));
     k_metrics<<<tiles->n_tiles, kTileThreads, smem, s>>>(*tiles, *v, out);
     return cuda_check("xpbd_metrics");

@@ -159,7 +159,7 @@ int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, f
     if (!aligned16(fine4) || !aligned16(coarse4) || !aligned16(coarse_prev4) || !aligned16(coarse_pin4))
         return fail(XPBD_ERR_ALIGN, "xpbd_mg_restrict: [n][4] buffers must be 16-byte aligned");
     const size_t smem = size_t(cage->max_block) * sizeof(float4);
-    if (smem > 48 * 1024)
+    if (smem > kSmemOptIn)
         cudaFuncSetAttribute(k_mg_restrict, cudaFuncAttributeMaxDynamicSharedMemorySize, int(8192 * sizeof(float4)));
     k_mg_residual<<<(cage->n_fine + kMgThreads - 1) / kMgThreads, kMgThreads, 0, (cudaStream_t)stream>>>(
         *cage, reinterpret_cast<const float4*>(fine4), reinterpret_cast<const float4*>(coarse4));

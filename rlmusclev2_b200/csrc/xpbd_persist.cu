@@ -132,7 +132,7 @@ int launch_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, cons
              cudaStream_t s, bool query_only, int* fits) {
     auto kern = k_iterate_persistent<DAMP, MINB, CSET, PF>;
     const size_t smem = size_t(T->max_tile_verts) * kSmemPerVert;
-    if (smem > 48 * 1024 &&
+    if (smem > kSmemOptIn &&
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return cuda_check("xpbd_iterate_persistent: smem attribute");
     int dev = 0, n_sm = 0, per_sm = 0;
