@@ -184,8 +184,13 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
         const float h = __fdividef(0.5f, g * det);  // 1 / (2 g det)
         const float a = 0.5f * g;
         const float3 y0 = a * x0 + h * c0, y1 = a * x1 + h * c1, y2 = a * x2 + h * c2;
-        const float3 e0 = y0 - x0, e1 = y1 - x1, e2 = y2 - x2;
-        const float ch = dot(e0, e0) + dot(e1, e1) + dot(e2, e2);
+        // The first step is never tested: from F it stops only for tets already
+        // at a rotation, which a second step leaves in place.
+        float ch = 1.f;
+        if (it > 0) {
+            const float3 e0 = y0 - x0, e1 = y1 - x1, e2 = y2 - x2;
+            ch = dot(e0, e0) + dot(e1, e1) + dot(e2, e2);
+        }
         x0 = y0;
         x1 = y1;
         x2 = y2;
