@@ -160,6 +160,21 @@ enum : uint32_t {
     MAT_DAMPED = 1u << 4,  // some constraint of this material reads pprev
 };
 
+// One scaled Newton step on the columns x0..x2 of X, given c0 = x1 x x2 and
+// det = det X > 0.  Scaling g ~ det^(-1/3) only sets the convergence speed: at
+// the fixed point det = 1, and a relative error e in g moves the iterate by
+// O(e^2), so the fast approximate power and divide are enough.
+__device__ __forceinline__ void polar_newton_step(const float3& x0, const float3& x1, const float3& x2,
+                                                  const float3& c0, float det, float3& y0, float3& y1, float3& y2) {
+    const float3 c1 = cross(x2, x0), c2 = cross(x0, x1);
+    const float g = __powf(det, -0.33333334f);
+    const float h = __fdividef(0.5f, g * det);  // 1 / (2 g det)
+    const float a = 0.5f * g;
+    y0 = a * x0 + h * c0;
+    y1 = a * x1 + h * c1;
+    y2 = a * x2 + h * c2;
+}
+
 // Rotation factor R of F = R S for det F > 0, by Higham's scaled Newton
 // iteration X <- (g X + (g X)^-T) / 2, g = |det X|^(-1/3) (N. J. Higham,
 // "Computing the polar decomposition with applications", SIAM J. Sci. Stat.
@@ -173,24 +188,20 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
     const float n2 = dot(x0, x0) + dot(x1, x1) + dot(x2, x2);
     float3 c0 = cross(x1, x2);
     float det = dot(x0, c0);
-    if (!(det > 1e-6f * n2 * sqrtf(n2))) return false;
+    // det > 1e-6 |F|_F^3, squared to avoid the square root
+    if (!(det > 0.f && det * det > 1e-12f * (n2 * n2 * n2))) return false;
+    // The first step is not tested: from F it stops only for tets already at
+    // a rotation, which a second step leaves in place.
+    polar_newton_step(x0, x1, x2, c0, det, x0, x1, x2);
+    c0 = cross(x1, x2);
+    det = dot(x0, c0);
+    if (!(det > 0.f)) return false;
 #pragma unroll 1
-    for (int it = 0; it < 10; ++it) {
-        const float3 c1 = cross(x2, x0), c2 = cross(x0, x1);
-        // Scaling g ~ det^(-1/3) only sets the convergence speed: at the fixed
-        // point det = 1, and a relative error e in g moves the iterate by
-        // O(e^2), so the fast approximate power and divide are enough.
-        const float g = __powf(det, -0.33333334f);
-        const float h = __fdividef(0.5f, g * det);  // 1 / (2 g det)
-        const float a = 0.5f * g;
-        const float3 y0 = a * x0 + h * c0, y1 = a * x1 + h * c1, y2 = a * x2 + h * c2;
-        // The first step is never tested: from F it stops only for tets already
-        // at a rotation, which a second step leaves in place.
-        float ch = 1.f;
-        if (it > 0) {
-            const float3 e0 = y0 - x0, e1 = y1 - x1, e2 = y2 - x2;
-            ch = dot(e0, e0) + dot(e1, e1) + dot(e2, e2);
-        }
+    for (int it = 1; it < 10; ++it) {
+        float3 y0, y1, y2;
+        polar_newton_step(x0, x1, x2, c0, det, y0, y1, y2);
+        const float3 e0 = y0 - x0, e1 = y1 - x1, e2 = y2 - x2;
+        const float ch = dot(e0, e0) + dot(e1, e1) + dot(e2, e2);
         x0 = y0;
         x1 = y1;
         x2 = y2;
