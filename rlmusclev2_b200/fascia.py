@@ -1,9 +1,11 @@
-"""Fascia shell sub-solver, ride mode (the reference's Fascia with
-fascia_mode="ride", fascia/fascia.py:179-572): a Stable Neo-Hookean shell
-whose vertices near the muscle are bound barycentrically to the closest
-muscle-surface triangle (plus the signed normal gap) and follow it every
-substep; the muscle is never pushed.  The shell runs on its own tile engine
-(one more XpbdSolver on the parent's stream)."""
+"""Fascia shell sub-solvers (the reference's Fascia, fascia/fascia.py:179-572).
+
+Ride mode (FasciaRide): a Stable Neo-Hookean shell whose vertices near the
+muscle are bound barycentrically to the closest muscle-surface triangle (plus
+the signed normal gap) and follow it every substep; the muscle is never
+pushed.  Squeeze mode (FasciaSqueeze): a shrunk ARAP + volume shell carried by
+the bones that pulls the muscle surface with one-way glue.  Each shell runs on
+its own tile engine (one more XpbdSolver on the parent's stream)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -101,6 +103,8 @@ class FasciaSqueeze:
         from scipy.spatial import cKDTree
 
         from .engine import XpbdSolver
+        if not rest_scale > 0.0:
+            raise ValueError(f"fascia_arap.rest_scale must be > 0, got {rest_scale}")
         self.parent = parent
         self.iterations = int(iterations)
         verts = np.asarray(verts, np.float32)
