@@ -61,3 +61,41 @@ def test_noalloc_rejects_oversized_meshes(lib):
     verts.n = capi.NOALLOC_MAX_VERTS + 1
     assert lib.xpbd_iterate_noalloc(C.byref(prm), C.byref(tiles), C.byref(verts), None) == ERR_LIMIT
     assert "XPBD_NOALLOC_MAX_VERTS" in _msg(lib)
+
+
+def test_bone_glue_fascia_checks(lib):
+    A, M8, M4 = 16, 8, 4  # aligned dummy, 8-byte (not 16), 4-byte (not 8): never dereferenced
+    f = C.c_float
+    # bone binding
+    assert lib.xpbd_bone_bind(-1, A, 3, A, 1, A, f(1.0), A, A, A, None) == ERR_ARG
+    assert lib.xpbd_bone_bind(1, A, 3, A, 0, A, f(1.0), A, A, A, None) == ERR_ARG         # no triangles
+    assert lib.xpbd_bone_bind(1, M8, 3, A, 1, A, f(1.0), A, A, A, None) == ERR_ALIGN      # query4
+    assert lib.xpbd_bone_bind(1, A, 3, A, 1, A, f(1.0), A, M4, A, None) == ERR_ALIGN      # uv
+    assert lib.xpbd_bone_bind(0, None, 3, A, 1, A, f(1.0), None, None, None, None) == 0
+    # sliding targets: re-projection needs the muscle positions and anchors; some target is required
+    assert lib.xpbd_bone_slide_targets(1, None, A, A, A, A, A, f(0.01), 1, f(1.0), 3, A, 1, A, A, A, None) == ERR_ARG
+    assert lib.xpbd_bone_slide_targets(1, A, A, A, A, A, A, f(0.01), 0, f(1.0), 3, A, 1, A, None, None,
+                                       None) == ERR_ARG
+    assert lib.xpbd_bone_slide_targets(1, A, A, A, A, A, A, f(0.01), 0, f(1.0), 3, A, 1, A, M8, None,
+                                       None) == ERR_ALIGN
+    assert lib.xpbd_bone_slide_targets(0, None, None, None, None, None, None, f(0.01), 0, f(1.0), 3, A, 1, A,
+                                       None, None, None) == 0
+    assert lib.xpbd_bone_surface_pose(4, A, A, 0, A, A, None) == ERR_ARG                  # no bones
+    assert lib.xpbd_bone_surface_pose(4, A, A, 2, A, M8, None) == ERR_ALIGN
+    # fascia ride
+    assert lib.xpbd_surface_bind(1, A, 3, A, 0, A, f(1.0), A, A, A, A, None) == ERR_ARG
+    assert lib.xpbd_surface_bind(1, A, 3, A, 1, A, f(1.0), A, M4, A, A, None) == ERR_ALIGN
+    assert lib.xpbd_surface_ride(1, A, A, A, A, M8, A, A, None) == ERR_ALIGN
+    assert lib.xpbd_surface_ride(0, None, None, None, None, None, None, None, None) == 0
+    # fascia squeeze
+    assert lib.xpbd_fascia_advect(1, None, A, A, A, None) == ERR_ARG
+    assert lib.xpbd_fascia_advect(1, A, A, M8, A, None) == ERR_ALIGN
+    assert lib.xpbd_fascia_advect(0, None, None, None, None, None) == 0
+    assert lib.xpbd_fascia_anchor(1, A, None, A, A, A, None) == ERR_ARG
+    assert lib.xpbd_fascia_anchor(1, A, A, A, A, M8, None) == ERR_ALIGN
+    assert lib.xpbd_fascia_glue(1, A, A, A, A, A, A, f(0.0), f(1.0), None) == ERR_ARG      # dt <= 0
+    assert lib.xpbd_fascia_glue(1, A, A, A, A, A, M8, f(0.01), f(1.0), None) == ERR_ALIGN
+    # muscle-to-muscle glue
+    assert lib.xpbd_m2m_glue(1, A, A, A, A, A, f(-1.0), f(1.0), None) == ERR_ARG
+    assert lib.xpbd_m2m_glue(1, A, A, A, A, M8, f(0.01), f(1.0), None) == ERR_ALIGN
+    assert lib.xpbd_m2m_glue(0, None, None, None, None, None, f(0.01), f(1.0), None) == 0
