@@ -99,3 +99,23 @@ def test_bone_glue_fascia_checks(lib):
     assert lib.xpbd_m2m_glue(1, A, A, A, A, A, f(-1.0), f(1.0), None) == ERR_ARG
     assert lib.xpbd_m2m_glue(1, A, A, A, A, M8, f(0.01), f(1.0), None) == ERR_ALIGN
     assert lib.xpbd_m2m_glue(0, None, None, None, None, None, f(0.01), f(1.0), None) == 0
+
+
+def test_dcd_checks(lib):
+    sz = capi.XpbdDcdWorkspaceSizes()
+    assert lib.xpbd_dcd_workspace_query(0, C.byref(sz)) == ERR_ARG
+    assert lib.xpbd_dcd_workspace_query(1000, C.byref(sz)) == 0
+    assert sz.hist > 4 and sz.split >= 4 and sz.keys == 1000   # the sort's 4 barrier words end ws_hist
+    assert lib.xpbd_dcd_broadphase(None, 16, 0, None) == ERR_ARG
+    d = capi.XpbdDcd()
+    d.n_tris, d.n_verts, d.max_pairs, d.max_contacts = 10, 12, 64, 64
+    for name, typ in capi.XpbdDcd._fields_:
+        if typ is C.c_void_p:
+            setattr(d, name, 16)                                   # aligned dummies, never dereferenced
+    assert lib.xpbd_dcd_broadphase(C.byref(d), 8, 0, None) == ERR_ARG    # pos4 misaligned
+    d.max_pairs = 0
+    assert lib.xpbd_dcd_broadphase(C.byref(d), 16, 0, None) == ERR_ARG   # no pair capacity
+    d.max_pairs, d.ws_split = 64, 8
+    assert lib.xpbd_dcd_broadphase(C.byref(d), 16, 0, None) == ERR_ALIGN
+    d.ws_split, d.tris = 16, None
+    assert lib.xpbd_dcd_narrow_respond(C.byref(d), 16, None) == ERR_ARG
