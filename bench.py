@@ -132,64 +132,41 @@ class ClockSampler:
 
 
 class CpuBaseline:
-    """The CPU oracle (OpenMP, all host threads) on the same mesh and constraint
-    set; a step times a bounded sample (``sample_iters`` Jacobi iterations of the
-    full mesh plus one predict/velocity pass) scaled to one frame."""
+    """The CPU oracle stepping whole frames of the benchmark's program
+    (OracleMultiGridSim.step_frame, the reference's MultiGridSim frame
+    mg.py:1322-1418 restated in C with OpenMP over all host threads): bone
+    targets and belly-attach targets, the 256^3 SDF bake, the hard pin, then
+    per substep the prediction, the Jacobi iterations (every constraint, the
+    averaged apply and the re-pin after each), the SDF push-out and the
+    velocity update.  The same frames and inputs as the GPU arm."""
 
     def __init__(self, cfg, scene):
         from oracle import oracle as O
-        from rlmusclev2_b200.builder import tet_rest_data
-        from rlmusclev2_b200.mg import find_constraint
-        verts, tets = scene.verts, scene.tets
-        _, V0, valid = tet_rest_data(verts, tets)
-        rho = float(cfg["total_mass"]) / float(V0[valid].astype(np.float64).sum())
-        rv, B, mass, tot = O.precompute_rest(verts, tets, rho, "f32")
-        arap = find_constraint(cfg, "arap")
-        fib = find_constraint(cfg, "fiber")
-        cons = [dict(type="tetarapsvd", name="arap", stiffness=arap["stiffness"],
-                     dampingratio=arap.get("dampingratio", 0.0))]
-        masks = {}
-        if fib:
-            cons.append(dict(type="aniso_arap", name="fiber", stiffness=fib["stiffness"]))
-            masks["fiber"] = scene.tet_part == scene.aniso_muscle
-        t = O.table_from_configs(verts, tets, cons, masks)
-        belly = find_constraint(cfg, "belly_attach")
-        if belly:
-            src = np.nonzero(scene.v_tendon <= 0.5)[0]
-            rvv = np.ones((src.shape[0], 4))
-            rvv[:, :3] = verts[src]
-            pts = np.full((src.shape[0], 4), -1, np.int32)
-            pts[:, 0] = src
-            t.add(O.T_ATTACH, pts, belly["stiffness"], belly.get("dampingratio", 0.0), np.full(src.shape[0], -1),
-                  np.zeros(src.shape[0]), restvector=rvv)
-        t.finalize()
-        dt = float(cfg["delta_t"]) / int(cfg["nsubsteps"])
-        self.s = O.OracleSolver(verts, tets, t, mass, np.zeros(verts.shape[0], np.int32), B, dt=dt,
-                                gravity_vec=(0, 0, 0), v_fiber=scene.v_fiber, tendonmask=np.zeros(tets.shape[0]),
-                                contraction_ratio=0.4, prec="f32")
-        self.s.pos += np.float32(1e-4) * np.sin(np.arange(self.s.pos.size, dtype=np.float32)).reshape(self.s.pos.shape)
+        self.orc = O.OracleMultiGridSim(cfg, scene, prec="f32")
+        self.frame = int(cfg.get("start_frame", 1))
         self.n_iter = int(cfg["nsubsteps"]) * int(cfg["fine_iterations"])
         self.nsub = int(cfg["nsubsteps"])
-        self.n_tets = int(tets.shape[0])
-        self.s.project()  # first touch of the scratch buffers
+        self.n_tets = int(scene.tets.shape[0])
 
-    def sample(self, sample_iters: int = 1) -> float:
-        s = self.s
+    def frame_ms(self) -> float:
+        """One whole frame (the next frame of the sequence), wall time in ms."""
         t0 = time.perf_counter()
-        for _ in range(sample_iters):
-            s.project()
-            s.apply_dP()
-        t_iter = (time.perf_counter() - t0) / sample_iters
-        t1 = time.perf_counter()
-        s.integrate()
-        s.update_velocities()
-        t_vert = time.perf_counter() - t1
-        return (t_iter * self.n_iter + t_vert * self.nsub) * 1e3
+        self.orc.step_frame(self.frame)
+        self.frame += 1
+        return (time.perf_counter() - t0) * 1e3
 
-    def describe(self, value: float, sample_iters: int) -> dict:
+    def run(self, warmup: int, steps: int) -> float:
+        for _ in range(warmup):
+            self.frame_ms()
+        self.times = [self.frame_ms() for _ in range(steps)]
+        return float(np.mean(self.times))
+
+    def describe(self, value: float, warmup: int, steps: int) -> dict:
         return {"value": round(value, 3), "unit": "ms/frame", "cores": _omp_threads(), "kind": "port",
-                "sample": f"{sample_iters} Jacobi iteration(s) + 1 predict/velocity pass of the full {self.n_tets}-tet "
-                          f"mesh on the FP32 oracle, scaled to {self.n_iter} iterations and {self.nsub} substeps/frame"}
+                "sample": f"{steps} whole frame(s) after {warmup} untimed, mean wall time: the {self.n_tets}-tet "
+                          f"mesh through the FP32 oracle's frame program (targets, SDF bake, pins, "
+                          f"{self.nsub} substeps x {self.n_iter // self.nsub} Jacobi iterations, push-out, "
+                          f"velocities)"}
 
 
 def _omp_threads() -> int:
@@ -211,6 +188,9 @@ def _dist_setup():
 
 
 def run_reference(args):
+    """The reference arm: the oracle's restatement of the reference's CPU
+    path (the reference itself runs on NVIDIA Warp, which cannot be installed
+    here), whole frames of the benchmark workload, rank 0 only."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -219,18 +199,16 @@ def run_reference(args):
     cfg = load_config(str(CONFIG))
     scene = scene_from_cfg(cfg)
     cb = CpuBaseline(cfg, scene)
-    for _ in range(args.warmup):
-        cb.sample(1)
-    vals = [cb.sample(1) for _ in range(max(1, args.steps))]
-    v = float(np.median(vals))
+    v = cb.run(args.warmup, max(1, args.steps))
+    steps = max(1, args.steps)
     line = {"impl": "reference", "metric": "ms/frame", "value": round(v, 3), "unit": "ms/frame", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n_verts": int(scene.verts.shape[0]), "n_tets": int(scene.tets.shape[0])},
-            "cpu_baseline": cb.describe(v, 1),
+            "cpu_baseline": cb.describe(v, args.warmup, steps),
             "e2e": {"value": round(v, 3), "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference runs on NVIDIA Warp, which cannot be installed here; its CPU path is restated "
-                    "by the C oracle (OpenMP) and timed on a bounded sample scaled to one frame"}
+            "note": "the reference runs on NVIDIA Warp (warp-lang 1.13.0), which is not installable offline here; "
+                    "its CPU path is restated by the C oracle (OpenMP) and timed on whole frames"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -433,7 +411,7 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config == "humanv2":
         cb = CpuBaseline(cfg, sc)
-        line["cpu_baseline"] = cb.describe(cb.sample(2), 2)
+        line["cpu_baseline"] = cb.describe(cb.run(1, 2), 1, 2)
     sim.release_graphs()
     if world > 1:
         torch.distributed.barrier()

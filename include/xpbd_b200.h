@@ -89,8 +89,9 @@ typedef struct XpbdParams {
                                     32-bit integers round(d * acc_scale) (native integer atomics; shared
                                     float atomics cost ~5x more) and read the sums back as float(sum) /
                                     acc_scale; xpbd_acc_scale_for_extent gives the value for a mesh */
-    int32_t* status;             /* optional [1]: XPBD_STATUS_ACC_RANGE is or-ed in when a single tet's
-                                    correction exceeds 1/64 of the fixed-point range (sums may wrap) */
+    int32_t* status;             /* optional [1]: XPBD_STATUS_ACC_RANGE is or-ed in when the sum of a single
+                                    tet's 12 correction magnitudes exceeds 1/64 of the fixed-point range, or
+                                    is NaN or Inf (a vertex sum can then wrap only with > 64 such tets) */
     XpbdMaterial materials[XPBD_MAX_MATERIALS];
     XpbdAttachMaterial attach[XPBD_MAX_ATTACH_MATERIALS];
 } XpbdParams;
@@ -188,8 +189,9 @@ int xpbd_abi_version(void);
  * in magnitude: the largest power of two s with s x max_coord <= 2^26.  The
  * quantum 1/s is then at most half an FP32 ulp of the largest coordinate (the
  * position update cannot resolve finer steps there), a vertex's correction
- * sum may reach 32 x max_coord before the 32-bit range ends, and one tet's
- * correction above max_coord / 2 sets XPBD_STATUS_ACC_RANGE.
+ * sum may reach 32 x max_coord before the 32-bit range ends, and one tet
+ * whose correction magnitudes sum above max_coord / 2 (or to NaN/Inf) sets
+ * XPBD_STATUS_ACC_RANGE.
  * Library-specific (the reference sums corrections with float atomics). */
 float xpbd_acc_scale_for_extent(float max_coord);
 
@@ -468,9 +470,14 @@ int xpbd_dcd_narrow_respond(const XpbdDcd* dcd, float* pos4, xpbd_stream_t strea
  * the accumulator is instead a fixed device array of XPBD_NOALLOC_MAX_VERTS
  * float4 (4 MiB) that every GPU loading the library holds until process
  * exit.  Meshes with more than XPBD_NOALLOC_MAX_VERTS vertices are rejected
- * with XPBD_ERR_LIMIT.  The first call on a device looks up that array's
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race. */
+ * with XPBD_ERR_LIMIT.  Every call made outside stream capture looks up that
+ * array's address (cudaGetSymbolAddress) on the current device; a call made
+ * during capture reuses the last one found there, so the first call on a
+ * device, and the first after a device reset, must come before any stream
+ * capture (otherwise XPBD_ERR_ARG).  The array starts zeroed and each call
+ * leaves it zeroed; it is cleared again only after a call that failed between
+ * its two launches.  All calls share the array: calls that overlap on the GPU
+ * race. */
 #define XPBD_NOALLOC_MAX_VERTS 262144
 int xpbd_iterate_noalloc(const XpbdParams* prm, const XpbdTiles* tiles, const XpbdVerts* v, xpbd_stream_t stream);
 

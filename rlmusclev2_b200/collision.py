@@ -222,6 +222,13 @@ class DcdBuffers:
     def narrow_respond(self, pos4: torch.Tensor, stream) -> None:
         capi.check(self.lib.xpbd_dcd_narrow_respond(C.byref(self.d), C.c_void_p(pos4.data_ptr()), stream))
 
+    def reset(self) -> None:
+        """Zero the counters (pair and contact counts, status word) and the
+        sort's grid-barrier words, on the current stream: after a barrier
+        timeout the next broadphase then runs with full barriers."""
+        self.t["counters"].zero_()
+        self.t["hist"].zero_()
+
     def counters(self) -> dict:
         c = self.t["counters"].cpu().numpy()
         return {"n_pairs": int(c[0]), "n_contacts": int(c[1]), "status": int(c[2])}
@@ -265,8 +272,11 @@ class UdcfDcdCollider:
         c = self.buf.counters()
         p = self.params
         if c["status"] & capi.STATUS_BARRIER_TIMEOUT:
+            with torch.cuda.stream(self.sim._stream):
+                self.buf.reset()
+            self.sim._stream.synchronize()
             raise RuntimeError("[udcf_dcd] the broadphase sort gave up waiting at a grid barrier; "
-                               "pairs are invalid (zero the workspace before the next call)")
+                               "pairs were invalid (the counters and barrier words have been cleared)")
         if c["status"] & capi.STATUS_STACK_OVERFLOW:
             print("[udcf_dcd] WARNING: BVH traversal stack overflow")
         if c["n_pairs"] > p.max_pairs or c["n_contacts"] > p.max_contacts:

@@ -163,10 +163,14 @@ __device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const X
                                                    (prm.tile_variant & 2) != 0))
             nact += 1;
         if (nact != 0) {
-            float dmax = 0.f;
+            // Range check on the sum of the 12 |components| (not their maximum:
+            // a sum carries a NaN or Inf component through, fmaxf drops NaN).
+            // Each converted component is then below 2^25 = 2^31/64, so a vertex
+            // sum wraps unflagged only with more than 64 such tets on it.
+            float dabs = 0.f;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) dmax = fmaxf(dmax, fmaxf(fabsf(d[i].x), fmaxf(fabsf(d[i].y), fabsf(d[i].z))));
-            if (!(dmax * acc_scale <= 33554432.f) && prm.status) atomicOr(prm.status, XPBD_STATUS_ACC_RANGE);  // 2^31/64
+            for (int i = 0; i < 4; ++i) dabs += (fabsf(d[i].x) + fabsf(d[i].y)) + fabsf(d[i].z);
+            if (!(dabs * acc_scale <= 33554432.f) && prm.status) atomicOr(prm.status, XPBD_STATUS_ACC_RANGE);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 atomicAdd(&s_ax[l[i]], __float2int_rn(d[i].x * acc_scale));

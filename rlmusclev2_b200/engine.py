@@ -33,6 +33,28 @@ def _ptr(t) -> int | None:
     return None if t is None else int(t.data_ptr())
 
 
+def status_error(tile_status: int, dcd_status: int = 0) -> str | None:
+    """The error a frame must raise for its status words, or None.
+
+    ``tile_status``: the XPBD_STATUS_* word of the tile passes and the
+    persistent pass; ``dcd_status``: the DCD's word.  Fatal: a grid barrier
+    that gave up (its later barriers race), a fixed-point correction beyond
+    the accumulator's safe range (the sums wrap), a DCD sort that gave up
+    (the broadphase finds no pairs until the words are cleared).  Overflow
+    bits of the DCD are warnings (UdcfDcdCollider.stats reports them)."""
+    msgs = []
+    if tile_status & capi.STATUS_BARRIER_TIMEOUT:
+        msgs.append("the persistent Jacobi pass gave up waiting at a grid barrier (positions are invalid)")
+    if tile_status & capi.STATUS_ACC_RANGE:
+        msgs.append("a tet correction left the fixed-point accumulator's range (positions are invalid: "
+                    "the state probably diverged or acc_scale is too large)")
+    if dcd_status & capi.STATUS_BARRIER_TIMEOUT:
+        msgs.append("the DCD broadphase sort gave up waiting at a grid barrier (contacts were skipped)")
+    if not msgs:
+        return None
+    return "; ".join(msgs) + ". The status words have been cleared for the next launch."
+
+
 
 class XpbdEngine:
     """State-independent substep primitives plus the program runner."""
@@ -96,6 +118,9 @@ class XpbdEngine:
         self._ring = torch.zeros((3, nv, 4), dtype=f32, device=dev)
         self._psync = torch.zeros(4, dtype=torch.int32, device=dev)
         self._pstatus = torch.zeros(1, dtype=torch.int32, device=dev)
+        # host copies of the status words, queued behind every frame (see _post_status)
+        self._status_host = torch.zeros(2, dtype=torch.int32).pin_memory()
+        self._status_event = None
         self._t_own = T(L.tile_own)
         self.use_persistent = True
         self._metrics_buf = torch.zeros(8, dtype=torch.float64, device=dev)  # >= sizeof(XpbdMetrics)
@@ -322,6 +347,7 @@ class XpbdEngine:
         ring and barrier words are cleared for the next launch."""
         self._stream.synchronize()
         st = int(self._pstatus.item())
+        self._status_pending = False  # this read supersedes the copy queued behind the last frame
         if st and reset:
             with torch.cuda.stream(self._stream):
                 self._ring.zero_()
@@ -330,8 +356,50 @@ class XpbdEngine:
             self._stream.synchronize()
         return st
 
+    def _post_status(self) -> None:
+        """Queue copies of the device status words (the tile passes' word and,
+        with a DCD attached, the DCD's) into pinned host memory behind the
+        work launched so far, with an event; no synchronisation."""
+        with torch.cuda.stream(self._stream):
+            self._status_host[0:1].copy_(self._pstatus, non_blocking=True)
+            dcd = getattr(self, "dcd", None)
+            if dcd is not None:
+                self._status_host[1:2].copy_(dcd.buf.t["counters"][2:3], non_blocking=True)
+        if self._status_event is None:
+            self._status_event = torch.cuda.Event()
+        self._status_event.record(self._stream)
+        self._status_pending = True
+
+    def _check_status(self) -> None:
+        """Raise if the last status copy that has landed shows a fatal bit.
+
+        A barrier timeout leaves the persistent pass's later barriers giving
+        up early (the bit is sticky), and a fixed-point range overflow
+        wraps the sums: both make every later result wrong without any other
+        sign.  Called before each frame (non-blocking: a copy still in flight
+        is checked at the next call) and after every synchronising read.
+        Before raising, the barrier words, ring, status word and the DCD's
+        counters are cleared, so the next launch runs with full barriers."""
+        if not getattr(self, "_status_pending", False) or not self._status_event.query():
+            return
+        self._status_pending = False
+        st, sd = (int(x) for x in self._status_host.tolist())
+        msg = status_error(st, sd if getattr(self, "dcd", None) is not None else 0)
+        if msg is None:
+            return
+        with torch.cuda.stream(self._stream):
+            self._ring.zero_()
+            self._psync.zero_()
+            self._pstatus.zero_()
+            dcd = getattr(self, "dcd", None)
+            if dcd is not None:
+                dcd.buf.reset()
+        self._stream.synchronize()
+        raise RuntimeError(msg)
+
     def synchronize(self) -> None:
         self._stream.synchronize()
+        self._check_status()
 
     # ------------------------------------------- reference engine primitives
     def integrate(self) -> None:
@@ -428,7 +496,7 @@ class XpbdEngine:
 
     # ------------------------------------------------------ user-order views
     def _to_user(self, t4: torch.Tensor, ncol: int = 3) -> np.ndarray:
-        self._stream.synchronize()
+        self.synchronize()
         a = t4[:, :ncol].cpu().numpy()
         out = np.empty_like(a)
         out[self.layout.perm] = a

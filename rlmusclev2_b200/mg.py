@@ -594,7 +594,7 @@ class MultiGridSim(MuscleSim):
                                          3, self._sp))
         with torch.cuda.stream(self._stream):
             self._pos_host.copy_(self._pos_user, non_blocking=True)
-        self._stream.synchronize()
+        self.synchronize()  # raises on a fatal status bit of the frames before
         out = torch.empty((self.NV, 3), dtype=torch.float32)
         out.copy_(self._pos_host)  # multi-threaded host copy out of the pinned buffer
         return out.numpy()
@@ -714,7 +714,10 @@ class MultiGridSim(MuscleSim):
                 fn(it)
 
     def step_frame(self, frame: int) -> None:
-        """mg.py:1409-1418: kinematic step then nsubsteps substeps at that pose."""
+        """mg.py:1409-1418: kinematic step then nsubsteps substeps at that pose.
+        Raises if an earlier frame's status word (checked without waiting)
+        shows a barrier timeout or an accumulator overflow."""
+        self._check_status()
         if self._frame_loaded != frame:
             self.load_frame_targets(frame)
         if self._fusable():
@@ -725,4 +728,5 @@ class MultiGridSim(MuscleSim):
                 self.fascia.advect()
             for _ in range(self.nsubsteps):
                 self.substep()
+        self._post_status()
         self.step_cnt += 1

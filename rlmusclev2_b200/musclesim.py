@@ -129,12 +129,14 @@ class MuscleSim(XpbdEngine):
 
     def step(self):
         """One frame (musclesim.py:136-142)."""
+        self._check_status()
         if self._hooks():
             if getattr(self, "program", None) is None:
                 self.build_program()
             self.run_program()
         else:
             self._graph("frame", self._frame_fused)
+        self._post_status()
         self.step_cnt += 1
 
     def step_eager(self):

@@ -216,3 +216,32 @@ def test_config3_full_size_runs():
     print(f"config3 full: dcd {st}, metrics {m}, coarse nv {sim.mg.coarse.n_verts}")
     assert np.isfinite(p).all() and m["n_nonfinite"] == 0
     assert st["status"] == 0 and st["n_pairs"] > 10000
+
+
+def test_status_bit_raises_and_next_frame_runs_full_barriers():
+    """A barrier timeout bit in the status word (set from the host here: no
+    wait is made to run out) makes the next synchronising read raise; the
+    check clears the barrier words, ring and status, so a frame stepped
+    after it from the same state as an untouched simulator gives the same
+    positions (full barriers again, not the early exits a sticky bit causes)."""
+    from rlmusclev2_b200 import _capi as capi
+    cfg, sc = _small()
+    a, b = MultiGridSim(cfg, scene=sc), MultiGridSim(cfg, scene=sc)
+    for s in (a, b):
+        s.step_frame(1)
+    with torch.cuda.stream(a._stream):
+        a._pstatus.fill_(capi.STATUS_BARRIER_TIMEOUT)
+    a.step_frame(2)  # every barrier of this frame gives up after a few polls
+    with pytest.raises(RuntimeError, match="grid barrier"):
+        a.positions_np()
+    assert a.persistent_status(reset=False) == 0
+    assert int(a._psync.abs().sum().item()) == 0
+    b.step_frame(2)
+    a.set_positions(b.positions_np(), also_prev=True)
+    a.set_velocities(b.vel.numpy())
+    for s in (a, b):
+        s.step_frame(3)
+    err = float(np.abs(a.positions_np() - b.positions_np()).max())
+    tol = 1e-5 * bbox_diag(sc.verts)
+    print(f"after the cleared timeout: max |a - b| = {err:.3e} m (tol {tol:.3e})")
+    assert err <= tol
