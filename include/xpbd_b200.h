@@ -84,11 +84,19 @@ typedef struct XpbdParams {
     int32_t tile_variant;        /* bit 0: flip the tile pass's CTAs/SM (default 3 at 80 regs for the
                                     ARAP/aniso set, 2 at up to 128 regs with volume/SNH/damping);
                                     bit 1: ARAP-SVD through the SVD even where the polar rotation applies;
-                                    bit 2: persistent pass loads the next tet's streams ahead (prefetch) */
+                                    bit 2: persistent pass loads the next tet's streams ahead (prefetch);
+                                    bit 3: persistent pass of the light set one tet per thread (default:
+                                    two tets per thread on packed FP32x2 arithmetic) */
     float acc_scale;             /* > 0: the tile passes sum each tet's corrections into shared memory as
                                     32-bit integers round(d * acc_scale) (native integer atomics; shared
                                     float atomics cost ~5x more) and read the sums back as float(sum) /
                                     acc_scale; xpbd_acc_scale_for_extent gives the value for a mesh */
+    float arap_skip_ssq;         /* ARAP-SVD leaves a tet out (no correction, not counted in the Jacobi
+                                    divisor) when sum((sigma-1)^2) is below a threshold: 0 selects the
+                                    reference's 1e-12 (solve_kernels.py:1257-1259), > 0 that value, < 0
+                                    no threshold (only an exact rotation is left out).  Whether a
+                                    near-rest tet passes 1e-12 is decided by FP32 rounding; parity tests
+                                    disable it to compare everything else at rounding level */
     int32_t* status;             /* optional [1]: XPBD_STATUS_ACC_RANGE is or-ed in when the sum of a single
                                     tet's 12 correction magnitudes exceeds 1/64 of the fixed-point range, or
                                     is NaN or Inf (a vertex sum can then wrap only with > 64 such tets) */

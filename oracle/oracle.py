@@ -765,3 +765,15 @@ def fascia_glue(pf, pm, restlen, compliance, fascia4, muscle4, dt, omega=1.0):
                       _p(np.ascontiguousarray(restlen, np.float32)), _p(np.ascontiguousarray(compliance, np.float32)),
                       _p(np.ascontiguousarray(fascia4, np.float32)), _p(m4), C.c_float(dt), C.c_float(omega))
     return m4
+
+
+def set_arap_skip(v: float) -> None:
+    """ARAP-SVD skip threshold on sum((sigma-1)^2) of both precisions: 0 the
+    reference's 1e-12, > 0 that value, < 0 none (an exact rotation only).
+    Process-wide state of the oracle library: restore 0 after use."""
+    L = lib()
+    for p in ("f32", "f64"):
+        f = getattr(L, f"orc_set_arap_skip_{p}")
+        f.argtypes = [C.c_double]
+        f.restype = None
+        f(float(v))

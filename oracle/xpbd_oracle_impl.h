@@ -292,6 +292,13 @@ typedef struct {
     REAL dt, contraction_ratio, fiber_stiffness_scale;
 } FN(ctx);
 
+/* ARAP-SVD skip threshold on sum((sigma-1)^2): the reference's 1e-12 unless a
+ * parity test disables it (orc_set_arap_skip; the CUDA path's
+ * XpbdParams.arap_skip_ssq < 0) to compare both sides without the FP32
+ * rounding decision it makes on near-rest tets. */
+static REAL FN(arap_skip) = (REAL)1.0e-12;
+void FN(orc_set_arap_skip)(double v) { FN(arap_skip) = v == 0.0 ? (REAL)1.0e-12 : (v < 0.0 ? (REAL)1.0e-38 : (REAL)v); }
+
 static int FN(con_arapsvd)(const FN(ctx) * X, int c, REAL out[4][3]) {
     REAL k = X->c_stiffness[c];
     if (k <= (REAL)0) return 0;
@@ -306,7 +313,7 @@ static int FN(con_arapsvd)(const FN(ctx) * X, int c, REAL out[4][3]) {
     FN(svdm)(F, &U, &s, &V);
     VEC sm1 = FN(mk)(s.x - (REAL)1, s.y - (REAL)1, s.z - (REAL)1);
     REAL ssq = sm1.x * sm1.x + sm1.y * sm1.y + sm1.z * sm1.z;
-    if (ssq < (REAL)1.0e-12) return 0;
+    if (ssq < FN(arap_skip)) return 0;
     REAL C = SQRT(ssq);
     REAL invC = (REAL)1 / C;
     REAL d0 = invC * sm1.x, d1 = invC * sm1.y, d2 = invC * sm1.z;

@@ -39,7 +39,7 @@ class XpbdParams(C.Structure):
                 ("quasi_static", C.c_int32), ("omega", C.c_float), ("contraction_ratio", C.c_float),
                 ("fiber_stiffness_scale", C.c_float), ("n_materials", C.c_int32),
                 ("n_attach_materials", C.c_int32), ("tile_variant", C.c_int32), ("acc_scale", C.c_float),
-                ("status", C.c_void_p),
+                ("arap_skip_ssq", C.c_float), ("status", C.c_void_p),
                 ("materials", XpbdMaterial * MAX_MATERIALS),
                 ("attach", XpbdAttachMaterial * MAX_ATTACH_MATERIALS)]
 

@@ -438,7 +438,7 @@ int launch_project(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V
 
 extern "C" {
 
-int xpbd_abi_version(void) { return 1; }
+int xpbd_abi_version(void) { return 2; }
 
 float xpbd_acc_scale_for_extent(float max_coord) {
     const double e = max_coord > 1e-9f ? double(max_coord) : 1e-9;

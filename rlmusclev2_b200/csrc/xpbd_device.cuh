@@ -232,8 +232,12 @@ __device__ __forceinline__ float arap_alpha_tilde(float k, float dt) {
     return alpha / (dt * dt);
 }
 
-__device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float at, float3 (&acc)[4],
-                                            bool force_svd = false) {
+__device__ __forceinline__ float arap_skip_threshold(float v) {
+    return v == 0.f ? 1.0e-12f : (v < 0.f ? 1.0e-38f : v);
+}
+
+__device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float at, float skip_ssq,
+                                            float3 (&acc)[4], bool force_svd = false) {
     M3 G;
     M3 R;
     float ssq;
@@ -246,7 +250,7 @@ __device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, cons
                 G.m[i][j] = F.m[i][j] - R.m[i][j];
                 ssq += G.m[i][j] * G.m[i][j];
             }
-        if (ssq < 1.0e-12f) return false;
+        if (ssq < skip_ssq) return false;
         const float invC = rsqrtf(ssq);
 #pragma unroll
         for (int i = 0; i < 3; ++i)
@@ -256,7 +260,7 @@ __device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, cons
         const Svd3 s = svd3(F);
         const float a = s.s0 - 1.f, b = s.s1 - 1.f, c = s.s2 - 1.f;
         ssq = a * a + b * b + c * c;
-        if (ssq < 1.0e-12f) return false;
+        if (ssq < skip_ssq) return false;
         const float invC = 1.f / sqrtf(ssq);
         const float d0 = invC * a, d1 = invC * b, d2 = invC * c;
         const float U[3][3] = {{s.u0.x, s.u1.x, s.u2.x}, {s.u0.y, s.u1.y, s.u2.y}, {s.u0.z, s.u1.z, s.u2.z}};

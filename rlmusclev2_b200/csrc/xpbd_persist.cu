@@ -18,6 +18,7 @@
 #include "xpbd_common.cuh"
 #include "xpbd_grid.cuh"
 #include "xpbd_tile.cuh"
+#include "xpbd_tile_x2.cuh"
 
 using namespace xpbd;
 
@@ -26,7 +27,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr size_t kSmemPerVert = 4 * sizeof(float4) + 4 * sizeof(float) + 2 * sizeof(int);  // 88 bytes
 
-template <bool DAMP, int MINB, int CSET, bool PF>
+template <bool DAMP, int MINB, int CSET, bool PF, bool X2>
 __global__ void __launch_bounds__(kThreads, MINB)
     k_iterate_persistent(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdTiles T,
                          const __grid_constant__ XpbdVerts V, const __grid_constant__ XpbdPersist P, int n_iters) {
@@ -85,7 +86,10 @@ __global__ void __launch_bounds__(kThreads, MINB)
             s_cnt[i] = 0;
         }
         __syncthreads();
-        project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at);
+        if constexpr (X2 && CSET == CSET_LIGHT && !DAMP)
+            project_tile_tets_x2(prm, T, tile, s_pos, s_ax, s_ay, s_az, s_cnt, s_arap_at);
+        else
+            project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at);
         __syncthreads();
         for (int i = threadIdx.x; i < nint; i += blockDim.x) {
             float4 pp = s_pos[i];
@@ -127,10 +131,10 @@ uint32_t material_union(const XpbdParams* p) {
     return u;
 }
 
-template <bool DAMP, int MINB, int CSET, bool PF>
+template <bool DAMP, int MINB, int CSET, bool PF, bool X2 = false>
 int launch_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, const XpbdPersist* P, int n_iters,
              cudaStream_t s, bool query_only, int* fits) {
-    auto kern = k_iterate_persistent<DAMP, MINB, CSET, PF>;
+    auto kern = k_iterate_persistent<DAMP, MINB, CSET, PF, X2>;
     const size_t smem = size_t(T->max_tile_verts) * kSmemPerVert;
     if (smem > kSmemOptIn &&
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
@@ -183,6 +187,9 @@ int dispatch(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, cons
         if (damp) return flip ? XPBD_LAUNCH(true, 3, CSET_VOL) : XPBD_LAUNCH(true, 2, CSET_VOL);
         return flip ? XPBD_LAUNCH(false, 3, CSET_VOL) : XPBD_LAUNCH(false, 2, CSET_VOL);
     }
+    // the light set runs the two-tet packed pass (2 CTAs/SM at up to 128
+    // registers) unless tile_variant bit 3 asks for the one-tet pass
+    if (!(prm->tile_variant & 8)) return launch_v<false, 2, CSET_LIGHT, false, true>(prm, T, V, P, n_iters, s, query_only, fits);
     return flip ? XPBD_LAUNCH(false, 2, CSET_LIGHT) : XPBD_LAUNCH(false, 3, CSET_LIGHT);
 #undef XPBD_LAUNCH
 }

@@ -86,6 +86,7 @@ __device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const X
                                                   const float4* s_pos, const float4* s_prev, int* s_ax, int* s_ay,
                                                   int* s_az, int* s_cnt, const float* s_arap_at) {
     const float acc_scale = prm.acc_scale;
+    const float arap_skip = arap_skip_threshold(prm.arap_skip_ssq);
     const int t1 = T.tile_tptr[tile + 1];
     const uint4* tq = reinterpret_cast<const uint4*>(T.tet_q);
     const float4* tb0 = reinterpret_cast<const float4*>(T.tet_b0);
@@ -159,8 +160,8 @@ __device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const X
                           prm.fiber_stiffness_scale, prm.dt, d))
                 nact += 1;
         }
-        if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, s_arap_at[min(int(q.z & 0xffu), XPBD_MAX_MATERIALS - 1)], d,
-                                                   (prm.tile_variant & 2) != 0))
+        if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, s_arap_at[min(int(q.z & 0xffu), XPBD_MAX_MATERIALS - 1)],
+                                                   arap_skip, d, (prm.tile_variant & 2) != 0))
             nact += 1;
         if (nact != 0) {
             // Range check on the sum of the 12 |components| (not their maximum:

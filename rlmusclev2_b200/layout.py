@@ -75,13 +75,11 @@ class TileLayout:
 
 
 def ctas_per_sm(materials: list[dict]) -> int:
-    """Resident CTAs per SM of the tile pass the library launches for these
-    materials: 3 for the light constraint set (ARAP-SVD / aniso only, no
-    damping), 2 when any material has volume, SNH or damping."""
-    u = 0
-    for m in materials:
-        u |= int(m["flags"])
-    return 2 if u & (capi.MAT_VOLUME | capi.MAT_SNH | capi.MAT_DAMPED) else 3
+    """Resident CTAs per SM of the persistent tile pass the library launches
+    for these materials: 2 for every set (the light set -- ARAP-SVD / aniso
+    only, no damping -- runs two tets per thread at up to 128 registers; the
+    sets with volume, SNH or damping one tet per thread at up to 128)."""
+    return 2
 
 
 def default_tile_tets(n_tets: int, n_sm: int = 148, ctas: int = 3, max_tile: int = 2048) -> int:

@@ -28,7 +28,7 @@ def test_library_loads_and_exports_declared_symbols():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(capi.exported_symbols()) <= declared | set()
-    assert lib.xpbd_abi_version() == 1
+    assert lib.xpbd_abi_version() == 2
 
 
 def test_struct_sizes_match_header_layout():
