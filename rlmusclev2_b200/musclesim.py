@@ -1,11 +1,13 @@
 """MuscleSim on the sm_100a engine (reference: src/muscle/musclesim.py).
 
 ``MuscleSim.from_procedural`` (musclesim.py:181-287) is the no-asset entry
-point; file-based construction needs the reference's Houdini/USD readers,
-which are not part of this project.
+point; ``MuscleSim(cfg)`` (musclesim.py:44-92) reads the rest mesh from a
+Houdini ``.geo`` file at ``cfg.geo_path`` (USD needs ``pxr``, which is not
+installed here).
 """
 from __future__ import annotations
 
+from pathlib import Path
 from types import SimpleNamespace
 
 import numpy as np
@@ -18,9 +20,34 @@ from .engine import XpbdEngine
 class MuscleSim(XpbdEngine):
     """XPBD muscle simulator: one Jacobi projection per substep."""
 
-    def __init__(self, cfg):
-        raise NotImplementedError("MuscleSim(cfg) loads .geo/.usd assets, which this project does not read; "
-                                  "use MuscleSim.from_procedural(...)")
+    def __init__(self, cfg, device: str = "cuda:0"):
+        """MuscleSim(cfg) (musclesim.py:44-92): the rest mesh from ``cfg.geo_path``
+        (a Houdini ``.geo`` tet mesh: points, tets, the ``materialW`` fiber field
+        and ``tendonmask``, read by geo.scene_from_geo), the constraint blocks of
+        ``cfg.constraints``, ``dt`` / ``num_substeps``, ``density``,
+        ``veldamping``, ``gravity`` (along Y), ``contraction_ratio``,
+        ``fiber_stiffness_scale``.  ``cfg`` is a dict or an attribute object
+        (the reference's SimConfig)."""
+        get = (lambda k, d=None: cfg.get(k, d)) if isinstance(cfg, dict) else (lambda k, d=None: getattr(cfg, k, d))
+        path = get("geo_path")
+        if not path:
+            raise ValueError("MuscleSim(cfg) needs cfg.geo_path (or use MuscleSim.from_procedural)")
+        path = Path(path)
+        if path.suffix.lower() != ".geo":
+            raise NotImplementedError(f"{path.name}: only Houdini .geo rest meshes are read (USD needs pxr, which is "
+                                      "not installed)")
+        if not path.exists():
+            raise FileNotFoundError(f"geo_path {path} does not exist")
+        from .geo import scene_from_geo
+        sc = scene_from_geo(path)
+        tendon_tet = (sc.v_tendon[sc.tets].astype(np.float32).sum(1) / np.float32(4.0)).astype(np.float32)
+        self._build(sc.verts, sc.tets, sc.v_fiber, cfg=cfg, constraint_configs=list(get("constraints") or []),
+                    dts=float(get("dt", 1.0 / 24.0)), num_substeps=int(get("num_substeps", 1)), device=device,
+                    density=float(get("density", 1060.0)), veldamping=float(get("veldamping", 0.02)),
+                    gravity=float(get("gravity", 0.0)), contraction_ratio=float(get("contraction_ratio", 0.4)),
+                    fiber_stiffness_scale=float(get("fiber_stiffness_scale", 10000.0)),
+                    quasi_static=bool(get("quasi_static", False)), tet_tendonmask=tendon_tet,
+                    v_tendonmask=sc.v_tendon)
 
     @classmethod
     def from_procedural(cls, vertices, tets, fiber_dirs_per_tet, bone_targets=None, *, constraint_configs, dts,
@@ -57,36 +84,51 @@ class MuscleSim(XpbdEngine):
             activation=0.0, nsteps=1, sigma0=sigma0, lambda_opt=lambda_opt, v_max_norm=v_max_norm, d_damp=d_damp,
             relaxation=relaxation)
         sim = object.__new__(cls)
-        sim.cfg = cfg
-        sim.constraint_configs = cfg.constraints
-        sim.pos0_np = vertices
-        sim.tet_np = tets
-        sim.v_fiber_np = vf
-        sim.v_tendonmask_np = None
-        sim.n_verts = n_v
-        sim.bone_pos = (np.asarray(bone_targets, np.float32) if bone_targets is not None
-                        else np.zeros((0, 3), np.float32))
-        sim.use_jacobi = True
-        sim.use_colored_gs = False
-        sim.contraction_ratio = contraction_ratio
-        sim.fiber_stiffness_scale = fiber_stiffness_scale
-        sim.has_compressstiffness = False
-        sim.num_substeps = int(num_substeps)
-        sim.quasi_static = False
-        sim.step_cnt = 0
-        sim.renderer = None
-        mass, rest_volume = lumped_mass(vertices, tets, density)
-        sim.rest_volume_np = rest_volume
-        sim.total_rest_volume = float(rest_volume.astype(np.float64).sum())
-        table = collect_raw_constraints(vertices, tets, sim.constraint_configs, tet_masks).sorted_by_type()
-        sim.raw_constraints = table
-        st = np.zeros(n_v, np.int32) if stopped is None else np.asarray(stopped, np.int32)
-        sim._setup_device(device, mass=mass, stopped=st, table=table, v_fiber=vf, tet_tendonmask=None,
-                          dt=float(dts) / int(num_substeps), gravity_vec=(0.0, float(gravity), 0.0),
-                          veldamping=float(veldamping), quasi_static=False, omega=float(relaxation),
-                          contraction_ratio=contraction_ratio, fiber_stiffness_scale=fiber_stiffness_scale,
-                          tile_tets=tile_tets)
+        sim._build(vertices, tets, vf, cfg=cfg, constraint_configs=cfg.constraints, dts=dts,
+                   num_substeps=num_substeps, device=device, density=density, veldamping=veldamping, gravity=gravity,
+                   contraction_ratio=contraction_ratio, fiber_stiffness_scale=fiber_stiffness_scale, stopped=stopped,
+                   relaxation=relaxation, tile_tets=tile_tets, tet_masks=tet_masks, bone_targets=bone_targets)
         return sim
+
+    def _build(self, vertices, tets, v_fiber, *, cfg, constraint_configs, dts, num_substeps, device, density,
+               veldamping, gravity, contraction_ratio, fiber_stiffness_scale, stopped=None, relaxation=1.0,
+               tile_tets=None, tet_masks=None, bone_targets=None, quasi_static=False, tet_tendonmask=None,
+               v_tendonmask=None) -> None:
+        """Common set-up of both constructors: constraint table, lumped mass,
+        device state."""
+        vertices = np.asarray(vertices, dtype=np.float32)
+        tets = np.asarray(tets, dtype=np.int32)
+        n_v = vertices.shape[0]
+        self.cfg = cfg
+        self.constraint_configs = list(constraint_configs)
+        self.pos0_np = vertices
+        self.tet_np = tets
+        self.v_fiber_np = np.asarray(v_fiber, np.float32)
+        self.v_tendonmask_np = v_tendonmask
+        self.n_verts = n_v
+        self.bone_pos = (np.asarray(bone_targets, np.float32) if bone_targets is not None
+                         else np.zeros((0, 3), np.float32))
+        self.use_jacobi = True
+        self.use_colored_gs = False
+        self.contraction_ratio = contraction_ratio
+        self.fiber_stiffness_scale = fiber_stiffness_scale
+        self.has_compressstiffness = False
+        self.num_substeps = int(num_substeps)
+        self.quasi_static = bool(quasi_static)
+        self.step_cnt = 0
+        self.renderer = None
+        mass, rest_volume = lumped_mass(vertices, tets, density)
+        self.rest_volume_np = rest_volume
+        self.total_rest_volume = float(rest_volume.astype(np.float64).sum())
+        table = collect_raw_constraints(vertices, tets, self.constraint_configs, tet_masks).sorted_by_type()
+        self.raw_constraints = table
+        st = np.zeros(n_v, np.int32) if stopped is None else np.asarray(stopped, np.int32)
+        self._setup_device(device, mass=mass, stopped=st, table=table, v_fiber=self.v_fiber_np,
+                           tet_tendonmask=tet_tendonmask, dt=float(dts) / int(num_substeps),
+                           gravity_vec=(0.0, float(gravity), 0.0), veldamping=float(veldamping),
+                           quasi_static=bool(quasi_static), omega=float(relaxation),
+                           contraction_ratio=contraction_ratio, fiber_stiffness_scale=fiber_stiffness_scale,
+                           tile_tets=tile_tets)
 
     # ---------------------------------------------------------------- program
     def build_program(self):

@@ -6,7 +6,7 @@ parsed by the reference's own reader (src/muscle/util/geo_io.py GeoFile); its
 results go to geo_small_ref.npz.  Run from the repository root in a container
 that has the reference checkout:
 
-    python tests/golden/make_geo_golden.py /root/reference
+    python tests/golden/make_geo_golden.py <reference checkout>
 """
 import sys
 from pathlib import Path
@@ -52,4 +52,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of the reference checkout>")
+    main(sys.argv[1])

@@ -4,7 +4,7 @@ src/muscle/util/mesh_utils.py, src/muscle/util/activation.py,
 src/muscle/defs.py).  Those modules need only numpy and scipy, so they are
 imported from a checkout of the reference; the Warp kernels are not.
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 writes builder_small.npz.  The fixture is committed; the tests read only the
 .npz and never the reference.
@@ -91,4 +91,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of the reference checkout>")
+    main(sys.argv[1])

@@ -61,3 +61,30 @@ def test_geo_asset_with_cons_frames_matches_the_synthetic_run(tmp_path):
     print(f"geo asset run vs synthetic run: max |diff| {err:.2e} m")
     assert np.isfinite(pg).all()
     assert err < 1e-6
+
+
+def test_musclesim_from_geo_config_matches_from_procedural(tmp_path):
+    """MuscleSim(cfg) (musclesim.py:44-92) on a .geo rest mesh: the box muscle
+    written out with its per-vertex fiber field steps exactly like
+    MuscleSim.from_procedural on the same arrays."""
+    from rlmusclev2_b200 import MuscleSim
+    from tests._cases import CFG1, CFG1_CONSTRAINTS, cfg1_mesh
+    m = cfg1_mesh()
+    vf = np.tile(np.array([0.0, 0.0, 1.0], np.float32), (m.verts.shape[0], 1))
+    write_geo(tmp_path / "box.geo", m.verts, m.tets, point_attrs={"materialW": vf})
+    cfg = dict(geo_path=str(tmp_path / "box.geo"), constraints=CFG1_CONSTRAINTS, dt=CFG1["dts"],
+               num_substeps=CFG1["num_substeps"], density=CFG1["density"], veldamping=CFG1["veldamping"],
+               gravity=CFG1["gravity"], contraction_ratio=0.0, fiber_stiffness_scale=1.0)
+    a = MuscleSim(cfg)
+    b = MuscleSim.from_procedural(m.verts, m.tets, m.fiber_per_tet, constraint_configs=CFG1_CONSTRAINTS,
+                                  device="cuda:0", **CFG1)
+    for s in (a, b):
+        s.stopped = m.stopped
+    for _ in range(2):
+        a.step()
+        b.step()
+    err = float(np.abs(a.positions_np() - b.positions_np()).max())
+    print(f"MuscleSim(cfg) from .geo vs from_procedural: max |diff| {err:.2e} m")
+    assert err <= 1e-7
+    with pytest.raises(NotImplementedError, match="only Houdini .geo"):
+        MuscleSim(dict(cfg, geo_path=str(tmp_path / "box.usd")))
