@@ -414,7 +414,11 @@ class OracleMultiGridSim(OracleSolver):
     def _init_mg(self, mu):
         from rlmusclev2_b200.meshgen import build_cage  # synthetic input geometry only
         cfg, P = self.cfg, self.P
-        cage = build_cage(self.scene, spacing=float(cfg.get("mg_cage_spacing", 0.016)))
+        cage = build_cage(self.scene, spacing=float(cfg.get("mg_cage_spacing", 0.016)),
+                          operator=str(cfg.get("mg_restrict_operator", "tikhonov")))
+        # "residual": prior + Minv P^T (x - P prior); "direct": Minv P^T x, the
+        # reference's scatter + block solve (mg/kernel.py:137-178) as written
+        self.mg_form = str(cfg.get("mg_restrict_form", "residual"))
         self.cage = cage
         emb = np.nonzero(cage.cage_idx >= 0)[0]
         self.mg_emb = emb
@@ -459,6 +463,8 @@ class OracleMultiGridSim(OracleSolver):
         P = self.P
         nc = self.cage.coarse_pos.shape[0]
         prior = prior.astype(P.dt)
+        if getattr(self, "mg_form", "residual") == "direct":
+            prior = np.zeros_like(prior)
         w, t = self.mg_w, self.mg_t
         xe = x[self.mg_emb].astype(P.dt)
         r = xe - (((w[:, 0:1] * prior[t[:, 0]] + w[:, 1:2] * prior[t[:, 1]]) + w[:, 2:3] * prior[t[:, 2]])

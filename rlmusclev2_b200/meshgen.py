@@ -531,10 +531,14 @@ def _bary(p, a, b, c, d):
     return np.concatenate([(1.0 - w.sum(-1))[..., None], w], -1)
 
 
-def build_cage(scene: "Scene", spacing: float = 0.016, rel_lam: float = 1e-3) -> Cage:
+def build_cage(scene: "Scene", spacing: float = 0.016, rel_lam: float = 1e-3, operator: str = "tikhonov") -> Cage:
     """Coarse cage: for every muscle a ``spacing`` hex lattice in the muscle's
     local frame over the cells that hold its fine vertices; fascia vertices are
-    not embedded."""
+    not embedded.  ``operator`` picks the per-muscle restriction block:
+    "pinv" the reference's pinv(P^T P, rcond=1e-8) (tools/gen_coarse_cage.py:221),
+    "tikhonov" inv(P^T P + lam I) with lam = rel_lam x the median diagonal."""
+    if operator not in ("tikhonov", "pinv"):
+        raise ValueError(f"operator must be 'tikhonov' or 'pinv', got {operator!r}")
     nv = scene.verts.shape[0]
     cage_idx = np.full(nv, -1, np.int64)
     uvw = np.zeros((nv, 3))
@@ -610,8 +614,12 @@ def build_cage(scene: "Scene", spacing: float = 0.016, rel_lam: float = 1e-3) ->
     # a small Tikhonov weight toward the previous coarse state, so that cage
     # corners carrying almost no fine weight stay where they were instead of
     # amplifying FP32 noise (lam = rel_lam x median diagonal of P^T P).
-    lam = rel_lam * float(np.median(np.concatenate([np.diag(B) for B in blocks])))
-    blocks = [np.linalg.inv(B + lam * np.eye(B.shape[0])) for B in blocks]
+    if operator == "pinv":
+        lam = 0.0
+        blocks = [np.linalg.pinv(B, rcond=1e-8) for B in blocks]
+    else:
+        lam = rel_lam * float(np.median(np.concatenate([np.diag(B) for B in blocks])))
+        blocks = [np.linalg.inv(B + lam * np.eye(B.shape[0])) for B in blocks]
     blk_base, blk_dim, blk_matoff, flat = [], [], [], []
     off = base = 0
     for B in blocks:
