@@ -17,6 +17,7 @@
 #include "xpbd_common.cuh"
 #include "xpbd_device.cuh"
 #include "xpbd_tile.cuh"
+#include "xpbd_tile_x2.cuh"
 
 using namespace xpbd;
 
@@ -32,7 +33,7 @@ namespace {
 constexpr int kTileThreads = 256;
 constexpr int kVertThreads = 256;
 
-template <int MODE, bool DAMP, int MINB, int CSET>
+template <int MODE, bool DAMP, int MINB, int CSET, bool X2 = false>
 __global__ void __launch_bounds__(kTileThreads, MINB)
     k_project_tiles(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdTiles T,
                     const __grid_constant__ XpbdVerts V, uint32_t finish_ops) {
@@ -68,7 +69,10 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     }
     __syncthreads();
 
-    project_tile_tets<DAMP, CSET>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at);
+    if constexpr (X2 && CSET != CSET_FULL && !DAMP)
+        project_tile_tets_x2<CSET == CSET_VOL>(prm, T, tile, s_pos, s_ax, s_ay, s_az, s_cnt, s_arap_at);
+    else
+        project_tile_tets<DAMP, CSET>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at);
     __syncthreads();
 
     float4* pos4w = reinterpret_cast<float4*>(V.pos);
@@ -393,7 +397,7 @@ bool any_aniso(const XpbdParams* p) {
     return false;
 }
 
-template <int MODE, bool DAMP, int MINB, int CSET>
+template <int MODE, bool DAMP, int MINB, int CSET, bool X2 = false>
 int launch_project_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
     const size_t smem = size_t(T->max_tile_verts) * sizeof(float4) * (DAMP ? 3 : 2);  // pos, [prev], 4 x float acc
     if (smem > kSmemOptIn) {
@@ -401,12 +405,12 @@ int launch_project_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts*
         int dev = 0;
         cudaGetDevice(&dev);
         if (dev < 0 || dev >= 64 || !done[dev]) {
-            cudaFuncSetAttribute(k_project_tiles<MODE, DAMP, MINB, CSET>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_project_tiles<MODE, DAMP, MINB, CSET, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(XPBD_MAX_TILE_VERTS * sizeof(float4) * 3));
             if (dev >= 0 && dev < 64) done[dev] = 1;
         }
     }
-    k_project_tiles<MODE, DAMP, MINB, CSET><<<T->n_tiles, kTileThreads, smem, s>>>(*prm, *T, *V, fops);
+    k_project_tiles<MODE, DAMP, MINB, CSET, X2><<<T->n_tiles, kTileThreads, smem, s>>>(*prm, *T, *V, fops);
     return cuda_check("xpbd_project");
 }
 
@@ -416,13 +420,19 @@ uint32_t material_union(const XpbdParams* p) {
     return u;
 }
 
-// Instance choice: the smallest constraint set covering the materials; the
-// light set runs 3 CTAs per SM (80 registers, no spills), the others 2
-// (bit 0 of tile_variant flips that choice).
+// Instance choice: the smallest constraint set covering the materials.
+// Undamped light and volume sets run two tets per thread on packed FP32x2
+// arithmetic (2 CTAs per SM) unless bit 3 of tile_variant asks for one tet
+// per thread; there the light set runs 3 CTAs per SM (80 registers, no
+// spills), the others 2 (bit 0 of tile_variant flips that choice).
 template <int MODE, bool DAMP>
 int launch_project(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
     const uint32_t u = material_union(prm);
     const bool flip = (prm->tile_variant & 1) != 0;
+    if (!DAMP && !(prm->tile_variant & 8) && !(u & XPBD_MAT_SNH)) {
+        if (u & XPBD_MAT_VOLUME) return launch_project_v<MODE, false, 2, CSET_VOL, true>(prm, T, V, fops, s);
+        return launch_project_v<MODE, false, 2, CSET_LIGHT, true>(prm, T, V, fops, s);
+    }
     if (u & XPBD_MAT_SNH)
         return flip ? launch_project_v<MODE, DAMP, 3, CSET_FULL>(prm, T, V, fops, s)
                     : launch_project_v<MODE, DAMP, 2, CSET_FULL>(prm, T, V, fops, s);

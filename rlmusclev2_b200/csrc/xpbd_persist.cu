@@ -86,8 +86,8 @@ __global__ void __launch_bounds__(kThreads, MINB)
             s_cnt[i] = 0;
         }
         __syncthreads();
-        if constexpr (X2 && CSET == CSET_LIGHT && !DAMP)
-            project_tile_tets_x2(prm, T, tile, s_pos, s_ax, s_ay, s_az, s_cnt, s_arap_at);
+        if constexpr (X2 && CSET != CSET_FULL && !DAMP)
+            project_tile_tets_x2<CSET == CSET_VOL>(prm, T, tile, s_pos, s_ax, s_ay, s_az, s_cnt, s_arap_at);
         else
             project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at);
         __syncthreads();
@@ -185,6 +185,7 @@ int dispatch(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, cons
     }
     if (u & XPBD_MAT_VOLUME) {
         if (damp) return flip ? XPBD_LAUNCH(true, 3, CSET_VOL) : XPBD_LAUNCH(true, 2, CSET_VOL);
+        if (!(prm->tile_variant & 8)) return launch_v<false, 2, CSET_VOL, false, true>(prm, T, V, P, n_iters, s, query_only, fits);
         return flip ? XPBD_LAUNCH(false, 3, CSET_VOL) : XPBD_LAUNCH(false, 2, CSET_VOL);
     }
     // the light set runs the two-tet packed pass (2 CTAs/SM at up to 128

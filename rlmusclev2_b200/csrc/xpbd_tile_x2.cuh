@@ -145,7 +145,10 @@ __device__ __forceinline__ void acc_tet(const int (&l)[4], const float3 (&d)[4],
 
 // Projects the tile's tets two per thread per round: tets a = t0 + tid +
 // 2 k T and b = a + T (T threads).  Same contract as project_tile_tets for
-// the light constraint set (ARAP-SVD and aniso_arap, no damping).
+// the light constraint set (ARAP-SVD and aniso_arap) and, with VOL, the
+// volume constraint too; no damping (damped materials read pprev and take
+// the one-tet pass).
+template <bool VOL>
 __device__ __forceinline__ void project_tile_tets_x2(const XpbdParams& prm, const XpbdTiles& T, int tile,
                                                      const float4* s_pos, int* s_ax, int* s_ay, int* s_az,
                                                      int* s_cnt, const float* s_arap_at) {
@@ -277,6 +280,52 @@ __device__ __forceinline__ void project_tile_tets_x2(const XpbdParams& prm, cons
                     db[2] = make_float3(e2.x.y, e2.y.y, e2.z.y);
                     db[3] = make_float3(e3.x.y, e3.y.y, e3.z.y);
                     nb = 1;
+                }
+            }
+        }
+        // volume (tet_volume_update_xpbd_fn, solve_kernels.py:187-281, undamped):
+        // gradients are the face cross products / 6 (pt3 reference), C = V - V0
+        if constexpr (VOL) {
+            const bool vola = (fa & XPBD_MAT_VOLUME) != 0, volb = hb && (fb & XPBD_MAT_VOLUME) != 0;
+            if (vola || volb) {
+                const f2 sixth = pk(1.f / 6.f, 1.f / 6.f);
+                const V2 c0 = vcross2(d1, d2), c1 = vcross2(d2, d0), c2 = vcross2(d0, d1);
+                const f2 vol = mul2(vdot2(c2, d2), sixth);
+                const V2 v0 = {mul2(c0.x, sixth), mul2(c0.y, sixth), mul2(c0.z, sixth)};
+                const V2 v1 = {mul2(c1.x, sixth), mul2(c1.y, sixth), mul2(c1.z, sixth)};
+                const V2 v2 = {mul2(c2.x, sixth), mul2(c2.y, sixth), mul2(c2.z, sixth)};
+                const V2 s01 = {add2(v0.x, v1.x), add2(v0.y, v1.y), add2(v0.z, v1.z)};
+                const V2 v3 = {neg2(add2(s01.x, v2.x)), neg2(add2(s01.y, v2.y)), neg2(add2(s01.z, v2.z))};
+                f2 ws = mul2(w0, vdot2(v0, v0));
+                ws = fma2(w1, vdot2(v1, v1), ws);
+                ws = fma2(w2, vdot2(v2, v2), ws);
+                ws = fma2(w3, vdot2(v3, v3), ws);
+                const bool oka = vola && ws.x > 1e-9f, okb = volb && ws.y > 1e-9f;
+                if (oka || okb) {
+                    const float dt2 = prm.dt * prm.dt;
+                    const f2 alpha = pk((1.f / prm.materials[ma].vol_k) / dt2, (1.f / prm.materials[mb].vol_k) / dt2);
+                    const f2 C = sub2(vol, pk(__uint_as_float(qa.w), __uint_as_float(qb.w)));
+                    const f2 den = add2(ws, alpha);
+                    const f2 dl = pk(-C.x / den.x, -C.y / den.y);
+                    const f2 s0 = mul2(dl, w0), s1 = mul2(dl, w1), s2 = mul2(dl, w2), s3 = mul2(dl, w3);
+                    const V2 e0 = {mul2(s0, v0.x), mul2(s0, v0.y), mul2(s0, v0.z)};
+                    const V2 e1 = {mul2(s1, v1.x), mul2(s1, v1.y), mul2(s1, v1.z)};
+                    const V2 e2 = {mul2(s2, v2.x), mul2(s2, v2.y), mul2(s2, v2.z)};
+                    const V2 e3 = {mul2(s3, v3.x), mul2(s3, v3.y), mul2(s3, v3.z)};
+                    if (oka) {
+                        da[0] = da[0] + make_float3(e0.x.x, e0.y.x, e0.z.x);
+                        da[1] = da[1] + make_float3(e1.x.x, e1.y.x, e1.z.x);
+                        da[2] = da[2] + make_float3(e2.x.x, e2.y.x, e2.z.x);
+                        da[3] = da[3] + make_float3(e3.x.x, e3.y.x, e3.z.x);
+                        na += 1;
+                    }
+                    if (okb) {
+                        db[0] = db[0] + make_float3(e0.x.y, e0.y.y, e0.z.y);
+                        db[1] = db[1] + make_float3(e1.x.y, e1.y.y, e1.z.y);
+                        db[2] = db[2] + make_float3(e2.x.y, e2.y.y, e2.z.y);
+                        db[3] = db[3] + make_float3(e3.x.y, e3.y.y, e3.z.y);
+                        nb += 1;
+                    }
                 }
             }
         }
