@@ -111,12 +111,16 @@ class MultiGridSim(MuscleSim):
                                       "(supported: 'aniso_arap')")
         if scene is None and "synthetic" not in cfg and cfg.get("rest_path"):
             rp = Path(cfg["rest_path"])
-            if rp.suffix.lower() != ".geo":
-                raise NotImplementedError(f"rest mesh {rp.name}: only Houdini .geo assets are read (no USD)")
+            if rp.suffix.lower() not in (".geo", ".usda", ".usd"):
+                raise NotImplementedError(f"rest mesh {rp.name}: Houdini .geo assets and text USD layers are read")
             if not rp.exists():
                 raise FileNotFoundError(f"rest_path {rp} does not exist")
-            from .geo import scene_from_geo
-            scene = scene_from_geo(rp)
+            if rp.suffix.lower() == ".geo":
+                from .geo import scene_from_geo
+                scene = scene_from_geo(rp)
+            else:
+                from .usd import scene_from_usda
+                scene = scene_from_usda(rp, cfg.get("rest_prim_path"))
         self.scene = scene if scene is not None else scene_from_cfg(cfg)
         sc = self.scene
         # kinematic targets (mg.py:436-446)

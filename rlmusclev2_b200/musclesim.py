@@ -2,8 +2,8 @@
 
 ``MuscleSim.from_procedural`` (musclesim.py:181-287) is the no-asset entry
 point; ``MuscleSim(cfg)`` (musclesim.py:44-92) reads the rest mesh from a
-Houdini ``.geo`` file at ``cfg.geo_path`` (USD needs ``pxr``, which is not
-installed here).
+Houdini ``.geo`` file or a text USD layer (``.usda``, read without pxr) at
+``cfg.geo_path``.
 """
 from __future__ import annotations
 
@@ -22,8 +22,9 @@ class MuscleSim(XpbdEngine):
 
     def __init__(self, cfg, device: str = "cuda:0"):
         """MuscleSim(cfg) (musclesim.py:44-92): the rest mesh from ``cfg.geo_path``
-        (a Houdini ``.geo`` tet mesh: points, tets, the ``materialW`` fiber field
-        and ``tendonmask``, read by geo.scene_from_geo), the constraint blocks of
+        (a Houdini ``.geo`` tet mesh, geo.scene_from_geo, or the TetMesh of a text
+        USD layer, usd.scene_from_usda, with ``cfg.geo_prim_path`` choosing the
+        prim: points, tets, the ``materialW`` fiber field and ``tendonmask``), the constraint blocks of
         ``cfg.constraints``, ``dt`` / ``num_substeps``, ``density``,
         ``veldamping``, ``gravity`` (along Y), ``contraction_ratio``,
         ``fiber_stiffness_scale``.  ``cfg`` is a dict or an attribute object
@@ -33,13 +34,17 @@ class MuscleSim(XpbdEngine):
         if not path:
             raise ValueError("MuscleSim(cfg) needs cfg.geo_path (or use MuscleSim.from_procedural)")
         path = Path(path)
-        if path.suffix.lower() != ".geo":
-            raise NotImplementedError(f"{path.name}: only Houdini .geo rest meshes are read (USD needs pxr, which is "
-                                      "not installed)")
+        if path.suffix.lower() not in (".geo", ".usda", ".usd"):
+            raise NotImplementedError(f"{path.name}: rest meshes are read from Houdini .geo files and text USD "
+                                      "layers (.usda)")
         if not path.exists():
             raise FileNotFoundError(f"geo_path {path} does not exist")
-        from .geo import scene_from_geo
-        sc = scene_from_geo(path)
+        if path.suffix.lower() == ".geo":
+            from .geo import scene_from_geo
+            sc = scene_from_geo(path)
+        else:
+            from .usd import scene_from_usda
+            sc = scene_from_usda(path, get("geo_prim_path"))
         tendon_tet = (sc.v_tendon[sc.tets].astype(np.float32).sum(1) / np.float32(4.0)).astype(np.float32)
         self._build(sc.verts, sc.tets, sc.v_fiber, cfg=cfg, constraint_configs=list(get("constraints") or []),
                     dts=float(get("dt", 1.0 / 24.0)), num_substeps=int(get("num_substeps", 1)), device=device,

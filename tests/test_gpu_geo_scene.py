@@ -64,9 +64,9 @@ def test_geo_asset_with_cons_frames_matches_the_synthetic_run(tmp_path):
 
 
 def test_musclesim_from_geo_config_matches_from_procedural(tmp_path):
-    """MuscleSim(cfg) (musclesim.py:44-92) on a .geo rest mesh: the box muscle
-    written out with its per-vertex fiber field steps exactly like
-    MuscleSim.from_procedural on the same arrays."""
+    """MuscleSim(cfg) (musclesim.py:44-92) on a .geo rest mesh and on a text
+    USD TetMesh: the box muscle written out with its per-vertex fiber field
+    steps exactly like MuscleSim.from_procedural on the same arrays."""
     from rlmusclev2_b200 import MuscleSim
     from tests._cases import CFG1, CFG1_CONSTRAINTS, cfg1_mesh
     m = cfg1_mesh()
@@ -86,5 +86,15 @@ def test_musclesim_from_geo_config_matches_from_procedural(tmp_path):
     err = float(np.abs(a.positions_np() - b.positions_np()).max())
     print(f"MuscleSim(cfg) from .geo vs from_procedural: max |diff| {err:.2e} m")
     assert err <= 1e-7
-    with pytest.raises(NotImplementedError, match="only Houdini .geo"):
-        MuscleSim(dict(cfg, geo_path=str(tmp_path / "box.usd")))
+    # the same mesh from a text USD layer (util/mesh_io.py:93-150 without pxr)
+    from rlmusclev2_b200.usd import write_usda_tetmesh
+    write_usda_tetmesh(tmp_path / "box.usda", m.verts, m.tets, {"materialW": vf})
+    c = MuscleSim(dict(cfg, geo_path=str(tmp_path / "box.usda")))
+    c.stopped = m.stopped
+    for _ in range(2):
+        c.step()
+    err_u = float(np.abs(c.positions_np() - b.positions_np()).max())
+    print(f"MuscleSim(cfg) from .usda vs from_procedural: max |diff| {err_u:.2e} m")
+    assert err_u <= 1e-7
+    with pytest.raises(NotImplementedError, match="rest meshes are read from"):
+        MuscleSim(dict(cfg, geo_path=str(tmp_path / "box.obj")))
