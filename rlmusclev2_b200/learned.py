@@ -276,6 +276,23 @@ class LearnedWarmStart:
                                                   C.c_void_p(vf) if vf else None, C.c_void_p(pt) if pt else None,
                                                   self.sp))
 
+    def ideal_warm_start(self) -> None:
+        """The warm start a perfect network would give: the cage moved by the
+        substep's true correction (``self.target``, from target_from_state),
+        prolongated onto the fine mesh (+ fine pins).  An evaluation device: it
+        bounds what any cage correction can do for the iterations after it."""
+        sim, mg = self.sim, self.mg
+        capi.check(self.lib.xpbd_cage_apply(self.nc, C.c_void_p(self._lib_d.data_ptr()),
+                                            C.c_void_p(mg.prev.data_ptr()), C.c_void_p(self.target.data_ptr()), 3,
+                                            C.c_float(1.0 / SCALE_MM), C.c_void_p(mg.coarse._pos4.data_ptr()),
+                                            self.sp))
+        vf = sim._vflags.data_ptr() if (self.pin and sim._vflags is not None) else None
+        pt = sim._pin_tgt.data_ptr() if (self.pin and sim._pin_tgt is not None) else None
+        capi.check(self.lib.xpbd_mg_prolong_delta(C.byref(mg.g), C.c_void_p(mg.coarse._pos4.data_ptr()),
+                                                  C.c_void_p(mg.prev.data_ptr()), C.c_void_p(sim._pos4.data_ptr()),
+                                                  C.c_void_p(vf) if vf else None, C.c_void_p(pt) if pt else None,
+                                                  self.sp))
+
     def iterate(self, n: int) -> None:
         self.sim._fused_iterations(n)
 
@@ -401,20 +418,21 @@ def train(net: CageMLP, X, Y, steps: int, lr: float = 1e-3, seed: int = 0, log=p
     return hist
 
 
-def evaluate(ws: LearnedWarmStart, seeds, frames: int, ns, conv_iters: int = 200, log=print):
+def evaluate(ws: LearnedWarmStart, seeds, frames: int, ns, conv_iters: int = 200, log=print, ideal: bool = False):
     """Max fine-vertex error (mm) against the converged solve from the same
     prediction, for the plain form and the learned form after n iterations
     (n in ns), on every substep of the held-out trajectories (which follow
-    the converged solve)."""
+    the converged solve).  With ``ideal``, also the form warm-started by the
+    substep's true cage correction (what a perfect network would give)."""
     sim = ws.sim
     base = sim.scene
     ns = sorted(ns)
-    forms = ("plain", "learned", "learned_raw")
+    forms = ("plain", "learned", "learned_raw") + (("ideal",) if ideal else ())
     err = {f: {n: [] for n in ns} for f in forms}
     rms = {f: {n: [] for n in ns} for f in forms}
     xpred = torch.zeros_like(sim._pos4)
     cpred = torch.zeros_like(ws.mg.coarse._pos4)
-    cprev = torch.zeros_like(ws.mg.coarse._pos4)
+    cstar = torch.zeros_like(ws.mg.coarse._pos4)
     for seed in seeds:
         ws.reset(reseed_motion(base, seed))
         for f in range(1, frames + 1):
@@ -424,35 +442,36 @@ def evaluate(ws: LearnedWarmStart, seeds, frames: int, ns, conv_iters: int = 200
                 with torch.cuda.stream(sim._stream):
                     xpred.copy_(sim._pos4)
                     cpred.copy_(ws.mg.coarse._pos4)
-                    cprev.copy_(ws._cprev)
-                outs = {}
+                # the converged solve first: its restriction is the true correction
+                ws.iterate(conv_iters)
+                with torch.cuda.stream(sim._stream):
+                    ref = sim._pos4[:, :3].clone()
+                    refp = sim._pos4.clone()
+                    ws.mg.coarse._pos4.copy_(cpred)
+                ws.target_from_state()
+                with torch.cuda.stream(sim._stream):
+                    cstar.copy_(ws.mg.coarse._pos4)
                 for form in forms:
                     with torch.cuda.stream(sim._stream):
                         sim._pos4.copy_(xpred)
                         ws.mg.coarse._pos4.copy_(cpred)
-                    if form != "plain":
+                    if form == "ideal":
+                        ws.ideal_warm_start()
+                    elif form != "plain":
                         ws.features()
                         ws.warm_start(fallback=(form == "learned"))
                     done = 0
-                    snaps = []
                     for n in ns:
                         ws.iterate(n - done)
                         done = n
                         with torch.cuda.stream(sim._stream):
-                            snaps.append(sim._pos4[:, :3].clone())
-                    outs[form] = snaps
-                with torch.cuda.stream(sim._stream):
-                    sim._pos4.copy_(xpred)
-                ws.iterate(conv_iters)
-                with torch.cuda.stream(sim._stream):
-                    ref = sim._pos4[:, :3].clone()
-                    for form in outs:
-                        for n, s in zip(ns, outs[form]):
-                            d = (s - ref).norm(dim=1)
+                            d = (sim._pos4[:, :3] - ref).norm(dim=1)
                             err[form][n].append(d.max())
                             rms[form][n].append(d.pow(2).mean().sqrt())
-                    ws.mg.coarse._pos4.copy_(cpred)
-                ws.target_from_state()
+                # the trajectory follows the converged solve
+                with torch.cuda.stream(sim._stream):
+                    sim._pos4.copy_(refp)
+                    ws.mg.coarse._pos4.copy_(cstar)
             ws.end_frame()
         log(f"  eval seed {seed} done")
     sim.synchronize()
@@ -460,6 +479,21 @@ def evaluate(ws: LearnedWarmStart, seeds, frames: int, ns, conv_iters: int = 200
     cv = lambda e: {form: {n: (torch.stack(v) * SCALE_MM).cpu().numpy() for n, v in d.items()}  # noqa: E731
                     for form, d in e.items()}
     return cv(err), cv(rms)
+
+
+def iterations_to(err_by_n: dict, tol_mm: float):
+    """Smallest n (log-linear interpolation between the evaluated counts) at
+    which the worst substep's max error reaches tol_mm; None if none does."""
+    ns = sorted(err_by_n)
+    worst = [float(np.max(err_by_n[n])) for n in ns]
+    for k, (n, e) in enumerate(zip(ns, worst)):
+        if e <= tol_mm:
+            if k == 0:
+                return float(n)
+            n0, e0 = ns[k - 1], worst[k - 1]
+            t = (math.log(e0) - math.log(tol_mm)) / max(math.log(e0) - math.log(e), 1e-12)
+            return float(n0 + t * (n - n0))
+    return None
 
 
 def time_frame(ws: LearnedWarmStart, n_iters: int, learned: bool, frames=(5, 6, 7), fallback: bool = True) -> float:
