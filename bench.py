@@ -43,6 +43,8 @@ CONFIGS["batched"] = (ROOT / "rlmusclev2_b200" / "configs" / "batched_256.json",
 CONFIGS["learned"] = (ROOT / "rlmusclev2_b200" / "configs" / "humanv2_synth_mg_dcd.json",
                       "humanv2_synth_535k_tets, config-3 mesh and cage, learned coarse warm start + 10 Jacobi "
                       "iterations per substep vs the plain solver at 20 (no DCD)")
+CONFIGS["box"] = (None, "box_muscle_8x8x32_12288_tets (ARAP-SVD + volume, 10 substeps x 1 Jacobi iteration, "
+                         "gravity, 5 % end pins)")
 CONFIG = CONFIGS["humanv2"][0]
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC = ROOT / "profiles" / "ncu_traffic.json"
@@ -140,9 +142,9 @@ class CpuBaseline:
     averaged apply and the re-pin after each), the SDF push-out and the
     velocity update.  The same frames and inputs as the GPU arm."""
 
-    def __init__(self, cfg, scene):
+    def __init__(self, cfg, scene, batched: bool = False):
         from oracle import oracle as O
-        self.orc = O.OracleMultiGridSim(cfg, scene, prec="f32")
+        self.orc = (O.OracleBatchSim if batched else O.OracleMultiGridSim)(cfg, scene, prec="f32")
         self.frame = int(cfg.get("start_frame", 1))
         self.n_iter = int(cfg["nsubsteps"]) * int(cfg["fine_iterations"])
         self.nsub = int(cfg["nsubsteps"])
@@ -196,11 +198,17 @@ def run_reference(args):
     if rank != 0:
         return 0
     from rlmusclev2_b200.mg import load_config, scene_from_cfg
+    steps = max(1, args.steps)
+    if args.config == "learned":
+        print(json.dumps({"impl": "reference", "unavailable": "the learned warm start has no counterpart in the "
+                          "reference (it replaces the V-cycle warm start); time --config humanv2_mg_dcd instead"}))
+        return 0
+    if args.config == "box":
+        return _run_reference_box(args, world, steps)
     cfg = load_config(str(CONFIG))
     scene = scene_from_cfg(cfg)
-    cb = CpuBaseline(cfg, scene)
-    v = cb.run(args.warmup, max(1, args.steps))
-    steps = max(1, args.steps)
+    cb = CpuBaseline(cfg, scene, batched=args.config == "batched")
+    v = cb.run(args.warmup, steps)
     line = {"impl": "reference", "metric": "ms/frame", "value": round(v, 3), "unit": "ms/frame", "n_gpus": world,
             "steps": steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -209,6 +217,37 @@ def run_reference(args):
             "e2e": {"value": round(v, 3), "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference runs on NVIDIA Warp (warp-lang 1.13.0), which is not installable offline here; "
                     "its CPU path is restated by the C oracle (OpenMP) and timed on whole frames"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _run_reference_box(args, world, steps):
+    """Reference arm of the box muscle: the FP32 oracle's MuscleSim program
+    (musclesim.py:107-142), whole frames."""
+    from oracle import oracle as O
+    from rlmusclev2_b200.meshgen import box_muscle
+    m = box_muscle()
+    cons = [{"type": "tetarapsvd", "name": "arap", "compliance": 1e-7},
+            {"type": "volume", "name": "volume", "compliance": 0.0}]
+    orc = O.OracleMuscleSim(m.verts, m.tets, m.fiber_per_tet, constraint_configs=cons, stopped=m.stopped,
+                            dts=1.0 / 24.0, num_substeps=10, density=1060.0, veldamping=0.02, gravity=-9.8, prec="f32")
+    for _ in range(args.warmup):
+        orc.step()
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        orc.step()
+        ts.append((time.perf_counter() - t0) * 1e3)
+    v = float(np.mean(ts))
+    cb = {"value": round(v, 3), "unit": "ms/frame", "cores": _omp_threads(), "kind": "port",
+          "sample": f"{steps} whole frame(s) after {args.warmup} untimed: the 12,288-tet box through the FP32 oracle's "
+                    "MuscleSim program (10 substeps x 1 Jacobi iteration)"}
+    line = {"impl": "reference", "metric": "ms/frame", "value": round(v, 3), "unit": "ms/frame", "n_gpus": world,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_verts": int(m.verts.shape[0]), "n_tets": int(m.tets.shape[0])},
+            "cpu_baseline": cb,
+            "e2e": {"value": round(v, 3), "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -453,6 +492,79 @@ def run_profile_case(args):
     return 0
 
 
+def run_box(args):
+    """The box muscle (8x8x32 hexes, 2,673 verts / 12,288 tets, ARAP-SVD + volume,
+    dt = 1/24 s in 10 substeps of one Jacobi iteration, the end 5 % pinned):
+    ms/frame of MuscleSim.step() (one CUDA graph per frame) with the state on
+    the GPU, and end to end with the positions read back every frame."""
+    import torch
+
+    from rlmusclev2_b200 import MuscleSim
+    from rlmusclev2_b200.meshgen import box_muscle
+
+    world, rank, local = _dist_setup()
+    torch.cuda.set_device(local)
+    m = box_muscle()
+    cons = [{"type": "tetarapsvd", "name": "arap", "compliance": 1e-7},
+            {"type": "volume", "name": "volume", "compliance": 0.0}]
+    sim = MuscleSim.from_procedural(m.verts, m.tets, m.fiber_per_tet, constraint_configs=cons,
+                                    device=f"cuda:{local}", stopped=m.stopped, dts=1.0 / 24.0, num_substeps=10,
+                                    density=1060.0, veldamping=0.02, gravity=-9.8)
+    s = sim._stream
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    for _ in range(args.warmup):
+        sim.step()
+    s.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    evs = [(ev(), ev()) for _ in range(args.steps)]
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for a, b in evs:
+            a.record(s)
+            sim.step()
+            b.record(s)
+        s.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+    evs2 = [(ev(), ev()) for _ in range(args.steps)]
+    for a, b in evs2:
+        a.record(s)
+        sim.step()
+        sim.positions_np()
+        b.record(s)
+    s.synchronize()
+    ms_e2e = sum(a.elapsed_time(b) for a, b in evs2) / args.steps
+    if world > 1:
+        t = torch.tensor([ms, ms_e2e], device=sim.device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms, ms_e2e = (float(x) for x in t.tolist())
+    L = sim.layout
+    alg = L.n_tets * 56 + L.n_verts * 40
+    peak, peak_kind = _peak_hbm()
+    it_s = ms * 1e-3 / 10
+    line = {
+        "metric": "ms/frame", "value": round(ms, 4), "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_verts": L.n_verts, "n_tets": L.n_tets, "n_tiles": L.n_tiles,
+                   "parallelism": f"replicas x{world}", "l2": "the 0.8 MB working set stays in L2"},
+        "substeps_per_s": round(10e3 / ms, 1), "tets_per_s": round(L.n_tets * 10 / (ms * 1e-3), 1),
+        "e2e": {"value": round(ms_e2e, 4), "unit": "ms/frame", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": L.n_verts * 12},
+        "roofline": {"bound": "launch", "achieved": round(alg / it_s / 1e9, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(alg / it_s / 1e9 / peak, 5), "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "whole substep (prediction, tile pass, boundary finish): launch-bound at 12k tets",
+                     "algorithmic_bytes": alg},
+        "clocks": clk.summary(), "gpu_launches": int(21 * args.steps),
+    }
+    sim.release_graphs()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_learned(args):
     """The learned coarse warm start against the plain solver on config 3's
     mesh and cage, measured in this run on held-out motion seed 41 (frames
@@ -557,6 +669,8 @@ def main():
         return run_reference(args)
     if args.config == "learned":
         return run_learned(args)
+    if args.config == "box":
+        return run_box(args)
     return run_ours(args)
 
 

@@ -85,8 +85,9 @@ typedef struct XpbdParams {
                                     ARAP/aniso set, 2 at up to 128 regs with volume/SNH/damping);
                                     bit 1: ARAP-SVD through the SVD even where the polar rotation applies;
                                     bit 2: persistent pass loads the next tet's streams ahead (prefetch);
-                                    bit 3: persistent pass of the light set one tet per thread (default:
-                                    two tets per thread on packed FP32x2 arithmetic) */
+                                    bit 3: undamped light and volume sets two tets per thread on packed
+                                    FP32x2 arithmetic (slower on B200: the register pairing costs as
+                                    many moves as it saves FP32 instructions) */
     float acc_scale;             /* > 0: the tile passes sum each tet's corrections into shared memory as
                                     32-bit integers round(d * acc_scale) (native integer atomics; shared
                                     float atomics cost ~5x more) and read the sums back as float(sum) /

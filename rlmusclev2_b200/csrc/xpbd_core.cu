@@ -370,7 +370,7 @@ int check_params(const XpbdParams* p) {
         p->n_attach_materials > XPBD_MAX_ATTACH_MATERIALS)
         return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range");
     if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0");
-    if (p->tile_variant < 0 || p->tile_variant > 7) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..7");
+    if (p->tile_variant < 0 || p->tile_variant > 15) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..15");
     if (!(p->acc_scale > 0.f) || !(p->acc_scale < 3.0e38f))
         return fail(XPBD_ERR_ARG, "XpbdParams: acc_scale must be a finite value > 0 (xpbd_acc_scale_for_extent)");
     return XPBD_OK;
@@ -420,16 +420,17 @@ uint32_t material_union(const XpbdParams* p) {
     return u;
 }
 
-// Instance choice: the smallest constraint set covering the materials.
-// Undamped light and volume sets run two tets per thread on packed FP32x2
-// arithmetic (2 CTAs per SM) unless bit 3 of tile_variant asks for one tet
-// per thread; there the light set runs 3 CTAs per SM (80 registers, no
-// spills), the others 2 (bit 0 of tile_variant flips that choice).
+// Instance choice: the smallest constraint set covering the materials; the
+// light set runs 3 CTAs per SM (80 registers, no spills), the others 2 (bit 0
+// of tile_variant flips that choice).  Bit 3 runs undamped light and volume
+// sets two tets per thread on packed FP32x2 arithmetic (2 CTAs per SM;
+// slower on B200, measured: the register pairing costs as many moves as the
+// packing saves).
 template <int MODE, bool DAMP>
 int launch_project(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, uint32_t fops, cudaStream_t s) {
     const uint32_t u = material_union(prm);
     const bool flip = (prm->tile_variant & 1) != 0;
-    if (!DAMP && !(prm->tile_variant & 8) && !(u & XPBD_MAT_SNH)) {
+    if (!DAMP && (prm->tile_variant & 8) && !(u & XPBD_MAT_SNH)) {
         if (u & XPBD_MAT_VOLUME) return launch_project_v<MODE, false, 2, CSET_VOL, true>(prm, T, V, fops, s);
         return launch_project_v<MODE, false, 2, CSET_LIGHT, true>(prm, T, V, fops, s);
     }

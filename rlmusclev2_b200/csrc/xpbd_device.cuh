@@ -179,8 +179,13 @@ __device__ __forceinline__ void polar_newton_step(const float3& x0, const float3
 // iteration X <- (g X + (g X)^-T) / 2, g = |det X|^(-1/3) (N. J. Higham,
 // "Computing the polar decomposition with applications", SIAM J. Sci. Stat.
 // Comput. 7, 1986).  X^-T = cof(X)/det X with the cofactor columns as cross
-// products of X's columns.  Returns false (caller falls back to the SVD) for
-// det F <= tiny or when 10 steps do not converge.
+// products of X's columns.  The iteration keeps det X > 0 when it starts
+// there, so after the start test the first two steps run untested: nearly
+// every tet needs two or three, and a warp runs as many as its slowest lane
+// needs, so testing them only adds work (and a converged tet stays put under
+// a further step).  From the third step on the step length is tested.
+// Returns false (caller falls back to the SVD) for det F <= tiny or when 10
+// steps do not converge.
 __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
     float3 x0 = make_float3(F.m[0][0], F.m[1][0], F.m[2][0]);
     float3 x1 = make_float3(F.m[0][1], F.m[1][1], F.m[2][1]);
@@ -190,14 +195,15 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
     float det = dot(x0, c0);
     // det > 1e-6 |F|_F^3, squared to avoid the square root
     if (!(det > 0.f && det * det > 1e-12f * (n2 * n2 * n2))) return false;
-    // The first step is not tested: from F it stops only for tets already at
-    // a rotation, which a second step leaves in place.
     polar_newton_step(x0, x1, x2, c0, det, x0, x1, x2);
     c0 = cross(x1, x2);
     det = dot(x0, c0);
-    if (!(det > 0.f)) return false;
+    polar_newton_step(x0, x1, x2, c0, det, x0, x1, x2);
+    c0 = cross(x1, x2);
+    det = dot(x0, c0);
 #pragma unroll 1
-    for (int it = 1; it < 10; ++it) {
+    for (int it = 2; it < 10; ++it) {
+        if (!(det > 0.f)) return false;
         float3 y0, y1, y2;
         polar_newton_step(x0, x1, x2, c0, det, y0, y1, y2);
         const float3 e0 = y0 - x0, e1 = y1 - x1, e2 = y2 - x2;
@@ -215,7 +221,6 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
         }
         c0 = cross(x1, x2);
         det = dot(x0, c0);
-        if (!(det > 0.f)) return false;
     }
     return false;
 }
@@ -236,8 +241,12 @@ __device__ __forceinline__ float arap_skip_threshold(float v) {
     return v == 0.f ? 1.0e-12f : (v < 0.f ? 1.0e-38f : v);
 }
 
+// The per-vertex delta is added as (dL w_i scale) grad_i with grad built from
+// the unnormalised G = F - R and 1/C folded into that scale factor (the scale
+// is the caller's fixed-point factor, a power of two, so it changes no
+// rounding); acc receives the scaled deltas.
 __device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, const M3& F, float at, float skip_ssq,
-                                            float3 (&acc)[4], bool force_svd = false) {
+                                            float scale, float3 (&acc)[4], bool force_svd = false) {
     M3 G;
     M3 R;
     float ssq;
@@ -251,42 +260,39 @@ __device__ __forceinline__ bool con_arapsvd(const float4 p[4], const M3& B, cons
                 ssq += G.m[i][j] * G.m[i][j];
             }
         if (ssq < skip_ssq) return false;
-        const float invC = rsqrtf(ssq);
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) G.m[i][j] *= invC;
     } else {
+        // F - U V^T = U diag(s - 1) V^T
         const Svd3 s = svd3(F);
         const float a = s.s0 - 1.f, b = s.s1 - 1.f, c = s.s2 - 1.f;
         ssq = a * a + b * b + c * c;
         if (ssq < skip_ssq) return false;
-        const float invC = 1.f / sqrtf(ssq);
-        const float d0 = invC * a, d1 = invC * b, d2 = invC * c;
         const float U[3][3] = {{s.u0.x, s.u1.x, s.u2.x}, {s.u0.y, s.u1.y, s.u2.y}, {s.u0.z, s.u1.z, s.u2.z}};
         const float V[3][3] = {{s.v0.x, s.v1.x, s.v2.x}, {s.v0.y, s.v1.y, s.v2.y}, {s.v0.z, s.v1.z, s.v2.z}};
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
-            for (int j = 0; j < 3; ++j) G.m[i][j] = U[i][0] * V[j][0] * d0 + U[i][1] * V[j][1] * d1 + U[i][2] * V[j][2] * d2;
+            for (int j = 0; j < 3; ++j) G.m[i][j] = U[i][0] * V[j][0] * a + U[i][1] * V[j][1] * b + U[i][2] * V[j][2] * c;
     }
-    const float C = sqrtf(ssq);
+    const float invC = rsqrtf(ssq);
+    const float C = ssq * invC;
+    // raw gradient rows (F - R) B^T; the constraint gradient is invC times them
     float3 g[4];
     g[0] = grad_row(G, B, 0);
     g[1] = grad_row(G, B, 1);
     g[2] = grad_row(G, B, 2);
     g[3] = (-g[0] - g[1]) - g[2];
-    const float wsum = p[0].w * dot(g[0], g[0]) + p[1].w * dot(g[1], g[1]) + p[2].w * dot(g[2], g[2]) + p[3].w * dot(g[3], g[3]);
-    if (wsum == 0.f) return false;
-    const float dL = -C / (wsum + at);
+    const float wraw = p[0].w * dot(g[0], g[0]) + p[1].w * dot(g[1], g[1]) + p[2].w * dot(g[2], g[2]) + p[3].w * dot(g[3], g[3]);
+    if (wraw == 0.f) return false;
+    const float dL = -C / (wraw * (invC * invC) + at);
+    const float k = dL * invC * scale;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) acc[i] = acc[i] + (dL * p[i].w) * g[i];
+    for (int i = 0; i < 4; ++i) acc[i] = acc[i] + (k * p[i].w) * g[i];
     return true;
 }
 
 // solve_tetvolume_kernel + tet_volume_update_xpbd_fn, solve_kernels.py:553-585, 187-281.
 __device__ __forceinline__ bool con_volume(const float4 p[4], const float4* q, float V0, float k, float kd, float dt,
-                                           float3 (&acc)[4]) {
+                                           float scale, float3 (&acc)[4]) {
     const float3 p3 = f3(p[3]);
     const float3 d0 = f3(p[0]) - p3, d1 = f3(p[1]) - p3, d2 = f3(p[2]) - p3;
     float3 g[4];
@@ -309,7 +315,7 @@ __device__ __forceinline__ bool con_volume(const float4 p[4], const float4* q, f
         dsum = dsum * gamma;
         gamma = gamma + 1.f;
     }
-    const float dl = (-C - dsum) / (gamma * ws + alpha);
+    const float dl = (-C - dsum) / (gamma * ws + alpha) * scale;
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[i] = acc[i] + (dl * p[i].w) * g[i];
     return true;
@@ -319,7 +325,8 @@ __device__ __forceinline__ bool con_volume(const float4 p[4], const float4* q, f
 // normalised mean fiber direction of the tet's 4 vertices (static, built at
 // upload); a zero f0 marks a tet whose mean fiber vanished (fn < 1e-9).
 __device__ __forceinline__ bool con_aniso(const float4 p[4], const M3& B, const M3& F, float3 f0, float tendon,
-                                          float act, float k, float ratio, float kscale, float dt, float3 (&acc)[4]) {
+                                          float act, float k, float ratio, float kscale, float dt, float scale,
+                                          float3 (&acc)[4]) {
     const float3 d = make_float3(F.m[0][0] * f0.x + F.m[0][1] * f0.y + F.m[0][2] * f0.z,
                                  F.m[1][0] * f0.x + F.m[1][1] * f0.y + F.m[1][2] * f0.z,
                                  F.m[2][0] * f0.x + F.m[2][1] * f0.y + F.m[2][2] * f0.z);
@@ -347,7 +354,7 @@ __device__ __forceinline__ bool con_aniso(const float4 p[4], const M3& B, const 
     if (wsum < 1.0e-20f) return false;
     const float sv = k * kscale;
     const float at = (1.f / sv) / (dt * dt);
-    const float dL = -C / (wsum + at);
+    const float dL = -C / (wsum + at) * scale;
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[i] = acc[i] + (dL * p[i].w) * g[i];
     return true;
@@ -355,7 +362,7 @@ __device__ __forceinline__ bool con_aniso(const float4 p[4], const M3& B, const 
 
 // solve_tetsnh_kernel + tet_snh_update_xpbd_fn, solve_kernels.py:1587-1617, 1429-1584.
 __device__ __forceinline__ bool con_snh(const float4 p[4], const float4* q, const M3& B, const M3& F, float V0,
-                                        float mu, float lam, float kd, float dt, float3 (&acc)[4]) {
+                                        float mu, float lam, float kd, float dt, float scale, float3 (&acc)[4]) {
     float Ic = 0.f;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -421,8 +428,8 @@ __device__ __forceinline__ bool con_snh(const float4 p[4], const float4* q, cons
     const float invd = 1.f / detA;
     const float db = -dC - ddamp;
     const float hb = -hC - hdamp;
-    const float ddL = invd * (Ayy * db - dh * hb);
-    const float hdL = invd * (Axx * hb - dh * db);
+    const float ddL = invd * (Ayy * db - dh * hb) * scale;
+    const float hdL = invd * (Axx * hb - dh * db) * scale;
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[i] = acc[i] + p[i].w * (ddL * dg[i] + hdL * hg[i]);
     return true;

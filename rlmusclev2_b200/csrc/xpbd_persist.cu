@@ -185,12 +185,12 @@ int dispatch(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, cons
     }
     if (u & XPBD_MAT_VOLUME) {
         if (damp) return flip ? XPBD_LAUNCH(true, 3, CSET_VOL) : XPBD_LAUNCH(true, 2, CSET_VOL);
-        if (!(prm->tile_variant & 8)) return launch_v<false, 2, CSET_VOL, false, true>(prm, T, V, P, n_iters, s, query_only, fits);
+        if (prm->tile_variant & 8) return launch_v<false, 2, CSET_VOL, false, true>(prm, T, V, P, n_iters, s, query_only, fits);
         return flip ? XPBD_LAUNCH(false, 3, CSET_VOL) : XPBD_LAUNCH(false, 2, CSET_VOL);
     }
-    // the light set runs the two-tet packed pass (2 CTAs/SM at up to 128
-    // registers) unless tile_variant bit 3 asks for the one-tet pass
-    if (!(prm->tile_variant & 8)) return launch_v<false, 2, CSET_LIGHT, false, true>(prm, T, V, P, n_iters, s, query_only, fits);
+    // tile_variant bit 3: the two-tet packed pass (2 CTAs/SM at up to 128
+    // registers; slower on B200, measured)
+    if (prm->tile_variant & 8) return launch_v<false, 2, CSET_LIGHT, false, true>(prm, T, V, P, n_iters, s, query_only, fits);
     return flip ? XPBD_LAUNCH(false, 2, CSET_LIGHT) : XPBD_LAUNCH(false, 3, CSET_LIGHT);
 #undef XPBD_LAUNCH
 }

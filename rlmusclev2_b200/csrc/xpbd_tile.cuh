@@ -149,34 +149,36 @@ __device__ __forceinline__ void project_tile_tets(const XpbdParams& prm, const X
         int nact = 0;
         const uint32_t fl = m.flags;
         // Same type order as the reference table (ascending ConstraintType tag).
+        // the deltas arrive already multiplied by acc_scale (a power of two)
         if (CSET >= CSET_FULL && (fl & XPBD_MAT_SNH) &&
-            con_snh(p, pq, B, F, V0, m.snh_mu, m.snh_lam, m.snh_damp, prm.dt, d))
+            con_snh(p, pq, B, F, V0, m.snh_mu, m.snh_lam, m.snh_damp, prm.dt, acc_scale, d))
             nact += 1;
-        if (CSET >= CSET_VOL && (fl & XPBD_MAT_VOLUME) && con_volume(p, pq, V0, m.vol_k, m.vol_damp, prm.dt, d))
+        if (CSET >= CSET_VOL && (fl & XPBD_MAT_VOLUME) &&
+            con_volume(p, pq, V0, m.vol_k, m.vol_damp, prm.dt, acc_scale, d))
             nact += 1;
         if (fl & XPBD_MAT_ANISO) {
             const float4 fb = reinterpret_cast<const float4*>(T.tet_fiber)[t];
             if (con_aniso(p, B, F, f3(fb), fb.w, T.tet_act[t], m.aniso_k, prm.contraction_ratio,
-                          prm.fiber_stiffness_scale, prm.dt, d))
+                          prm.fiber_stiffness_scale, prm.dt, acc_scale, d))
                 nact += 1;
         }
         if ((fl & XPBD_MAT_ARAPSVD) && con_arapsvd(p, B, F, s_arap_at[min(int(q.z & 0xffu), XPBD_MAX_MATERIALS - 1)],
-                                                   arap_skip, d, (prm.tile_variant & 2) != 0))
+                                                   arap_skip, acc_scale, d, (prm.tile_variant & 2) != 0))
             nact += 1;
         if (nact != 0) {
-            // Range check on the sum of the 12 |components| (not their maximum:
-            // a sum carries a NaN or Inf component through, fmaxf drops NaN).
-            // Each converted component is then below 2^25 = 2^31/64, so a vertex
-            // sum wraps unflagged only with more than 64 such tets on it.
+            // Range check on the sum of the 12 scaled |components| (not their
+            // maximum: a sum carries a NaN or Inf component through, fmaxf
+            // drops NaN).  Each converted component is then below 2^25 = 2^31/64,
+            // so a vertex sum wraps unflagged only with more than 64 such tets on it.
             float dabs = 0.f;
 #pragma unroll
             for (int i = 0; i < 4; ++i) dabs += (fabsf(d[i].x) + fabsf(d[i].y)) + fabsf(d[i].z);
-            if (!(dabs * acc_scale <= 33554432.f) && prm.status) atomicOr(prm.status, XPBD_STATUS_ACC_RANGE);
+            if (!(dabs <= 33554432.f) && prm.status) atomicOr(prm.status, XPBD_STATUS_ACC_RANGE);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                atomicAdd(&s_ax[l[i]], __float2int_rn(d[i].x * acc_scale));
-                atomicAdd(&s_ay[l[i]], __float2int_rn(d[i].y * acc_scale));
-                atomicAdd(&s_az[l[i]], __float2int_rn(d[i].z * acc_scale));
+                atomicAdd(&s_ax[l[i]], __float2int_rn(d[i].x));
+                atomicAdd(&s_ay[l[i]], __float2int_rn(d[i].y));
+                atomicAdd(&s_az[l[i]], __float2int_rn(d[i].z));
                 atomicAdd(&s_cnt[l[i]], nact);
             }
         }

@@ -341,7 +341,7 @@ __device__ __forceinline__ void project_tile_tets_x2(const XpbdParams& prm, cons
             B.m[2][0] = lane ? B20.y : B20.x; B.m[2][1] = lane ? B21.y : B21.x; B.m[2][2] = lane ? B22.y : B22.x;
             const float4 fbv = reinterpret_cast<const float4*>(T.tet_fiber)[t];
             if (con_aniso(pp, B, F, f3(fbv), fbv.w, T.tet_act[t], prm.materials[m].aniso_k, prm.contraction_ratio,
-                          prm.fiber_stiffness_scale, prm.dt, dd))
+                          prm.fiber_stiffness_scale, prm.dt, 1.f, dd))
                 n += 1;
         };
         if (fa & XPBD_MAT_ANISO) aniso(pa, ta, ma, 0, da, na);

@@ -75,11 +75,13 @@ class TileLayout:
 
 
 def ctas_per_sm(materials: list[dict]) -> int:
-    """Resident CTAs per SM of the persistent tile pass the library launches
-    for these materials: 2 for every set (the light set -- ARAP-SVD / aniso
-    only, no damping -- runs two tets per thread at up to 128 registers; the
-    sets with volume, SNH or damping one tet per thread at up to 128)."""
-    return 2
+    """Resident CTAs per SM of the tile pass the library launches for these
+    materials: 3 for the light constraint set (ARAP-SVD / aniso only, no
+    damping), 2 when any material has volume, SNH or damping."""
+    u = 0
+    for m in materials:
+        u |= int(m["flags"])
+    return 2 if u & (capi.MAT_VOLUME | capi.MAT_SNH | capi.MAT_DAMPED) else 3
 
 
 def default_tile_tets(n_tets: int, n_sm: int = 148, ctas: int = 3, max_tile: int = 2048) -> int:
@@ -141,6 +143,18 @@ def tet_materials(n_tets: int, tets: np.ndarray, table: ConstraintTable):
     return mats, mat_of.astype(np.int32).ravel(), V0
 
 
+# Relative projection cost of a tet by constraint (the polar iteration of
+# ARAP-SVD dominates; the shared loads, deformation gradient and
+# accumulation are the base), from instruction counts of the tile pass.
+_COST_BASE, _COST = 0.35, {capi.MAT_ARAPSVD: 0.65, capi.MAT_SNH: 0.35, capi.MAT_VOLUME: 0.15, capi.MAT_ANISO: 0.25}
+
+
+def tet_cost(materials: list[dict], mat_of_tet: np.ndarray) -> np.ndarray:
+    """Estimated relative cost of projecting each tet (1.0 for an ARAP-SVD tet)."""
+    mc = np.array([_COST_BASE + sum(c for bit, c in _COST.items() if int(m["flags"]) & bit) for m in materials])
+    return mc[mat_of_tet]
+
+
 def fiber_f0(v_fiber: np.ndarray, tets: np.ndarray) -> np.ndarray:
     """Normalised mean fiber direction per tet in float32, in the order of
     solve_tet_aniso_arap_kernel (solve_kernels.py:1348-1353); zero where the
@@ -194,17 +208,28 @@ def build_layout(pos0: np.ndarray, tets: np.ndarray, table: ConstraintTable, *, 
     tet_inv = np.empty(nt, np.int64)
     tet_inv[tet_perm] = np.arange(nt)
     tets_s = tets[tet_perm]
-    # 2. tiles of consecutive tets (cut at group starts, equal tiles within a
-    # group); split any tile whose vertex set would not fit
+    # 2. tiles of consecutive tets (cut at group starts), as many as equal
+    # counts of tile_tets give, cut at equal shares of the estimated projection
+    # cost so that tiles holding dearer constraint sets (the aniso muscle's
+    # fiber term, volume) hold fewer tets and all tiles reach the per-iteration
+    # grid barrier together; split any tile whose vertex set would not fit
+    cost = tet_cost(mats, mat_of_user_tet[tet_perm])
+    ccum = np.r_[0.0, np.cumsum(cost)]
+
+    def cut(a: int, b: int, k: int) -> list[int]:
+        share = ccum[a] + (ccum[b] - ccum[a]) * np.arange(1, k) / k
+        inner = np.clip(np.searchsorted(ccum, share, side="left"), a + 1, b - 1) if k > 1 else []
+        return [int(x) for x in inner] + [b]
+
     if tgroup is None:
-        bounds = list(range(0, nt, tile_tets)) + [nt]
+        bounds = [0] + cut(0, nt, int(np.ceil(nt / tile_tets)))
     else:
         gs = tgroup[tet_perm]
         starts = np.r_[0, np.nonzero(np.diff(gs))[0] + 1, nt]
         bounds = [0]
         for a, b in zip(starts[:-1], starts[1:]):
-            k = int(np.ceil((b - a) / tile_tets))
-            bounds += [int(a + (b - a) * j // k) for j in range(1, k + 1)]
+            bounds += cut(int(a), int(b), int(np.ceil((b - a) / tile_tets)))
+    bounds = sorted(set(bounds))
     tptr = [0]
     for a, b in zip(bounds[:-1], bounds[1:]):
         s = a

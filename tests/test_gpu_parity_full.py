@@ -10,10 +10,13 @@ divisor, and whole frames drift apart by far more than rounding.  The
 comparison is therefore split:
 
 * with the threshold disabled on both sides (XpbdParams.arap_skip_ssq < 0,
-  oracle.set_arap_skip(-1); nothing else changes), every vertex after one
-  frame (10 substeps) lies within 1e-5 x bbox diagonal of the FP64 and the
-  FP32 oracle, the max ARAP residual matches to 1e-4 relative and the volume
-  drift to 1e-4 of the rest volume: the kernels' arithmetic at rounding level;
+  oracle.set_arap_skip(-1); nothing else changes), every vertex after three
+  frames (30 substeps) lies within 1e-5 x bbox diagonal of the FP64 and the
+  FP32 oracle, the max ARAP residual of the GPU's metric kernel matches the
+  FP64 oracle's on the same positions to 1e-4 relative (on each side's own
+  positions to 1e-2: the max sits on a thin tet whose residual moves with
+  sub-micron position differences), and the volume drift matches to 1e-4 of
+  the rest volume: the kernels' arithmetic at rounding level;
 * with the reference threshold, the GPU is as close to the FP64 oracle as
   the FP32 oracle is (three times its spread at most), and one Jacobi
   iteration from the frame's end state takes < 1 % of vertices into a
@@ -44,9 +47,12 @@ def scenes():
     return out
 
 
+FRAMES = (1, 2, 3)  # frame 1 starts at the rest pose; bones and activation move from frame 2
+
+
 def _frame(cfg, sc, skip):
-    """One frame (frame 1) on the GPU and on the FP32 / FP64 oracle with the
-    ARAP skip threshold ``skip`` (0: the reference's 1e-12, < 0: none)."""
+    """Frames 1-3 (30 substeps) on the GPU and on the FP32 / FP64 oracle with
+    the ARAP skip threshold ``skip`` (0: the reference's 1e-12, < 0: none)."""
     O.set_arap_skip(skip)
     try:
         sim = MultiGridSim(cfg, scene=sc)
@@ -55,10 +61,11 @@ def _frame(cfg, sc, skip):
             sim.mg.coarse._prm.arap_skip_ssq = skip
         o32 = O.OracleMultiGridSim(cfg, sc, prec="f32")
         o64 = O.OracleMultiGridSim(cfg, sc, prec="f64")
-        sim.set_fiber_activation(sc.activation(1))
-        sim.step_frame(1)
-        o32.step_frame(1)
-        o64.step_frame(1)
+        for f in FRAMES:
+            sim.set_fiber_activation(sc.activation(f))
+            sim.step_frame(f)
+            o32.step_frame(f)
+            o64.step_frame(f)
         p = sim.positions_np()
     except Exception:
         O.set_arap_skip(0.0)
@@ -66,12 +73,19 @@ def _frame(cfg, sc, skip):
     return sim, o32, o64, p
 
 
-def _metrics(sim, o64):
+def _metrics(sim, o64, p):
+    """GPU metrics, the FP64 oracle's max ARAP residual and volume drift on its
+    own positions, and its max residual on the GPU's positions (the metric
+    kernel's parity, free of the position differences)."""
     mt = sim.metrics()
-    r64 = o64.arap_residual()
+    r64 = float(o64.arap_residual().max())
     drift_gpu = (mt["vol_sum"] - sim.total_rest_volume) / sim.total_rest_volume
     drift_64 = (o64.total_volume() - o64.total_rest_volume) / o64.total_rest_volume
-    return mt, float(r64.max()), drift_gpu, drift_64
+    own = o64.pos.copy()
+    o64.pos[:] = p
+    r64_at_gpu = float(o64.arap_residual().max())
+    o64.pos[:] = own
+    return mt, r64, drift_gpu, drift_64, r64_at_gpu
 
 
 @pytest.mark.parametrize("name", ["config2", "config3"])
@@ -85,12 +99,14 @@ def test_full_frame_rounding_level_without_skip_threshold(scenes, name, parity_r
         e32 = np.abs(p - o32.pos).max(1)
         spread = np.abs(o32.pos - o64.pos).max(1)
         moved = float(np.abs(o64.pos - sc.verts).max())
-        mt, rmax64, drift_gpu, drift_64 = _metrics(sim, o64)
+        mt, rmax64, drift_gpu, drift_64, r_at_gpu = _metrics(sim, o64, p)
         rel_r = abs(mt["resid_max"] - rmax64) / rmax64
-        rec = dict(n_verts=sim.NV, n_tets=sim.NT, diag_m=diag, tol_m=tol, max_gpu_o64_m=e64.max(),
-                   max_gpu_o32_m=e32.max(), max_o32_o64_m=spread.max(), max_gpu_o64_over_diag=e64.max() / diag,
-                   p99_gpu_o64_m=np.percentile(e64, 99), moved_m=moved, resid_max_rel=rel_r,
-                   drift_gpu=drift_gpu, drift_o64=drift_64)
+        rel_metric = abs(mt["resid_max"] - r_at_gpu) / r_at_gpu
+        rec = dict(n_verts=sim.NV, n_tets=sim.NT, frames=len(FRAMES), diag_m=diag, tol_m=tol,
+                   max_gpu_o64_m=e64.max(), max_gpu_o32_m=e32.max(), max_o32_o64_m=spread.max(),
+                   max_gpu_o64_over_diag=e64.max() / diag, p99_gpu_o64_m=np.percentile(e64, 99), moved_m=moved,
+                   resid_max_gpu=mt["resid_max"], resid_max_o64=rmax64, resid_max_rel=rel_r,
+                   resid_metric_rel_same_positions=rel_metric, drift_gpu=drift_gpu, drift_o64=drift_64)
         if getattr(sim, "dcd", None) is not None:
             st = sim.dcd.stats()
             rec.update(dcd_pairs_gpu=st["n_pairs"], dcd_pairs_o32=int(o32.dcd_last[0]))
@@ -98,7 +114,10 @@ def test_full_frame_rounding_level_without_skip_threshold(scenes, name, parity_r
         assert moved > 100 * tol
         assert mt["n_nonfinite"] == 0
         assert e64.max() <= tol and e32.max() <= tol
-        assert rel_r <= 1e-4
+        # the metric kernel on the same positions; on each side's own positions the
+        # max sits on a thin tet whose residual moves with sub-micron differences
+        assert rel_metric <= 1e-4
+        assert rel_r <= 1e-2
         assert abs(drift_gpu - drift_64) <= 1e-4
     finally:
         O.set_arap_skip(0.0)
@@ -114,7 +133,7 @@ def test_full_frame_reference_threshold(scenes, name, parity_record):
     sim, o32, o64, p = _frame(cfg, sc, 0.0)
     e64 = np.abs(p - o64.pos).max(1)
     spread = np.abs(o32.pos - o64.pos).max(1)
-    mt, rmax64, drift_gpu, drift_64 = _metrics(sim, o64)
+    mt, rmax64, drift_gpu, drift_64, r_at_gpu = _metrics(sim, o64, p)
     r32 = float(o32.arap_residual().max())
     # one Jacobi iteration (the constraint sums) from the frame's end state on all three
     for o in (o32, o64):
@@ -131,14 +150,16 @@ def test_full_frame_reference_threshold(scenes, name, parity_record):
     flips_3264 = float((o32.dPw != o64.dPw).mean())
     avg = dP / np.maximum(dPw, 1)[:, None]
     err_same = np.abs(avg - o64.dP / np.maximum(o64.dPw, 1)[:, None]).max(1)[same].max()
-    parity_record(f"{name}_reference_threshold", diag_m=diag, tol_m=tol, max_gpu_o64_m=e64.max(),
+    parity_record(f"{name}_reference_threshold", frames=len(FRAMES), diag_m=diag, tol_m=tol, max_gpu_o64_m=e64.max(),
                   max_o32_o64_m=spread.max(), p99_gpu_o64_m=np.percentile(e64, 99),
                   p99_o32_o64_m=np.percentile(spread, 99), resid_max_gpu=mt["resid_max"], resid_max_o64=rmax64,
                   resid_max_o32=r32, drift_gpu=drift_gpu, drift_o64=drift_64, iteration_flip_frac=flips,
-                  iteration_flip_frac_o32_o64=flips_3264, iteration_err_same_count_m=err_same)
+                  iteration_flip_frac_o32_o64=flips_3264, iteration_err_same_count_m=err_same,
+                  resid_metric_rel_same_positions=abs(mt["resid_max"] - r_at_gpu) / r_at_gpu)
     assert mt["n_nonfinite"] == 0
     assert e64.max() <= max(tol, 3.0 * spread.max())
-    assert abs(mt["resid_max"] - rmax64) <= max(1e-4 * rmax64, 3.0 * abs(r32 - rmax64))
+    assert abs(mt["resid_max"] - r_at_gpu) <= 1e-4 * r_at_gpu
+    assert abs(mt["resid_max"] - rmax64) <= max(1e-2 * rmax64, 3.0 * abs(r32 - rmax64))
     assert abs(drift_gpu - drift_64) <= 1e-4
     assert flips < 0.01
     assert err_same <= tol
