@@ -464,7 +464,8 @@ def run_profile_case(args):
     """Small deterministic workloads for ncu (no timing, no output line).
 
     humanv2: ``--steps`` frames of the benchmark configuration (the frame's
-    launches issued eagerly, without the graph).  box3m: a 64x64x120-hex box (2.95M tets, ~150 MB of tet
+    launches issued eagerly, without the graph); batched: ``--steps`` frames of
+    the 256-instance batch on the per-iteration tile pass.  box3m: a 64x64x120-hex box (2.95M tets, ~150 MB of tet
     streams, larger than L2) and ``--steps`` Jacobi iterations of its tet pass."""
     import torch
     if args.profile_case in ("humanv2", "humanv2_mg_dcd"):
@@ -474,6 +475,15 @@ def run_profile_case(args):
         for f in range(sim.start_frame, sim.start_frame + args.steps):
             sim.set_fiber_activation(sim.scene.activation(f))
             sim.step_frame(f)
+        sim.synchronize()
+    elif args.profile_case == "batched":
+        from rlmusclev2_b200.batch import BatchSim
+        from rlmusclev2_b200.mg import load_config
+        sim = BatchSim(load_config(str(CONFIGS["batched"][0])))
+        sim.use_graphs = False
+        sim.use_persistent = False  # the per-iteration tile pass the autotuner picks at 1 iteration per substep
+        for f in range(sim.start_frame, sim.start_frame + args.steps):
+            sim.step_frame_inputs(f)
         sim.synchronize()
     elif args.profile_case == "box3m":
         from rlmusclev2_b200 import MuscleSim
@@ -656,7 +666,7 @@ def main():
     ap.add_argument("--config", choices=sorted(CONFIGS), default="humanv2",
                     help="workload (default: the 535k-tet configuration the metric is quoted on)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-case", choices=["humanv2", "humanv2_mg_dcd", "box3m"], default=None,
+    ap.add_argument("--profile-case", choices=["humanv2", "humanv2_mg_dcd", "batched", "box3m"], default=None,
                     help="run a small fixed workload for ncu and exit")
     args = ap.parse_args()
     global CONFIG, WORKLOAD
