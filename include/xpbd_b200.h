@@ -87,7 +87,9 @@ typedef struct XpbdParams {
                                     bit 2: persistent pass loads the next tet's streams ahead (prefetch);
                                     bit 3: undamped light and volume sets two tets per thread on packed
                                     FP32x2 arithmetic (slower on B200: the register pairing costs as
-                                    many moves as it saves FP32 instructions) */
+                                    many moves as it saves FP32 instructions);
+                                    bit 4: persistent pass keeps the runtime shared-memory layout for
+                                    tiles of <= 768 vertices (default: compile-time offsets) */
     float acc_scale;             /* > 0: the tile passes sum each tet's corrections into shared memory as
                                     32-bit integers round(d * acc_scale) (native integer atomics; shared
                                     float atomics cost ~5x more) and read the sums back as float(sum) /

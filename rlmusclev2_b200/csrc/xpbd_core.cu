@@ -370,7 +370,7 @@ int check_params(const XpbdParams* p) {
         p->n_attach_materials > XPBD_MAX_ATTACH_MATERIALS)
         return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range");
     if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0");
-    if (p->tile_variant < 0 || p->tile_variant > 15) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..15");
+    if (p->tile_variant < 0 || p->tile_variant > 31) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..31");
     if (!(p->acc_scale > 0.f) || !(p->acc_scale < 3.0e38f))
         return fail(XPBD_ERR_ARG, "XpbdParams: acc_scale must be a finite value > 0 (xpbd_acc_scale_for_extent)");
     return XPBD_OK;

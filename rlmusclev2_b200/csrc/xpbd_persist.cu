@@ -26,8 +26,13 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr size_t kSmemPerVert = 4 * sizeof(float4) + 4 * sizeof(float) + 2 * sizeof(int);  // 88 bytes
+// Tiles of at most kFixV vertices put the accumulators and the positions at
+// compile-time offsets of the shared block, so the 16 shared atomics and the
+// 4 position loads of a tet address their vertex by one register plus an
+// immediate (no per-array base register arithmetic).
+constexpr int kFixV = 768;
 
-template <bool DAMP, int MINB, int CSET, bool PF, bool X2>
+template <bool DAMP, int MINB, int CSET, bool PF, bool X2, bool FIXED = false>
 __global__ void __launch_bounds__(kThreads, MINB)
     k_iterate_persistent(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdTiles T,
                          const __grid_constant__ XpbdVerts V, const __grid_constant__ XpbdPersist P, int n_iters) {
@@ -43,17 +48,33 @@ __global__ void __launch_bounds__(kThreads, MINB)
     // global id and the vertex flags: 88 bytes.  Everything but the position
     // and the accumulators is constant for the launch.
     const int mtv = T.max_tile_verts;
-    float4* s_pos = smem;
-    float4* s_prev = smem + mtv;
-    float4* s_att = smem + 2 * mtv;
-    float4* s_pin = smem + 3 * mtv;
-    int* s_ax = reinterpret_cast<int*>(smem + 4 * mtv);
-    int* s_ay = s_ax + mtv;
-    int* s_az = s_ay + mtv;
-    int* s_cnt = s_az + mtv;
+    float4 *s_pos, *s_prev, *s_att, *s_pin;
+    int *s_ax, *s_ay, *s_az, *s_cnt, *s_g, *s_f;
+    if constexpr (FIXED) {
+        // [4 x kFixV accumulator ints][kFixV positions][prev, attach, pin: mtv each][ids, flags]
+        s_ax = reinterpret_cast<int*>(smem);
+        s_ay = s_ax + kFixV;
+        s_az = s_ay + kFixV;
+        s_cnt = s_az + kFixV;
+        s_pos = smem + kFixV;
+        s_prev = smem + 2 * kFixV;
+        s_att = s_prev + mtv;
+        s_pin = s_att + mtv;
+        s_g = reinterpret_cast<int*>(s_pin + mtv);
+        s_f = s_g + mtv;
+    } else {
+        s_pos = smem;
+        s_prev = smem + mtv;
+        s_att = smem + 2 * mtv;
+        s_pin = smem + 3 * mtv;
+        s_ax = reinterpret_cast<int*>(smem + 4 * mtv);
+        s_ay = s_ax + mtv;
+        s_az = s_ay + mtv;
+        s_cnt = s_az + mtv;
+        s_g = s_cnt + mtv;
+        s_f = s_g + mtv;
+    }
     const float inv_scale = 1.f / prm.acc_scale;
-    int* s_g = s_cnt + mtv;
-    int* s_f = s_g + mtv;
     const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
     const float4* prev4 = reinterpret_cast<const float4*>(V.pprev);
     float4* pos4w = reinterpret_cast<float4*>(V.pos);
@@ -131,11 +152,13 @@ uint32_t material_union(const XpbdParams* p) {
     return u;
 }
 
-template <bool DAMP, int MINB, int CSET, bool PF, bool X2 = false>
+template <bool DAMP, int MINB, int CSET, bool PF, bool X2 = false, bool FIXED = false>
 int launch_v(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, const XpbdPersist* P, int n_iters,
              cudaStream_t s, bool query_only, int* fits) {
-    auto kern = k_iterate_persistent<DAMP, MINB, CSET, PF, X2>;
-    const size_t smem = size_t(T->max_tile_verts) * kSmemPerVert;
+    auto kern = k_iterate_persistent<DAMP, MINB, CSET, PF, X2, FIXED>;
+    const size_t smem = FIXED ? size_t(kFixV) * (4 * sizeof(int) + sizeof(float4)) +
+                                    size_t(T->max_tile_verts) * (3 * sizeof(float4) + 2 * sizeof(int))
+                              : size_t(T->max_tile_verts) * kSmemPerVert;
     if (smem > kSmemOptIn &&
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return cuda_check("xpbd_iterate_persistent: smem attribute");
@@ -176,9 +199,12 @@ int dispatch(const XpbdParams* prm, const XpbdTiles* T, const XpbdVerts* V, cons
         if (prm->materials[i].flags & XPBD_MAT_DAMPED) damp = true;
     const bool flip = (prm->tile_variant & 1) != 0;
     const bool pf = (prm->tile_variant & 4) != 0;
+    // tile_variant bit 4: the runtime shared layout even for small tiles
+    const bool fixed = T->max_tile_verts <= kFixV && !(prm->tile_variant & 16);
 #define XPBD_LAUNCH(D, M, C) \
     (pf ? launch_v<D, M, C, true>(prm, T, V, P, n_iters, s, query_only, fits) \
-        : launch_v<D, M, C, false>(prm, T, V, P, n_iters, s, query_only, fits))
+        : (fixed ? launch_v<D, M, C, false, false, true>(prm, T, V, P, n_iters, s, query_only, fits) \
+                 : launch_v<D, M, C, false>(prm, T, V, P, n_iters, s, query_only, fits)))
     if (u & XPBD_MAT_SNH) {
         if (damp) return flip ? XPBD_LAUNCH(true, 3, CSET_FULL) : XPBD_LAUNCH(true, 2, CSET_FULL);
         return flip ? XPBD_LAUNCH(false, 3, CSET_FULL) : XPBD_LAUNCH(false, 2, CSET_FULL);

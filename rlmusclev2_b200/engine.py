@@ -33,6 +33,9 @@ def _ptr(t) -> int | None:
     return None if t is None else int(t.data_ptr())
 
 
+ACC_HEADROOM = 8.0
+
+
 def status_error(tile_status: int, dcd_status: int = 0) -> str | None:
     """The error a frame must raise for its status words, or None.
 
@@ -158,9 +161,13 @@ class XpbdEngine:
         for i, m in enumerate(L.materials):
             for k, v in m.items():
                 setattr(prm.materials[i], k, v)
-        # fixed-point accumulation scale of the tile passes: quantum at most half an
-        # FP32 ulp of the largest rest coordinate
-        prm.acc_scale = float(self._lib.xpbd_acc_scale_for_extent(float(np.abs(self.pos0_np).max())))
+        # fixed-point accumulation scale of the tile passes, sized for coordinates up
+        # to ACC_HEADROOM x the largest rest coordinate (a mesh may travel or stretch
+        # that far: the 1-iteration box muscle sags to 5x its length, with single-tet
+        # corrections of 10 cm): a quantum of at most 4 FP32 ulps of the largest rest
+        # coordinate, far below the parity tolerance, and vertex sums up to 256x it
+        prm.acc_scale = float(self._lib.xpbd_acc_scale_for_extent(
+            ACC_HEADROOM * float(np.abs(self.pos0_np).max())))
         prm.status = self._pstatus.data_ptr()
         prm.n_attach_materials = len(self._attach_mats)
         for i, (k, d) in enumerate(self._attach_mats):
