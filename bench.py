@@ -402,11 +402,9 @@ def run_ours(args):
     achieved = alg_bytes / (it_ms * 1e-3) / 1e9
     peak, peak_kind = _peak_hbm()
     traffic = None
-    try:
-        tr = json.loads(TRAFFIC.read_text())
-        if args.config in tr.get("configs", ["humanv2"]):
-            traffic = tr.get("bytes_per_iteration")
-    except Exception:
+    try:  # ncu DRAM bytes per iteration of this workload's tile pass, when captured
+        traffic = json.loads(TRAFFIC.read_text()).get(args.config, {}).get("bytes_per_iteration")
+    except (OSError, ValueError):
         pass
     per_iter = 2 + (3 if getattr(sim, "dcd", None) is not None else 0)
     fine = len(sim._persist) if persistent else sim.fine_iters * per_iter
