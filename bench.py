@@ -592,7 +592,7 @@ def run_learned(args):
     sim = MultiGridSim(LW.learned_config(), device=f"cuda:{local}")
     ws = LW.LearnedWarmStart(sim)
     meta = LW.load_weights(ws)
-    ns = [10, 20, 40, 80, 120, 160]
+    ns = [10, 20, 40, 80, 120, 160, 180, 200]
     err, rms = LW.evaluate(ws, [41], 4, ns, ideal=True)
     n_to = {form: LW.iterations_to(err[form], 0.1) for form in ("plain", "learned", "ideal")}
     base = sim.scene
