@@ -503,6 +503,16 @@ typedef struct XpbdPersist {
                                      be closed (no vertex shared with tiles outside it, e.g. whole instances of a
                                      batch) and keeps its own sync words; vertices in no tet are finished by the
                                      launch whose range ends at n_tiles */
+    /* Optional neighbour synchronisation (all three set, or all NULL for the grid-wide
+     * barrier): tile t shares boundary vertices with tiles nbr_idx[nbr_ptr[t] ..
+     * nbr_ptr[t+1]) (all inside the launched range); after its boundary sums a tile
+     * publishes its iteration count in tile_cnt[t] and waits only until those
+     * neighbours have published theirs, instead of waiting for every tile.  tile_cnt
+     * holds one counter per tile, all zero before the first call and all equal between
+     * calls (zero them with the ring and sync words after a barrier timeout). */
+    const int32_t* nbr_ptr;  /* [n_tiles+1] */
+    const int32_t* nbr_idx;  /* [nbr_ptr[n_tiles]] */
+    uint32_t* tile_cnt;      /* [n_tiles] */
 } XpbdPersist;
 
 /* n_iters fused Jacobi iterations in ONE cooperative launch: the same

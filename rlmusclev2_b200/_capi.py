@@ -125,7 +125,8 @@ class XpbdCageFeatures(C.Structure):
 
 class XpbdPersist(C.Structure):
     _fields_ = [("tile_own", C.c_void_p), ("ring", C.c_void_p), ("sync", C.c_void_p), ("status", C.c_void_p),
-                ("tile_begin", C.c_int32), ("tile_end", C.c_int32)]
+                ("tile_begin", C.c_int32), ("tile_end", C.c_int32), ("nbr_ptr", C.c_void_p),
+                ("nbr_idx", C.c_void_p), ("tile_cnt", C.c_void_p)]
 
 
 P = C.c_void_p

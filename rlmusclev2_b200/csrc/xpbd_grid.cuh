@@ -78,4 +78,41 @@ __device__ __forceinline__ void grid_barrier(GridBarrier& b, int32_t* status) {
     __syncthreads();
 }
 
+// Neighbour synchronisation of the persistent pass: tile `self` publishes
+// that it finished iteration `it` (its counter becomes c0 + it + 1, c0 being
+// the counter at launch start, equal for all tiles) and waits until each of
+// its neighbours has published at least that.  A tile only reads ring slots
+// of vertices it shares with those neighbours, so this orders every partial
+// sum it reads (and, two iterations on, every clear) as the grid-wide barrier
+// does, without waiting for tiles elsewhere.  The lanes of warp 0 poll the
+// neighbour counters in parallel.  Bounded like grid_barrier: after kSpinLimit
+// polls the bit is set and the wait ends; a set bit ends later waits early.
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void neighbour_sync(uint32_t* cnt, const int32_t* nbr, int n_nbr, int self, uint32_t target,
+                                               int32_t* status) {
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) st_release(cnt + self, target);
+        for (int j = int(threadIdx.x); j < n_nbr; j += 32) {
+            const uint32_t* c = cnt + nbr[j];
+            uint32_t spins = 0;
+            while (int32_t(ld_acquire(c) - target) < 0) {
+                if (++spins % kSpinCheck == 0u) {
+                    if (spins > kSpinLimit) {
+                        atomicOr(status, XPBD_STATUS_BARRIER_TIMEOUT);
+                        break;
+                    }
+                    if (*reinterpret_cast<volatile int32_t*>(status) & XPBD_STATUS_BARRIER_TIMEOUT) break;
+                    __nanosleep(32);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+}
+
 }  // namespace xpbd

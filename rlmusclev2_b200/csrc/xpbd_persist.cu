@@ -81,7 +81,18 @@ __global__ void __launch_bounds__(kThreads, MINB)
     float4* ring = reinterpret_cast<float4*>(P.ring);
     const size_t nv = size_t(V.n);
     const uint32_t phase0 = P.sync[2];
-    GridBarrier bar = grid_barrier_begin(P.sync);
+    const bool nsync = P.nbr_ptr != nullptr;
+    GridBarrier bar = {nullptr, 0u, 0u};
+    uint32_t c0 = 0;
+    const int32_t* nbr = nullptr;
+    int n_nbr = 0;
+    if (nsync) {
+        c0 = __ldcg(P.tile_cnt + tile);
+        nbr = P.nbr_idx + P.nbr_ptr[tile];
+        n_nbr = P.nbr_ptr[tile + 1] - P.nbr_ptr[tile];
+    } else {
+        bar = grid_barrier_begin(P.sync);
+    }
     const uint32_t ops = XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_PIN;
     __shared__ float s_arap_at[XPBD_MAX_MATERIALS];
     fill_arap_at(prm, s_arap_at);
@@ -130,7 +141,10 @@ __global__ void __launch_bounds__(kThreads, MINB)
             finish_vertex(prm, V, g, pp, make_float4(0.f, 0.f, 0.f, 0.f), ops);
             pos4w[g] = pp;
         }
-        grid_barrier(bar, P.status);
+        if (nsync)
+            neighbour_sync(P.tile_cnt, nbr, n_nbr, tile, c0 + uint32_t(it) + 1u, P.status);
+        else
+            grid_barrier(bar, P.status);
         for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
             float4 pp = s_pos[i];
             finish_core(prm, s_f[i], s_att[i], s_prev[i], s_pin[i], pp, __ldcg(&rc[s_g[i]]), ops);
@@ -143,7 +157,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
         if (i < nint || (g >= own_lo && g < own_hi)) pos4w[g] = s_pos[i];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) P.sync[2] = (phase0 + uint32_t(n_iters)) % 3u;
-    grid_barrier_end(P.sync, bar);
+    if (!nsync) grid_barrier_end(P.sync, bar);
 }
 
 uint32_t material_union(const XpbdParams* p) {
@@ -235,6 +249,8 @@ extern "C" int xpbd_iterate_persistent(const XpbdParams* prm, const XpbdTiles* t
         return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: tiles/verts");
     if (!ps->tile_own || !ps->ring || !ps->sync || !ps->status)
         return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: XpbdPersist pointers");
+    if ((ps->nbr_ptr == nullptr) != (ps->nbr_idx == nullptr) || (ps->nbr_ptr == nullptr) != (ps->tile_cnt == nullptr))
+        return fail(XPBD_ERR_ARG, "xpbd_iterate_persistent: nbr_ptr, nbr_idx and tile_cnt must be set together");
     XpbdPersist P = *ps;
     if (P.tile_begin == 0 && P.tile_end == 0) P.tile_end = tiles->n_tiles;
     if (P.tile_begin < 0 || P.tile_end > tiles->n_tiles || P.tile_begin >= P.tile_end)

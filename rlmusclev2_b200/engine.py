@@ -257,23 +257,53 @@ class XpbdEngine:
             capi.check(self._lib.xpbd_graph_destroy(g))
         self._graphs = {}
 
+    #: synchronisation between the iterations of the persistent pass: "grid"
+    #: (one grid-wide barrier) or "neighbour" (each tile waits for the tiles it
+    #: shares boundary vertices with)
+    persistent_sync = "grid"
+
+    def _tile_neighbours(self):
+        """CSR of the tiles each tile shares a boundary vertex with (itself excluded)."""
+        import scipy.sparse as sp
+        L = self.layout
+        nt = L.n_tiles
+        counts = np.diff(L.tile_vptr)
+        tile_of = np.repeat(np.arange(nt), counts)
+        local = np.arange(L.tile_verts.shape[0]) - np.repeat(L.tile_vptr[:-1], counts)
+        bnd = local >= np.repeat(L.tile_nint, counts)
+        M = sp.csr_matrix((np.ones(int(bnd.sum()), np.int8), (tile_of[bnd], L.tile_verts[bnd])),
+                          shape=(nt, L.n_verts))
+        A = (M @ M.T).tocsr()
+        A.setdiag(0)
+        A.eliminate_zeros()
+        A.sort_indices()
+        return A.indptr.astype(np.int32), A.indices.astype(np.int32)
+
     def _build_persist(self, slots: int) -> None:
         """Persistent-pass launch descriptors for tile ranges of at most
         ``slots`` tiles (one set of barrier words per range)."""
         ranges = self._persist_ranges(int(slots))
         if 4 * len(ranges) > self._psync.numel():
             self._psync = torch.zeros(4 * len(ranges), dtype=torch.int32, device=self.device)
+        ptr, idx = self._tile_neighbours()
+        self._t_nbr_ptr = torch.from_numpy(ptr).to(self.device)
+        self._t_nbr_idx = torch.from_numpy(idx if idx.size else np.zeros(1, np.int32)).to(self.device)
+        self._t_cnt = torch.zeros(self.layout.n_tiles, dtype=torch.int32, device=self.device)
         # a vertex's ring slots follow its range's phase word: start all over
         with torch.cuda.stream(self._stream):
             self._ring.zero_()
             self._psync.zero_()
         self._stream.synchronize()
         self._persist = []
+        nb = self.persistent_sync == "neighbour"
         for k, (b, e) in enumerate(ranges):
             ps = capi.XpbdPersist()
             ps.tile_own, ps.ring, ps.status = _ptr(self._t_own), _ptr(self._ring), _ptr(self._pstatus)
             ps.sync = self._psync.data_ptr() + 16 * k
             ps.tile_begin, ps.tile_end = b, e
+            if nb:
+                ps.nbr_ptr, ps.nbr_idx, ps.tile_cnt = (_ptr(self._t_nbr_ptr), _ptr(self._t_nbr_idx),
+                                                       _ptr(self._t_cnt))
             self._persist.append(ps)
         self._persist_fits = bool(ranges)
 
@@ -359,6 +389,7 @@ class XpbdEngine:
             with torch.cuda.stream(self._stream):
                 self._ring.zero_()
                 self._psync.zero_()
+                self._t_cnt.zero_()
                 self._pstatus.zero_()
             self._stream.synchronize()
         return st
@@ -397,6 +428,7 @@ class XpbdEngine:
         with torch.cuda.stream(self._stream):
             self._ring.zero_()
             self._psync.zero_()
+            self._t_cnt.zero_()
             self._pstatus.zero_()
             dcd = getattr(self, "dcd", None)
             if dcd is not None:
