@@ -491,6 +491,8 @@ def iterations_to(err_by_n: dict, tol_mm: float):
             if k == 0:
                 return float(n)
             n0, e0 = ns[k - 1], worst[k - 1]
+            if e <= 0.0:  # the reference itself (n = conv_iters): interpolate linearly
+                return float(n0 + (e0 - tol_mm) / e0 * (n - n0))
             t = (math.log(e0) - math.log(tol_mm)) / max(math.log(e0) - math.log(e), 1e-12)
             return float(n0 + t * (n - n0))
     return None
