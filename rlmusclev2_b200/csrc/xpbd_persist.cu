@@ -107,34 +107,54 @@ __global__ void __launch_bounds__(kThreads, MINB)
         s_att[i] = (f & XPBD_VF_ATTACH_MASK) ? reinterpret_cast<const float4*>(V.attach_target)[g] : z4;
         s_pin[i] = (f & XPBD_VF_PIN) ? reinterpret_cast<const float4*>(V.pin_target)[g] : z4;
     }
+    // The accumulators start zeroed and each vertex's are zeroed again where
+    // they are read (the finish or the boundary push), so no clearing pass
+    // runs between iterations.
+    for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
+        s_ax[i] = 0;
+        s_ay[i] = 0;
+        s_az[i] = 0;
+        s_cnt[i] = 0;
+    }
+    // Finish of tile vertex i from its sum a; only the staged data its flags use is read.
+    auto finish_local = [&](int i, float4 a) {
+        const int f = s_f[i];
+        float4 at = z4, pv = z4, pin = z4;
+        if (f & XPBD_VF_ATTACH_MASK) {
+            at = s_att[i];
+            pv = s_prev[i];
+        }
+        if (f & XPBD_VF_PIN) pin = s_pin[i];
+        float4 pp = s_pos[i];
+        finish_core(prm, f, at, pv, pin, pp, a, ops);
+        s_pos[i] = pp;
+    };
+    auto take_acc = [&](int i) {
+        const float4 a = tile_acc(s_ax, s_ay, s_az, s_cnt, i, inv_scale);
+        s_ax[i] = 0;
+        s_ay[i] = 0;
+        s_az[i] = 0;
+        s_cnt[i] = 0;
+        return a;
+    };
     for (int it = 0; it < n_iters; ++it) {
         const uint32_t cur = (phase0 + uint32_t(it)) % 3u, nxt = (phase0 + uint32_t(it) + 1u) % 3u;
         float4* rc = ring + cur * nv;
         float4* rn = ring + nxt * nv;
-        for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
-            s_ax[i] = 0;
-            s_ay[i] = 0;
-            s_az[i] = 0;
-            s_cnt[i] = 0;
-        }
-        __syncthreads();
+        __syncthreads();  // staged or finished positions, zeroed accumulators
         if constexpr (X2 && CSET != CSET_FULL && !DAMP)
             project_tile_tets_x2<CSET == CSET_VOL>(prm, T, tile, s_pos, s_ax, s_ay, s_az, s_cnt, s_arap_at);
         else
             project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at);
         __syncthreads();
-        for (int i = threadIdx.x; i < nint; i += blockDim.x) {
-            float4 pp = s_pos[i];
-            finish_core(prm, s_f[i], s_att[i], s_prev[i], s_pin[i], pp,
-                        tile_acc(s_ax, s_ay, s_az, s_cnt, i, inv_scale), ops);
-            s_pos[i] = pp;
-        }
+        // boundary partial sums first, so their L2 atomics overlap the interior finish
         for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
             const int g = s_g[i];
-            const float4 a = tile_acc(s_ax, s_ay, s_az, s_cnt, i, inv_scale);
+            const float4 a = take_acc(i);
             if (a.w != 0.f) atomicAdd(&rc[g], a);
             if (g >= own_lo && g < own_hi) rn[g] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
+        for (int i = threadIdx.x; i < nint; i += blockDim.x) finish_local(i, take_acc(i));
         // vertices in no tet: attach and pin only, each handled by one thread
         for (int g = orph_lo + int(blockIdx.x) * blockDim.x + threadIdx.x; g < V.n; g += gridDim.x * blockDim.x) {
             float4 pp = pos4[g];
@@ -145,11 +165,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
             neighbour_sync(P.tile_cnt, nbr, n_nbr, tile, c0 + uint32_t(it) + 1u, P.status);
         else
             grid_barrier(bar, P.status);
-        for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {
-            float4 pp = s_pos[i];
-            finish_core(prm, s_f[i], s_att[i], s_prev[i], s_pin[i], pp, __ldcg(&rc[s_g[i]]), ops);
-            s_pos[i] = pp;
-        }
+        for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) finish_local(i, __ldcg(&rc[s_g[i]]));
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
