@@ -160,32 +160,20 @@ enum : uint32_t {
     MAT_DAMPED = 1u << 4,  // some constraint of this material reads pprev
 };
 
-// One scaled Newton step on the columns x0..x2 of X, given c0 = x1 x x2 and
-// det = det X > 0.  Scaling g ~ det^(-1/3) only sets the convergence speed: at
-// the fixed point det = 1, and a relative error e in g moves the iterate by
-// O(e^2), so the fast approximate power and divide are enough.
-__device__ __forceinline__ void polar_newton_step(const float3& x0, const float3& x1, const float3& x2,
-                                                  const float3& c0, float det, float3& y0, float3& y1, float3& y2) {
-    const float3 c1 = cross(x2, x0), c2 = cross(x0, x1);
-    const float g = __powf(det, -0.33333334f);
-    const float h = __fdividef(0.5f, g * det);  // 1 / (2 g det)
-    const float a = 0.5f * g;
-    y0 = a * x0 + h * c0;
-    y1 = a * x1 + h * c1;
-    y2 = a * x2 + h * c2;
-}
-
 // Rotation factor R of F = R S for det F > 0, by Higham's scaled Newton
-// iteration X <- (g X + (g X)^-T) / 2, g = |det X|^(-1/3) (N. J. Higham,
+// iteration X <- (g X + (g X)^-T) / 2, g = det(X)^(-1/3) (N. J. Higham,
 // "Computing the polar decomposition with applications", SIAM J. Sci. Stat.
-// Comput. 7, 1986).  X^-T = cof(X)/det X with the cofactor columns as cross
-// products of X's columns.  The iteration keeps det X > 0 when it starts
-// there, so after the start test the first two steps run untested: nearly
-// every tet needs two or three, and a warp runs as many as its slowest lane
-// needs, so testing them only adds work (and a converged tet stays put under
-// a further step).  From the third step on the step length is tested.
-// Returns false (caller falls back to the SVD) for det F <= tiny or when 10
-// steps do not converge.
+// Comput. 7, 1986).  With the cofactor matrix C = det(X) X^-T (columns: cross
+// products of X's columns) the step is X <- (g/2) (X + g C).  The iteration is
+// invariant to a positive factor on X (g X does not change), so the factor
+// g/2 is dropped and X <- X + g C is iterated (one FMA per entry); only the
+// result is scaled by the last g/2.  The iteration keeps det X > 0 when it
+// starts there, so after the start test the first two steps run untested:
+// nearly every tet needs two or three, a warp runs as many as its slowest
+// lane, and a converged tet stays put under a further step.  From the third
+// step on, the step of the unit-determinant iterates, (g/2)(g C - X), is
+// tested.  Returns false (caller falls back to the SVD) for det F <= tiny or
+// when 10 steps do not converge.
 __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
     float3 x0 = make_float3(F.m[0][0], F.m[1][0], F.m[2][0]);
     float3 x1 = make_float3(F.m[0][1], F.m[1][1], F.m[2][1]);
@@ -195,28 +183,33 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
     float det = dot(x0, c0);
     // det > 1e-6 |F|_F^3, squared to avoid the square root
     if (!(det > 0.f && det * det > 1e-12f * (n2 * n2 * n2))) return false;
-    polar_newton_step(x0, x1, x2, c0, det, x0, x1, x2);
-    c0 = cross(x1, x2);
-    det = dot(x0, c0);
-    polar_newton_step(x0, x1, x2, c0, det, x0, x1, x2);
-    c0 = cross(x1, x2);
-    det = dot(x0, c0);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const float3 c1 = cross(x2, x0), c2 = cross(x0, x1);
+        const float g = __powf(det, -0.33333334f);
+        x0 = x0 + g * c0;
+        x1 = x1 + g * c1;
+        x2 = x2 + g * c2;
+        c0 = cross(x1, x2);
+        det = dot(x0, c0);
+    }
 #pragma unroll 1
     for (int it = 2; it < 10; ++it) {
         if (!(det > 0.f)) return false;
-        float3 y0, y1, y2;
-        polar_newton_step(x0, x1, x2, c0, det, y0, y1, y2);
-        const float3 e0 = y0 - x0, e1 = y1 - x1, e2 = y2 - x2;
-        const float ch = dot(e0, e0) + dot(e1, e1) + dot(e2, e2);
-        x0 = y0;
-        x1 = y1;
-        x2 = y2;
+        const float3 c1 = cross(x2, x0), c2 = cross(x0, x1);
+        const float g = __powf(det, -0.33333334f);
+        const float3 d0 = g * c0 - x0, d1 = g * c1 - x1, d2 = g * c2 - x2;
+        const float dd = dot(d0, d0) + dot(d1, d1) + dot(d2, d2);
+        x0 = (x0 + x0) + d0;  // X + g C
+        x1 = (x1 + x1) + d1;
+        x2 = (x2 + x2) + d2;
         // step <= 1e-4: Newton's quadratic convergence leaves an error ~|step|^2/2 = 5e-9
         // after this update, below the FP32 resolution of R's entries
-        if (ch <= 1e-8f) {
-            R.m[0][0] = x0.x; R.m[1][0] = x0.y; R.m[2][0] = x0.z;
-            R.m[0][1] = x1.x; R.m[1][1] = x1.y; R.m[2][1] = x1.z;
-            R.m[0][2] = x2.x; R.m[1][2] = x2.y; R.m[2][2] = x2.z;
+        if (dd * (g * g) <= 4e-8f) {
+            const float h = 0.5f * g;
+            R.m[0][0] = h * x0.x; R.m[1][0] = h * x0.y; R.m[2][0] = h * x0.z;
+            R.m[0][1] = h * x1.x; R.m[1][1] = h * x1.y; R.m[2][1] = h * x1.z;
+            R.m[0][2] = h * x2.x; R.m[1][2] = h * x2.y; R.m[2][2] = h * x2.z;
             return true;
         }
         c0 = cross(x1, x2);

@@ -52,7 +52,7 @@ __device__ __forceinline__ V2 vaxpy2(f2 s, const V2& a, f2 t, const V2& c) {
 }
 
 // One scaled Newton step X <- g X / 2 + (g X)^-T / 2 on the columns of both
-// tets' X (polar_newton_step in xpbd_device.cuh, per lane).  c0 = x1 x x2 and
+// tets' X (Higham's scaled Newton step, per lane).  c0 = x1 x x2 and
 // det = x0 . c0 come in; the new columns overwrite x0..x2 and the squared
 // step norm is returned.
 __device__ __forceinline__ f2 polar_step2(V2& x0, V2& x1, V2& x2, const V2& c0, f2 det) {
