@@ -385,7 +385,7 @@ def run_ours(args):
         for it in range(sim.fine_iters):
             a, b = ev(), ev()
             a.record(stream)
-            sim._fused_iteration()
+            sim._hook_iteration()
             b.record(stream)
             iters.append((a, b, 1))
             for fn in sim.collision_solvers_iter:
@@ -406,7 +406,9 @@ def run_ours(args):
         traffic = json.loads(TRAFFIC.read_text()).get(args.config, {}).get("bytes_per_iteration")
     except (OSError, ValueError):
         pass
-    per_iter = 2 + (3 if getattr(sim, "dcd", None) is not None else 0)
+    hook_persistent = bool(sim._persist_fits and getattr(sim, "persistent_between_hooks", False)
+                           and sim.use_persistent)
+    per_iter = (1 if hook_persistent else 2) + (3 if getattr(sim, "dcd", None) is not None else 0)
     fine = len(sim._persist) if persistent else sim.fine_iters * per_iter
     coarse = 0
     if sim.mg is not None:
@@ -438,7 +440,10 @@ def run_ours(args):
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": ("k_iterate_persistent (all Jacobi iterations of a substep in one launch; "
                                 "time per iteration, inside a frame)") if persistent else
-                               "k_project_tiles + k_apply_list (one Jacobi iteration, timed inside a frame)",
+                               ("k_iterate_persistent (one launch per iteration, a hook between iterations)"
+                                if (sim._persist_fits and getattr(sim, "persistent_between_hooks", False)
+                                    and sim.collision_solvers_iter and sim.use_persistent)
+                                else "k_project_tiles + k_apply_list (one Jacobi iteration, timed inside a frame)"),
                      "algorithmic_bytes": alg_bytes, "iteration_us": round(it_ms * 1e3, 2),
                      "frame_roofline_ms": round(alg_bytes * n_iter / (peak * 1e9) * 1e3, 4)},
         "clocks": clk.summary(),

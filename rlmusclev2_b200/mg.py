@@ -59,6 +59,9 @@ def scene_from_cfg(cfg: dict) -> Scene:
 class MultiGridSim(MuscleSim):
     """One-way pin-to-target XPBD solver (mg.py:85)."""
 
+    #: iterations followed by a hook (the DCD) as one-iteration persistent launches
+    persistent_between_hooks = True
+
     def __init__(self, cfg: dict, device: str | None = "cuda:0", scene: Scene | None = None):
         self.cfg = cfg
         self._device_str = device or "cuda:0"
@@ -713,9 +716,19 @@ class MultiGridSim(MuscleSim):
             self._fused_iterations(self.fine_iters)
             return
         for it in range(self.fine_iters):
-            self._fused_iteration()
+            self._hook_iteration()
             for fn in self.collision_solvers_iter:
                 fn(it)
+
+    def _hook_iteration(self) -> None:
+        """One fused iteration before a hook: a one-iteration persistent launch
+        (one kernel, vertices staged once) when the tiles fit and
+        ``persistent_between_hooks`` is set, else the per-iteration tile pass
+        and boundary launch."""
+        if self.persistent_between_hooks:
+            self._fused_iterations(1)
+        else:
+            self._fused_iteration()
 
     def step_frame(self, frame: int) -> None:
         """mg.py:1409-1418: kinematic step then nsubsteps substeps at that pose.
