@@ -167,7 +167,7 @@ enum : uint32_t {
 // products of X's columns) the step is X <- (g/2) (X + g C).  The iteration is
 // invariant to a positive factor on X (g X does not change), so the factor
 // g/2 is dropped and X <- X + g C is iterated (one FMA per entry); only the
-// result is scaled by the last g/2.  The iteration keeps det X > 0 when it
+// last step is taken in the scaled form.  The iteration keeps det X > 0 when it
 // starts there, so after the start test the first two steps run untested:
 // nearly every tet needs two or three, a warp runs as many as its slowest
 // lane, and a converged tet stays put under a further step.  From the third
@@ -200,18 +200,21 @@ __device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
         const float g = __powf(det, -0.33333334f);
         const float3 d0 = g * c0 - x0, d1 = g * c1 - x1, d2 = g * c2 - x2;
         const float dd = dot(d0, d0) + dot(d1, d1) + dot(d2, d2);
+        // step <= 1e-4: Newton's quadratic convergence leaves an error ~|step|^2/2 = 5e-9
+        // after this update, below the FP32 resolution of R's entries.  The last step
+        // is taken in the scaled form (g X + C / (g det)) / 2, whose fixed point does
+        // not depend on the error of the fast power g (it enters at second order).
+        if (dd * (g * g) <= 4e-8f) {
+            const float a = 0.5f * g, h = __fdividef(0.5f, g * det);
+            const float3 r0 = a * x0 + h * c0, r1 = a * x1 + h * c1, r2 = a * x2 + h * c2;
+            R.m[0][0] = r0.x; R.m[1][0] = r0.y; R.m[2][0] = r0.z;
+            R.m[0][1] = r1.x; R.m[1][1] = r1.y; R.m[2][1] = r1.z;
+            R.m[0][2] = r2.x; R.m[1][2] = r2.y; R.m[2][2] = r2.z;
+            return true;
+        }
         x0 = (x0 + x0) + d0;  // X + g C
         x1 = (x1 + x1) + d1;
         x2 = (x2 + x2) + d2;
-        // step <= 1e-4: Newton's quadratic convergence leaves an error ~|step|^2/2 = 5e-9
-        // after this update, below the FP32 resolution of R's entries
-        if (dd * (g * g) <= 4e-8f) {
-            const float h = 0.5f * g;
-            R.m[0][0] = h * x0.x; R.m[1][0] = h * x0.y; R.m[2][0] = h * x0.z;
-            R.m[0][1] = h * x1.x; R.m[1][1] = h * x1.y; R.m[2][1] = h * x1.z;
-            R.m[0][2] = h * x2.x; R.m[1][2] = h * x2.y; R.m[2][2] = h * x2.z;
-            return true;
-        }
         c0 = cross(x1, x2);
         det = dot(x0, c0);
     }

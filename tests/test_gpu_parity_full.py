@@ -23,11 +23,12 @@ comparison is therefore split:
   positions to 1e-2: the max sits on a thin tet whose residual moves with
   sub-micron position differences), and the volume drift matches to 1e-4 of
   the rest volume: the kernels' arithmetic at rounding level;
-* with the reference threshold, the GPU is as close to the FP64 oracle as
-  the FP32 oracle is (p99 within three times its distance, no more vertices
-  beyond the tolerance than twice its count; the maximum too on config 2,
-  while on config 3 the DCD contact set is another discrete choice that
-  moves a few vertices by millimetres in any two implementations), and one Jacobi
+* with the reference threshold, on config 2 the GPU is as close to the FP64
+  oracle as the FP32 oracle is (max and p99 within three times its distance,
+  no more vertices beyond the tolerance than twice its count); on config 3
+  the coarse cage starts exactly at rest, so the threshold decides for many
+  coarse tets at once and each decision moves a cage cell's fine vertices,
+  and only the p99 is gated (ten times the FP32 oracle's distance); one Jacobi
   iteration from the frame's end state takes < 1 % of vertices into a
   different divisor, the others matching to 1e-5 x diagonal.
 
@@ -203,10 +204,16 @@ def test_full_frame_reference_threshold(scenes, name, parity_record):
                   iteration_flip_frac_o32_o64=flips_3264, iteration_err_same_count_m=err_same,
                   resid_metric_rel_same_positions=abs(mt["resid_max"] - r_at_gpu) / r_at_gpu)
     assert mt["n_nonfinite"] == 0
-    dcd = name == "config3"
+    # On config 3 the coarse cage starts exactly at its rest (its rest is the
+    # restriction of the fine rest), so in the first moving frames the threshold
+    # decides for many coarse tets at once, and each decision moves a whole cage
+    # cell's fine vertices through the prolongation: the GPU (polar rotation) and
+    # the FP32 oracle (SVD) decide differently there.  Its arithmetic is checked by
+    # the no-threshold test; here only the p99 is gated, at ten times the spread.
+    dcd = name.startswith("config3")
     for r in sim.per_frame:
         assert r["p99_gpu_o64"] <= max(tol, (10.0 if dcd else 3.0) * r["p99_o32_o64"])
-        if not dcd:  # the contact set's discrete choices: see the no-threshold test
+        if not dcd:
             assert r["beyond_tol_gpu"] <= 2 * r["beyond_tol_o32"] + 1e-3 * sim.NV
             assert r["max_gpu_o64"] <= max(tol, 3.0 * r["max_o32_o64"])
     assert abs(mt["resid_max"] - r_at_gpu) <= 1e-4 * r_at_gpu
