@@ -60,7 +60,9 @@ class MultiGridSim(MuscleSim):
     """One-way pin-to-target XPBD solver (mg.py:85)."""
 
     #: iterations followed by a hook (the DCD) as one-iteration persistent launches
-    persistent_between_hooks = True
+    #: (one kernel instead of two; 1 % slower on config 3's 535k-tet scene, whose
+    #: one-iteration launches pay the cooperative launch and a grid barrier)
+    persistent_between_hooks = False
 
     def __init__(self, cfg: dict, device: str | None = "cuda:0", scene: Scene | None = None):
         self.cfg = cfg

@@ -9,10 +9,10 @@ per-operation rounding.  The gates are:
   * one Jacobi iteration from an identical state: vertices whose count agrees
     match dP/dPw to 1e-5 x bbox diagonal; count mismatches are confined to
     vertices with a near-threshold constraint and to < 1 % of vertices;
-  * whole frames: within the reference's own FP32 run-to-run gate, 1e-4 m
-    (tests/test_engine_parity.py:25 of the reference), or three times the
-    oracle's own FP32/FP64 spread where that is larger; the FP64 distance is
-    printed beside it;
+  * whole frames: within 1e-5 x bbox diagonal of both oracles, or within three
+    times the FP32 oracle's own distance from FP64 where that is larger (max and
+    p99); the reference's own FP32 run-to-run gate is 1e-4 m
+    (tests/test_engine_parity.py:25 of the reference);
   * max and RMS ARAP residual to 1e-4 / 1e-2 relative or three times the
     oracle's FP32/FP64 spread, relative volume drift to 1e-4.
 """
@@ -98,7 +98,7 @@ def test_one_iteration_from_identical_state():
     assert moved > 100 * tol
 
 
-def test_frames_fused_graph_vs_oracle():
+def test_frames_fused_graph_vs_oracle(parity_record):
     cfg, sc = _small()
     sim = MultiGridSim(cfg, scene=sc)
     o32 = O.OracleMultiGridSim(cfg, sc, prec="f32")
@@ -111,12 +111,18 @@ def test_frames_fused_graph_vs_oracle():
         o64.step_frame(frame)
         p = sim.positions_np()
         e32 = np.abs(p - o32.pos).max()
-        e64 = np.abs(p - o64.pos).max()
-        f3264 = np.abs(o32.pos - o64.pos).max()
-        print(f"frame {frame}: |gpu-o32| {e32:.3e} |gpu-o64| {e64:.3e} |o32-o64| {f3264:.3e} "
-              f"(1e-5 diag {1e-5 * bbox_diag(sc.verts):.3e}, ref atol {REF_ATOL})")
-        gate = max(REF_ATOL, 3.0 * f3264)
+        d64 = np.abs(p - o64.pos).max(1)
+        e64 = d64.max()
+        s3264 = np.abs(o32.pos - o64.pos).max(1)
+        f3264 = s3264.max()
+        tol = 1e-5 * bbox_diag(sc.verts)
+        parity_record(f"small_scene_frame{frame}", gpu_o32_m=e32, gpu_o64_m=e64, o32_o64_m=f3264,
+                      p99_gpu_o64_m=np.percentile(d64, 99), p99_o32_o64_m=np.percentile(s3264, 99), tol_m=tol)
+        # 1e-5 x diagonal, or as close to FP64 as the FP32 oracle is (the ARAP skip
+        # threshold and rounding make every FP32 implementation drift from FP64)
+        gate = max(tol, 3.0 * f3264)
         assert e32 <= gate and e64 <= gate
+        assert np.percentile(d64, 99) <= max(tol, 3.0 * np.percentile(s3264, 99))
     mt = sim.metrics()
     r64, r32 = o64.arap_residual(), o32.arap_residual()
     # the max residual sits on a few extreme tets that the count flips move:
