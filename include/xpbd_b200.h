@@ -196,13 +196,13 @@ enum {
 
 int xpbd_abi_version(void);
 
-/* XpbdParams.acc_scale for positions whose coordinates stay below max_coord
- * in magnitude: the largest power of two s with s x max_coord <= 2^26.  The
- * quantum 1/s is then at most half an FP32 ulp of the largest coordinate (the
- * position update cannot resolve finer steps there), a vertex's correction
- * sum may reach 32 x max_coord before the 32-bit range ends, and one tet
- * whose correction magnitudes sum above max_coord / 2 (or to NaN/Inf) sets
- * XPBD_STATUS_ACC_RANGE.
+/* XpbdParams.acc_scale for the length max_coord: the largest power of two s
+ * with s x max_coord <= 2^26.  One tet whose 12 correction magnitudes sum
+ * above 2^25 / s (between max_coord / 2 and max_coord), or to NaN/Inf, sets
+ * XPBD_STATUS_ACC_RANGE; a vertex's sum may reach 64 such tets before the
+ * 32-bit range ends; the quantum is 1/s.  The engine passes 128 x the longest
+ * rest edge of the mesh (a projection moves a sane tet's vertices by a few
+ * edge lengths), which gives 1/s = 1.5e-8 m on a mesh of 5.5 mm edges.
  * Library-specific (the reference sums corrections with float atomics). */
 float xpbd_acc_scale_for_extent(float max_coord);
 
@@ -237,6 +237,21 @@ int xpbd_apply_all(const XpbdParams* prm, const XpbdVerts* v, uint32_t ops, xpbd
 int xpbd_pin_overwrite_masked(int32_t n, const int32_t* pts, const float* target, const float* offset,
                               const int32_t* active, float* pos4, xpbd_stream_t stream);
 
+/* SVD inversion repair, XpbdEngine.repair_inverted_tets (engine.py:831-856):
+ * iters passes of (accumulate, apply).  Accumulate
+ * (_svd_clamp_accumulate_kernel, engine.py:293-367): every tet whose
+ * sign-fixed singular values of F = Ds B are not all >= sigma_min takes the
+ * edge matrix U diag(max(s, sigma_min)) V^T inverse(B), its differences
+ * d0..d2 from the current edges p_i - p3, shifted by (d0 + d1 + d2) / 4 so
+ * the centroid stays (d3 = -shift), and adds them with a count of 1 to the
+ * accumulator of each vertex that is not stopped (vel.w == 0).  Apply
+ * (_apply_svd_clamp_kernel, engine.py:370-380): pos += alpha dP / w where
+ * w > 0.  The accumulator is zeroed first and left zeroed; a no-op when
+ * iters == 0 or alpha <= 0.  Sums use float atomics (order-dependent in
+ * the last bits; the repair is off the hot pass). */
+int xpbd_svd_clamp(const XpbdTiles* tiles, const XpbdVerts* v, float sigma_min, float alpha, int32_t iters,
+                   xpbd_stream_t stream);
+
 /* Mesh metrics into out (device XpbdMetrics, zeroed by this call). */
 int xpbd_metrics(const XpbdTiles* tiles, const XpbdVerts* v, XpbdMetrics* out, xpbd_stream_t stream);
 
@@ -253,6 +268,19 @@ int xpbd_metrics(const XpbdTiles* tiles, const XpbdVerts* v, XpbdMetrics* out, x
 int xpbd_bone_targets(int32_t n, int32_t n_bones, const float* transforms, const int32_t* vert_bone,
                       const float* vert_w, const float* rest4, float* pin_target, float* attach_target,
                       xpbd_stream_t stream);
+
+/* Soft pull toward per-vertex targets: for i < n, v = idx[i] (idx NULL: v = i,
+ * n <= n_verts), pos4[v].xyz += beta (target4[v].xyz - pos4[v].xyz), one
+ * fma per component; beta finite (1 snaps, < 1 follows partly); idx entries
+ * outside [0, n_verts) are skipped.  Two reference kernels are this operation:
+ * presubframe_pintotarget_kernel (mg/kernel.py:229-257; MultiGridSim
+ * .apply_pintotarget_all, mg/mg.py:1386-1397: every constraint point blended
+ * toward target_pos + rest_offset once per kinematic step, after the hard
+ * pin) and dense_soft_attach_kernel (mg/kernel.py:64-84; the coarse cage's
+ * Neumann attach after each coarse ARAP sweep, mg/mg.py:1047-1062, idx = the
+ * coarse nodes with a nonzero restriction column). */
+int xpbd_blend_to_target(int32_t n, const int32_t* idx, int32_t n_verts, float* pos4, const float* target4,
+                         float beta, xpbd_stream_t stream);
 
 /* Bone-surface binding, the reference's target_mode="mesh" driver.  A bone
  * surface is a triangle mesh: bone4 [n_bverts][4] (x, y, z, -), btris

@@ -238,6 +238,48 @@ class OracleSolver:
         f.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, self.P.ct]
         f(self.nv, _p(self.pos), _p(self.dP), _p(self.dPw), self.P.ct(self.omega))
 
+    def svd_clamp(self, sigma_min, alpha, iters):
+        """XpbdEngine.repair_inverted_tets (engine.py:831-856): iters passes of
+        _svd_clamp_accumulate_kernel (engine.py:293-367) and
+        _apply_svd_clamp_kernel (engine.py:370-380).  The sign-fixed SVD (U, V
+        rotations, s sorted descending, sign(s2) = sign(det F)) and the target
+        edges are taken in float64; the per-vertex sums are added in tet order in
+        the oracle's precision."""
+        if alpha <= 0.0 or iters <= 0:
+            return
+        P = self.P
+        t = self.tets.astype(np.int64)
+        B = self.B.reshape(-1, 3, 3).astype(np.float64)
+        Dm = np.linalg.inv(B)
+        free = self.stopped == 0
+        for _ in range(iters):
+            x = self.pos
+            c = np.stack([x[t[:, k]] - x[t[:, 3]] for k in range(3)], -1).astype(P.dt)  # columns p_k - p3
+            F = np.einsum("nij,njk->nik", c.astype(np.float64), B)
+            U, sv, Vt = np.linalg.svd(F)
+            fu = np.linalg.det(U) < 0
+            U[fu, :, 2] *= -1
+            sv[fu, 2] *= -1
+            fv = np.linalg.det(Vt) < 0
+            Vt[fv, 2, :] *= -1
+            sv[fv, 2] *= -1
+            bad = (sv < sigma_min).any(1)
+            dP = np.zeros_like(self.pos)
+            w = np.zeros(self.nv, P.dt)
+            if bad.any():
+                Ft = np.einsum("nij,nj,njk->nik", U[bad], np.maximum(sv[bad], sigma_min), Vt[bad])
+                Dt = np.einsum("nij,njk->nik", Ft, Dm[bad])
+                d = Dt - c[bad].astype(np.float64)
+                shift = (d[:, :, 0] + d[:, :, 1] + d[:, :, 2]) * 0.25
+                corr = np.stack([d[:, :, 0] - shift, d[:, :, 1] - shift, d[:, :, 2] - shift, -shift], 1).astype(P.dt)
+                tb = t[bad]
+                for k in range(4):
+                    m = free[tb[:, k]]
+                    np.add.at(dP, tb[m, k], corr[m, k])
+                    np.add.at(w, tb[m, k], P.dt(1))
+            on = w > 0
+            self.pos[on] = (self.pos[on] + (P.dt(alpha) * dP[on]) / w[on, None]).astype(P.dt)
+
     # metrics
     def count_inverted(self):
         f = self.P.fn("orc_count_inverted")
@@ -259,7 +301,8 @@ class OracleMuscleSim(OracleSolver):
 
     def __init__(self, vertices, tets, fiber_dirs_per_tet, *, constraint_configs, dts, num_substeps=1,
                  density=1060.0, veldamping=0.02, gravity=0.0, stopped=None, relaxation=1.0,
-                 contraction_ratio=0.0, fiber_stiffness_scale=1.0, tet_masks=None, prec="f32"):
+                 contraction_ratio=0.0, fiber_stiffness_scale=1.0, tet_masks=None, repair_alpha=0.0, repair_iters=0,
+                 repair_sigma_min=0.1, prec="f32"):
         vertices = np.asarray(vertices, np.float32)
         tets = np.asarray(tets, np.int32)
         nv = vertices.shape[0]
@@ -282,11 +325,15 @@ class OracleMuscleSim(OracleSolver):
                          v_fiber=vf, contraction_ratio=contraction_ratio,
                          fiber_stiffness_scale=fiber_stiffness_scale, prec=prec)
         self.num_substeps = int(num_substeps)
+        self.repair = (float(repair_sigma_min), float(repair_alpha), int(repair_iters))
 
     def substep(self):
+        """integrate_phase, solve_phase, finalize_phase (musclesim.py:107-130)
+        with the SVD inversion repair before the velocity update."""
         self.integrate()
         self.project()
         self.apply_dP()
+        self.svd_clamp(*self.repair)
         self.update_velocities()
 
     def step(self):
@@ -407,6 +454,10 @@ class OracleMultiGridSim(OracleSolver):
         self.mg = None
         scfg = (cfg.get("demo") or {}).get("self_collision") or {}
         self.dcd = scfg if str(scfg.get("method", "none")).lower() == "udcf" else None
+        # soft pin of every vertex toward its target after the hard pin, once per
+        # kinematic step (mg.py:133, 1386-1397; presubframe_pintotarget_kernel,
+        # mg/kernel.py:229-257)
+        self.presub = float(cfg.get("presubframe_pintotarget", 0.0))
         if cfg.get("use_multigrid", False):
             self._init_mg(float(arap["stiffness"]))
 
@@ -448,6 +499,10 @@ class OracleMultiGridSim(OracleSolver):
             frac = np.where(wacc > 1e-9, pacc / wacc, 0.0)
         pin = ((frac >= float(cfg.get("mg_coarse_pin_frac", 0.5))) & (wacc > 1e-9)).astype(np.int32)
         self.mg_pin = pin.astype(bool)
+        # coarse soft attach of the nodes with a nonzero restriction column after
+        # every coarse sweep (mg.py:216, 836-841, 1047-1062)
+        self.mg_beta = float(cfg.get("mg_coarse_attach_beta", 0.0))
+        self.mg_attach = wacc > 1e-9
         t = Table()
         V0, _ = signed_rest_volume(q0, cage.coarse_tet)
         t.add(T_TETARAPSVD, cage.coarse_tet, mu, 0.0, np.arange(cage.coarse_tet.shape[0]), V0)
@@ -477,8 +532,17 @@ class OracleMultiGridSim(OracleSolver):
             out[base:base + dim] = M @ b[base:base + dim]
         return prior + out
 
+    def blend(self, pos, tgt, beta):
+        """pos + beta (tgt - pos) with one rounding per component, as the device's
+        fma (the FP32 product is exact in float64)."""
+        P = self.P
+        d = (tgt.astype(P.dt) - pos).astype(P.dt)
+        return (pos.astype(np.float64) + np.float64(P.dt(beta)) * d.astype(np.float64)).astype(P.dt)
+
     def vcycle(self):
-        """_hpbd_vcycle (mg.py:1064-1079) with beta = 0 (no coarse soft attach)."""
+        """_hpbd_vcycle (mg.py:1064-1079): restrict, kinematic pin, coarse sweeps
+        each followed by the soft attach when mg_coarse_attach_beta != 0
+        (dense_soft_attach_kernel, mg/kernel.py:64-84), delta prolongation."""
         co = self.mg
         co.pos[:] = self.restrict(self.pos, co.pos)
         prev = co.pos.copy()
@@ -487,6 +551,9 @@ class OracleMultiGridSim(OracleSolver):
         for _ in range(self.mg_iters):
             co.project()
             co.apply_dP()
+            if self.mg_beta != 0.0:
+                m = self.mg_attach
+                co.pos[m] = self.blend(co.pos[m], tgt[m], self.mg_beta)
         d = co.pos - prev
         e = self.mg_emb
         w = self.mg_w
@@ -537,6 +604,8 @@ class OracleMultiGridSim(OracleSolver):
             # coarse Dirichlet targets, restricted once per target change (mg.py:1028-1045)
             self.mg_target = self.restrict(self.target, self.mg_target)
         self.apply_pins()
+        if self.presub > 0.0:
+            self.pos[:] = self.blend(self.pos, self.target, self.presub)
         if self.coll:
             self._sdf_bake(T)
         for _ in range(self.nsub):

@@ -152,6 +152,8 @@ _SIGS = {
     "xpbd_pin_overwrite_masked": ([C.c_int32, P, P, P, P, P, P], C.c_int),
     "xpbd_metrics": ([C.POINTER(XpbdTiles), C.POINTER(XpbdVerts), P, P], C.c_int),
     "xpbd_bone_targets": ([C.c_int32, C.c_int32, P, P, P, P, P, P, P], C.c_int),
+    "xpbd_blend_to_target": ([C.c_int32, P, C.c_int32, P, P, C.c_float, P], C.c_int),
+    "xpbd_svd_clamp": ([P, P, C.c_float, C.c_float, C.c_int32, P], C.c_int),
     "xpbd_sdf_bake_capsules": ([C.POINTER(XpbdSdf), C.c_int32, P, P, C.c_float, P], C.c_int),
     "xpbd_sdf_bake_capsules_batched": ([C.POINTER(XpbdSdfBatch), C.c_int32, P, P, C.c_float, P], C.c_int),
     "xpbd_vertex_step_batched": ([C.POINTER(XpbdParams), C.POINTER(XpbdVerts), C.c_uint32, C.POINTER(XpbdSdfBatch),

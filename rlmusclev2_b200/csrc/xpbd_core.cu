@@ -299,6 +299,109 @@ __global__ void k_pin_masked(int n, const int32_t* pts, const float* target, con
 }
 
 // ---------------------------------------------------------------------------
+// SVD inversion repair (XpbdEngine.repair_inverted_tets, engine.py:831-856):
+// per tet with a signed singular value below sigma_min, the edge matrix of
+// U diag(max(s, sigma_min)) V^T Dm (Dm = inverse of the rest matrix B, as
+// _svd_clamp_accumulate_kernel, engine.py:293-367, computes it), its
+// per-vertex difference from the current edges with the centroid kept
+// (shift = (d0 + d1 + d2) / 4), added to the Jacobi accumulator of every
+// vertex that is not stopped (vel.w == 0) with a count of 1.  Float atomics:
+// the repair is a rare correction, not the hot pass.
+__device__ __forceinline__ M3 inverse3(const M3& A) {
+    M3 C;
+    C.m[0][0] = A.m[1][1] * A.m[2][2] - A.m[1][2] * A.m[2][1];
+    C.m[0][1] = A.m[0][2] * A.m[2][1] - A.m[0][1] * A.m[2][2];
+    C.m[0][2] = A.m[0][1] * A.m[1][2] - A.m[0][2] * A.m[1][1];
+    C.m[1][0] = A.m[1][2] * A.m[2][0] - A.m[1][0] * A.m[2][2];
+    C.m[1][1] = A.m[0][0] * A.m[2][2] - A.m[0][2] * A.m[2][0];
+    C.m[1][2] = A.m[0][2] * A.m[1][0] - A.m[0][0] * A.m[1][2];
+    C.m[2][0] = A.m[1][0] * A.m[2][1] - A.m[1][1] * A.m[2][0];
+    C.m[2][1] = A.m[0][1] * A.m[2][0] - A.m[0][0] * A.m[2][1];
+    C.m[2][2] = A.m[0][0] * A.m[1][1] - A.m[0][1] * A.m[1][0];
+    const float d = A.m[0][0] * C.m[0][0] + A.m[0][1] * C.m[1][0] + A.m[0][2] * C.m[2][0];
+    const float inv = 1.f / d;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) C.m[i][j] *= inv;
+    return C;
+}
+
+__global__ void __launch_bounds__(kTileThreads)
+    k_svd_clamp(const __grid_constant__ XpbdTiles T, const __grid_constant__ XpbdVerts V, float sigma_min) {
+    const int tile = blockIdx.x;
+    const int vbeg = T.tile_vptr[tile];
+    const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
+    const float4* vel4 = reinterpret_cast<const float4*>(V.vel);
+    float4* acc = reinterpret_cast<float4*>(V.accum);
+    const uint4* tq = reinterpret_cast<const uint4*>(T.tet_q);
+    const float4* tb0 = reinterpret_cast<const float4*>(T.tet_b0);
+    const float4* tb1 = reinterpret_cast<const float4*>(T.tet_b1);
+    for (int t = T.tile_tptr[tile] + threadIdx.x; t < T.tile_tptr[tile + 1]; t += blockDim.x) {
+        const uint4 q = tq[t];
+        const int g[4] = {T.tile_verts[vbeg + int(q.x & 0xffffu)], T.tile_verts[vbeg + int(q.x >> 16)],
+                          T.tile_verts[vbeg + int(q.y & 0xffffu)], T.tile_verts[vbeg + int(q.y >> 16)]};
+        const float4 b0 = tb0[t], b1 = tb1[t];
+        M3 B;
+        B.m[0][0] = b0.x; B.m[0][1] = b0.y; B.m[0][2] = b0.z;
+        B.m[1][0] = b0.w; B.m[1][1] = b1.x; B.m[1][2] = b1.y;
+        B.m[2][0] = b1.z; B.m[2][1] = b1.w; B.m[2][2] = T.tet_b2[t];
+        const float3 p3 = f3(pos4[g[3]]);
+        const float3 c[3] = {f3(pos4[g[0]]) - p3, f3(pos4[g[1]]) - p3, f3(pos4[g[2]]) - p3};
+        const Svd3 sv = svd3(deformation(c[0], c[1], c[2], B));
+        if (sv.s0 >= sigma_min && sv.s1 >= sigma_min && sv.s2 >= sigma_min) continue;
+        const float kk[3] = {fmaxf(sv.s0, sigma_min), fmaxf(sv.s1, sigma_min), fmaxf(sv.s2, sigma_min)};
+        M3 Ft;  // U diag(clamped s) V^T
+        const float U[3][3] = {{sv.u0.x, sv.u1.x, sv.u2.x}, {sv.u0.y, sv.u1.y, sv.u2.y}, {sv.u0.z, sv.u1.z, sv.u2.z}};
+        const float W[3][3] = {{sv.v0.x, sv.v1.x, sv.v2.x}, {sv.v0.y, sv.v1.y, sv.v2.y}, {sv.v0.z, sv.v1.z, sv.v2.z}};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                Ft.m[i][j] = U[i][0] * kk[0] * W[j][0] + U[i][1] * kk[1] * W[j][1] + U[i][2] * kk[2] * W[j][2];
+        const M3 Dm = inverse3(B);
+        float3 d[4];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float3 e = make_float3(Ft.m[0][0] * Dm.m[0][j] + Ft.m[0][1] * Dm.m[1][j] + Ft.m[0][2] * Dm.m[2][j],
+                                         Ft.m[1][0] * Dm.m[0][j] + Ft.m[1][1] * Dm.m[1][j] + Ft.m[1][2] * Dm.m[2][j],
+                                         Ft.m[2][0] * Dm.m[0][j] + Ft.m[2][1] * Dm.m[1][j] + Ft.m[2][2] * Dm.m[2][j]);
+            d[j] = e - c[j];
+        }
+        const float3 shift = 0.25f * ((d[0] + d[1]) + d[2]);
+        d[0] = d[0] - shift;
+        d[1] = d[1] - shift;
+        d[2] = d[2] - shift;
+        d[3] = -shift;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (vel4[g[i]].w != 0.f) continue;  // stopped
+            float* a = reinterpret_cast<float*>(acc + g[i]);
+            atomicAdd(a + 0, d[i].x);
+            atomicAdd(a + 1, d[i].y);
+            atomicAdd(a + 2, d[i].z);
+            atomicAdd(a + 3, 1.f);
+        }
+    }
+}
+
+// _apply_svd_clamp_kernel (engine.py:370-380): pos += alpha dP / w where
+// w > 0, then the accumulator is zeroed for the next pass.
+__global__ void k_svd_clamp_apply(int n, float4* pos, float4* acc, float alpha) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = acc[i];
+    if (a.w > 0.f) {
+        float4 p = pos[i];
+        p.x += (alpha * a.x) / a.w;
+        p.y += (alpha * a.y) / a.w;
+        p.z += (alpha * a.z) / a.w;
+        pos[i] = p;
+    }
+    acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kTileThreads)
     k_metrics(const __grid_constant__ XpbdTiles T, const __grid_constant__ XpbdVerts V, XpbdMetrics* out) {
     extern __shared__ float4 smem[];
@@ -565,6 +668,27 @@ int xpbd_metrics(const XpbdTiles* tiles, const XpbdVerts* v, XpbdMetrics* out, x
         cudaFuncSetAttribute(k_metrics, cudaFuncAttributeMaxDynamicSharedMemorySize, int(XPBD_MAX_TILE_VERTS * sizeof(float4)));
     k_metrics<<<tiles->n_tiles, kTileThreads, smem, s>>>(*tiles, *v, out);
     return cuda_check("xpbd_metrics");
+}
+
+int xpbd_svd_clamp(const XpbdTiles* tiles, const XpbdVerts* v, float sigma_min, float alpha, int32_t iters,
+                   xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_tiles(tiles)) || (rc = check_verts(v))) return rc;
+    if (!v->accum || !v->vel) return fail(XPBD_ERR_ARG, "xpbd_svd_clamp: accum and vel required");
+    if (!std::isfinite(sigma_min) || !std::isfinite(alpha) || iters < 0)
+        return fail(XPBD_ERR_ARG, "xpbd_svd_clamp: finite sigma_min and alpha, iters >= 0");
+    if (iters == 0 || alpha <= 0.f) return XPBD_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    // clear_dP_kernel before the first pass (engine.py:845-847); each apply pass
+    // leaves the accumulator zeroed for the next
+    if (cudaMemsetAsync(v->accum, 0, size_t(v->n) * sizeof(float4), s) != cudaSuccess)
+        return cuda_check("xpbd_svd_clamp memset");
+    for (int it = 0; it < iters; ++it) {
+        k_svd_clamp<<<tiles->n_tiles, kTileThreads, 0, s>>>(*tiles, *v, sigma_min);
+        k_svd_clamp_apply<<<(v->n + kVertThreads - 1) / kVertThreads, kVertThreads, 0, s>>>(
+            v->n, reinterpret_cast<float4*>(v->pos), reinterpret_cast<float4*>(v->accum), alpha);
+    }
+    return cuda_check("xpbd_svd_clamp");
 }
 
 int xpbd_graph_begin(xpbd_stream_t stream) {

@@ -220,10 +220,13 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_coop(XpbdDcd D, int chunk
             const int d = threadIdx.x & 255, q = threadIdx.x >> 8;
             constexpr int kQ = kSortThreads / 256;
             int tot = 0, pre = 0;
+            // the CTAs' counts are independent L2 reads: unrolled so that several
+            // are in flight at once instead of one latency per CTA
+#pragma unroll 8
             for (int bb = q; bb < G; bb += kQ) {
                 const int h = __ldcg(&hist[bb * 256 + d]);
                 tot += h;
-                if (bb < b) pre += h;
+                pre += bb < b ? h : 0;
             }
             part[q][d] = tot;
             wcnt[q][d] = pre;

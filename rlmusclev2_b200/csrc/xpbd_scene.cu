@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdio.h>
 
+#include <cmath>
+
 #include "../../include/xpbd_b200.h"
 #include "xpbd_common.cuh"
 #include "xpbd_device.cuh"
@@ -40,6 +42,22 @@ __global__ void k_bone_targets(int n, int nb, const float* __restrict__ tr, cons
         a.x = t.x; a.y = t.y; a.z = t.z;
         att[i] = a;
     }
+}
+
+// pos.xyz += beta (target.xyz - pos.xyz) on vertex v = idx[i] (or i), with
+// one rounding per component (fma); indices outside [0, nv) are skipped.
+__global__ void k_blend_to_target(int n, const int* __restrict__ idx, int nv, float4* pos,
+                                  const float4* __restrict__ tgt, float beta) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int v = idx ? idx[i] : i;
+    if (v < 0 || v >= nv) return;
+    const float4 t = tgt[v];
+    float4 p = pos[v];
+    p.x = __fmaf_rn(beta, t.x - p.x, p.x);
+    p.y = __fmaf_rn(beta, t.y - p.y, p.y);
+    p.z = __fmaf_rn(beta, t.z - p.z, p.z);
+    pos[v] = p;
 }
 
 constexpr int kBrick = 8;      // 8^3 nodes per CTA
@@ -160,6 +178,18 @@ int xpbd_bone_targets(int32_t n, int32_t n_bones, const float* transforms, const
         reinterpret_cast<float4*>(pin_target),
         reinterpret_cast<float4*>(attach_target));
     return cuda_check("xpbd_bone_targets");
+}
+
+int xpbd_blend_to_target(int32_t n, const int32_t* idx, int32_t n_verts, float* pos4, const float* target4,
+                         float beta, xpbd_stream_t stream) {
+    if (n < 0 || n_verts < 0 || (!idx && n > n_verts) || (n > 0 && (!pos4 || !target4)) || !std::isfinite(beta))
+        return fail(XPBD_ERR_ARG, "xpbd_blend_to_target: bad arguments (finite beta, n <= n_verts without idx)");
+    if (!aligned16(pos4) || !aligned16(target4))
+        return fail(XPBD_ERR_ALIGN, "xpbd_blend_to_target: [n][4] arrays must be 16-byte aligned");
+    if (n == 0 || beta == 0.f) return XPBD_OK;
+    k_blend_to_target<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        n, idx, n_verts, reinterpret_cast<float4*>(pos4), reinterpret_cast<const float4*>(target4), beta);
+    return cuda_check("xpbd_blend_to_target");
 }
 
 int xpbd_sdf_bake_capsules(const XpbdSdf* sdf, int32_t n_caps, const XpbdCapsule* caps, const float* transforms,

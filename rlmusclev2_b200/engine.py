@@ -33,7 +33,20 @@ def _ptr(t) -> int | None:
     return None if t is None else int(t.data_ptr())
 
 
-ACC_HEADROOM = 8.0
+#: the fixed-point accumulator's per-tet range: a tet whose 12 correction
+#: magnitudes sum above half to one times the larger of ACC_RANGE_EDGES longest
+#: rest edges and the largest rest coordinate raises ACC_RANGE
+ACC_RANGE_EDGES = 128.0
+
+
+def max_rest_edge(pos: np.ndarray, tets: np.ndarray) -> float:
+    """Longest of the six edges over all tets of a rest mesh."""
+    x = np.asarray(pos, np.float64)
+    t = np.asarray(tets, np.int64)
+    m = 0.0
+    for a, b in ((0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)):
+        m = max(m, float(np.sqrt(((x[t[:, a]] - x[t[:, b]]) ** 2).sum(1)).max(initial=0.0)))
+    return m
 
 
 def status_error(tile_status: int, dcd_status: int = 0) -> str | None:
@@ -161,13 +174,23 @@ class XpbdEngine:
         for i, m in enumerate(L.materials):
             for k, v in m.items():
                 setattr(prm.materials[i], k, v)
-        # fixed-point accumulation scale of the tile passes, sized for coordinates up
-        # to ACC_HEADROOM x the largest rest coordinate (a mesh may travel or stretch
-        # that far: the 1-iteration box muscle sags to 5x its length, with single-tet
-        # corrections of 10 cm): a quantum of at most 4 FP32 ulps of the largest rest
-        # coordinate, far below the parity tolerance, and vertex sums up to 256x it
-        prm.acc_scale = float(self._lib.xpbd_acc_scale_for_extent(
-            ACC_HEADROOM * float(np.abs(self.pos0_np).max())))
+        # fixed-point accumulation scale of the tile passes.  Its range must hold one
+        # tet's corrections: a few edge lengths while the state is sane (the box
+        # muscle's first sagging iterations reach 33 edges, 97 mm, summed over a
+        # tet's 12 components), or a pin's jump between two poses, bounded by the
+        # scene's extent.  Its quantum 1/acc_scale must stay well below the FP32
+        # rounding of the corrections: corrections below half a quantum are lost,
+        # a dead zone that an eighth as fine a scale showed on the 535k-tet
+        # multigrid scene (stiff fibre tets at the tendon pins settled into a
+        # different state).  Range = 64-128 longest rest edges or 0.5-1 x the
+        # largest rest coordinate, whichever is larger: quantum 1.5e-8 m on the
+        # 535k-tet scene, 7.5e-9 m on the box.
+        e = getattr(self, "_acc_range", None)
+        if e is None:
+            e = max_rest_edge(self.pos0_np, self.tet_np) if self.tet_np.size else 0.0
+            e = max(ACC_RANGE_EDGES * e, float(np.abs(self.pos0_np).max()))
+        e = max(float(e), 1e-9)
+        prm.acc_scale = float(self._lib.xpbd_acc_scale_for_extent(e))
         prm.status = self._pstatus.data_ptr()
         prm.n_attach_materials = len(self._attach_mats)
         for i, (k, d) in enumerate(self._attach_mats):
@@ -218,7 +241,9 @@ class XpbdEngine:
             flags |= np.where(np.asarray(has) != 0, capi.VF_PIN, 0).astype(np.int32)
             pin4[:, :3] = tgt
             pin4[:, 3] = (np.asarray(act) != 0)
-        if flags.any():
+        # the soft pin of all constraint points (presubframe_pintotarget) reads the
+        # pin targets even where no vertex is pinned or attached
+        if flags.any() or (pin is not None and float(getattr(self, "presubframe_pintotarget", 0.0)) > 0.0):
             dev = self.device
             self._vflags = torch.from_numpy(flags[L.perm]).to(dev)
             self._attach_tgt = torch.from_numpy(att[L.perm]).to(dev)
@@ -486,7 +511,7 @@ class XpbdEngine:
     def post_smooth(self) -> None:
         """XpbdEngine.post_smooth (engine.py:1072-1100): extra Jacobi sweeps of the
         non-fiber constraints (every type on this path)."""
-        n = int(getattr(self, "post_smooth_iters", 0))
+        n = int(self._option("post_smooth_iters", 0))
         for _ in range(n):
             self.clear()
             self.solve_constraints(run_extras=False)
@@ -496,13 +521,33 @@ class XpbdEngine:
     def freeze_near_inverted(self) -> None:
         """XpbdEngine.freeze_near_inverted (engine.py:1102-1124): disabled on CUDA
         devices in the reference (races on shared vertices); same here."""
-        if float(getattr(self, "freeze_detF_threshold", 0.0)) > 0.0 and not getattr(self, "_freeze_warned", False):
+        if float(self._option("freeze_detF_threshold", 0.0)) > 0.0 and not getattr(self, "_freeze_warned", False):
             log.warning("freeze_near_inverted skipped on GPU (race condition on shared vertices)")
             self._freeze_warned = True
 
+    def _option(self, name: str, default):
+        """An engine option: an attribute of the engine, else of its config (a
+        dict or the reference's SimConfig object)."""
+        if hasattr(self, name):
+            return getattr(self, name)
+        cfg = getattr(self, "cfg", None)
+        if isinstance(cfg, dict):
+            return cfg.get(name, default)
+        return getattr(cfg, name, default)
+
     def repair_inverted_tets(self) -> None:
-        if float(getattr(self, "repair_alpha", 0.0)) > 0.0 and int(getattr(self, "repair_iters", 0)) > 0:
-            raise NotImplementedError("SVD inversion repair is not on the sm_100a path")
+        """XpbdEngine.repair_inverted_tets (engine.py:831-856): repair_iters
+        passes of the SVD clamp (singular values raised to repair_sigma_min,
+        Jacobi-averaged, blended by repair_alpha); off unless repair_alpha > 0
+        and repair_iters > 0."""
+        alpha = float(self._option("repair_alpha", 0.0))
+        iters = int(self._option("repair_iters", 0))
+        if alpha <= 0.0 or iters <= 0:
+            return
+        sigma_min = float(self._option("repair_sigma_min", 0.1))
+        capi.check(self._lib.xpbd_svd_clamp(C.byref(self._tiles), C.byref(self._verts), C.c_float(sigma_min),
+                                            C.c_float(alpha), iters, self._sp))
+        self._accum_dirty = False  # the clamp leaves the accumulator zeroed
 
     def run_program(self) -> None:
         """XpbdEngine.run_program (engine.py:1126-1134)."""
@@ -647,7 +692,11 @@ class XpbdSolver(XpbdEngine):
     def __init__(self, verts, tets, table: ConstraintTable, *, mass, dt, stopped=None, gravity=(0.0, 0.0, 0.0),
                  veldamping=0.0, quasi_static=False, relaxation=1.0, v_fiber=None, tet_tendonmask=None,
                  contraction_ratio=0.0, fiber_stiffness_scale=1.0, device="cuda:0", tile_tets=None, pins=None,
-                 num_substeps=1, total_rest_volume=None, stream=None):
+                 num_substeps=1, total_rest_volume=None, stream=None, acc_range=None):
+        """``acc_range``: the length the fixed-point accumulator's per-tet range is
+        sized for (default: the larger of 128 longest rest edges and the largest
+        rest coordinate)."""
+        self._acc_range = acc_range
         self.pos0_np = np.asarray(verts, np.float32)
         self.tet_np = np.asarray(tets, np.int32)
         self.n_verts = self.pos0_np.shape[0]

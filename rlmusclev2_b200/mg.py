@@ -84,9 +84,9 @@ class MultiGridSim(MuscleSim):
         self.dt_frame = float(cfg["delta_t"])
         self.nsubsteps = int(cfg["nsubsteps"])
         self.num_substeps = self.nsubsteps
+        # soft pin of every constraint point toward its bone target after the hard
+        # pin, once per kinematic step (mg.py:133, 1386-1397); 0 = off
         self.presubframe_pintotarget = float(cfg.get("presubframe_pintotarget", 0.0))
-        if self.presubframe_pintotarget > 0.0:
-            raise NotImplementedError("presubframe_pintotarget > 0 is not on the sm_100a path")
         self.fine_iters = int(cfg["fine_iterations"])
         # density: total_mass spread over the signed rest volume (mg.py:736-740),
         # or a fixed "density" (kg/m^3, the MuscleSim.from_procedural form)
@@ -320,9 +320,11 @@ class MultiGridSim(MuscleSim):
         self._act_event.record(self._stream)
         self._h2d_event = torch.cuda.Event()
         self._h2d_event.record(self._stream)
+        self._presub_idx = None  # constraint points of the soft pin: all vertices
         if self.target_mode == "points":
             self._pts_tgt = torch.zeros((self.NV, 3), dtype=torch.float32, device=dev)
             self._pts_host = torch.zeros((self.NV, 3), dtype=torch.float32).pin_memory()
+            self._presub_idx = torch.from_numpy(L.inv[self._cons_pts].astype(np.int32)).to(dev)
         if self.target_mode == "mesh":
             self._setup_surface_binding()
 
@@ -614,6 +616,21 @@ class MultiGridSim(MuscleSim):
         if self._has_pins:
             self._apply_all(capi.APPLY_PIN)
 
+    def apply_pintotarget_all(self) -> None:
+        """Soft pin (apply_pintotarget_all, mg/mg.py:1386-1397): every constraint
+        point moves by presubframe_pintotarget x (target - pos) toward its pin
+        target (target_pos + rest_offset); a no-op when the factor is <= 0.  The
+        constraint points are all vertices, or the cons file's points when
+        target_mode="points"."""
+        b = self.presubframe_pintotarget
+        if b <= 0.0 or self._pin_tgt is None:
+            return
+        idx = getattr(self, "_presub_idx", None)
+        n = self.n_verts if idx is None else int(idx.shape[0])
+        capi.check(self._lib.xpbd_blend_to_target(n, C.c_void_p(idx.data_ptr()) if idx is not None else None,
+                                                  self.n_verts, C.c_void_p(self._pos4.data_ptr()),
+                                                  C.c_void_p(self._pin_tgt.data_ptr()), C.c_float(b), self._sp))
+
     def _vstep_sdf_only(self, coll) -> None:
         sdf = coll.struct()
         capi.check(self._lib.xpbd_vertex_step(C.byref(self._prm), C.byref(self._verts), capi.OP_SDF, C.byref(sdf),
@@ -659,7 +676,7 @@ class MultiGridSim(MuscleSim):
         self.mg.vcycle(pin_fine=False)
 
     def _kinematic_step(self, t: float) -> None:
-        """mg.py:1396-1407: targets for frame t, hard pin (presubframe soft pin is 0)."""
+        """mg.py:1399-1407: targets for frame t, hard pin, soft pin of all points."""
         if self._frame_loaded != t:
             self.load_frame_targets(t)
         self._targets_kernel()
@@ -668,6 +685,7 @@ class MultiGridSim(MuscleSim):
         if getattr(self, "bone_collider", None) is not None:
             self.bone_collider.bake()
         self.apply_pintotarget()
+        self.apply_pintotarget_all()
 
     def _fusable(self) -> bool:
         cs = getattr(self, "collision_solvers", None) or []
@@ -690,6 +708,7 @@ class MultiGridSim(MuscleSim):
         pin = capi.OP_PIN if self._has_pins else 0
         if pin:
             self._vstep(capi.OP_PIN)
+        self.apply_pintotarget_all()
         vel = 0 if self.quasi_static else capi.OP_VELOCITY
         push = capi.OP_SDF if sdf is not None else 0
         for sub in range(self.nsubsteps):

@@ -3,8 +3,10 @@
 Per substep, after the prediction: restrict the fine state onto the cage
 (Galerkin least squares, snapshot q_j, kinematic pin of the coarse Dirichlet
 nodes), ``mg_coarse_iters`` Jacobi ARAP-SVD sweeps of the cage (its own tile
-engine, pins held by zero inverse mass), then add the coarse displacement
-back onto the fine vertices (delta prolongation) and re-pin.  The restricted
+engine, pins held by zero inverse mass; with mg_coarse_attach_beta != 0 each
+sweep is followed by the soft attach of the referenced nodes), then add the
+coarse displacement back onto the fine vertices (delta prolongation) and
+re-pin.  The restricted
 bone target that drives the coarse pins is recomputed once per frame (it is
 constant across a frame's substeps).
 """
@@ -80,13 +82,21 @@ class DeviceMultigrid:
             frac = np.where(wacc > 1e-9, pacc / wacc, 0.0)
         pin_frac = float(cfg.get("mg_coarse_pin_frac", 0.5))
         self.coarse_pin = ((frac >= pin_frac) & (wacc > 1e-9)).astype(np.int32)
+        # coarse Neumann attach (mg.py:216, 1047-1062): after every coarse sweep the
+        # nodes with a nonzero restriction column move by beta x (target - pos)
+        # toward their restricted bone target; 0 = pure ARAP relax
         self.beta = float(cfg.get("mg_coarse_attach_beta", 0.0))
-        if self.beta != 0.0:
-            raise NotImplementedError("mg_coarse_attach_beta != 0 is not on the sm_100a path")
+        self.attach_nodes = np.nonzero(wacc > 1e-9)[0]
         table = collect_raw_constraints(q0, cage.coarse_tet, [dict(type="tetarapsvd", name="arap",
                                                                     stiffness=sim.mu)]).sorted_by_type()
+        # the cage's per-tet corrections stay far below its extent (its cells are
+        # 16 mm, a smooth correction of the fine state), so its accumulator is
+        # sized by the extent alone: a quantum of 1.5e-8 m on the 535k-tet scenes,
+        # where 128 cage edges (3.5 m) would give 6e-8 m.  Coarse corrections
+        # below half a quantum are lost (a dead zone), and the multigrid scene's
+        # stiff tendon tets are sensitive to that at 6e-8 m.
         self.coarse = XpbdSolver(q0, cage.coarse_tet, table, mass=mass, dt=sim.dt, stopped=self.coarse_pin,
-                                 device=sim.device, stream=sim._stream)
+                                 device=sim.device, stream=sim._stream, acc_range=float(np.abs(q0).max()))
         self.iters = int(sim.mg_coarse_iters)
         self._build_device()
 
@@ -132,6 +142,7 @@ class DeviceMultigrid:
         pin4[:, :3] = self.q0  # prior of the first target restriction
         pin4[:, 3] = self.coarse_pin
         self.pin4 = T(pin4[cl.perm])
+        self.attach_idx = T(cl.inv[self.attach_nodes].astype(np.int32))
 
     def refresh_target(self):
         """Coarse Dirichlet targets = restriction of the fine bone targets (mg.py:1028-1045)."""
@@ -145,7 +156,16 @@ class DeviceMultigrid:
         capi.check(s._lib.xpbd_mg_restrict(C.byref(self.g), C.c_void_p(s._pos4.data_ptr()),
                                            C.c_void_p(co._pos4.data_ptr()), C.c_void_p(self.prev.data_ptr()),
                                            C.c_void_p(self.pin4.data_ptr()), s._sp))
-        co._fused_iterations(self.iters)
+        if self.beta != 0.0:
+            for _ in range(self.iters):  # ARAP sweep, then the soft attach (mg.py:1057-1062)
+                co._fused_iterations(1)
+                capi.check(s._lib.xpbd_blend_to_target(int(self.attach_idx.shape[0]),
+                                                       C.c_void_p(self.attach_idx.data_ptr()), co.n_verts,
+                                                       C.c_void_p(co._pos4.data_ptr()),
+                                                       C.c_void_p(self.pin4.data_ptr()), C.c_float(self.beta),
+                                                       s._sp))
+        else:
+            co._fused_iterations(self.iters)
         vf = s._vflags.data_ptr() if (pin_fine and s._vflags is not None) else None
         pt = s._pin_tgt.data_ptr() if (pin_fine and s._pin_tgt is not None) else None
         capi.check(s._lib.xpbd_mg_prolong_delta(C.byref(self.g), C.c_void_p(co._pos4.data_ptr()),

@@ -161,7 +161,8 @@ class MuscleSim(XpbdEngine):
         self.program = [integrate_phase, solve_phase, finalize_phase]
 
     def _hooks(self) -> bool:
-        return bool(getattr(self, "constraint_solvers", None)) or int(getattr(self, "post_smooth_iters", 0)) > 0
+        return (bool(getattr(self, "constraint_solvers", None)) or int(self._option("post_smooth_iters", 0)) > 0
+                or (float(self._option("repair_alpha", 0.0)) > 0.0 and int(self._option("repair_iters", 0)) > 0))
 
     def _frame_fused(self) -> None:
         """One frame, fused: [predict] (tile pass + boundary finish) ... with the

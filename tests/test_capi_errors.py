@@ -119,3 +119,21 @@ def test_dcd_checks(lib):
     assert lib.xpbd_dcd_broadphase(C.byref(d), 16, 0, None) == ERR_ALIGN
     d.ws_split, d.tris = 16, None
     assert lib.xpbd_dcd_narrow_respond(C.byref(d), 16, None) == ERR_ARG
+
+
+def test_blend_to_target_checks(lib):
+    f = lib.xpbd_blend_to_target
+    assert f(-1, None, 4, None, None, C.c_float(0.5), None) == ERR_ARG           # negative count
+    assert f(8, None, 4, 16, 16, C.c_float(0.5), None) == ERR_ARG                # n > n_verts without idx
+    assert f(2, None, 4, None, 16, C.c_float(0.5), None) == ERR_ARG              # null positions
+    assert f(2, None, 4, 16, 16, C.c_float(float("nan")), None) == ERR_ARG     # non-finite beta
+    assert "beta" in _msg(lib)
+    assert f(2, None, 4, 8, 16, C.c_float(0.5), None) == ERR_ALIGN               # misaligned positions
+    assert f(0, None, 4, 16, 16, C.c_float(0.5), None) == 0                      # nothing to do
+    assert f(2, None, 4, 16, 16, C.c_float(0.0), None) == 0                      # beta 0: no launch
+
+
+def test_svd_clamp_checks(lib):
+    tiles, verts = capi.XpbdTiles(), capi.XpbdVerts()
+    assert lib.xpbd_svd_clamp(None, None, C.c_float(0.1), C.c_float(1.0), 1, None) == ERR_ARG
+    assert lib.xpbd_svd_clamp(C.byref(tiles), C.byref(verts), C.c_float(0.1), C.c_float(1.0), 1, None) == ERR_ARG

@@ -1,0 +1,82 @@
+"""Kinematic options of MultiGridSim on the GPU against the oracle:
+presubframe_pintotarget (the soft pin of every constraint point toward its
+bone target after the hard pin, mg/mg.py:1386-1407, mg/kernel.py:229-257) and
+mg_coarse_attach_beta (the coarse cage's soft attach after each coarse sweep,
+mg/mg.py:1047-1062, mg/kernel.py:64-84), on the small synthetic scene with
+the multigrid on, three frames.  Gates as for the other small-scene frame
+tests: within 1e-5 x bbox diagonal of the FP64 oracle, or three times the FP32
+oracle's own distance from it (max and p99)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rlmusclev2_b200.meshgen import humanv2_scene
+from rlmusclev2_b200.mg import MultiGridSim, load_config
+from tests._cases import bbox_diag
+
+pytestmark = pytest.mark.gpu
+CFG3 = "rlmusclev2_b200/configs/humanv2_synth_mg_dcd.json"
+
+
+def _scene(presub, beta):
+    cfg = load_config(CFG3)
+    cfg["demo"]["collision"]["sdf_res"] = 96
+    cfg["demo"]["self_collision"]["method"] = "none"
+    cfg["presubframe_pintotarget"] = presub
+    cfg["mg_coarse_attach_beta"] = beta
+    sc = humanv2_scene(seed=1, n_muscles=5, n_bones=4, target_tets=20000, fascia_tets=3000, box=(0.35, 0.35, 0.35))
+    return cfg, sc
+
+
+def _run(cfg, sc, eager=False):
+    sim = MultiGridSim(cfg, scene=sc)
+    if eager:
+        sim.build_program()
+    out = []
+    for frame in (1, 2, 3):
+        sim.set_fiber_activation(sc.activation(frame))
+        sim.step_frame(frame)
+        out.append(sim.positions_np())
+    return sim, out
+
+
+@pytest.mark.parametrize("presub,beta", [(0.5, 0.0), (0.0, 0.3), (1.0, 0.3)])
+def test_soft_pins_vs_oracle(presub, beta, parity_record):
+    cfg, sc = _scene(presub, beta)
+    sim, ps = _run(cfg, sc)
+    o32 = O.OracleMultiGridSim(cfg, sc, prec="f32")
+    o64 = O.OracleMultiGridSim(cfg, sc, prec="f64")
+    _, base = _run(*_scene(0.0, 0.0))
+    tol = 1e-5 * bbox_diag(sc.verts)
+    for frame, p, q in zip((1, 2, 3), ps, base):
+        o32.step_frame(frame)
+        o64.step_frame(frame)
+        d64 = np.abs(p - o64.pos).max(1)
+        spr = np.abs(o32.pos - o64.pos).max(1)
+        parity_record(f"soft_pins_p{presub}_b{beta}_frame{frame}", max_gpu_o64_m=d64.max(), max_o32_o64_m=spr.max(),
+                      p99_gpu_o64_m=np.percentile(d64, 99), p99_o32_o64_m=np.percentile(spr, 99),
+                      moved_by_option_m=float(np.abs(p - q).max()), tol_m=tol)
+        assert np.isfinite(p).all()
+        assert d64.max() <= max(tol, 3.0 * spr.max())
+        assert np.percentile(d64, 99) <= max(tol, 3.0 * np.percentile(spr, 99))
+    # the options act: the end state differs from the run without them by far more than the gate
+    assert np.abs(ps[-1] - base[-1]).max() > 100 * tol
+
+
+def test_soft_pin_eager_program_matches_fused():
+    cfg, sc = _scene(0.5, 0.3)
+    _, a = _run(cfg, sc)
+    _, b = _run(cfg, sc, eager=True)
+    assert np.abs(a[-1] - b[-1]).max() <= 1e-4
+
+
+def test_presubframe_one_snaps_every_vertex_before_the_substeps():
+    """With the factor 1 the kinematic step leaves every vertex on its target
+    (to the rounding of p + (t - p))."""
+    cfg, sc = _scene(1.0, 0.0)
+    sim = MultiGridSim(cfg, scene=sc)
+    sim._kinematic_step(2)
+    sim.synchronize()
+    pos = sim._pos4[:, :3].cpu().numpy()
+    tgt = sim._pin_tgt[:, :3].cpu().numpy()
+    assert np.abs(pos - tgt).max() <= 2.5e-7

@@ -1,0 +1,100 @@
+"""SVD inversion repair (XpbdEngine.repair_inverted_tets, engine.py:831-856)
+on the GPU against the oracle: a box muscle squashed to a tenth of its height
+along z (singular values ~0.1 below repair_sigma_min = 0.3) and one with a
+layer of inverted tets, stepped with the repair in the finalize phase."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rlmusclev2_b200 import MuscleSim
+from rlmusclev2_b200.meshgen import box_muscle
+from tests._cases import bbox_diag
+
+pytestmark = pytest.mark.gpu
+CONS = [{"type": "tetarapsvd", "name": "arap", "compliance": 1e-7},
+        {"type": "volume", "name": "volume", "compliance": 0.0}]
+KW = dict(dts=1.0 / 24.0, num_substeps=10, density=1060.0, veldamping=0.02, gravity=-9.8)
+
+
+def _pair(start, alpha, iters, sigma_min):
+    m = box_muscle()
+    sim = MuscleSim.from_procedural(m.verts, m.tets, m.fiber_per_tet, constraint_configs=CONS, device="cuda:0",
+                                    stopped=m.stopped, **KW)
+    sim.repair_alpha, sim.repair_iters, sim.repair_sigma_min = alpha, iters, sigma_min
+    orc = O.OracleMuscleSim(m.verts, m.tets, m.fiber_per_tet, constraint_configs=CONS, stopped=m.stopped,
+                            repair_alpha=alpha, repair_iters=iters, repair_sigma_min=sigma_min, prec="f32", **KW)
+    sim.set_positions(start, also_prev=True)
+    orc.pos[:] = start
+    orc.pprev[:] = start
+    return m, sim, orc
+
+
+def _squashed(m):
+    c = m.verts.mean(0)
+    return (c + (m.verts - c) * np.array([1.0, 1.0, 0.1], np.float32)).astype(np.float32)
+
+
+def test_clamp_pass_matches_oracle():
+    """One repair call from the squashed state (no constraint step between)."""
+    m = box_muscle()
+    start = _squashed(m)
+    _, sim, orc = _pair(start, 1.0, 2, 0.3)
+    sim.repair_inverted_tets()
+    orc.svd_clamp(0.3, 1.0, 2)
+    p = sim.positions_np()
+    moved = np.abs(orc.pos - start).max()
+    assert moved > 1e-4
+    # float atomics add the per-vertex sums in any order: rounding level
+    assert np.abs(p - orc.pos).max() <= 1e-6 * max(1.0, float(np.abs(start).max()))
+    assert np.array_equal(p[m.stopped != 0], start[m.stopped != 0])
+
+
+@pytest.mark.parametrize("case", ["squashed", "inverted"])
+def test_steps_with_repair_match_oracle(case):
+    """Two frames with the repair in every substep.  Both starts are violent (the
+    squashed box re-expands through inverted states, the mirrored layer unfolds),
+    so the FP32 and FP64 oracles themselves part by 3e-5 m and by millimetres;
+    the GPU is gated against the FP64 oracle at three times that spread (max and
+    p99), and its inverted-tet count at three times the oracles' difference."""
+    m = box_muscle()
+    start = _squashed(m)
+    if case == "inverted":
+        # mirror the upper fifth of the box through its mid-plane: its tets invert
+        z = m.verts[:, 2]
+        lo, hi = z.min(), z.max()
+        cut = hi - 0.2 * (hi - lo)
+        start = m.verts.copy()
+        up = z > cut
+        start[up, 2] = (2 * cut - z[up]).astype(np.float32)
+    _, sim, o32 = _pair(start, 1.0, 2, 0.3)
+    o64 = O.OracleMuscleSim(m.verts, m.tets, m.fiber_per_tet, constraint_configs=CONS, stopped=m.stopped,
+                            repair_alpha=1.0, repair_iters=2, repair_sigma_min=0.3, prec="f64", **KW)
+    o64.pos[:] = start
+    o64.pprev[:] = start
+    inv0 = o64.count_inverted()
+    tol = 1e-5 * bbox_diag(m.verts)
+    for _ in range(2):
+        sim.step()
+        o32.step()
+        o64.step()
+        p = sim.positions_np()
+        e = np.abs(p - o64.pos).max(1)
+        spr = np.abs(o32.pos - o64.pos).max(1)
+        print(f"{case}: |gpu-o64| max {e.max():.3e} p99 {np.percentile(e, 99):.3e}; "
+              f"|o32-o64| max {spr.max():.3e} p99 {np.percentile(spr, 99):.3e}")
+        assert np.isfinite(p).all()
+        assert e.max() <= max(tol, 3.0 * spr.max())
+        assert np.percentile(e, 99) <= max(tol, 3.0 * np.percentile(spr, 99))
+    n_gpu, n32, n64 = sim.count_inverted(), o32.count_inverted(), o64.count_inverted()
+    print(f"{case}: inverted at start {inv0}, after gpu {n_gpu} o32 {n32} o64 {n64}")
+    assert abs(n_gpu - n64) <= max(3 * abs(n32 - n64), 0.005 * m.tets.shape[0])
+    if case == "inverted":
+        assert inv0 > 0 and n64 < inv0
+
+
+def test_repair_off_is_a_noop():
+    m = box_muscle()
+    start = _squashed(m)
+    _, sim, _ = _pair(start, 0.0, 2, 0.3)
+    sim.repair_inverted_tets()
+    assert np.array_equal(sim.positions_np(), start)

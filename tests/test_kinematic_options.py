@@ -1,0 +1,59 @@
+"""Host side of the soft pins (presubframe_pintotarget, mg_coarse_attach_beta)
+on the oracle, CPU only: the blend arithmetic, the coarse attach set, and that
+both options change the oracle's frames."""
+import numpy as np
+
+from oracle import oracle as O
+from rlmusclev2_b200.meshgen import humanv2_scene
+from rlmusclev2_b200.mg import load_config
+
+CFG3 = "rlmusclev2_b200/configs/humanv2_synth_mg_dcd.json"
+
+
+def _cfg(presub=0.0, beta=0.0):
+    cfg = load_config(CFG3)
+    cfg["demo"]["collision"]["sdf_res"] = 48
+    cfg["demo"]["self_collision"]["method"] = "none"
+    cfg["presubframe_pintotarget"] = presub
+    cfg["mg_coarse_attach_beta"] = beta
+    return cfg
+
+
+def _scene():
+    return humanv2_scene(seed=2, n_muscles=3, n_bones=3, target_tets=4000, fascia_tets=800, box=(0.25, 0.25, 0.25))
+
+
+def test_blend_is_one_fma():
+    sc = _scene()
+    o = O.OracleMultiGridSim(_cfg(), sc, prec="f32")
+    rng = np.random.default_rng(0)
+    p = rng.standard_normal((1000, 3)).astype(np.float32)
+    t = rng.standard_normal((1000, 3)).astype(np.float32)
+    got = o.blend(p, t, 0.3)
+    d = (t - p).astype(np.float32)
+    want = (p.astype(np.float64) + np.float64(np.float32(0.3)) * d.astype(np.float64)).astype(np.float32)
+    assert got.dtype == np.float32 and np.array_equal(got, want)
+    assert np.abs(o.blend(p, t, 1.0) - t).max() <= 4.8e-7  # snaps to the rounding of p + (t - p)
+    assert np.array_equal(o.blend(p, t, 0.0), p)
+
+
+def test_coarse_attach_set_is_the_referenced_nodes():
+    sc = _scene()
+    o = O.OracleMultiGridSim(_cfg(beta=0.3), sc, prec="f32")
+    ref = np.zeros(o.mg.nv, bool)
+    ref[np.unique(o.mg_t[np.abs(o.mg_w) > 0])] = True
+    assert np.array_equal(o.mg_attach, ref)
+    assert o.mg_attach.any()
+
+
+def test_options_change_the_frames():
+    sc = _scene()
+    runs = {}
+    for key in ((0.0, 0.0), (0.5, 0.0), (0.0, 0.3)):
+        o = O.OracleMultiGridSim(_cfg(*key), sc, prec="f32")
+        for f in (1, 2):
+            o.step_frame(f)
+        assert np.isfinite(o.pos).all()
+        runs[key] = o.pos.copy()
+    assert np.abs(runs[(0.5, 0.0)] - runs[(0.0, 0.0)]).max() > 1e-5
+    assert np.abs(runs[(0.0, 0.3)] - runs[(0.0, 0.0)]).max() > 1e-6
