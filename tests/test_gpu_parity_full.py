@@ -23,14 +23,13 @@ comparison is therefore split:
   positions to 1e-2: the max sits on a thin tet whose residual moves with
   sub-micron position differences), and the volume drift matches to 1e-4 of
   the rest volume: the kernels' arithmetic at rounding level;
-* with the reference threshold, on config 2 the GPU is as close to the FP64
-  oracle as the FP32 oracle is (max and p99 within three times its distance,
-  no more vertices beyond the tolerance than twice its count); on config 3
-  the coarse cage starts exactly at rest, so the threshold decides for many
-  coarse tets at once and each decision moves a cage cell's fine vertices,
-  and only the p99 is gated (ten times the FP32 oracle's distance); one Jacobi
-  iteration from the frame's end state takes < 1 % of vertices into a
-  different divisor, the others matching to 1e-5 x diagonal.
+* with the reference threshold the GPU is as close to the FP64 oracle as the
+  FP32 oracle is (max within three times its distance, no more vertices beyond
+  the tolerance than twice its count; p99 within three times, five on config 3,
+  whose coarse cage starts exactly at rest, so the threshold decides for many
+  coarse tets at once and each decision moves a cage cell's fine vertices);
+  one Jacobi iteration from the frame's end state takes < 1 % of vertices into
+  a different divisor, the others matching to 1e-5 x diagonal.
 
 Each test records its figures (parity_record), printed at the end of the
 session.
@@ -143,18 +142,16 @@ def test_full_frame_rounding_level_without_skip_threshold(scenes, name, parity_r
         assert mt["n_nonfinite"] == 0
         # Rounding differences grow with the motion in every FP32 implementation:
         # the FP32 oracle drifts from the FP64 one too, most on the few lattice-corner
-        # vertices held by two tets.  Per frame the GPU is as close to FP64 as the FP32
-        # oracle is (max and p99 within 3x its distance, or within the tolerance), and
-        # it leaves the tolerance on no more vertices than twice the FP32 oracle does
-        # (with the DCD, config 3's contact set is another discrete choice: a contact
-        # taken by one implementation and not the other moves a few vertices by
-        # millimetres, so there only the p99 is gated, at ten times the spread)
-        dcd = name == "config3"
+        # vertices held by two tets (config 2) and, with the multigrid, by millimetres
+        # on a few stiff fibre tets beside the tendon pins (config 3).  Per frame the
+        # GPU is as close to FP64 as the FP32 oracle is (max and p99 within 3x its
+        # distance, or within the tolerance), and it leaves the tolerance on no more
+        # vertices than twice the FP32 oracle does; with the DCD (config 3) the contact
+        # set is one more discrete choice, under the same gates.
         for r in pf:
-            if not dcd:
-                assert r["max_gpu_o64"] <= max(tol, 3.0 * r["max_o32_o64"])
-                assert r["beyond_tol_gpu"] <= 2 * r["beyond_tol_o32"] + 1e-3 * sim.NV
-            assert r["p99_gpu_o64"] <= max(tol, (10.0 if dcd else 3.0) * r["p99_o32_o64"])
+            assert r["max_gpu_o64"] <= max(tol, 3.0 * r["max_o32_o64"])
+            assert r["beyond_tol_gpu"] <= 2 * r["beyond_tol_o32"] + 1e-3 * sim.NV
+            assert r["p99_gpu_o64"] <= max(tol, 3.0 * r["p99_o32_o64"])
         # frame 2 holds the first 10 substeps of motion (frame 1 starts and stays at
         # rest): there 99 % of the vertices are within 1e-5 x diagonal of FP64
         if name == "config2":
@@ -162,9 +159,8 @@ def test_full_frame_rounding_level_without_skip_threshold(scenes, name, parity_r
         # the metric kernel on the same positions; on each side's own positions the
         # max sits on a thin tet whose residual moves with sub-micron differences
         assert rel_metric <= 1e-4
-        if not dcd:
-            assert rel_r <= 1e-2
-            assert abs(drift_gpu - drift_64) <= 1e-4
+        assert rel_r <= 1e-2
+        assert abs(drift_gpu - drift_64) <= 1e-4
     finally:
         O.set_arap_skip(0.0)
         del sim
@@ -208,18 +204,17 @@ def test_full_frame_reference_threshold(scenes, name, parity_record):
     # restriction of the fine rest), so in the first moving frames the threshold
     # decides for many coarse tets at once, and each decision moves a whole cage
     # cell's fine vertices through the prolongation: the GPU (polar rotation) and
-    # the FP32 oracle (SVD) decide differently there.  Its arithmetic is checked by
-    # the no-threshold test; here only the p99 is gated, at ten times the spread.
-    dcd = name.startswith("config3")
+    # the FP32 oracle (SVD) decide differently there, which lifts the p99 (measured
+    # 2.9-3.1x the FP32 oracle's) but not the max or the count beyond tolerance.
+    # Its arithmetic is checked by the no-threshold test.
+    mg = name.startswith("config3")
     for r in sim.per_frame:
-        assert r["p99_gpu_o64"] <= max(tol, (10.0 if dcd else 3.0) * r["p99_o32_o64"])
-        if not dcd:
-            assert r["beyond_tol_gpu"] <= 2 * r["beyond_tol_o32"] + 1e-3 * sim.NV
-            assert r["max_gpu_o64"] <= max(tol, 3.0 * r["max_o32_o64"])
+        assert r["p99_gpu_o64"] <= max(tol, (5.0 if mg else 3.0) * r["p99_o32_o64"])
+        assert r["beyond_tol_gpu"] <= 2 * r["beyond_tol_o32"] + 1e-3 * sim.NV
+        assert r["max_gpu_o64"] <= max(tol, 3.0 * r["max_o32_o64"])
     assert abs(mt["resid_max"] - r_at_gpu) <= 1e-4 * r_at_gpu
-    if not dcd:
-        assert abs(mt["resid_max"] - rmax64) <= max(1e-2 * rmax64, 3.0 * abs(r32 - rmax64))
-        assert abs(drift_gpu - drift_64) <= 1e-4
+    assert abs(mt["resid_max"] - rmax64) <= max(1e-2 * rmax64, 3.0 * abs(r32 - rmax64))
+    assert abs(drift_gpu - drift_64) <= 1e-4
     assert flips < 0.01
     assert err_same <= tol
     del sim
