@@ -3,9 +3,13 @@ presubframe_pintotarget (the soft pin of every constraint point toward its
 bone target after the hard pin, mg/mg.py:1386-1407, mg/kernel.py:229-257) and
 mg_coarse_attach_beta (the coarse cage's soft attach after each coarse sweep,
 mg/mg.py:1047-1062, mg/kernel.py:64-84), on the small synthetic scene with
-the multigrid on, three frames.  Gates as for the other small-scene frame
-tests: within 1e-5 x bbox diagonal of the FP64 oracle, or three times the FP32
-oracle's own distance from it (max and p99)."""
+the multigrid on, three frames.  The ARAP skip threshold is off on both sides
+(XpbdParams.arap_skip_ssq < 0, oracle.set_arap_skip(-1)): the cage starts
+exactly at rest, where FP32 rounding decides the threshold for whole groups of
+coarse tets, and one such decision moves a cage node by a fraction of a
+millimetre.  Gates as for the full-size frame tests: within 1e-5 x bbox
+diagonal of the FP64 oracle, or three times the FP32 oracle's own distance from
+it (max and p99)."""
 import numpy as np
 import pytest
 
@@ -30,6 +34,8 @@ def _scene(presub, beta):
 
 def _run(cfg, sc, eager=False):
     sim = MultiGridSim(cfg, scene=sc)
+    sim._prm.arap_skip_ssq = -1.0
+    sim.mg.coarse._prm.arap_skip_ssq = -1.0
     if eager:
         sim.build_program()
     out = []
@@ -48,11 +54,18 @@ def test_soft_pins_vs_oracle(presub, beta, parity_record):
     o64 = O.OracleMultiGridSim(cfg, sc, prec="f64")
     _, base = _run(*_scene(0.0, 0.0))
     tol = 1e-5 * bbox_diag(sc.verts)
-    for frame, p, q in zip((1, 2, 3), ps, base):
-        o32.step_frame(frame)
-        o64.step_frame(frame)
-        d64 = np.abs(p - o64.pos).max(1)
-        spr = np.abs(o32.pos - o64.pos).max(1)
+    r32, r64 = [], []
+    O.set_arap_skip(-1.0)
+    try:
+        for frame in (1, 2, 3):
+            for o, out in ((o32, r32), (o64, r64)):
+                o.step_frame(frame)
+                out.append(o.pos.copy())
+    finally:
+        O.set_arap_skip(0.0)
+    for frame, p, q, a32, a64 in zip((1, 2, 3), ps, base, r32, r64):
+        d64 = np.abs(p - a64).max(1)
+        spr = np.abs(a32 - a64).max(1)
         parity_record(f"soft_pins_p{presub}_b{beta}_frame{frame}", max_gpu_o64_m=d64.max(), max_o32_o64_m=spr.max(),
                       p99_gpu_o64_m=np.percentile(d64, 99), p99_o32_o64_m=np.percentile(spr, 99),
                       moved_by_option_m=float(np.abs(p - q).max()), tol_m=tol)
