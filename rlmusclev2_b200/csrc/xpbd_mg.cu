@@ -55,7 +55,12 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_gather(const __grid_constant_
 // is staged in shared memory, each warp computes rows
 // delta[r] = sum_j Minv[r][j] b_j with lanes striding j (coalesced rows) and
 // the new coarse position prior + delta.
-constexpr int kRestrictRows = 8;  // one row per warp: blocks of a few hundred rows want CTAs, not long warps
+#ifndef XPBD_RESTRICT_ROWS
+#define XPBD_RESTRICT_ROWS 8
+#endif
+// rows of one block per CTA (one row per warp at 8); every CTA stages the block's
+// right-hand side in shared memory, so fewer rows per CTA mean more staging reads
+constexpr int kRestrictRows = XPBD_RESTRICT_ROWS;
 __global__ void __launch_bounds__(kMgThreads)
     k_mg_restrict(const __grid_constant__ XpbdCage G, float4* coarse, float4* prev, const float4* __restrict__ pin) {
     extern __shared__ float4 sb[];
