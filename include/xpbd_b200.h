@@ -89,7 +89,10 @@ typedef struct XpbdParams {
                                     FP32x2 arithmetic (slower on B200: the register pairing costs as
                                     many moves as it saves FP32 instructions);
                                     bit 4: persistent pass keeps the runtime shared-memory layout for
-                                    tiles of <= 768 vertices (default: compile-time offsets) */
+                                    tiles of <= 768 vertices (default: compile-time offsets);
+                                    bit 5: the per-iteration tile pass asks the copy engine for an L2
+                                    prefetch of its tile's tet streams (cp.async.bulk.prefetch.L2)
+                                    before staging the tile's vertices */
     float acc_scale;             /* > 0: the tile passes sum each tet's corrections into shared memory as
                                     32-bit integers round(d * acc_scale) (native integer atomics; shared
                                     float atomics cost ~5x more) and read the sums back as float(sum) /

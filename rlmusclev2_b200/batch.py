@@ -99,9 +99,11 @@ class BatchSim(MultiGridSim):
     # ------------------------------------------------------------- autotune
     def _candidates(self):
         """Persistent ranges without/with tet-stream prefetch; per-iteration
-        launches at the default and the flipped CTAs/SM."""
+        launches at the default and the flipped CTAs/SM, and with the bulk L2
+        prefetch of each tile's tet streams (tile_variant bit 5)."""
         return [dict(persistent=True, variant=0), dict(persistent=True, variant=4),
-                dict(persistent=False, variant=0), dict(persistent=False, variant=1)]
+                dict(persistent=False, variant=0), dict(persistent=False, variant=1),
+                dict(persistent=False, variant=32), dict(persistent=False, variant=33)]
 
     def _time_iterations(self, n_iters: int, reps: int) -> float:
         """ms per Jacobi iteration with the frame's own grouping: ``reps``
@@ -120,7 +122,8 @@ class BatchSim(MultiGridSim):
     def _tune_key(self) -> str:
         name = torch.cuda.get_device_name(self.device)
         flags = sorted({int(m["flags"]) for m in self.layout.materials})
-        return f"{name}|nv={self.NV}|nt={self.NT}|inst={self.n_inst}|flags={flags}|iters={self.fine_iters}"
+        cands = len(self._candidates())
+        return f"{name}|nv={self.NV}|nt={self.NT}|inst={self.n_inst}|flags={flags}|iters={self.fine_iters}|cands={cands}"
 
     def autotune(self, use_cache: bool = True) -> dict:
         """Pick the fastest tet-pass configuration for this batch: persistent

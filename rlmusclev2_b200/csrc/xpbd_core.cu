@@ -33,6 +33,33 @@ namespace {
 constexpr int kTileThreads = 256;
 constexpr int kVertThreads = 256;
 
+// L2 prefetch of the bytes [begin, end) of one array through the bulk-copy
+// engine: the range is shrunk to whole 16-byte units inside it (the
+// instruction wants a 16-byte aligned address and a size in 16-byte units)
+// and issued in pieces of at most 32 KB.  A prefetch has no destination and
+// no completion to wait for.
+__device__ __forceinline__ void prefetch_l2_range(const void* begin, const void* end) {
+    uintptr_t a = (reinterpret_cast<uintptr_t>(begin) + 15u) & ~uintptr_t(15);
+    const uintptr_t e = reinterpret_cast<uintptr_t>(end) & ~uintptr_t(15);
+    while (a < e) {
+        const uint32_t n = uint32_t(e - a < 32768u ? e - a : 32768u);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(n) : "memory");
+        a += n;
+    }
+}
+
+// The tet streams of one tile: indices and rest matrices, and the fibre
+// streams when the tiles carry them.
+__device__ __forceinline__ void prefetch_tile_tets(const XpbdTiles& T, int tile) {
+    const int t0 = T.tile_tptr[tile], t1 = T.tile_tptr[tile + 1];
+    prefetch_l2_range(T.tet_q + 4 * size_t(t0), T.tet_q + 4 * size_t(t1));
+    prefetch_l2_range(T.tet_b0 + 4 * size_t(t0), T.tet_b0 + 4 * size_t(t1));
+    prefetch_l2_range(T.tet_b1 + 4 * size_t(t0), T.tet_b1 + 4 * size_t(t1));
+    prefetch_l2_range(T.tet_b2 + t0, T.tet_b2 + t1);
+    if (T.tet_fiber) prefetch_l2_range(T.tet_fiber + 4 * size_t(t0), T.tet_fiber + 4 * size_t(t1));
+    if (T.tet_act) prefetch_l2_range(T.tet_act + t0, T.tet_act + t1);
+}
+
 template <int MODE, bool DAMP, int MINB, int CSET, bool X2 = false>
 __global__ void __launch_bounds__(kTileThreads, MINB)
     k_project_tiles(const __grid_constant__ XpbdParams prm, const __grid_constant__ XpbdTiles T,
@@ -57,6 +84,8 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
     const float4* prev4 = reinterpret_cast<const float4*>(V.pprev);
     __shared__ float s_arap_at[XPBD_MAX_MATERIALS];
+    // the tet streams are read after the vertex gather: ask for them first
+    if ((prm.tile_variant & 32) && threadIdx.x == 0) prefetch_tile_tets(T, tile);
     fill_arap_at(prm, s_arap_at);
     for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
         const int g = T.tile_verts[vbeg + i];
@@ -473,7 +502,7 @@ int check_params(const XpbdParams* p) {
         p->n_attach_materials > XPBD_MAX_ATTACH_MATERIALS)
         return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range");
     if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0");
-    if (p->tile_variant < 0 || p->tile_variant > 31) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..31");
+    if (p->tile_variant < 0 || p->tile_variant > 63) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..63");
     if (!(p->acc_scale > 0.f) || !(p->acc_scale < 3.0e38f))
         return fail(XPBD_ERR_ARG, "XpbdParams: acc_scale must be a finite value > 0 (xpbd_acc_scale_for_extent)");
     return XPBD_OK;

@@ -107,3 +107,26 @@ def test_fixed_point_range_check_flags_oversized_scale():
     sim.set_positions(deformed)
     sim._fused_iterations(1)
     assert sim.persistent_status() & capi.STATUS_ACC_RANGE
+
+
+@pytest.mark.parametrize("base", [0, 1])
+def test_tile_pass_with_l2_prefetch_is_bit_identical(base):
+    """tile_variant bit 5 only adds a bulk L2 prefetch of each tile's tet
+    streams: the per-iteration pass gives the same positions bit for bit, at
+    either CTAs-per-SM choice (bit 0)."""
+    variant = base | 32
+    verts, tets, table, mass, vf, act, tendon, deformed, prev = _mixed_problem()
+    kw = dict(dt=1.0 / 240.0, contraction_ratio=0.4, fiber_stiffness_scale=3.0)
+    out = []
+    for tv in (base, variant):
+        sim = XpbdSolver(verts, tets, table, mass=mass, v_fiber=vf, tet_tendonmask=tendon, device="cuda:0",
+                         tile_tets=64, **kw)
+        sim._prm.tile_variant = tv
+        sim.set_activation(act)
+        sim.set_positions(prev, also_prev=True)
+        sim.set_positions(deformed)
+        for _ in range(3):
+            sim._fused_iteration()
+        out.append(sim.positions_np())
+    assert np.array_equal(out[0], out[1])
+    assert np.abs(out[0] - deformed).max() > 0
