@@ -583,7 +583,8 @@ typedef struct XpbdGemm {
     int32_t lda, ldb, m, n, k, act;
     const float* bias;
     const float* gelu_grad_of;
-    int32_t ld_g, ld_pre, ld_f32, ld_bf16, ld_bf16_t, reserved;
+    int32_t ld_g, ld_pre, ld_f32, ld_bf16, ld_bf16_t;
+    int32_t flags;   /* XPBD_GEMM_THREAD_STAGED: operands staged by the CTA's threads instead of TMA */
     float* out_pre;
     float* out_f32;
     uint16_t* out_bf16;
@@ -591,7 +592,13 @@ typedef struct XpbdGemm {
     int32_t* status; /* XPBD_STATUS_MMA_TIMEOUT, optional */
 } XpbdGemm;
 
-/* One CTA per 128 x n_tile block of C (n_tile a multiple of 16, <= 256). */
+#define XPBD_GEMM_THREAD_STAGED 1
+
+/* One CTA per 128 x n_tile block of C (n_tile a multiple of 16, <= 256).  The
+ * operands come into shared memory through the tensor memory accelerator
+ * (cp.async.bulk.tensor 2-D boxes, up to four 64-wide k blocks in flight),
+ * unless flags has XPBD_GEMM_THREAD_STAGED or the driver offers no tensor-map
+ * encoder, in which case the CTA's threads copy them (two stages). */
 int xpbd_gemm_bf16(const XpbdGemm* g, int32_t n_tile, xpbd_stream_t stream);
 
 /* db[o] = sum_{s < m} dzt[o][s] for o < n_out (BF16 rows of length >= m). */

@@ -111,7 +111,7 @@ class XpbdGemm(C.Structure):
     _fields_ = [("a", C.c_void_p), ("b", C.c_void_p), ("lda", C.c_int32), ("ldb", C.c_int32), ("m", C.c_int32),
                 ("n", C.c_int32), ("k", C.c_int32), ("act", C.c_int32), ("bias", C.c_void_p),
                 ("gelu_grad_of", C.c_void_p), ("ld_g", C.c_int32), ("ld_pre", C.c_int32), ("ld_f32", C.c_int32),
-                ("ld_bf16", C.c_int32), ("ld_bf16_t", C.c_int32), ("reserved", C.c_int32), ("out_pre", C.c_void_p),
+                ("ld_bf16", C.c_int32), ("ld_bf16_t", C.c_int32), ("flags", C.c_int32), ("out_pre", C.c_void_p),
                 ("out_f32", C.c_void_p), ("out_bf16", C.c_void_p), ("out_bf16_t", C.c_void_p),
                 ("status", C.c_void_p)]
 

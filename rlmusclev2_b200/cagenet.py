@@ -31,9 +31,10 @@ def _p(t):
 
 
 def gemm(lib, stream, a, b, m, n, k, *, lda=None, ldb=None, bias=None, act=0, gelu_grad_of=None, out_pre=None,
-         out_f32=None, out_bf16=None, out_bf16_t=None, status=None, n_tile=None):
+         out_f32=None, out_bf16=None, out_bf16_t=None, status=None, n_tile=None, flags=0):
     """C = A B^T (+ epilogue) through xpbd_gemm_bf16; tensors are CUDA, BF16
-    operands row-major along k.  Output row strides are the tensors' own."""
+    operands row-major along k.  Output row strides are the tensors' own.
+    ``flags``: XpbdGemm.flags (1: thread-staged operands instead of TMA)."""
     g = capi.XpbdGemm()
     g.a, g.b = a.data_ptr(), b.data_ptr()
     g.lda = lda if lda is not None else a.shape[-1]
@@ -51,6 +52,7 @@ def gemm(lib, stream, a, b, m, n, k, *, lda=None, ldb=None, bias=None, act=0, ge
     if out_bf16_t is not None:
         g.out_bf16_t, g.ld_bf16_t = out_bf16_t.data_ptr(), out_bf16_t.shape[-1]
     g.status = None if status is None else status.data_ptr()
+    g.flags = int(flags)
     if n_tile is None:
         n_tile = min(256, ((int(n) + 15) // 16) * 16)
     capi.check(lib.xpbd_gemm_bf16(C.byref(g), int(n_tile), stream))

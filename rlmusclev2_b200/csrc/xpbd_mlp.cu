@@ -20,6 +20,8 @@
 // Every mbarrier wait is bounded; on timeout the status word gets
 // XPBD_STATUS_MMA_TIMEOUT, the CTA waits (bounded) once more for its MMAs and
 // frees its tensor memory before returning.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -49,10 +51,11 @@ __device__ __forceinline__ uint32_t kmajor_off(int r, int k) {
 
 // Shared-memory matrix descriptor: start address, LBO, SBO (all >> 4),
 // version 1 (sm100), base offset 0, no swizzle.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((kLbo >> 4) & 0x3FFFu) << 16) |
-           (uint64_t((kSbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+__device__ __forceinline__ uint64_t smem_desc_lbo_sbo(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
 }
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) { return smem_desc_lbo_sbo(addr, kLbo, kSbo); }
 
 // Instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 D, M = 128.
 __host__ __device__ constexpr uint32_t instr_desc(int n) {
@@ -125,6 +128,82 @@ __device__ __forceinline__ void load_block(const uint16_t* __restrict__ g, int l
     }
 }
 
+// Epilogue: warp w reads TMEM lanes 32w..32w+31 (rows m0 + 32w + lane of the
+// tile) 16 columns at a time, adds the bias, multiplies by the GELU derivative
+// of a stored pre-activation (backward), applies GELU, and writes the FP32,
+// BF16 and transposed BF16 outputs that are set.
+__device__ __forceinline__ void gemm_epilogue(const XpbdGemm& G, uint32_t tmem, int m0, int n0, int n_tile, int warp,
+                                              int lane) {
+    const int row = m0 + warp * 32 + lane;
+    const bool rv = row < G.m;
+    // 16-byte vector stores of a row's 16 columns where the chunk is whole
+    // and the row strides keep them aligned
+    const bool vec_h = G.out_bf16 && (G.ld_bf16 % 8) == 0 && aligned_ptr16(G.out_bf16);
+    const bool vec_f = G.out_f32 && (G.ld_f32 % 4) == 0 && aligned_ptr16(G.out_f32);
+    const bool vec_p = G.out_pre && (G.ld_pre % 4) == 0 && aligned_ptr16(G.out_pre);
+    for (int c0 = 0; c0 < n_tile; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), v);
+        if (!rv) continue;
+        const bool whole = n0 + c0 + 16 <= G.n;
+        float y[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int col = n0 + c0 + j;
+            float z = v[j];
+            if (col < G.n) {
+                if (G.bias) z += G.bias[col];
+                if (G.gelu_grad_of) z *= gelu_grad_f(G.gelu_grad_of[size_t(row) * G.ld_g + col]);
+            }
+            v[j] = z;
+            y[j] = G.act == 1 ? gelu_f(z) : z;
+        }
+        const size_t cb = size_t(n0 + c0);
+        if (G.out_pre) {
+            if (whole && vec_p) {
+                float4* d = reinterpret_cast<float4*>(G.out_pre + size_t(row) * G.ld_pre + cb);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            } else {
+                for (int j = 0; j < 16; ++j)
+                    if (n0 + c0 + j < G.n) G.out_pre[size_t(row) * G.ld_pre + cb + j] = v[j];
+            }
+        }
+        if (G.out_f32) {
+            if (whole && vec_f) {
+                float4* d = reinterpret_cast<float4*>(G.out_f32 + size_t(row) * G.ld_f32 + cb);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) d[q] = make_float4(y[4 * q], y[4 * q + 1], y[4 * q + 2], y[4 * q + 3]);
+            } else {
+                for (int j = 0; j < 16; ++j)
+                    if (n0 + c0 + j < G.n) G.out_f32[size_t(row) * G.ld_f32 + cb + j] = y[j];
+            }
+        }
+        if (G.out_bf16) {
+            __nv_bfloat16* hb = reinterpret_cast<__nv_bfloat16*>(G.out_bf16) + size_t(row) * G.ld_bf16 + cb;
+            if (whole && vec_h) {
+                uint4 pk[2];
+                uint32_t* w = reinterpret_cast<uint32_t*>(pk);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const __nv_bfloat162 h2 = __floats2bfloat162_rn(y[2 * q], y[2 * q + 1]);
+                    w[q] = *reinterpret_cast<const uint32_t*>(&h2);
+                }
+                reinterpret_cast<uint4*>(hb)[0] = pk[0];
+                reinterpret_cast<uint4*>(hb)[1] = pk[1];
+            } else {
+                for (int j = 0; j < 16; ++j)
+                    if (n0 + c0 + j < G.n) hb[j] = __float2bfloat16_rn(y[j]);
+            }
+        }
+        if (G.out_bf16_t) {
+            __nv_bfloat16* ht = reinterpret_cast<__nv_bfloat16*>(G.out_bf16_t);
+            for (int j = 0; j < 16; ++j)
+                if (n0 + c0 + j < G.n) ht[(cb + j) * G.ld_bf16_t + row] = __float2bfloat16_rn(y[j]);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(const __grid_constant__ XpbdGemm G, int n_tile, int tmem_cols) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t s_bar[2];
@@ -184,76 +263,145 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(const __grid_constant
         if (nkb > 0) mbar_wait(smem_u32(&s_bar[(nkb - 1) & 1]), uint32_t(((nkb - 1) >> 1) & 1));
     }
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (ok) {
-        const int row = m0 + warp * 32 + lane;
-        const bool rv = row < G.m;
-        // 16-byte vector stores of a row's 16 columns where the chunk is whole
-        // and the row strides keep them aligned
-        const bool vec_h = G.out_bf16 && (G.ld_bf16 % 8) == 0 && aligned_ptr16(G.out_bf16);
-        const bool vec_f = G.out_f32 && (G.ld_f32 % 4) == 0 && aligned_ptr16(G.out_f32);
-        const bool vec_p = G.out_pre && (G.ld_pre % 4) == 0 && aligned_ptr16(G.out_pre);
-        for (int c0 = 0; c0 < n_tile; c0 += 16) {
-            float v[16];
-            tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), v);
-            if (!rv) continue;
-            const bool whole = n0 + c0 + 16 <= G.n;
-            float y[16];
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int col = n0 + c0 + j;
-                float z = v[j];
-                if (col < G.n) {
-                    if (G.bias) z += G.bias[col];
-                    if (G.gelu_grad_of) z *= gelu_grad_f(G.gelu_grad_of[size_t(row) * G.ld_g + col]);
-                }
-                v[j] = z;
-                y[j] = G.act == 1 ? gelu_f(z) : z;
-            }
-            const size_t cb = size_t(n0 + c0);
-            if (G.out_pre) {
-                if (whole && vec_p) {
-                    float4* d = reinterpret_cast<float4*>(G.out_pre + size_t(row) * G.ld_pre + cb);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-                } else {
-                    for (int j = 0; j < 16; ++j)
-                        if (n0 + c0 + j < G.n) G.out_pre[size_t(row) * G.ld_pre + cb + j] = v[j];
-                }
-            }
-            if (G.out_f32) {
-                if (whole && vec_f) {
-                    float4* d = reinterpret_cast<float4*>(G.out_f32 + size_t(row) * G.ld_f32 + cb);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) d[q] = make_float4(y[4 * q], y[4 * q + 1], y[4 * q + 2], y[4 * q + 3]);
-                } else {
-                    for (int j = 0; j < 16; ++j)
-                        if (n0 + c0 + j < G.n) G.out_f32[size_t(row) * G.ld_f32 + cb + j] = y[j];
-                }
-            }
-            if (G.out_bf16) {
-                __nv_bfloat16* hb = reinterpret_cast<__nv_bfloat16*>(G.out_bf16) + size_t(row) * G.ld_bf16 + cb;
-                if (whole && vec_h) {
-                    uint4 pk[2];
-                    uint32_t* w = reinterpret_cast<uint32_t*>(pk);
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const __nv_bfloat162 h2 = __floats2bfloat162_rn(y[2 * q], y[2 * q + 1]);
-                        w[q] = *reinterpret_cast<const uint32_t*>(&h2);
-                    }
-                    reinterpret_cast<uint4*>(hb)[0] = pk[0];
-                    reinterpret_cast<uint4*>(hb)[1] = pk[1];
-                } else {
-                    for (int j = 0; j < 16; ++j)
-                        if (n0 + c0 + j < G.n) hb[j] = __float2bfloat16_rn(y[j]);
-                }
-            }
-            if (G.out_bf16_t) {
-                __nv_bfloat16* ht = reinterpret_cast<__nv_bfloat16*>(G.out_bf16_t);
-                for (int j = 0; j < 16; ++j)
-                    if (n0 + c0 + j < G.n) ht[(cb + j) * G.ld_bf16_t + row] = __float2bfloat16_rn(y[j]);
+    if (ok) gemm_epilogue(G, tmem, m0, n0, n_tile, warp, lane);
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(tmem_cols));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The same GEMM with its operands brought in by the tensor memory accelerator.
+// A k block of A (128 x 64) and of B (n_tile x 64) is eight 2-D boxes each
+// (8 k-elements = 16 bytes wide, 128 or n_tile rows high) that land as
+// row-after-row 16-byte lines: eight-row groups are core matrices 128 B apart
+// (SBO) and the eight 16-byte k chunks are rows x 16 B apart (LBO).  Rows
+// beyond m or n come in as zeros (the tensor map's out-of-bounds fill).  Up to
+// kTmaStages k blocks are in flight; one thread issues the copies, waits for
+// each block (mbarrier with transaction count), issues its four MMAs and
+// commits them to the block's "free" barrier before the stage is refilled.
+constexpr int kTmaStages = 4;
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_gemm_bf16_tma(const __grid_constant__ XpbdGemm G, const __grid_constant__ CUtensorMap ta,
+                    const __grid_constant__ CUtensorMap tb, int n_tile, int tmem_cols) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t s_full[kTmaStages];
+    __shared__ __align__(8) uint64_t s_free[kTmaStages];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_ok;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * n_tile;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t a_lbo = 128u * 16u, b_lbo = uint32_t(n_tile) * 16u;  // bytes per 16-byte k chunk of all rows
+    const uint32_t a_bytes = 8u * a_lbo, st_bytes = a_bytes + 8u * b_lbo;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&s_tmem)),
+                     "r"(tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kTmaStages; ++st) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s_full[st])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s_free[st])));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        s_ok = 1;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const int nkb = G.k / kKB;
+    if (threadIdx.x == 0) {
+        const uint32_t base = smem_u32(smem);
+        const uint32_t idesc = instr_desc(n_tile);
+        int issued = 0, committed = 0;
+        bool ok = true;
+        while (issued < nkb && issued < kTmaStages) {
+            const int kb = issued++;
+            const uint32_t sa = base + uint32_t(kb % kTmaStages) * st_bytes, sb = sa + a_bytes;
+            const uint32_t bar = smem_u32(&s_full[kb % kTmaStages]);
+            mbar_expect_tx(bar, st_bytes);
+            for (int kc = 0; kc < 8; ++kc) {
+                tma_load_2d(sa + uint32_t(kc) * a_lbo, &ta, kb * kKB + kc * 8, m0, bar);
+                tma_load_2d(sb + uint32_t(kc) * b_lbo, &tb, kb * kKB + kc * 8, n0, bar);
             }
         }
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int st = kb % kTmaStages;
+            const uint32_t par = uint32_t((kb / kTmaStages) & 1);
+            if (!mbar_wait(smem_u32(&s_full[st]), par)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t sa = base + uint32_t(st) * st_bytes, sb = sa + a_bytes;
+#pragma unroll
+            for (int ks = 0; ks < kKB / 16; ++ks) {
+                const uint64_t ad = smem_desc_lbo_sbo(sa + uint32_t(ks) * 2u * a_lbo, a_lbo, 128u);
+                const uint64_t bd = smem_desc_lbo_sbo(sb + uint32_t(ks) * 2u * b_lbo, b_lbo, 128u);
+                const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&s_free[st]))
+                         : "memory");
+            committed = kb + 1;
+            if (issued < nkb) {
+                // the stage's next k block may overwrite it only after these MMAs read it
+                if (!mbar_wait(smem_u32(&s_free[st]), par)) {
+                    ok = false;
+                    break;
+                }
+                const int nk = issued++;
+                const uint32_t bar = smem_u32(&s_full[st]);
+                mbar_expect_tx(bar, st_bytes);
+                for (int kc = 0; kc < 8; ++kc) {
+                    tma_load_2d(sa + uint32_t(kc) * a_lbo, &ta, nk * kKB + kc * 8, m0, bar);
+                    tma_load_2d(sb + uint32_t(kc) * b_lbo, &tb, nk * kKB + kc * 8, n0, bar);
+                }
+            }
+        }
+        // the accumulator is complete when the last commit's barrier completes
+        if (ok && committed > 0) {
+            const int kl = committed - 1;
+            ok = mbar_wait(smem_u32(&s_free[kl % kTmaStages]), uint32_t((kl / kTmaStages) & 1));
+        }
+        if (!ok) {
+            if (G.status) atomicOr(G.status, XPBD_STATUS_MMA_TIMEOUT);
+            // bounded waits for this CTA's copies and MMAs still in flight before the
+            // shared and tensor memory are released: the last load of every stage, the
+            // last commit
+            for (int kb = (issued > kTmaStages ? issued - kTmaStages : 0); kb < issued; ++kb)
+                mbar_wait(smem_u32(&s_full[kb % kTmaStages]), uint32_t((kb / kTmaStages) & 1));
+            if (committed > 0) {
+                const int kl = committed - 1;
+                mbar_wait(smem_u32(&s_free[kl % kTmaStages]), uint32_t((kl / kTmaStages) & 1));
+            }
+            s_ok = 0;
+        }
     }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (s_ok) gemm_epilogue(G, tmem, m0, n0, n_tile, warp, lane);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     if (warp == 0) {
@@ -314,6 +462,38 @@ __global__ void k_mse_grad(int m, int m_pad, int n_out, int ld, const float* __r
     if (dt) reinterpret_cast<__nv_bfloat16*>(dt)[size_t(c) * ld_dt + r] = h;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); null when the driver does not provide it.
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        cudaGetLastError();
+    }
+    return fn;
+}
+
+// Tensor map of a K-major BF16 operand [rows][ld] (k < ld used): boxes of
+// 8 k-elements (16 bytes) x box_rows rows, no swizzle, zero fill outside.
+// The caller has checked the 16-byte alignment of the base and of ld x 2.
+bool encode_kmajor(CUtensorMap* map, const uint16_t* ptr, int rows, int k, int ld, int box_rows) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_tiled();
+    if (!fn || rows <= 0 || k < 8 || box_rows <= 0 || box_rows > 256) return false;
+    const cuuint64_t dims[2] = {cuuint64_t(k), cuuint64_t(rows)};
+    const cuuint64_t strides[1] = {cuuint64_t(ld) * 2u};
+    const cuuint32_t box[2] = {8u, cuuint32_t(box_rows)};
+    const cuuint32_t es[2] = {1u, 1u};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<uint16_t*>(ptr), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 extern "C" {
@@ -328,18 +508,27 @@ int xpbd_gemm_bf16(const XpbdGemm* g, int32_t n_tile, xpbd_stream_t stream) {
     if (g->act != 0 && g->act != 1) return fail(XPBD_ERR_ARG, "xpbd_gemm_bf16: act");
     int tmem_cols = 32;
     while (tmem_cols < n_tile) tmem_cols <<= 1;
-    const size_t smem = size_t(2) * (128 + n_tile) * kKB * 2;
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
         if (cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(size_t(2) * (128 + 256) * kKB * 2)) != cudaSuccess)
+                                 int(size_t(2) * (128 + 256) * kKB * 2)) != cudaSuccess ||
+            cudaFuncSetAttribute(k_gemm_bf16_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(size_t(kTmaStages) * (128 + 256) * kKB * 2)) != cudaSuccess)
             return cuda_check("xpbd_gemm_bf16: smem attribute");
         attr_set[dev] = true;
     }
     dim3 grid((g->m + 127) / 128, (g->n + n_tile - 1) / n_tile);
-    k_gemm_bf16<<<grid, kThreads, smem, (cudaStream_t)stream>>>(*g, n_tile, tmem_cols);
+    CUtensorMap ta, tb;
+    if (!(g->flags & XPBD_GEMM_THREAD_STAGED) && encode_kmajor(&ta, g->a, g->m, g->k, g->lda, 128) &&
+        encode_kmajor(&tb, g->b, g->n, g->k, g->ldb, n_tile)) {
+        const size_t smem = size_t(kTmaStages) * (128 + n_tile) * kKB * 2;
+        k_gemm_bf16_tma<<<grid, kThreads, smem, (cudaStream_t)stream>>>(*g, ta, tb, n_tile, tmem_cols);
+    } else {
+        const size_t smem = size_t(2) * (128 + n_tile) * kKB * 2;
+        k_gemm_bf16<<<grid, kThreads, smem, (cudaStream_t)stream>>>(*g, n_tile, tmem_cols);
+    }
     return cuda_check("xpbd_gemm_bf16");
 }
 
