@@ -128,12 +128,13 @@ __device__ __forceinline__ void load_block(const uint16_t* __restrict__ g, int l
     }
 }
 
-// Epilogue: warp w reads TMEM lanes 32w..32w+31 (rows m0 + 32w + lane of the
-// tile) 16 columns at a time, adds the bias, multiplies by the GELU derivative
-// of a stored pre-activation (backward), applies GELU, and writes the FP32,
-// BF16 and transposed BF16 outputs that are set.
+// Epilogue: a warp of quarter q (its warp index mod 4, the TMEM lanes it may
+// read) reads lanes 32q..32q+31 (rows m0 + 32q + lane of the tile), 16 columns
+// at a time from column c_first in steps of c_step, adds the bias, multiplies
+// by the GELU derivative of a stored pre-activation (backward), applies GELU,
+// and writes the FP32, BF16 and transposed BF16 outputs that are set.
 __device__ __forceinline__ void gemm_epilogue(const XpbdGemm& G, uint32_t tmem, int m0, int n0, int n_tile, int warp,
-                                              int lane) {
+                                              int lane, int c_first = 0, int c_step = 16) {
     const int row = m0 + warp * 32 + lane;
     const bool rv = row < G.m;
     // 16-byte vector stores of a row's 16 columns where the chunk is whole
@@ -141,7 +142,7 @@ __device__ __forceinline__ void gemm_epilogue(const XpbdGemm& G, uint32_t tmem, 
     const bool vec_h = G.out_bf16 && (G.ld_bf16 % 8) == 0 && aligned_ptr16(G.out_bf16);
     const bool vec_f = G.out_f32 && (G.ld_f32 % 4) == 0 && aligned_ptr16(G.out_f32);
     const bool vec_p = G.out_pre && (G.ld_pre % 4) == 0 && aligned_ptr16(G.out_pre);
-    for (int c0 = 0; c0 < n_tile; c0 += 16) {
+    for (int c0 = c_first; c0 < n_tile; c0 += c_step) {
         float v[16];
         tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), v);
         if (!rv) continue;
@@ -283,6 +284,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_bf16(const __grid_constant
 // each block (mbarrier with transaction count), issues its four MMAs and
 // commits them to the block's "free" barrier before the stage is refilled.
 constexpr int kTmaStages = 4;
+// Eight warps: the epilogue (bias, GELU, conversions, stores) is most of the
+// kernel's time at the MLP's shapes, and two warps per TMEM lane quarter take
+// alternate 16-column chunks.
+constexpr int kTmaThreads = 256;
 
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
@@ -296,7 +301,7 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kTmaThreads, 1)
     k_gemm_bf16_tma(const __grid_constant__ XpbdGemm G, const __grid_constant__ CUtensorMap ta,
                     const __grid_constant__ CUtensorMap tb, int n_tile, int tmem_cols) {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -401,7 +406,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (s_ok) gemm_epilogue(G, tmem, m0, n0, n_tile, warp, lane);
+    if (s_ok) gemm_epilogue(G, tmem, m0, n0, n_tile, warp & 3, lane, 16 * (warp >> 2), 32);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     if (warp == 0) {
@@ -524,7 +529,7 @@ int xpbd_gemm_bf16(const XpbdGemm* g, int32_t n_tile, xpbd_stream_t stream) {
     if (!(g->flags & XPBD_GEMM_THREAD_STAGED) && encode_kmajor(&ta, g->a, g->m, g->k, g->lda, 128) &&
         encode_kmajor(&tb, g->b, g->n, g->k, g->ldb, n_tile)) {
         const size_t smem = size_t(kTmaStages) * (128 + n_tile) * kKB * 2;
-        k_gemm_bf16_tma<<<grid, kThreads, smem, (cudaStream_t)stream>>>(*g, ta, tb, n_tile, tmem_cols);
+        k_gemm_bf16_tma<<<grid, kTmaThreads, smem, (cudaStream_t)stream>>>(*g, ta, tb, n_tile, tmem_cols);
     } else {
         const size_t smem = size_t(2) * (128 + n_tile) * kKB * 2;
         k_gemm_bf16<<<grid, kThreads, smem, (cudaStream_t)stream>>>(*g, n_tile, tmem_cols);
