@@ -70,3 +70,22 @@ def test_acc_scale_for_extent_is_the_largest_safe_power_of_two():
         assert e * s <= 2.0 ** 26 < e * 2.0 * s
         # quantum at most half an FP32 ulp of the largest coordinate
         assert 1.0 / s <= np.spacing(np.float32(e)) / 2
+
+
+def test_engine_accumulator_range_rule():
+    """The engine sizes the fixed-point range by the larger of 128 longest rest
+    edges and the largest rest coordinate: the box muscle's measured worst tet
+    correction (97 mm summed over its 12 components) stays inside the range,
+    and the 535k-tet scene gets a quantum of at most 3e-8 m."""
+    from rlmusclev2_b200.engine import ACC_RANGE_EDGES, max_rest_edge
+    from rlmusclev2_b200.meshgen import box_muscle
+    lib = capi.load(build_if_missing=True)
+    x = np.array([[0, 0, 0], [1, 0, 0], [0, 2, 0], [0, 0, 3]], np.float32)
+    assert abs(max_rest_edge(x, np.array([[0, 1, 2, 3]])) - np.sqrt(13.0)) < 1e-6
+    m = box_muscle()
+    e = max(ACC_RANGE_EDGES * max_rest_edge(m.verts, m.tets), float(np.abs(m.verts).max()))
+    s = float(lib.xpbd_acc_scale_for_extent(e))
+    assert 2.0 ** 25 / s >= 0.097
+    # the 535k-tet scene: longest edge 9.7 mm, largest coordinate 0.96 m
+    s2 = float(lib.xpbd_acc_scale_for_extent(max(ACC_RANGE_EDGES * 0.00966, 0.958)))
+    assert 1.0 / s2 <= 3e-8 and 2.0 ** 25 / s2 >= 0.25
