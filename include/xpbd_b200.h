@@ -438,7 +438,10 @@ int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, f
 
 /* fine4.xyz += sum_k w_k (coarse4 - coarse_prev4)[p_idx_k] (prolong_delta_kernel,
  * mg/kernel.py:8-39), then the fine pin overwrite where vflags has
- * XPBD_VF_PIN and pin_target.w != 0 (vflags/pin_target may be NULL). */
+ * XPBD_VF_PIN and pin_target.w != 0 (vflags/pin_target may be NULL).  With
+ * coarse_prev4 NULL the prolongation is absolute, fine4.xyz = sum_k w_k
+ * coarse4[p_idx_k] (prolong_kernel, mg/kernel.py:181-203; mg_mode
+ * "projection"), on the embedded vertices only. */
 int xpbd_mg_prolong_delta(const XpbdCage* cage, const float* coarse4, const float* coarse_prev4, float* fine4,
                           const int32_t* vflags, const float* pin_target, xpbd_stream_t stream);
 

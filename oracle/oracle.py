@@ -542,7 +542,15 @@ class OracleMultiGridSim(OracleSolver):
     def vcycle(self):
         """_hpbd_vcycle (mg.py:1064-1079): restrict, kinematic pin, coarse sweeps
         each followed by the soft attach when mg_coarse_attach_beta != 0
-        (dense_soft_attach_kernel, mg/kernel.py:64-84), delta prolongation."""
+        (dense_soft_attach_kernel, mg/kernel.py:64-84), delta prolongation.
+        With mg_mode "projection" (mg.py:1263-1320): the restricted bone target
+        prolonged absolute onto the embedded fine vertices (prolong_kernel,
+        mg/kernel.py:181-203)."""
+        if str(self.cfg.get("mg_mode", "hpbd")).lower() == "projection":
+            c, w, t, e = self.mg_target, self.mg_w, self.mg_t, self.mg_emb
+            self.pos[e] = (((w[:, 0:1] * c[t[:, 0]] + w[:, 1:2] * c[t[:, 1]]) + w[:, 2:3] * c[t[:, 2]])
+                           + w[:, 3:4] * c[t[:, 3]]).astype(self.P.dt)
+            return
         co = self.mg
         co.pos[:] = self.restrict(self.pos, co.pos)
         prev = co.pos.copy()

@@ -120,7 +120,14 @@ __global__ void __launch_bounds__(kMgThreads)
     const int4 id = reinterpret_cast<const int4*>(G.p_idx)[i];
     float4 p = fine[i];
     bool wr = false;
-    if (id.x >= 0) {
+    if (id.x >= 0 && !prev) {  // absolute prolongation (prolong_kernel, mg/kernel.py:181-203)
+        const float4 w = reinterpret_cast<const float4*>(G.p_w)[i];
+        const float4 a0 = coarse[id.x], a1 = coarse[id.y], a2 = coarse[id.z], a3 = coarse[id.w];
+        p.x = ((w.x * a0.x + w.y * a1.x) + w.z * a2.x) + w.w * a3.x;
+        p.y = ((w.x * a0.y + w.y * a1.y) + w.z * a2.y) + w.w * a3.y;
+        p.z = ((w.x * a0.z + w.y * a1.z) + w.z * a2.z) + w.w * a3.z;
+        wr = true;
+    } else if (id.x >= 0) {
         const float4 w = reinterpret_cast<const float4*>(G.p_w)[i];
         const float4 a0 = coarse[id.x], b0 = prev[id.x], a1 = coarse[id.y], b1 = prev[id.y];
         const float4 a2 = coarse[id.z], b2 = prev[id.z], a3 = coarse[id.w], b3 = prev[id.w];
@@ -180,7 +187,7 @@ int xpbd_mg_prolong_delta(const XpbdCage* cage, const float* coarse4, const floa
                           const int32_t* vflags, const float* pin_target, xpbd_stream_t stream) {
     int rc;
     if ((rc = check_cage(cage))) return rc;
-    if (!coarse4 || !coarse_prev4 || !fine4) return fail(XPBD_ERR_ARG, "xpbd_mg_prolong_delta: null buffer");
+    if (!coarse4 || !fine4) return fail(XPBD_ERR_ARG, "xpbd_mg_prolong_delta: null buffer");
     if (!aligned16(coarse4) || !aligned16(coarse_prev4) || !aligned16(fine4) || !aligned16(pin_target))
         return fail(XPBD_ERR_ALIGN, "xpbd_mg_prolong_delta: [n][4] buffers must be 16-byte aligned");
     k_mg_prolong_delta<<<(cage->n_fine + kMgThreads - 1) / kMgThreads, kMgThreads, 0, (cudaStream_t)stream>>>(

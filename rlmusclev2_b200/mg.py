@@ -246,8 +246,6 @@ class MultiGridSim(MuscleSim):
         self.collision_solvers_iter = []
         self.mg = None
         if self.use_multigrid:
-            if self.mg_mode != "hpbd":
-                raise NotImplementedError("mg_mode='projection' is not on the sm_100a path (use 'hpbd')")
             from .multigrid import DeviceMultigrid
             self.mg = DeviceMultigrid(self, spacing=float(cfg.get("mg_cage_spacing", 0.016)))
         self.collision_solvers = []

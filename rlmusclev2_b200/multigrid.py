@@ -98,6 +98,9 @@ class DeviceMultigrid:
         self.coarse = XpbdSolver(q0, cage.coarse_tet, table, mass=mass, dt=sim.dt, stopped=self.coarse_pin,
                                  device=sim.device, stream=sim._stream, acc_range=float(np.abs(q0).max()))
         self.iters = int(sim.mg_coarse_iters)
+        # "hpbd": the cage is its own ARAP sim, delta-prolonged; "projection": the
+        # fine state is reset to the prolonged restricted bone target each substep
+        self.mode = str(getattr(sim, "mg_mode", "hpbd"))
         self._build_device()
 
     def _build_device(self):
@@ -151,8 +154,17 @@ class DeviceMultigrid:
                                            C.c_void_p(self.pin4.data_ptr()), None, None, s._sp))
 
     def vcycle(self, pin_fine: bool):
-        """Restrict + coarse solve + delta prolong (+ fine re-pin)."""
+        """Restrict + coarse solve + delta prolong (+ fine re-pin); with
+        mg_mode="projection" (mg.py:1263-1320) the restricted bone target,
+        prolonged absolute onto the embedded fine vertices (+ fine re-pin)."""
         s, co = self.sim, self.coarse
+        vf = s._vflags.data_ptr() if (pin_fine and s._vflags is not None) else None
+        pt = s._pin_tgt.data_ptr() if (pin_fine and s._pin_tgt is not None) else None
+        if self.mode == "projection":
+            capi.check(s._lib.xpbd_mg_prolong_delta(C.byref(self.g), C.c_void_p(self.pin4.data_ptr()), None,
+                                                    C.c_void_p(s._pos4.data_ptr()), C.c_void_p(vf) if vf else None,
+                                                    C.c_void_p(pt) if pt else None, s._sp))
+            return
         capi.check(s._lib.xpbd_mg_restrict(C.byref(self.g), C.c_void_p(s._pos4.data_ptr()),
                                            C.c_void_p(co._pos4.data_ptr()), C.c_void_p(self.prev.data_ptr()),
                                            C.c_void_p(self.pin4.data_ptr()), s._sp))
@@ -166,8 +178,6 @@ class DeviceMultigrid:
                                                        s._sp))
         else:
             co._fused_iterations(self.iters)
-        vf = s._vflags.data_ptr() if (pin_fine and s._vflags is not None) else None
-        pt = s._pin_tgt.data_ptr() if (pin_fine and s._pin_tgt is not None) else None
         capi.check(s._lib.xpbd_mg_prolong_delta(C.byref(self.g), C.c_void_p(co._pos4.data_ptr()),
                                                 C.c_void_p(self.prev.data_ptr()), C.c_void_p(s._pos4.data_ptr()),
                                                 C.c_void_p(vf) if vf else None, C.c_void_p(pt) if pt else None,

@@ -115,3 +115,38 @@ def test_mg_frames_run_and_stay_finite():
     print(f"mg frames: |gpu-o64| {err:.3e}  oracle FP32/FP64 spread {spread:.3e}")
     assert np.isfinite(p).all()
     assert err <= max(1e-4, 3.0 * spread)
+
+
+def test_projection_mode_frames_vs_oracle():
+    """mg_mode="projection" (mg.py:1263-1320): every substep the embedded fine
+    vertices restart from the prolonged restricted bone target.  Three frames on
+    the small scene without the skip threshold, against the FP64 oracle at three
+    times the FP32 oracle's distance (max and p99)."""
+    cfg = load_config("rlmusclev2_b200/configs/humanv2_synth_mg_dcd.json")
+    cfg["demo"]["collision"]["sdf_res"] = 96
+    cfg["demo"]["self_collision"]["method"] = "none"
+    cfg["mg_mode"] = "projection"
+    sc = humanv2_scene(seed=1, n_muscles=5, n_bones=4, target_tets=20000, fascia_tets=3000, box=(0.35, 0.35, 0.35))
+    sim = MultiGridSim(cfg, scene=sc)
+    sim._prm.arap_skip_ssq = -1.0
+    o32 = O.OracleMultiGridSim(cfg, sc, prec="f32")
+    o64 = O.OracleMultiGridSim(cfg, sc, prec="f64")
+    tol = 1e-5 * bbox_diag(sc.verts)
+    O.set_arap_skip(-1.0)
+    try:
+        for frame in (1, 2, 3):
+            sim.set_fiber_activation(sc.activation(frame))
+            sim.step_frame(frame)
+            o32.step_frame(frame)
+            o64.step_frame(frame)
+            p = sim.positions_np()
+            d = np.abs(p - o64.pos).max(1)
+            spr = np.abs(o32.pos - o64.pos).max(1)
+            print(f"projection frame {frame}: |gpu-o64| max {d.max():.3e} p99 {np.percentile(d, 99):.3e}; "
+                  f"|o32-o64| max {spr.max():.3e}")
+            assert np.isfinite(p).all()
+            assert d.max() <= max(tol, 3.0 * spr.max())
+            assert np.percentile(d, 99) <= max(tol, 3.0 * np.percentile(spr, 99))
+    finally:
+        O.set_arap_skip(0.0)
+    assert np.abs(o64.pos - sc.verts).max() > 100 * tol

@@ -57,3 +57,21 @@ def test_options_change_the_frames():
         runs[key] = o.pos.copy()
     assert np.abs(runs[(0.5, 0.0)] - runs[(0.0, 0.0)]).max() > 1e-5
     assert np.abs(runs[(0.0, 0.3)] - runs[(0.0, 0.0)]).max() > 1e-6
+
+
+def test_projection_mode_restarts_from_the_prolonged_target():
+    """mg_mode="projection" on the oracle: after one substep's V-cycle the
+    embedded vertices sit on the prolonged restricted target."""
+    sc = _scene()
+    cfg = _cfg()
+    cfg["mg_mode"] = "projection"
+    o = O.OracleMultiGridSim(cfg, sc, prec="f64")
+    o.target, _ = o.targets(2)
+    o.mg_target = o.restrict(o.target, o.mg_target)
+    o.pos[:] = o.pos + 0.01
+    o.vcycle()
+    e, w, t = o.mg_emb, o.mg_w, o.mg_t
+    want = sum(w[:, k:k + 1] * o.mg_target[t[:, k]] for k in range(4))
+    assert np.abs(o.pos[e] - want).max() < 1e-12
+    # the restricted target reproduces the bone target on the embedded vertices
+    assert np.abs(o.pos[e] - o.target[e]).max() < 5e-3
