@@ -168,6 +168,36 @@ def create_attach_constraints(src: np.ndarray, target: np.ndarray, restlength, s
         c_restvector=rv, c_restdir=np.zeros((n, 3), np.float32))
 
 
+def constraints_from_dicts(rows: list[dict]) -> ConstraintTable:
+    """A table from constraint dicts in the reference's schema (builder.py:164-175:
+    type, pts[4], stiffness, dampingratio, compressionstiffness, tetid, L[3],
+    restlength, restvector[4], restdir[3]); missing keys take the builder's
+    defaults (pts -1, compressionstiffness -1, tetid -1, restvector (0, 0, 0, 1))."""
+    n = len(rows)
+    t = ConstraintTable(
+        c_type=np.zeros(n, np.int32), c_pts=np.full((n, 4), -1, np.int32), c_stiffness=np.zeros(n, np.float32),
+        c_compressionstiffness=np.full(n, -1.0, np.float32), c_dampingratio=np.zeros(n, np.float32),
+        c_tetid=np.full(n, -1, np.int32), c_L=np.zeros((n, 3), np.float32), c_restlength=np.zeros(n, np.float32),
+        c_restvector=np.tile(np.array([0, 0, 0, 1], np.float32), (n, 1)), c_restdir=np.zeros((n, 3), np.float32))
+    for i, c in enumerate(rows):
+        t.c_type[i] = int(c["type"])
+        pts = list(c.get("pts", []))[:4]
+        t.c_pts[i, :len(pts)] = pts
+        t.c_stiffness[i] = float(c.get("stiffness", 0.0))
+        t.c_compressionstiffness[i] = float(c.get("compressionstiffness", -1.0))
+        t.c_dampingratio[i] = float(c.get("dampingratio", 0.0))
+        t.c_tetid[i] = int(c.get("tetid", -1))
+        if c.get("L") is not None:
+            t.c_L[i] = np.asarray(c["L"], np.float32)[:3]
+        t.c_restlength[i] = float(c.get("restlength", 0.0))
+        if c.get("restvector") is not None:
+            rv = np.asarray(c["restvector"], np.float32).reshape(-1)
+            t.c_restvector[i, :rv.shape[0]] = rv[:4]
+        if c.get("restdir") is not None:
+            t.c_restdir[i] = np.asarray(c["restdir"], np.float32)[:3]
+    return t
+
+
 def collect_raw_constraints(pos0, tets, constraint_configs, tet_masks: dict | None = None) -> ConstraintTable:
     """_collect_raw_constraints (builder.py:610-656) for the tet types of the
     sm_100a path.  ``tet_masks`` optionally restricts a named config to a tet

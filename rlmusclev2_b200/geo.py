@@ -326,4 +326,4 @@ def scene_from_geo(rest_path: str | Path):
     return Scene(verts=verts, tets=tets, tet_part=tpart, vert_part=vpart, v_tendon=tendon, v_fiber=fib,
                  surface_tris=surf, bone_center=z3, bone_axis=z3, bone_half=z1, bone_radius=z1,
                  vert_bone=np.zeros((nv, 2), np.int32), vert_bw=np.zeros(nv, np.float32), traj={}, aniso_muscle=-1,
-                 meta=dict(source=str(rest_path)))
+                 meta=dict(source=str(rest_path), muscle_names=list(g.prim_attr_strings("muscle_id"))))

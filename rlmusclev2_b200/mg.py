@@ -614,6 +614,58 @@ class MultiGridSim(MuscleSim):
         if self._has_pins:
             self._apply_all(capi.APPLY_PIN)
 
+    # ----------------------------------------------------------- helpers
+    def count_coarse_inverted(self) -> int:
+        """count_coarse_inverted (mg.py:954-965): cage tets with det F <= 0 at the
+        current cage positions; 0 without the hpbd cage."""
+        if self.mg is None or self.mg.mode != "hpbd":
+            return 0
+        return int(self.mg.coarse.count_inverted())
+
+    def belly_track_mm(self) -> tuple[float, float]:
+        """belly_track_mm (mg.py:967-977): median and mean distance in mm from
+        each constraint point to its bone-driven goal (target_pos + rest_offset);
+        one device sync."""
+        if self._pin_tgt is None:
+            raise RuntimeError("belly_track_mm needs pin targets (a muscleToBonePin or belly_attach block)")
+        goal = self._to_user(self._pin_tgt)
+        pos = self.positions_np()
+        idx = self._cons_pts if self.target_mode == "points" else slice(None)
+        d = np.linalg.norm(pos[idx] - goal[idx], axis=1)
+        return float(np.percentile(d, 50) * 1e3), float(d.mean() * 1e3)
+
+    def tet_mask_for_muscles(self, names) -> np.ndarray:
+        """tet_mask_for_muscles (mg.py:1083-1096): per-tet mask of the muscles
+        whose name contains any of ``names`` (the rest mesh's ``muscle_id``
+        strings), in the user's tet order."""
+        if isinstance(names, str):
+            names = [names]
+        strings = list(self.scene.meta.get("muscle_names") or [])
+        if not strings:
+            raise ValueError("the rest mesh has no 'muscle_id' prim attribute names")
+        sel = [i for i, m in enumerate(strings) if any(n in m for n in names)]
+        return np.isin(self.scene.tet_part, sel)
+
+    def preload_targets(self, frames=None) -> None:
+        """preload_targets (mg.py:1216-1231): read every frame's targets once
+        (the cons frames of target_mode="points"; the other modes compute theirs
+        on the device and have nothing to read)."""
+        if self.target_mode != "points":
+            return
+        if frames is None:
+            frames = range(self.start_frame, self.end_frame + 1)
+        for f in frames:
+            self._cons_targets(int(f))
+
+    def substep_at_frac_frame(self, t: float) -> None:
+        """substep_at_frac_frame (mg.py:1421-1432): the kinematic step at the
+        fractional frame t (bone targets sampled on the bones' path), then one
+        substep of the phase program."""
+        self._check_status()
+        self._kinematic_step(t)
+        self.substep()
+        self._post_status()
+
     def apply_pintotarget_all(self) -> None:
         """Soft pin (apply_pintotarget_all, mg/mg.py:1386-1397): every constraint
         point moves by presubframe_pintotarget x (target - pos) toward its pin

@@ -128,12 +128,29 @@ class MuscleSim(XpbdEngine):
         table = collect_raw_constraints(vertices, tets, self.constraint_configs, tet_masks).sorted_by_type()
         self.raw_constraints = table
         st = np.zeros(n_v, np.int32) if stopped is None else np.asarray(stopped, np.int32)
-        self._setup_device(device, mass=mass, stopped=st, table=table, v_fiber=self.v_fiber_np,
-                           tet_tendonmask=tet_tendonmask, dt=float(dts) / int(num_substeps),
-                           gravity_vec=(0.0, float(gravity), 0.0), veldamping=float(veldamping),
-                           quasi_static=bool(quasi_static), omega=float(relaxation),
-                           contraction_ratio=contraction_ratio, fiber_stiffness_scale=fiber_stiffness_scale,
-                           tile_tets=tile_tets)
+        self._setup_kw = dict(device=device, mass=mass, v_fiber=self.v_fiber_np, tet_tendonmask=tet_tendonmask,
+                              dt=float(dts) / int(num_substeps), gravity_vec=(0.0, float(gravity), 0.0),
+                              veldamping=float(veldamping), quasi_static=bool(quasi_static),
+                              omega=float(relaxation), contraction_ratio=contraction_ratio,
+                              fiber_stiffness_scale=fiber_stiffness_scale, tile_tets=tile_tets)
+        self._setup_device(stopped=st, table=table, **self._setup_kw)
+
+    def rebuild_constraints(self, extra_constraints=None) -> None:
+        """musclesim.py:289-321: the constraint table rebuilt from the raw
+        constraints plus ``extra_constraints`` (dicts in the reference's schema,
+        e.g. ATTACH rows added after the build), sorted by type.  The device
+        layout is rebuilt; positions, previous positions, velocities and the
+        stopped flags carry over."""
+        from .builder import ConstraintTable, constraints_from_dicts
+        extra = list(extra_constraints or [])
+        parts = [self.raw_constraints] + ([constraints_from_dicts(extra)] if extra else [])
+        table = ConstraintTable.concat(parts).sorted_by_type()
+        pos, prev, vel = self.positions_np(), self.pprev.numpy(), self.vel.numpy()
+        self.release_graphs()
+        self._setup_device(stopped=self._stopped_user.copy(), table=table, **self._setup_kw)
+        self.set_positions(prev, also_prev=True)
+        self.set_positions(pos)
+        self.set_velocities(vel)
 
     # ---------------------------------------------------------------- program
     def build_program(self):

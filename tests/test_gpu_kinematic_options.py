@@ -104,3 +104,33 @@ def test_presubframe_one_snaps_every_vertex_before_the_substeps():
     pos = sim._pos4[:, :3].cpu().numpy()
     tgt = sim._pin_tgt[:, :3].cpu().numpy()
     assert np.abs(pos - tgt).max() <= 2.5e-7
+
+
+def test_helpers_frac_frame_tracking_and_cage_inversions():
+    """substep_at_frac_frame, belly_track_mm, count_coarse_inverted and
+    tet_mask_for_muscles (mg.py:954-977, 1083-1096, 1421-1432)."""
+    cfg, sc = _scene(0.0, 0.0)
+    sim = MultiGridSim(cfg, scene=sc)
+    sim.set_fiber_activation(sc.activation(1))
+    sim.step_frame(1)
+    p50_0, mean_0 = sim.belly_track_mm()
+    assert 0.0 <= p50_0 and np.isfinite(mean_0)
+    assert sim.count_coarse_inverted() == 0
+    # sub-frame bone path: ten substeps easing from frame 1 to frame 2
+    for k in range(1, sim.nsubsteps + 1):
+        sim.substep_at_frac_frame(1.0 + k / sim.nsubsteps)
+    p = sim.positions_np()
+    ref = MultiGridSim(cfg, scene=sc)
+    ref.set_fiber_activation(sc.activation(1))
+    ref.step_frame(1)
+    ref.step_frame(2)
+    q = ref.positions_np()
+    assert np.isfinite(p).all()
+    # a different path to the same pose: near the whole-frame step (bones move at
+    # most 10 mm per frame), not equal to it
+    assert 0.0 < np.abs(p - q).max() < 1e-2
+    with pytest.raises(ValueError):
+        sim.tet_mask_for_muscles("biceps")  # the synthetic scene carries no muscle names
+    sim.scene.meta["muscle_names"] = [f"L_muscle{k}" for k in range(int(sc.tet_part.max()) + 1)]
+    m = sim.tet_mask_for_muscles(["muscle1", "muscle3"])
+    assert m.shape == (sc.tets.shape[0],) and np.array_equal(m, np.isin(sc.tet_part, [1, 3]))

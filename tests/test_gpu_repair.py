@@ -98,3 +98,28 @@ def test_repair_off_is_a_noop():
     _, sim, _ = _pair(start, 0.0, 2, 0.3)
     sim.repair_inverted_tets()
     assert np.array_equal(sim.positions_np(), start)
+
+
+def test_rebuild_constraints_keeps_state_and_adds_attach():
+    """MuscleSim.rebuild_constraints (musclesim.py:289-321): without extras the
+    rebuilt sim steps exactly as before; ATTACH rows added as reference-schema
+    dicts pull their vertices toward the targets."""
+    from rlmusclev2_b200.defs import ConstraintType
+    m = box_muscle()
+    mk = lambda: MuscleSim.from_procedural(m.verts, m.tets, m.fiber_per_tet, constraint_configs=CONS,  # noqa: E731
+                                           device="cuda:0", stopped=m.stopped, **KW)
+    a, b, c = mk(), mk(), mk()
+    for s in (a, b, c):
+        s.step()
+    b.rebuild_constraints()
+    np.testing.assert_array_equal(a.positions_np(), b.positions_np())
+    free = np.nonzero(m.stopped == 0)[0][:8]
+    tgt = m.verts[free] + np.array([0.0, 0.01, 0.0], np.float32)
+    rows = [dict(type=int(ConstraintType.ATTACH), pts=[int(v), -1, -1, -1], stiffness=1e6, dampingratio=0.0,
+                 restlength=0.0, restvector=[*map(float, t), 1.0]) for v, t in zip(free, tgt)]
+    c.rebuild_constraints(rows)
+    for s in (a, b, c):
+        s.step()
+    np.testing.assert_array_equal(a.positions_np(), b.positions_np())
+    pa, pc = a.positions_np()[free], c.positions_np()[free]
+    assert (np.linalg.norm(pc - tgt, axis=1) < np.linalg.norm(pa - tgt, axis=1)).all()
