@@ -302,7 +302,7 @@ class OracleMuscleSim(OracleSolver):
     def __init__(self, vertices, tets, fiber_dirs_per_tet, *, constraint_configs, dts, num_substeps=1,
                  density=1060.0, veldamping=0.02, gravity=0.0, stopped=None, relaxation=1.0,
                  contraction_ratio=0.0, fiber_stiffness_scale=1.0, tet_masks=None, repair_alpha=0.0, repair_iters=0,
-                 repair_sigma_min=0.1, prec="f32"):
+                 repair_sigma_min=0.1, attach=None, prec="f32"):
         vertices = np.asarray(vertices, np.float32)
         tets = np.asarray(tets, np.int32)
         nv = vertices.shape[0]
@@ -318,7 +318,17 @@ class OracleMuscleSim(OracleSolver):
         vf /= np.maximum(np.linalg.norm(vf, axis=1, keepdims=True), 1e-8)
         rv, B, mass, tot = precompute_rest(vertices, tets, density, prec)
         self.total_rest_volume = tot
-        table = table_from_configs(vertices, tets, constraint_configs, tet_masks).finalize()
+        table = table_from_configs(vertices, tets, constraint_configs, tet_masks)
+        if attach is not None:
+            # bone attach rows (builder.py:347-398): (src, target xyz, rest length, stiffness, damping)
+            src, tgt, rl, k, d = attach
+            n = len(src)
+            pts = np.full((n, 4), -1, np.int32)
+            pts[:, 0] = src
+            rv = np.ones((n, 4))
+            rv[:, :3] = tgt
+            table.add(T_ATTACH, pts, float(k), float(d), np.full(n, -1), np.asarray(rl, np.float64), restvector=rv)
+        table = table.finalize()
         st = np.zeros(nv, np.int32) if stopped is None else np.asarray(stopped, np.int32)
         super().__init__(vertices, tets, table, mass, st, B, dt=float(dts) / int(num_substeps),
                          gravity_vec=(0.0, float(gravity), 0.0), veldamping=veldamping, relaxation=relaxation,

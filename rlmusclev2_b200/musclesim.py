@@ -13,8 +13,24 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import _capi as capi
-from .builder import collect_raw_constraints, lumped_mass
+import torch
+
+from .builder import ConstraintTable, collect_raw_constraints, create_attach_constraints, lumped_mass
 from .engine import XpbdEngine
+
+
+class _GeoPointAttrs:
+    """Point attributes of a .geo rest mesh as attributes (the reference's
+    ``self.geo``, read by the attach blocks' ``mask_name``)."""
+
+    def __init__(self, geo):
+        self._geo = geo
+
+    def __getattr__(self, name):
+        geo = self.__dict__["_geo"]
+        if geo.has_point_attr(name):
+            return geo.point_attr(name)
+        raise AttributeError(name)
 
 
 class MuscleSim(XpbdEngine):
@@ -40,11 +56,14 @@ class MuscleSim(XpbdEngine):
         if not path.exists():
             raise FileNotFoundError(f"geo_path {path} does not exist")
         if path.suffix.lower() == ".geo":
-            from .geo import scene_from_geo
+            from .geo import GeoFile, scene_from_geo
             sc = scene_from_geo(path)
+            self.geo = _GeoPointAttrs(GeoFile(path))
         else:
             from .usd import scene_from_usda
             sc = scene_from_usda(path, get("geo_prim_path"))
+            self.geo = SimpleNamespace(tendonmask=sc.v_tendon)
+        self.bone_pos = np.zeros((0, 3), np.float32)
         tendon_tet = (sc.v_tendon[sc.tets].astype(np.float32).sum(1) / np.float32(4.0)).astype(np.float32)
         self._build(sc.verts, sc.tets, sc.v_fiber, cfg=cfg, constraint_configs=list(get("constraints") or []),
                     dts=float(get("dt", 1.0 / 24.0)), num_substeps=int(get("num_substeps", 1)), device=device,
@@ -89,6 +108,7 @@ class MuscleSim(XpbdEngine):
             activation=0.0, nsteps=1, sigma0=sigma0, lambda_opt=lambda_opt, v_max_norm=v_max_norm, d_damp=d_damp,
             relaxation=relaxation)
         sim = object.__new__(cls)
+        sim.geo = SimpleNamespace()  # point attributes for attach masks, as the reference's empty namespace
         sim._build(vertices, tets, vf, cfg=cfg, constraint_configs=cfg.constraints, dts=dts,
                    num_substeps=num_substeps, device=device, density=density, veldamping=veldamping, gravity=gravity,
                    contraction_ratio=contraction_ratio, fiber_stiffness_scale=fiber_stiffness_scale, stopped=stopped,
@@ -111,8 +131,12 @@ class MuscleSim(XpbdEngine):
         self.v_fiber_np = np.asarray(v_fiber, np.float32)
         self.v_tendonmask_np = v_tendonmask
         self.n_verts = n_v
-        self.bone_pos = (np.asarray(bone_targets, np.float32) if bone_targets is not None
-                         else np.zeros((0, 3), np.float32))
+        if bone_targets is not None:
+            self.bone_pos = np.asarray(bone_targets, np.float32).reshape(-1, 3)
+        elif not hasattr(self, "bone_pos"):
+            self.bone_pos = np.zeros((0, 3), np.float32)
+        if not hasattr(self, "geo"):
+            self.geo = SimpleNamespace()
         self.use_jacobi = True
         self.use_colored_gs = False
         self.contraction_ratio = contraction_ratio
@@ -125,7 +149,12 @@ class MuscleSim(XpbdEngine):
         mass, rest_volume = lumped_mass(vertices, tets, density)
         self.rest_volume_np = rest_volume
         self.total_rest_volume = float(rest_volume.astype(np.float64).sum())
-        table = collect_raw_constraints(vertices, tets, self.constraint_configs, tet_masks).sorted_by_type()
+        self._tet_masks = tet_masks
+        table = collect_raw_constraints(vertices, tets, self.constraint_configs, tet_masks)
+        attach = self._bone_attach_rows(vertices, tets)
+        if attach is not None:
+            table = ConstraintTable.concat([table, attach])
+        table = table.sorted_by_type()
         self.raw_constraints = table
         st = np.zeros(n_v, np.int32) if stopped is None else np.asarray(stopped, np.int32)
         self._setup_kw = dict(device=device, mass=mass, v_fiber=self.v_fiber_np, tet_tendonmask=tet_tendonmask,
@@ -135,13 +164,89 @@ class MuscleSim(XpbdEngine):
                               fiber_stiffness_scale=fiber_stiffness_scale, tile_tets=tile_tets)
         self._setup_device(stopped=st, table=table, **self._setup_kw)
 
+    # ------------------------------------------------------- bone attach
+    def load_bone_geo(self, target_path):
+        """load_bone_geo (musclesim.py:101-105): the bone geometry of an attach
+        block (a Houdini .geo) and its point positions, read once."""
+        if getattr(self, "_bone_geo_path", None) != str(target_path) or self.bone_pos.shape[0] == 0:
+            from .geo import GeoFile
+            self.bone_geo = GeoFile(target_path)
+            self.bone_pos = self.bone_geo.positions.astype(np.float32)
+            self._bone_geo_path = str(target_path)
+        return getattr(self, "bone_geo", None), self.bone_pos
+
+    def _bone_attach_rows(self, pos0, tets):
+        """create_attach_constraints (builder.py:347-398) for every enabled
+        "attach" block: the vertices whose point attribute ``mask_name`` exceeds
+        ``mask_threshold`` (0.75) attach to their nearest bone point (a k-d tree
+        over the bone points, from ``bone_targets`` or the block's
+        ``target_path``) with the rest length of that distance.  Bone point
+        groups (target_group) are not read: every bone point is a candidate."""
+        from scipy.spatial import cKDTree
+        rows = []
+        self._attach_src = np.zeros(0, np.int64)
+        self._attach_tgt_idx = np.zeros(0, np.int64)
+        for params in self.constraint_configs:
+            if not params.get("enable", True) or str(params.get("type", "")).lower() != "attach":
+                continue
+            if params.get("target_path") and self.bone_pos.shape[0] == 0:
+                self.load_bone_geo(params["target_path"])
+            mask = getattr(self.geo, str(params.get("mask_name")), None)
+            if mask is None or self.bone_pos.shape[0] == 0:
+                continue  # the reference warns and builds no rows
+            src = np.nonzero(np.asarray(mask, np.float32).reshape(-1) > float(params.get("mask_threshold", 0.75)))[0]
+            if src.size == 0:
+                continue
+            d, tgt = cKDTree(self.bone_pos).query(pos0[src], k=1)
+            tgt = np.asarray(tgt, np.int64)
+            first_tet = np.full(pos0.shape[0], -1, np.int64)
+            order = np.arange(tets.shape[0] * 4)[::-1]
+            first_tet[tets.reshape(-1)[order]] = order // 4
+            rows.append(create_attach_constraints(
+                src.astype(np.int32), self.bone_pos[tgt], np.asarray(d, np.float32),
+                float(params.get("stiffness", 1e10)), float(params.get("dampingratio", 0.0)),
+                tgt_idx=tgt.astype(np.int32), tetid=first_tet[src]))
+            self._attach_src = np.concatenate([self._attach_src, src])
+            self._attach_tgt_idx = np.concatenate([self._attach_tgt_idx, tgt])
+        return ConstraintTable.concat(rows) if rows else None
+
+    def update_attach_targets(self) -> None:
+        """update_attach_targets (musclesim.py:564-578): the bone-attach targets
+        follow the current bone points (``self.bone_pos``); uploaded only when
+        they changed."""
+        src = getattr(self, "_attach_src", None)
+        if src is None or src.size == 0 or self._attach_tgt is None or self.bone_pos.shape[0] == 0:
+            return
+        last = getattr(self, "_attach_bone_last", None)
+        if last is not None and last.shape == self.bone_pos.shape and np.array_equal(last, self.bone_pos):
+            return
+        self._attach_bone_last = self.bone_pos.copy()
+        lib_idx = torch.from_numpy(self.layout.inv[src].astype(np.int64)).to(self.device)
+        tgt = torch.from_numpy(np.ascontiguousarray(self.bone_pos[self._attach_tgt_idx], np.float32)).to(self.device)
+        with torch.cuda.stream(self._stream):
+            self._attach_tgt[lib_idx, :3] = tgt
+
+    def build_constraints(self) -> None:
+        """build_constraints (musclesim.py:365-389): the constraint blocks
+        collected again (with the current point attributes in ``self.geo`` and
+        bone points in ``self.bone_pos``) and the device rebuilt; the state
+        carries over."""
+        table = collect_raw_constraints(self.pos0_np, self.tet_np, self.constraint_configs,
+                                        getattr(self, "_tet_masks", None))
+        attach = self._bone_attach_rows(self.pos0_np, self.tet_np)
+        if attach is not None:
+            table = ConstraintTable.concat([table, attach])
+        self.raw_constraints = table.sorted_by_type()
+        self._attach_bone_last = None
+        self.rebuild_constraints()
+
     def rebuild_constraints(self, extra_constraints=None) -> None:
         """musclesim.py:289-321: the constraint table rebuilt from the raw
         constraints plus ``extra_constraints`` (dicts in the reference's schema,
         e.g. ATTACH rows added after the build), sorted by type.  The device
         layout is rebuilt; positions, previous positions, velocities and the
         stopped flags carry over."""
-        from .builder import ConstraintTable, constraints_from_dicts
+        from .builder import constraints_from_dicts
         extra = list(extra_constraints or [])
         parts = [self.raw_constraints] + ([constraints_from_dicts(extra)] if extra else [])
         table = ConstraintTable.concat(parts).sorted_by_type()
@@ -193,8 +298,10 @@ class MuscleSim(XpbdEngine):
         self._vstep(capi.OP_VELOCITY)
 
     def step(self):
-        """One frame (musclesim.py:136-142)."""
+        """One frame (musclesim.py:136-142): the bone-attach targets follow the
+        bones, then the substeps."""
         self._check_status()
+        self.update_attach_targets()
         if self._hooks():
             if getattr(self, "program", None) is None:
                 self.build_program()
@@ -206,6 +313,7 @@ class MuscleSim(XpbdEngine):
 
     def step_eager(self):
         """One frame through the phase program (no graph, unfused primitives)."""
+        self.update_attach_targets()
         if getattr(self, "program", None) is None:
             self.build_program()
         self.run_program()

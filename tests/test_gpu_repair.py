@@ -123,3 +123,40 @@ def test_rebuild_constraints_keeps_state_and_adds_attach():
     np.testing.assert_array_equal(a.positions_np(), b.positions_np())
     pa, pc = a.positions_np()[free], c.positions_np()[free]
     assert (np.linalg.norm(pc - tgt, axis=1) < np.linalg.norm(pa - tgt, axis=1)).all()
+
+
+def test_bone_attach_blocks_vs_oracle():
+    """An "attach" block (create_attach_constraints, builder.py:347-398): the
+    masked vertices attach to their nearest bone point at the rest distance;
+    when the bone points move, the targets follow (update_attach_targets,
+    musclesim.py:564-578).  Against the FP32 oracle with the same rows."""
+    from scipy.spatial import cKDTree
+    m = box_muscle()
+    z = m.verts[:, 2]
+    zr = (z - z.min()) / (z.max() - z.min())
+    mask = ((zr > 0.1) & (zr < 0.2)).astype(np.float32)
+    bones = (m.verts[mask > 0.5][::3] + np.array([0.0, 0.004, 0.0], np.float32)).astype(np.float32)
+    att = dict(type="attach", name="bone_attach", mask_name="attachmask", mask_threshold=0.5, stiffness=1e6,
+               dampingratio=0.0)
+    sim = MuscleSim.from_procedural(m.verts, m.tets, m.fiber_per_tet, bone_targets=bones,
+                                    constraint_configs=CONS + [att], device="cuda:0", stopped=m.stopped, **KW)
+    sim.geo.attachmask = mask
+    sim.build_constraints()
+    src = np.nonzero(mask > 0.5)[0]
+    d, tgt = cKDTree(bones).query(m.verts[src], k=1)
+    assert np.array_equal(np.sort(sim._attach_src), src)
+    orc = O.OracleMuscleSim(m.verts, m.tets, m.fiber_per_tet, constraint_configs=CONS, stopped=m.stopped,
+                            attach=(src, bones[tgt], d, 1e6, 0.0), prec="f32", **KW)
+    tol = 1e-5 * bbox_diag(m.verts)
+    rows = np.nonzero(orc.c_type == O.T_ATTACH)[0]
+    for frame in range(3):
+        if frame == 2:  # the bones move: the attach targets follow
+            moved = (bones + np.array([0.0, 0.0, 0.005], np.float32)).astype(np.float32)
+            sim.bone_pos = moved
+            orc.c_rv[rows, :3] = moved[tgt]
+        sim.step()
+        orc.step()
+        err = np.abs(sim.positions_np() - orc.pos).max()
+        print(f"bone attach frame {frame}: |gpu-o32| {err:.3e} (tol {tol:.3e})")
+        assert err <= tol
+    assert np.abs(orc.pos - m.verts).max() > 10 * tol
