@@ -7,13 +7,14 @@ Houdini ``.geo`` file or a text USD layer (``.usda``, read without pxr) at
 """
 from __future__ import annotations
 
+import ctypes as C
 from pathlib import Path
 from types import SimpleNamespace
 
 import numpy as np
+import torch
 
 from . import _capi as capi
-import torch
 
 from .builder import ConstraintTable, collect_raw_constraints, create_attach_constraints, lumped_mass
 from .engine import XpbdEngine
@@ -163,6 +164,80 @@ class MuscleSim(XpbdEngine):
                               omega=float(relaxation), contraction_ratio=contraction_ratio,
                               fiber_stiffness_scale=fiber_stiffness_scale, tile_tets=tile_tets)
         self._setup_device(stopped=st, table=table, **self._setup_kw)
+
+    # ------------------------------------------------------- state helpers
+    def reset(self) -> None:
+        """reset (musclesim.py:555-562): rest positions (also the previous ones),
+        zero velocities and activation, cleared accumulators, step count 1."""
+        self.set_positions(self.pos0_np, also_prev=True)
+        self.set_velocities(np.zeros_like(self.pos0_np))
+        if self._t_act is not None:
+            with torch.cuda.stream(self._stream):
+                self._t_act.zero_()
+        self.clear()
+        self.synchronize()
+        self.step_cnt = 1
+
+    def clear_forces(self) -> None:
+        """clear_forces (musclesim.py:580-582).  The explicit per-vertex force
+        accumulator only feeds the active fiber force (sigma0 > 0), which this
+        path does not run, so there is nothing to zero."""
+
+    def clear_reaction(self) -> None:
+        """clear_reaction (musclesim.py:676-679).  The attach reaction sums are
+        not accumulated on this path (get_insertion_force works from
+        positions), so there is nothing to zero."""
+
+    def save_predicted_positions(self, vertex_ids) -> None:
+        """save_predicted_positions (musclesim.py:612-615): the positions of
+        vertex_ids after integrate(), before the constraint solve."""
+        ids = np.asarray(vertex_ids)
+        self._predicted_pos = self.positions_np()[ids].copy()
+        self._predicted_ids = ids
+
+    def get_insertion_force(self, insertion_vids, dts) -> np.ndarray:
+        """get_insertion_force (musclesim.py:617-633): net force on the bone,
+        -sum m (x_corrected - x_predicted) / dts^2 over the insertion vertices
+        (save_predicted_positions must have run after integrate())."""
+        ids = np.asarray(insertion_vids)
+        corrected = self.positions_np()[ids].astype(np.float64)
+        masses = self._mass_user[ids].astype(np.float64)
+        forces = masses[:, None] * (corrected - self._predicted_pos.astype(np.float64)) / (float(dts) * float(dts))
+        return (-forces.sum(axis=0)).astype(np.float32)
+
+    def set_lbs_T_rel(self, T_rel_flat_np) -> None:
+        """set_lbs_T_rel (musclesim.py:635-644): per-bone relative transforms,
+        (n_bones * 12,) row-major in the reference's row-vector layout
+        [r00..r22, t0..t2] (q = p R + t), kept on the device as 3x4 [R^T | t]."""
+        T = np.asarray(T_rel_flat_np, np.float32).reshape(-1, 12)
+        M = np.concatenate([T[:, [0, 3, 6, 9]], T[:, [1, 4, 7, 10]], T[:, [2, 5, 8, 11]]], axis=1)
+        self._lbs_T = torch.from_numpy(np.ascontiguousarray(M)).to(self.device)
+
+    def apply_lbs(self, vertex_bone_field, blend: float = 1.0) -> None:
+        """apply_lbs (musclesim.py:646-656; lbs_apply_kernel, engine.py:641-661):
+        pos moves by ``blend`` toward its rest position carried by its bone's
+        T_rel (vertices with bone < 0 stay).  Two device launches: the targets
+        (xpbd_bone_targets) and the blend (xpbd_blend_to_target)."""
+        T = getattr(self, "_lbs_T", None)
+        if T is None:
+            return
+        vb = vertex_bone_field
+        if isinstance(vb, torch.Tensor):
+            vb = vb.detach().cpu().numpy()
+        vb = np.asarray(vb, np.int32).reshape(self.n_verts)[self.layout.perm]
+        vb2 = torch.from_numpy(np.ascontiguousarray(np.stack([vb, vb], 1))).to(self.device)
+        if getattr(self, "_rest4_lbs", None) is None:
+            r4 = np.zeros((self.n_verts, 4), np.float32)
+            r4[:, :3] = self.pos0_np
+            self._rest4_lbs = torch.from_numpy(r4[self.layout.perm]).to(self.device)
+        with torch.cuda.stream(self._stream):
+            tgt = self._pos4.clone()  # vertices without a bone blend toward themselves
+        capi.check(self._lib.xpbd_bone_targets(self.n_verts, int(T.shape[0]), C.c_void_p(T.data_ptr()),
+                                               C.c_void_p(vb2.data_ptr()), None, C.c_void_p(self._rest4_lbs.data_ptr()),
+                                               C.c_void_p(tgt.data_ptr()), None, self._sp))
+        capi.check(self._lib.xpbd_blend_to_target(self.n_verts, None, self.n_verts, C.c_void_p(self._pos4.data_ptr()),
+                                                  C.c_void_p(tgt.data_ptr()), C.c_float(blend), self._sp))
+        self.synchronize()
 
     # ------------------------------------------------------- bone attach
     def load_bone_geo(self, target_path):

@@ -160,3 +160,47 @@ def test_bone_attach_blocks_vs_oracle():
         print(f"bone attach frame {frame}: |gpu-o32| {err:.3e} (tol {tol:.3e})")
         assert err <= tol
     assert np.abs(orc.pos - m.verts).max() > 10 * tol
+
+
+def test_state_helpers_and_lbs_drive():
+    """reset, save_predicted_positions / get_insertion_force, set_lbs_T_rel /
+    apply_lbs (musclesim.py:555-656) against their numpy definitions."""
+    m = box_muscle()
+    sim = MuscleSim.from_procedural(m.verts, m.tets, m.fiber_per_tet, constraint_configs=CONS, device="cuda:0",
+                                    stopped=m.stopped, **KW)
+    sim.step()
+    sim.reset()
+    assert np.array_equal(sim.positions_np(), m.verts) and not sim.vel.numpy().any() and sim.step_cnt == 1
+    ids = np.arange(0, m.verts.shape[0], 7)
+    sim.integrate()
+    sim.save_predicted_positions(ids)
+    pred = sim.positions_np()[ids].astype(np.float64)
+    sim.solve_constraints(run_extras=False)
+    sim.apply_dP()
+    dts = 1.0 / 240.0
+    f = sim.get_insertion_force(ids, dts)
+    want = -(sim.mass[ids][:, None] * (sim.positions_np()[ids] - pred) / dts ** 2).sum(0)
+    np.testing.assert_allclose(f, want, rtol=1e-5, atol=1e-6)
+    # LBS drive: two bones, row-vector transforms q = p R + t
+    rng = np.random.default_rng(3)
+    Ts = []
+    for b in range(2):
+        a = rng.normal(size=3)
+        a /= np.linalg.norm(a)
+        ang = 0.3 * (b + 1)
+        K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+        R = np.eye(3) + np.sin(ang) * K + (1 - np.cos(ang)) * K @ K
+        Ts.append(np.concatenate([R.reshape(-1), rng.normal(scale=0.01, size=3)]))
+    T = np.asarray(Ts, np.float32).reshape(-1)
+    vb = rng.integers(-1, 2, size=m.verts.shape[0]).astype(np.int32)
+    cur = sim.positions_np().astype(np.float64)
+    sim.set_lbs_T_rel(T)
+    sim.apply_lbs(vb, blend=0.7)
+    got = sim.positions_np()
+    want = cur.copy()
+    T2 = T.reshape(2, 12).astype(np.float64)
+    for b in range(2):
+        sel = vb == b
+        q = m.verts[sel].astype(np.float64) @ T2[b, :9].reshape(3, 3) + T2[b, 9:]
+        want[sel] = (1 - 0.7) * cur[sel] + 0.7 * q
+    np.testing.assert_allclose(got, want, atol=2e-6)
