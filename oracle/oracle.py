@@ -473,10 +473,9 @@ class OracleMultiGridSim(OracleSolver):
 
     # ---- multigrid (mg/mg.py:744-1079, mg/kernel.py:8-178) --------------------
     def _init_mg(self, mu):
-        from rlmusclev2_b200.meshgen import build_cage  # synthetic input geometry only
+        from rlmusclev2_b200.meshgen import cage_for_config  # input geometry only
         cfg, P = self.cfg, self.P
-        cage = build_cage(self.scene, spacing=float(cfg.get("mg_cage_spacing", 0.016)),
-                          operator=str(cfg.get("mg_restrict_operator", "tikhonov")))
+        cage = cage_for_config(self.scene, cfg, operator=str(cfg.get("mg_restrict_operator", "tikhonov")))
         # "residual": prior + Minv P^T (x - P prior); "direct": Minv P^T x, the
         # reference's scatter + block solve (mg/kernel.py:137-178) as written
         self.mg_form = str(cfg.get("mg_restrict_form", "residual"))

@@ -808,3 +808,77 @@ def reseed_motion(sc: Scene, seed: int, n_frames: int = 64) -> Scene:
     knots = rng.uniform(0.0, 1.0, n_frames // 8 + 2).astype(np.float32)
     knots[0] = 0.0
     return dataclasses.replace(sc, traj=traj, act_sched=knots, meta=dict(sc.meta, motion_seed=int(seed)))
+
+
+# arrays of a baked cage file, as the reference's cage baker writes them
+# (tools/gen_coarse_cage.py:261) and its multigrid loads them (mg/mg.py:773-795)
+CAGE_NPZ_KEYS = ("coarse_pos", "coarse_tet", "cage_idx", "uvw", "minv_flat", "blk_base", "blk_dim",
+                 "blk_matoff", "mg_fine_nv")
+
+
+def save_cage_npz(cage: Cage, path) -> None:
+    """Write ``cage`` with the reference's cage-file keys plus ``lam`` (the
+    Tikhonov weight its restriction blocks were inverted with; absent in the
+    reference's files, whose blocks are pinv(P^T P), i.e. lam = 0)."""
+    with open(path, "wb") as f:  # a file object keeps the name as given (no ".npz" appended)
+        np.savez(f, coarse_pos=cage.coarse_pos.astype(np.float32), coarse_tet=cage.coarse_tet.astype(np.int32),
+                 cage_idx=cage.cage_idx.astype(np.int32), uvw=cage.uvw.astype(np.float32),
+                 minv_flat=cage.minv_flat.astype(np.float32), blk_base=cage.blk_base.astype(np.int32),
+                 blk_dim=cage.blk_dim.astype(np.int32), blk_matoff=cage.blk_matoff.astype(np.int32),
+                 mg_fine_nv=np.int64(cage.mg_fine_nv), lam=np.float64(cage.lam))
+
+
+def load_cage_npz(path, n_verts: int) -> Cage:
+    """Read a baked cage file (the reference's or ``save_cage_npz``'s).  Like
+    the reference (mg/mg.py:774-779) it refuses a cage baked for another fine
+    vertex count, and it checks that the block tables index inside the coarse
+    vertex and Minv arrays, since the device restriction trusts them."""
+    d = np.load(path)
+    missing = [k for k in CAGE_NPZ_KEYS if k not in d.files]
+    if missing:
+        raise ValueError(f"cage file {path} lacks {missing}")
+    nv = int(d["mg_fine_nv"])
+    if nv != int(n_verts):
+        raise ValueError(f"cage file {path} was built for fine NV={nv} but this scene has NV={int(n_verts)}")
+    cage = Cage(coarse_pos=np.asarray(d["coarse_pos"], np.float32).reshape(-1, 3),
+                coarse_tet=np.asarray(d["coarse_tet"], np.int32).reshape(-1, 4),
+                cage_idx=np.asarray(d["cage_idx"], np.int32).reshape(-1),
+                uvw=np.asarray(d["uvw"], np.float32).reshape(-1, 3),
+                minv_flat=np.asarray(d["minv_flat"], np.float32).reshape(-1),
+                blk_base=np.asarray(d["blk_base"], np.int32).reshape(-1),
+                blk_dim=np.asarray(d["blk_dim"], np.int32).reshape(-1),
+                blk_matoff=np.asarray(d["blk_matoff"], np.int32).reshape(-1),
+                mg_fine_nv=nv, lam=float(d["lam"]) if "lam" in d.files else 0.0)
+    nc, nt = cage.coarse_pos.shape[0], cage.coarse_tet.shape[0]
+    if cage.cage_idx.shape[0] != nv or cage.uvw.shape[0] != nv:
+        raise ValueError(f"cage file {path}: cage_idx/uvw must have one row per fine vertex ({nv})")
+    if cage.coarse_tet.size and (cage.coarse_tet.min() < 0 or cage.coarse_tet.max() >= nc):
+        raise ValueError(f"cage file {path}: coarse_tet indexes outside the {nc} coarse vertices")
+    if cage.cage_idx.size and (cage.cage_idx.min() < -1 or cage.cage_idx.max() >= nt):
+        raise ValueError(f"cage file {path}: cage_idx indexes outside the {nt} coarse tets")
+    if not (cage.blk_base.shape[0] == cage.blk_dim.shape[0] == cage.blk_matoff.shape[0] == nc):
+        raise ValueError(f"cage file {path}: blk_base/blk_dim/blk_matoff need one entry per coarse vertex")
+    ends = cage.blk_matoff.astype(np.int64) + cage.blk_dim.astype(np.int64) ** 2
+    if nc and (cage.blk_base.min() < 0 or (cage.blk_base.astype(np.int64) + cage.blk_dim).max() > nc
+               or cage.blk_dim.min() < 1 or cage.blk_matoff.min() < 0 or ends.max() > cage.minv_flat.shape[0]):
+        raise ValueError(f"cage file {path}: block table points outside the coarse vertices or minv_flat")
+    return cage
+
+
+def cage_for_config(scene: "Scene", cfg, operator: str = "tikhonov") -> Cage:
+    """The multigrid cage a config asks for: ``coarse_npz_path`` names a baked
+    cage file, which is loaded; a missing file is baked here (this package's
+    lattice cage, ``mg_cage_spacing``) and written there, as the reference
+    bakes a missing one on first use (mg/mg.py:759-772); without a path the
+    lattice cage is built in memory."""
+    import os
+    spacing = float(cfg.get("mg_cage_spacing", 0.016))
+    path = cfg.get("coarse_npz_path")
+    if not path:
+        return build_cage(scene, spacing=spacing, operator=operator)
+    path = str(path)
+    if not os.path.exists(path):
+        cage = build_cage(scene, spacing=spacing, operator=operator)
+        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+        save_cage_npz(cage, path)
+    return load_cage_npz(path, scene.verts.shape[0])

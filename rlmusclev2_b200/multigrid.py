@@ -20,7 +20,7 @@ import torch
 from . import _capi as capi
 from .builder import collect_raw_constraints
 from .engine import XpbdSolver
-from .meshgen import Cage, build_cage
+from .meshgen import Cage, cage_for_config
 
 
 def _restrict_host(cage: Cage, x: np.ndarray, prior: np.ndarray) -> np.ndarray:
@@ -61,7 +61,10 @@ class DeviceMultigrid:
     def __init__(self, sim, spacing: float = 0.016):
         self.sim = sim
         cfg = sim.cfg
-        cage = build_cage(sim.scene, spacing=spacing)
+        # a baked cage file (coarse_npz_path) or the lattice cage; "pinv" blocks
+        # are the reference's restriction as written, "tikhonov" the default
+        cage = cage_for_config(sim.scene, {**cfg, "mg_cage_spacing": spacing},
+                               operator=str(cfg.get("mg_restrict_operator", "tikhonov")))
         self.cage = cage
         ncoarse = cage.coarse_pos.shape[0]
         # FAS rest of the coarse ARAP = restriction of the fine rest (mg.py:813-829)

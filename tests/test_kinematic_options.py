@@ -75,3 +75,63 @@ def test_projection_mode_restarts_from_the_prolonged_target():
     assert np.abs(o.pos[e] - want).max() < 1e-12
     # the restricted target reproduces the bone target on the embedded vertices
     assert np.abs(o.pos[e] - o.target[e]).max() < 5e-3
+
+
+def test_baked_cage_file_round_trips_and_drives_the_same_frames(tmp_path):
+    """coarse_npz_path: a missing file is baked and written, a present one is
+    loaded with every array unchanged, and the oracle steps the same frames
+    from the file as from the in-memory cage."""
+    from rlmusclev2_b200.meshgen import CAGE_NPZ_KEYS, build_cage, cage_for_config, load_cage_npz
+    sc = _scene()
+    path = tmp_path / "cage" / "coarse_cage"   # no ".npz": the name is kept as given
+    cfg = _cfg()
+    cage_mem = build_cage(sc, spacing=float(cfg.get("mg_cage_spacing", 0.016)))
+    cfg["coarse_npz_path"] = str(path)
+    cage_file = cage_for_config(sc, cfg)
+    assert path.exists()
+    with np.load(path) as d:
+        assert set(CAGE_NPZ_KEYS) <= set(d.files)
+    for k in CAGE_NPZ_KEYS[:-1]:
+        assert np.array_equal(getattr(cage_file, k), getattr(cage_mem, k)), k
+    assert cage_file.mg_fine_nv == sc.verts.shape[0] and cage_file.lam == cage_mem.lam
+    runs = []
+    for c in (_cfg(), cfg):
+        o = O.OracleMultiGridSim(c, sc, prec="f32")
+        for f in (1, 2):
+            o.step_frame(f)
+        runs.append(o.pos.copy())
+    assert np.array_equal(runs[0], runs[1])
+    # a file without "lam" is a reference-baked pinv cage: lam = 0
+    ref = tmp_path / "ref.npz"
+    np.savez(ref, **{k: (np.int64(cage_mem.mg_fine_nv) if k == "mg_fine_nv" else getattr(cage_mem, k))
+                     for k in CAGE_NPZ_KEYS})
+    assert load_cage_npz(ref, sc.verts.shape[0]).lam == 0.0
+
+
+def test_cage_file_is_checked_before_use(tmp_path):
+    import pytest
+    from rlmusclev2_b200.meshgen import build_cage, load_cage_npz, save_cage_npz
+    sc = _scene()
+    cage = build_cage(sc)
+    nv = sc.verts.shape[0]
+    good = tmp_path / "good.npz"
+    save_cage_npz(cage, good)
+    with pytest.raises(ValueError, match="fine NV"):
+        load_cage_npz(good, nv + 1)
+    bad = dict(np.load(good))
+    bad["blk_matoff"] = bad["blk_matoff"].copy()
+    bad["blk_matoff"][-1] = bad["minv_flat"].shape[0]
+    np.savez(tmp_path / "bad_blk.npz", **bad)
+    with pytest.raises(ValueError, match="block table"):
+        load_cage_npz(tmp_path / "bad_blk.npz", nv)
+    bad = dict(np.load(good))
+    bad["coarse_tet"] = bad["coarse_tet"].copy()
+    bad["coarse_tet"][0, 0] = bad["coarse_pos"].shape[0]
+    np.savez(tmp_path / "bad_tet.npz", **bad)
+    with pytest.raises(ValueError, match="coarse_tet"):
+        load_cage_npz(tmp_path / "bad_tet.npz", nv)
+    bad = dict(np.load(good))
+    del bad["uvw"]
+    np.savez(tmp_path / "no_uvw.npz", **bad)
+    with pytest.raises(ValueError, match="lacks"):
+        load_cage_npz(tmp_path / "no_uvw.npz", nv)
