@@ -436,12 +436,26 @@ typedef struct XpbdCage {
 int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, float* coarse_prev4,
                      const float* coarse_pin4, xpbd_stream_t stream);
 
+/* Step 1 of the V-cycle without the Galerkin restriction (mg/mg.py:1006-1012,
+ * mg_restrict_mode "galerkin" = the restricted bone target copied in, "none" =
+ * the coarse keeps its own state; also after the coarse-in-fine readout of
+ * mg_sync_restrict "c2f", mg/mg.py:992-996): over the cage's n_coarse vertices
+ * (coarse library order) coarse4.xyz = src4.xyz when src4 is not NULL, then
+ * coarse_prev4 (optional) receives coarse4 and the coarse kinematic pin
+ * overwrites coarse4.xyz where coarse_pin4[c].w != 0, as xpbd_mg_restrict
+ * does after its block solve.  src4 must not alias coarse4. */
+int xpbd_mg_coarse_reset(const XpbdCage* cage, const float* src4, float* coarse4, float* coarse_prev4,
+                         const float* coarse_pin4, xpbd_stream_t stream);
+
 /* fine4.xyz += sum_k w_k (coarse4 - coarse_prev4)[p_idx_k] (prolong_delta_kernel,
  * mg/kernel.py:8-39), then the fine pin overwrite where vflags has
  * XPBD_VF_PIN and pin_target.w != 0 (vflags/pin_target may be NULL).  With
  * coarse_prev4 NULL the prolongation is absolute, fine4.xyz = sum_k w_k
  * coarse4[p_idx_k] (prolong_kernel, mg/kernel.py:181-203; mg_mode
- * "projection"), on the embedded vertices only. */
+ * "projection"), on the embedded vertices only.  Given a cage whose p_idx/p_w
+ * embed the coarse vertices in fine tets (n_fine = the coarse vertex count,
+ * p_idx = fine ids), the absolute form reads the coarse positions off the fine
+ * mesh (restrict_c2f_kernel, mg/kernel.py:43-60; mg_sync_restrict "c2f"). */
 int xpbd_mg_prolong_delta(const XpbdCage* cage, const float* coarse4, const float* coarse_prev4, float* fine4,
                           const int32_t* vflags, const float* pin_target, xpbd_stream_t stream);
 

@@ -519,6 +519,14 @@ class OracleMultiGridSim(OracleSolver):
         self.mg = OracleSolver(q0, cage.coarse_tet, t, m.astype(np.float32), pin, B, dt=self.dt, gravity_vec=(0, 0, 0),
                                prec=P.name)
         self.mg_iters = int(cfg.get("mg_coarse_iters", 15))
+        # step 1 of the V-cycle (mg.py:224-246, 1006-1012) and the coarse-in-fine
+        # embedding of the "c2f" state restriction (mg.py:897-938)
+        self.mg_restrict_mode = str(cfg.get("mg_restrict_mode", "direct")).lower()
+        self.mg_sync = str(cfg.get("mg_sync_restrict", "galerkin")).lower()
+        if self.mg_sync == "c2f":
+            from rlmusclev2_b200.meshgen import coarse_in_fine_embedding  # input geometry only
+            ct, cw = coarse_in_fine_embedding(self.scene.verts.astype(np.float32), self.scene.tets, cage.coarse_pos)
+            self.mg_c2f = (ct.astype(np.int64), cw.astype(P.dt))
 
     def restrict(self, x, prior):
         """Regularised Galerkin restriction prior + Minv P^T (x - P prior)
@@ -561,7 +569,15 @@ class OracleMultiGridSim(OracleSolver):
                            + w[:, 3:4] * c[t[:, 3]]).astype(self.P.dt)
             return
         co = self.mg
-        co.pos[:] = self.restrict(self.pos, co.pos)
+        if self.mg_restrict_mode == "direct" and self.mg_sync == "c2f":
+            t, w = self.mg_c2f  # restrict_c2f_kernel (mg/kernel.py:43-60)
+            x = self.pos
+            co.pos[:] = (((w[:, 0:1] * x[t[:, 0]] + w[:, 1:2] * x[t[:, 1]]) + w[:, 2:3] * x[t[:, 2]])
+                         + w[:, 3:4] * x[t[:, 3]]).astype(self.P.dt)
+        elif self.mg_restrict_mode == "direct":
+            co.pos[:] = self.restrict(self.pos, co.pos)
+        elif self.mg_restrict_mode == "galerkin":  # the restricted bone target (mg.py:1265-1295)
+            co.pos[:] = self.mg_target
         prev = co.pos.copy()
         tgt = self.mg_target
         co.pos[self.mg_pin] = tgt[self.mg_pin]

@@ -160,6 +160,7 @@ _SIGS = {
                                   P], C.c_int),
     "xpbd_gather": ([C.c_int32, C.c_int32, P, P, C.c_int32, P, C.c_int32, P], C.c_int),
     "xpbd_mg_restrict": ([C.POINTER(XpbdCage), P, P, P, P, P], C.c_int),
+    "xpbd_mg_coarse_reset": ([C.POINTER(XpbdCage), P, P, P, P, P], C.c_int),
     "xpbd_mg_prolong_delta": ([C.POINTER(XpbdCage), P, P, P, P, P, P], C.c_int),
     "xpbd_dcd_workspace_query": ([C.c_int32, C.POINTER(XpbdDcdWorkspaceSizes)], C.c_int),
     "xpbd_dcd_broadphase": ([C.POINTER(XpbdDcd), P, C.c_int32, P], C.c_int),

@@ -148,6 +148,35 @@ __global__ void __launch_bounds__(kMgThreads)
     if (wr) fine[i] = p;
 }
 
+// Step 1 of the V-cycle without the Galerkin restriction (mg_restrict_mode
+// "galerkin" / "none", or after the coarse-in-fine readout): the xyz lanes of
+// src (when given) replace the coarse position, prev receives the result and
+// the coarse kinematic pin overwrites the pinned nodes, as k_mg_restrict does
+// after its block solve.  One thread per coarse vertex (library order).
+__global__ void __launch_bounds__(kMgThreads)
+    k_mg_coarse_reset(int n, const float4* __restrict__ src, float4* coarse, float4* prev,
+                      const float4* __restrict__ pin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = coarse[i];
+    if (src) {
+        const float4 s = src[i];
+        p.x = s.x;
+        p.y = s.y;
+        p.z = s.z;
+    }
+    if (prev) prev[i] = make_float4(p.x, p.y, p.z, 0.f);
+    if (pin) {
+        const float4 t = pin[i];
+        if (t.w != 0.f) {
+            p.x = t.x;
+            p.y = t.y;
+            p.z = t.z;
+        }
+    }
+    coarse[i] = p;
+}
+
 int check_cage(const XpbdCage* g) {
     if (!g || g->n_fine <= 0 || g->n_coarse <= 0 || g->n_blocks <= 0 || !g->r_ptr || !g->r_fine || !g->r_w ||
         !g->blk_ptr || !g->blk_moff || !g->minv || !g->coarse_lib || !g->p_idx || !g->p_w || !g->resid)
@@ -181,6 +210,20 @@ int xpbd_mg_restrict(const XpbdCage* cage, const float* fine4, float* coarse4, f
         *cage, reinterpret_cast<float4*>(coarse4), reinterpret_cast<float4*>(coarse_prev4),
         reinterpret_cast<const float4*>(coarse_pin4));
     return cuda_check("xpbd_mg_restrict");
+}
+
+int xpbd_mg_coarse_reset(const XpbdCage* cage, const float* src4, float* coarse4, float* coarse_prev4,
+                         const float* coarse_pin4, xpbd_stream_t stream) {
+    int rc;
+    if ((rc = check_cage(cage))) return rc;
+    if (!coarse4) return fail(XPBD_ERR_ARG, "xpbd_mg_coarse_reset: null coarse buffer");
+    if (src4 == coarse4) return fail(XPBD_ERR_ARG, "xpbd_mg_coarse_reset: src4 must not alias coarse4");
+    if (!aligned16(src4) || !aligned16(coarse4) || !aligned16(coarse_prev4) || !aligned16(coarse_pin4))
+        return fail(XPBD_ERR_ALIGN, "xpbd_mg_coarse_reset: [n][4] buffers must be 16-byte aligned");
+    k_mg_coarse_reset<<<(cage->n_coarse + kMgThreads - 1) / kMgThreads, kMgThreads, 0, (cudaStream_t)stream>>>(
+        cage->n_coarse, reinterpret_cast<const float4*>(src4), reinterpret_cast<float4*>(coarse4),
+        reinterpret_cast<float4*>(coarse_prev4), reinterpret_cast<const float4*>(coarse_pin4));
+    return cuda_check("xpbd_mg_coarse_reset");
 }
 
 int xpbd_mg_prolong_delta(const XpbdCage* cage, const float* coarse4, const float* coarse_prev4, float* fine4,

@@ -882,3 +882,33 @@ def cage_for_config(scene: "Scene", cfg, operator: str = "tikhonov") -> Cage:
         os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
         save_cage_npz(cage, path)
     return load_cage_npz(path, scene.verts.shape[0])
+
+
+def coarse_in_fine_embedding(fine_pos, fine_tet, coarse_pos, k: int = 16):
+    """Coarse-in-fine embedding of the "c2f" state restriction
+    (_build_c2f_embedding, mg/mg.py:903-938): for every coarse vertex, among
+    the k fine rest tets with the nearest centroids, the one whose barycentric
+    weights have the largest minimum (the enclosing tet when there is one,
+    else the least extrapolating); weights ordered like the tet's corners,
+    the last one 1 - the others.  Returns (tet [nc, 4] int32 fine ids,
+    w [nc, 4] float32)."""
+    from scipy.spatial import cKDTree
+    fp = np.asarray(fine_pos, np.float64)
+    ft = np.asarray(fine_tet, np.int64)
+    cp = np.asarray(coarse_pos, np.float64)
+    k = int(min(k, ft.shape[0]))
+    _, cand = cKDTree(fp[ft].mean(1)).query(cp, k=k)
+    cand = cand.reshape(cp.shape[0], k)
+    best_w = np.zeros((cp.shape[0], 4))
+    best_t = ft[cand[:, 0]].copy()
+    best = np.full(cp.shape[0], -np.inf)
+    for j in range(k):
+        t = ft[cand[:, j]]
+        d = fp[t[:, 3]]
+        T = np.stack([fp[t[:, 0]] - d, fp[t[:, 1]] - d, fp[t[:, 2]] - d], axis=-1)
+        w3 = np.linalg.solve(T, (cp - d)[..., None])[..., 0]
+        w = np.concatenate([w3, (1.0 - w3.sum(1))[:, None]], axis=1)
+        score = w.min(1)
+        up = score > best
+        best[up], best_w[up], best_t[up] = score[up], w[up], t[up]
+    return best_t.astype(np.int32), best_w.astype(np.float32)

@@ -10,7 +10,9 @@ surfaces at the start frame and rides (optionally slides along) them
 (mg.py:1117-1174; the synthetic bones are capsule surfaces posed rigidly);
 target_mode="lbs" gives every vertex a smooth target blended between the two
 bones at its muscle's ends, computed on the device from the bone poses (the
-synthetic counterpart of the reference's precomputed LBS target sequence).
+synthetic counterpart of the reference's precomputed LBS target sequence), or,
+with ``lbs_target_npz``, read from such a sequence file (points (F, NV, 3),
+frames); target_mode="points" reads the cons_<frame>.geo pin-to-target frames.
 """
 from __future__ import annotations
 
@@ -145,6 +147,18 @@ class MultiGridSim(MuscleSim):
         self.tet_np = sc.tets.astype(np.int32)
         self.NV = self.n_verts = int(self.pos0_np.shape[0])
         self.NT = int(self.tet_np.shape[0])
+        # target_mode="lbs" with lbs_target_npz: a precomputed target sequence
+        # (F, NV, 3) for every vertex, read on the host (_build_lbs_target,
+        # mg.py:1176-1198); without it the lbs targets are computed on the device
+        self.lbs_target_npz = cfg.get("lbs_target_npz") if self.target_mode == "lbs" else None
+        if self.lbs_target_npz:
+            z = np.load(self.lbs_target_npz)
+            self._lbs_pts = np.asarray(z["points"], np.float32)
+            if self._lbs_pts.ndim != 3 or self._lbs_pts.shape[1:] != (self.NV, 3):
+                raise ValueError(f"lbs_target_npz points {self._lbs_pts.shape} != (F, NV={self.NV}, 3)")
+            self._lbs_f0 = int(np.asarray(z["frames"], np.int32)[0])
+        # targets that come from the host every frame (cons frames or the lbs file)
+        self._host_tgt = self.target_mode == "points" or bool(self.lbs_target_npz)
         self.use_jacobi = True
         self.use_colored_gs = False
         self.has_compressstiffness = False
@@ -213,6 +227,8 @@ class MultiGridSim(MuscleSim):
             in_cons = np.zeros(self.NV, bool)
             in_cons[self._cons_pts] = True
             active = (active.astype(bool) & in_cons).astype(np.int32)
+        elif self.lbs_target_npz:
+            self._cons_pts = np.arange(self.NV, dtype=np.int64)  # every vertex, rest_offset 0
         self.pin_active_np = active
         _belly = find_constraint(cfg, "belly_attach")
         self._belly_enabled = _belly is not None
@@ -285,7 +301,23 @@ class MultiGridSim(MuscleSim):
         tgt[self._cons_pts] = self._cons_cache[frame]
         return tgt
 
+    def _lbs_targets(self, frame: float) -> np.ndarray:
+        """_update_lbs_target (mg.py:1200-1214): the sequence's frame, clamped
+        to its range, linearly blended between the two frames around a
+        fractional frame (the weight is a float64 scalar, so the blend runs in
+        FP64 and is rounded to FP32 once)."""
+        f = float(frame)
+        n = self._lbs_pts.shape[0]
+        lo = min(max(int(np.floor(f)) - self._lbs_f0, 0), n - 1)
+        hi = min(max(int(np.ceil(f)) - self._lbs_f0, 0), n - 1)
+        if lo == hi:
+            return self._lbs_pts[lo].copy()
+        w = f - np.floor(f)
+        return ((1.0 - w) * self._lbs_pts[lo] + w * self._lbs_pts[hi]).astype(np.float32)
+
     def _host_targets(self, frame: float) -> np.ndarray:
+        if self.lbs_target_npz:
+            return self._lbs_targets(frame)
         if self.target_mode == "points":
             return self._cons_targets(int(frame))
         if self.target_mode == "mesh":
@@ -319,9 +351,10 @@ class MultiGridSim(MuscleSim):
         self._h2d_event = torch.cuda.Event()
         self._h2d_event.record(self._stream)
         self._presub_idx = None  # constraint points of the soft pin: all vertices
-        if self.target_mode == "points":
+        if self._host_tgt:
             self._pts_tgt = torch.zeros((self.NV, 3), dtype=torch.float32, device=dev)
             self._pts_host = torch.zeros((self.NV, 3), dtype=torch.float32).pin_memory()
+        if self.target_mode == "points":
             self._presub_idx = torch.from_numpy(L.inv[self._cons_pts].astype(np.int32)).to(dev)
         if self.target_mode == "mesh":
             self._setup_surface_binding()
@@ -530,9 +563,10 @@ class MultiGridSim(MuscleSim):
     def load_frame_targets(self, frame: float) -> None:
         """Bone poses of ``frame`` -> device (one pinned H2D copy), then the
         per-vertex pin/attach targets on the device (mg.py:1386-1407); with
-        target_mode="points" the frame's cons targets instead."""
-        if self.target_mode == "points":
-            tgt = (self._cons_targets(int(frame)) + self.rest_offset_np)[self.layout.perm]
+        target_mode="points" the frame's cons targets, with lbs_target_npz the
+        file's targets, instead."""
+        if self._host_tgt:
+            tgt = (self._host_targets(frame) + self.rest_offset_np)[self.layout.perm]
             self._h2d_event.synchronize()
             self._pts_host.copy_(torch.from_numpy(np.ascontiguousarray(tgt, np.float32)))
             with torch.cuda.stream(self._stream):
@@ -557,7 +591,7 @@ class MultiGridSim(MuscleSim):
 
     def _targets_kernel(self) -> None:
         v = self._verts
-        if self.target_mode == "points":
+        if self._host_tgt:
             with torch.cuda.stream(self._stream):
                 for t in (self._pin_tgt, self._attach_tgt):
                     if t is not None:

@@ -20,7 +20,7 @@ import torch
 from . import _capi as capi
 from .builder import collect_raw_constraints
 from .engine import XpbdSolver
-from .meshgen import Cage, cage_for_config
+from .meshgen import Cage, cage_for_config, coarse_in_fine_embedding
 
 
 def _restrict_host(cage: Cage, x: np.ndarray, prior: np.ndarray) -> np.ndarray:
@@ -104,6 +104,16 @@ class DeviceMultigrid:
         # "hpbd": the cage is its own ARAP sim, delta-prolonged; "projection": the
         # fine state is reset to the prolonged restricted bone target each substep
         self.mode = str(getattr(sim, "mg_mode", "hpbd"))
+        # step 1 of the V-cycle (mg.py:224-246, 1006-1012): "direct" restricts the
+        # fine state (Galerkin least squares, or with mg_sync_restrict "c2f" the
+        # coarse-in-fine barycentric readout), "galerkin" copies in the restricted
+        # bone target, "none" leaves the coarse on its own state
+        self.restrict_mode = str(cfg.get("mg_restrict_mode", "direct")).lower()
+        if self.restrict_mode not in ("direct", "galerkin", "none"):
+            raise ValueError(f"mg_restrict_mode must be 'direct', 'galerkin' or 'none', got {self.restrict_mode!r}")
+        self.sync_restrict = str(cfg.get("mg_sync_restrict", "galerkin")).lower()
+        if self.sync_restrict not in ("galerkin", "c2f"):
+            raise ValueError(f"mg_sync_restrict must be 'galerkin' or 'c2f', got {self.sync_restrict!r}")
         self._build_device()
 
     def _build_device(self):
@@ -149,6 +159,20 @@ class DeviceMultigrid:
         pin4[:, 3] = self.coarse_pin
         self.pin4 = T(pin4[cl.perm])
         self.attach_idx = T(cl.inv[self.attach_nodes].astype(np.int32))
+        self.g_c2f = None
+        if self.sync_restrict == "c2f":
+            # the coarse vertices embedded in fine rest tets (mg.py:897-898, 903-938):
+            # the absolute prolongation with the roles swapped reads them off the fine mesh
+            ct, cw = coarse_in_fine_embedding(sim.pos0_np, sim.tet_np, cage.coarse_pos)
+            c_idx = np.empty((ncoarse, 4), np.int32)
+            c_w = np.empty((ncoarse, 4), np.float32)
+            c_idx[cl.inv] = fl.inv[ct]
+            c_w[cl.inv] = cw
+            self._t["c2f_idx"], self._t["c2f_w"] = T(c_idx), T(c_w)
+            g2 = capi.XpbdCage.from_buffer_copy(g)
+            g2.n_fine = ncoarse
+            g2.p_idx, g2.p_w = self._t["c2f_idx"].data_ptr(), self._t["c2f_w"].data_ptr()
+            self.g_c2f = g2
 
     def refresh_target(self):
         """Coarse Dirichlet targets = restriction of the fine bone targets (mg.py:1028-1045)."""
@@ -168,9 +192,20 @@ class DeviceMultigrid:
                                                     C.c_void_p(s._pos4.data_ptr()), C.c_void_p(vf) if vf else None,
                                                     C.c_void_p(pt) if pt else None, s._sp))
             return
-        capi.check(s._lib.xpbd_mg_restrict(C.byref(self.g), C.c_void_p(s._pos4.data_ptr()),
-                                           C.c_void_p(co._pos4.data_ptr()), C.c_void_p(self.prev.data_ptr()),
-                                           C.c_void_p(self.pin4.data_ptr()), s._sp))
+        if self.restrict_mode == "direct" and self.g_c2f is None:
+            capi.check(s._lib.xpbd_mg_restrict(C.byref(self.g), C.c_void_p(s._pos4.data_ptr()),
+                                               C.c_void_p(co._pos4.data_ptr()), C.c_void_p(self.prev.data_ptr()),
+                                               C.c_void_p(self.pin4.data_ptr()), s._sp))
+        else:
+            src = None
+            if self.restrict_mode == "direct":  # restrict_c2f_kernel (mg/kernel.py:43-60)
+                capi.check(s._lib.xpbd_mg_prolong_delta(C.byref(self.g_c2f), C.c_void_p(s._pos4.data_ptr()), None,
+                                                        C.c_void_p(co._pos4.data_ptr()), None, None, s._sp))
+            elif self.restrict_mode == "galerkin":  # the restricted bone target (mg.py:1265-1295)
+                src = C.c_void_p(self.pin4.data_ptr())
+            capi.check(s._lib.xpbd_mg_coarse_reset(C.byref(self.g), src, C.c_void_p(co._pos4.data_ptr()),
+                                                   C.c_void_p(self.prev.data_ptr()),
+                                                   C.c_void_p(self.pin4.data_ptr()), s._sp))
         if self.beta != 0.0:
             for _ in range(self.iters):  # ARAP sweep, then the soft attach (mg.py:1057-1062)
                 co._fused_iterations(1)

@@ -137,3 +137,19 @@ def test_svd_clamp_checks(lib):
     tiles, verts = capi.XpbdTiles(), capi.XpbdVerts()
     assert lib.xpbd_svd_clamp(None, None, C.c_float(0.1), C.c_float(1.0), 1, None) == ERR_ARG
     assert lib.xpbd_svd_clamp(C.byref(tiles), C.byref(verts), C.c_float(0.1), C.c_float(1.0), 1, None) == ERR_ARG
+
+
+def test_multigrid_transfer_checks(lib):
+    g = capi.XpbdCage()
+    assert lib.xpbd_mg_coarse_reset(None, None, 16, None, None, None) == ERR_ARG      # no cage
+    assert lib.xpbd_mg_coarse_reset(C.byref(g), None, 16, None, None, None) == ERR_ARG  # empty cage
+    g.n_fine, g.n_coarse, g.n_blocks, g.max_block = 8, 4, 1, 4
+    for k in ("r_ptr", "r_fine", "r_w", "blk_ptr", "blk_moff", "minv", "coarse_lib", "p_idx", "p_w", "resid", "rhs"):
+        setattr(g, k, 16)  # aligned dummies, never dereferenced
+    assert lib.xpbd_mg_coarse_reset(C.byref(g), None, None, None, None, None) == ERR_ARG
+    assert "null coarse" in _msg(lib)
+    assert lib.xpbd_mg_coarse_reset(C.byref(g), 32, 32, None, None, None) == ERR_ARG  # src aliases coarse
+    assert lib.xpbd_mg_coarse_reset(C.byref(g), 40, 32, None, None, None) == ERR_ALIGN
+    assert lib.xpbd_mg_coarse_reset(C.byref(g), None, 32, 8, None, None) == ERR_ALIGN
+    assert lib.xpbd_mg_restrict(C.byref(g), None, 32, None, None, None) == ERR_ARG
+    assert lib.xpbd_mg_prolong_delta(C.byref(g), 32, None, 24, None, None, None) == ERR_ALIGN

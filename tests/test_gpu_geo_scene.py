@@ -98,3 +98,41 @@ def test_musclesim_from_geo_config_matches_from_procedural(tmp_path):
     assert err_u <= 1e-7
     with pytest.raises(NotImplementedError, match="rest meshes are read from"):
         MuscleSim(dict(cfg, geo_path=str(tmp_path / "box.obj")))
+
+
+def test_lbs_target_file_matches_the_device_lbs_run(tmp_path):
+    """target_mode="lbs" with lbs_target_npz (mg.py:1176-1214): a sequence
+    file holding, bit for bit, the targets the device computes for frames 1-4
+    drives the same frames as the device computation; a fractional frame
+    blends the two frames around it."""
+    sc = humanv2_scene(seed=1, n_muscles=5, n_bones=4, target_tets=20000, fascia_tets=0, box=(0.35, 0.35, 0.35))
+    base = load_config("rlmusclev2_b200/configs/humanv2_synth.json")
+    base["demo"]["collision"]["enabled"] = False
+    ref = MultiGridSim(dict(base, target_mode="lbs"), scene=sc)
+    frames = np.arange(1, 5, dtype=np.int32)
+    pts = np.empty((4, ref.NV, 3), np.float32)
+    for i, f in enumerate(frames):
+        ref.load_frame_targets(int(f))
+        ref._targets_kernel()
+        ref.synchronize()
+        pts[i][ref.layout.perm] = ref._pin_tgt[:, :3].cpu().numpy()
+    np.savez(tmp_path / "lbs.npz", points=pts, frames=frames)
+    sim = MultiGridSim(dict(base, target_mode="lbs", lbs_target_npz=str(tmp_path / "lbs.npz")), scene=sc)
+    sim.load_frame_targets(2.25)
+    sim._targets_kernel()
+    sim.synchronize()
+    got = np.empty((sim.NV, 3), np.float32)
+    got[sim.layout.perm] = sim._pin_tgt[:, :3].cpu().numpy()
+    np.testing.assert_array_equal(got, (0.75 * pts[1].astype(np.float64) + 0.25 * pts[2]).astype(np.float32))
+    for f in frames:
+        a = sc.activation(int(f))
+        for s in (ref, sim):
+            s.set_fiber_activation(a)
+            s.step_frame(int(f))
+    err = float(np.abs(ref.positions_np() - sim.positions_np()).max())
+    print(f"lbs target file vs device lbs: max |diff| {err:.2e} m")
+    assert np.isfinite(sim.positions_np()).all()
+    assert err < 1e-6
+    with pytest.raises(ValueError, match="lbs_target_npz"):
+        np.savez(tmp_path / "bad.npz", points=pts[:, :-1], frames=frames)
+        MultiGridSim(dict(base, target_mode="lbs", lbs_target_npz=str(tmp_path / "bad.npz")), scene=sc)

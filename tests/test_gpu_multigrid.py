@@ -150,3 +150,42 @@ def test_projection_mode_frames_vs_oracle():
     finally:
         O.set_arap_skip(0.0)
     assert np.abs(o64.pos - sc.verts).max() > 100 * tol
+
+
+@pytest.mark.parametrize("restrict_mode,sync", [("galerkin", "galerkin"), ("none", "galerkin"), ("direct", "c2f")])
+def test_restrict_modes_frames_vs_oracle(restrict_mode, sync):
+    """Step 1 of the V-cycle by mg_restrict_mode / mg_sync_restrict
+    (mg.py:224-246, 992-1012): the restricted bone target copied in, the coarse
+    left on its own state, and the coarse-in-fine readout.  Three frames on the
+    small scene without the skip threshold, against the FP64 oracle at three
+    times the FP32 oracle's distance (max and p99)."""
+    cfg = load_config("rlmusclev2_b200/configs/humanv2_synth_mg_dcd.json")
+    cfg["demo"]["collision"]["sdf_res"] = 96
+    cfg["demo"]["self_collision"]["method"] = "none"
+    cfg["mg_restrict_mode"], cfg["mg_sync_restrict"] = restrict_mode, sync
+    sc = humanv2_scene(seed=1, n_muscles=5, n_bones=4, target_tets=20000, fascia_tets=3000, box=(0.35, 0.35, 0.35))
+    sim = MultiGridSim(cfg, scene=sc)
+    # no skip threshold on either level: with "none" the cage relaxes across
+    # frames, and the threshold then leaves out (and uncounts) nearly rigid tets
+    sim._prm.arap_skip_ssq = -1.0
+    sim.mg.coarse._prm.arap_skip_ssq = -1.0
+    o32 = O.OracleMultiGridSim(cfg, sc, prec="f32")
+    o64 = O.OracleMultiGridSim(cfg, sc, prec="f64")
+    tol = 1e-5 * bbox_diag(sc.verts)
+    O.set_arap_skip(-1.0)
+    try:
+        for frame in (1, 2, 3):
+            sim.set_fiber_activation(sc.activation(frame))
+            sim.step_frame(frame)
+            o32.step_frame(frame)
+            o64.step_frame(frame)
+            p = sim.positions_np()
+            d = np.abs(p - o64.pos).max(1)
+            spr = np.abs(o32.pos - o64.pos).max(1)
+            print(f"{restrict_mode}/{sync} frame {frame}: |gpu-o64| max {d.max():.3e} p99 "
+                  f"{np.percentile(d, 99):.3e}; |o32-o64| max {spr.max():.3e}")
+            assert np.isfinite(p).all()
+            assert d.max() <= max(tol, 3.0 * spr.max())
+            assert np.percentile(d, 99) <= max(tol, 3.0 * np.percentile(spr, 99))
+    finally:
+        O.set_arap_skip(0.0)

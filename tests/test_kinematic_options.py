@@ -135,3 +135,57 @@ def test_cage_file_is_checked_before_use(tmp_path):
     np.savez(tmp_path / "no_uvw.npz", **bad)
     with pytest.raises(ValueError, match="lacks"):
         load_cage_npz(tmp_path / "no_uvw.npz", nv)
+
+
+def test_lbs_target_file_frames_clamp_and_blend():
+    """_lbs_targets (mg.py:1200-1214): frames before and after the sequence
+    clamp to its ends, integer frames are the stored frame, fractional frames
+    blend the two around them in FP32."""
+    from types import SimpleNamespace
+    from rlmusclev2_b200.mg import MultiGridSim
+    rng = np.random.default_rng(3)
+    pts = rng.standard_normal((3, 50, 3)).astype(np.float32)
+    s = SimpleNamespace(_lbs_pts=pts, _lbs_f0=5)
+    f = MultiGridSim._lbs_targets
+    assert np.array_equal(f(s, 2), pts[0]) and np.array_equal(f(s, 9.5), pts[2])
+    assert np.array_equal(f(s, 6), pts[1])
+    got = f(s, 5.4)
+    w = 5.4 - np.floor(5.4)  # a float64 weight: the blend runs in FP64, rounded once
+    assert got.dtype == np.float32
+    assert np.array_equal(got, ((1.0 - w) * pts[0].astype(np.float64) + w * pts[1]).astype(np.float32))
+
+
+def test_coarse_in_fine_embedding_reads_interior_points_exactly():
+    """coarse_in_fine_embedding (mg.py:903-938): a point inside the fine mesh
+    (a fine tet's centroid) gets its enclosing tet with non-negative weights
+    that reproduce it; a point outside extrapolates (a negative weight)."""
+    from rlmusclev2_b200.meshgen import coarse_in_fine_embedding
+    sc = _scene()
+    x = sc.verts.astype(np.float64)
+    probe = x[sc.tets[::97]].mean(1)
+    far = x.max(0) + 0.05
+    t, w = coarse_in_fine_embedding(sc.verts, sc.tets, np.vstack([probe, far[None]]))
+    rec = np.einsum("nk,nkd->nd", w.astype(np.float64), x[t])
+    assert np.abs(rec - np.vstack([probe, far[None]])).max() < 1e-5
+    assert (w[:-1] >= -1e-5).all() and np.allclose(w.sum(1), 1.0, atol=1e-5)
+    assert w[-1].min() < 0
+
+
+def test_restrict_modes_change_the_frames():
+    """mg_restrict_mode "galerkin" / "none" and mg_sync_restrict "c2f"
+    (mg.py:224-246, 1006-1012) each give different frames from the default
+    state restriction on the oracle."""
+    sc = _scene()
+    runs = {}
+    for key in (("direct", "galerkin"), ("galerkin", "galerkin"), ("none", "galerkin"), ("direct", "c2f")):
+        cfg = _cfg()
+        cfg["mg_restrict_mode"], cfg["mg_sync_restrict"] = key
+        o = O.OracleMultiGridSim(cfg, sc, prec="f32")
+        for f in (1, 2):
+            o.step_frame(f)
+        runs[key] = o.pos.copy()
+    base = runs[("direct", "galerkin")]
+    for key, p in runs.items():
+        print(key, np.isfinite(p).all(), np.abs(p - base).max())
+        if key != ("direct", "galerkin"):
+            assert not np.array_equal(p, base), key
