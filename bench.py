@@ -598,16 +598,18 @@ def run_learned(args):
     ws = LW.LearnedWarmStart(sim)
     meta = LW.load_weights(ws)
     ns = [10, 20, 40, 80, 120, 160, 180, 200]
-    err, rms = LW.evaluate(ws, [41], 4, ns, ideal=True)
+    ws.plain_taken.zero_()
+    err, rms = LW.evaluate(ws, [41], 4, ns, ideal=True, checked_ns=(10, 20))
+    checked_taken = int(ws.plain_taken.item())
     n_to = {form: LW.iterations_to(err[form], 0.1) for form in ("plain", "learned", "ideal")}
     base = sim.scene
     s = sim._stream
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
 
-    def timed(n, learned):
+    def timed(n, learned, fallback=True):
         ws.reset(reseed_motion(base, 41))
         for f in range(1, 1 + args.warmup):
-            ws.frame(f, n, learned)
+            ws.frame(f, n, learned, fallback)
         times = []
         with ClockSampler(torch.cuda.current_device()) as clk:
             for f in range(1 + args.warmup, 1 + args.warmup + args.steps):
@@ -615,7 +617,7 @@ def run_learned(args):
                 a, b = ev(), ev()
                 a.record(s)
                 for sub in range(sim.nsubsteps):
-                    ws.substep(sub, n, learned)
+                    ws.substep(sub, n, learned, fallback)
                 b.record(s)
                 ws.end_frame()
                 b.synchronize()
@@ -626,10 +628,11 @@ def run_learned(args):
     t_p10, _ = timed(10, False)
     t_p20, _ = timed(n_p, False)
     t_learn, clocks = timed(n_l, True)
+    t_checked, _ = timed(n_l, True, "residual")
     if world > 1:
-        t = torch.tensor([t_learn, t_p20, t_p10], device=sim.device)
+        t = torch.tensor([t_learn, t_p20, t_p10, t_checked], device=sim.device)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_learn, t_p20, t_p10 = (float(x) for x in t.tolist())
+        t_learn, t_p20, t_p10, t_checked = (float(x) for x in t.tolist())
     t_iter = (t_p20 - t_p10) / (10 * sim.nsubsteps)  # ms per fine iteration
     fixed = (t_learn - t_p10) / sim.nsubsteps  # ms per substep: restriction, features, network, prolongation
     frame_ms = lambda n, extra: sim.nsubsteps * (extra + n * t_iter) + (t_p10 - 10 * t_iter * sim.nsubsteps)  # noqa: E731
@@ -647,6 +650,12 @@ def run_learned(args):
         "error_vs_200_iteration_solve": {form: {str(n): summ(err[form][n]) for n in ns}
                                          for form in ("plain", "learned", "ideal")},
         "iterations_to_0.1mm": {k: (None if v is None else round(v, 1)) for k, v in n_to.items()},
+        # the fallback rule as stated: every substep also runs the plain solve and
+        # keeps it when the learned post-iteration ARAP residual is higher
+        "residual_checked_fallback": {
+            "ms_per_frame": round(t_checked, 4), "iterations": n_l,
+            "error_vs_200_iteration_solve": {str(n): summ(err["checked"][n]) for n in (10, 20)},
+            "plain_taken": checked_taken, "checks": int(2 * err["checked"][10].shape[0])},
         "ms_per_frame_at_0.1mm": est,
         "gate_0.1mm_at_2x": bool(est["learned"] is not None and est["plain"] is not None
                                  and est["learned"] <= 0.5 * est["plain"]),

@@ -17,6 +17,13 @@ Per substep, after the inertial prediction x_pred of the fine mesh:
   6. N plain fine Jacobi iterations (the persistent pass);
   7. restrict the result to the cage: the next substep's c_prev.
 
+With ``fallback="residual"`` the fallback is the plain solver itself: the
+substep also runs N plain iterations from x_pred, and the learned result is
+replaced by the plain one whenever its post-iteration fine ARAP residual
+exceeds the plain solver's (a device-side choice).  That is the rule as
+stated for the learned form, at the price of the plain solve on every
+substep; the cage rule above is its cheap stand-in.
+
 The training data are the plain solver's own trajectories: for seeds of bone
 motion and fiber activation, each substep's features and its converged cage
 correction, generated and kept on the GPU; training runs the library's
@@ -151,8 +158,10 @@ class LearnedWarmStart:
         self.set_norm(None)
         self._cprev = torch.zeros_like(co._pos4)
         self._saved = torch.zeros_like(sim._pos4)
+        self._saved_plain = torch.zeros_like(sim._pos4)
         self._mbuf = torch.zeros((2, 8), dtype=torch.float64, device=dev)
         self.fallbacks = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.plain_taken = torch.zeros(1, dtype=torch.int32, device=dev)  # residual-rule fallbacks
         self.target = torch.zeros((self.nc, 3), dtype=torch.float32, device=dev)
         cfg = sim.cfg
         coll = (cfg.get("demo") or {}).get("collision") or {}
@@ -314,20 +323,48 @@ class LearnedWarmStart:
                                              C.c_float(SCALE_MM), C.c_void_p(self.target.data_ptr()), self.sp))
 
     # ------------------------------------------------------- one substep
-    def substep(self, sub: int, n_iters: int, learned: bool, fallback: bool = True) -> None:
+    def substep(self, sub: int, n_iters: int, learned: bool, fallback=True) -> None:
         """One substep of the learned form, or of the plain form (prediction and
-        iterations only: the plain solver needs no cage)."""
+        iterations only: the plain solver needs no cage).  ``fallback``: True
+        the cage rule, False none, "residual" the plain solver's residual."""
         if not learned:
             self.sim._vstep(capi.OP_PREDICT | self.pin | ((self.push | self.vel) if sub > 0 else 0))
             self.iterate(n_iters)
             return
         self.predict(sub)
-        self.features()
-        self.warm_start(fallback)
-        self.iterate(n_iters)
+        if fallback == "residual":
+            self.plain_checked(n_iters)
+        else:
+            self.features()
+            self.warm_start(bool(fallback))
+            self.iterate(n_iters)
         self.restrict_final()
 
-    def frame(self, frame: int, n_iters: int, learned: bool, fallback: bool = True) -> None:
+    def plain_checked(self, n_iters: int) -> None:
+        """From x_pred (after predict): the plain solve (n_iters iterations,
+        its fine metrics and result kept), then the learned solve from the same
+        x_pred; the plain result replaces the learned one when the learned
+        post-iteration ARAP residual exceeds the plain one or is not finite
+        (xpbd_fallback_select, counted in ``plain_taken``)."""
+        sim = self.sim
+        with torch.cuda.stream(sim._stream):
+            self._saved.copy_(sim._pos4)
+        self.iterate(n_iters)
+        self._metrics_into(1)
+        with torch.cuda.stream(sim._stream):
+            self._saved_plain.copy_(sim._pos4)
+            sim._pos4.copy_(self._saved)
+        self.features()
+        self.warm_start(fallback=False)
+        self.iterate(n_iters)
+        self._metrics_into(0)
+        capi.check(self.lib.xpbd_fallback_select(sim.n_verts, C.c_void_p(self._mbuf[0].data_ptr()),
+                                                 C.c_void_p(self._mbuf[1].data_ptr()), C.c_float(1.0),
+                                                 C.c_void_p(self._saved_plain.data_ptr()),
+                                                 C.c_void_p(sim._pos4.data_ptr()),
+                                                 C.c_void_p(self.plain_taken.data_ptr()), self.sp))
+
+    def frame(self, frame: int, n_iters: int, learned: bool, fallback=True) -> None:
         self.begin_frame(frame)
         for sub in range(self.sim.nsubsteps):
             self.substep(sub, n_iters, learned, fallback)
@@ -418,18 +455,24 @@ def train(net: CageMLP, X, Y, steps: int, lr: float = 1e-3, seed: int = 0, log=p
     return hist
 
 
-def evaluate(ws: LearnedWarmStart, seeds, frames: int, ns, conv_iters: int = 200, log=print, ideal: bool = False):
+def evaluate(ws: LearnedWarmStart, seeds, frames: int, ns, conv_iters: int = 200, log=print, ideal: bool = False,
+             checked_ns=()):
     """Max fine-vertex error (mm) against the converged solve from the same
     prediction, for the plain form and the learned form after n iterations
     (n in ns), on every substep of the held-out trajectories (which follow
     the converged solve).  With ``ideal``, also the form warm-started by the
-    substep's true cage correction (what a perfect network would give)."""
+    substep's true cage correction (what a perfect network would give); for
+    n in ``checked_ns`` the learned form checked against the plain solver's
+    residual (``fallback="residual"``, form "checked")."""
     sim = ws.sim
     base = sim.scene
     ns = sorted(ns)
     forms = ("plain", "learned", "learned_raw") + (("ideal",) if ideal else ())
     err = {f: {n: [] for n in ns} for f in forms}
     rms = {f: {n: [] for n in ns} for f in forms}
+    if checked_ns:
+        err["checked"] = {n: [] for n in checked_ns}
+        rms["checked"] = {n: [] for n in checked_ns}
     xpred = torch.zeros_like(sim._pos4)
     cpred = torch.zeros_like(ws.mg.coarse._pos4)
     cstar = torch.zeros_like(ws.mg.coarse._pos4)
@@ -468,6 +511,15 @@ def evaluate(ws: LearnedWarmStart, seeds, frames: int, ns, conv_iters: int = 200
                             d = (sim._pos4[:, :3] - ref).norm(dim=1)
                             err[form][n].append(d.max())
                             rms[form][n].append(d.pow(2).mean().sqrt())
+                for n in checked_ns:
+                    with torch.cuda.stream(sim._stream):
+                        sim._pos4.copy_(xpred)
+                        ws.mg.coarse._pos4.copy_(cpred)
+                    ws.plain_checked(n)
+                    with torch.cuda.stream(sim._stream):
+                        d = (sim._pos4[:, :3] - ref).norm(dim=1)
+                        err["checked"][n].append(d.max())
+                        rms["checked"][n].append(d.pow(2).mean().sqrt())
                 # the trajectory follows the converged solve
                 with torch.cuda.stream(sim._stream):
                     sim._pos4.copy_(refp)

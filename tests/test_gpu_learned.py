@@ -67,6 +67,7 @@ def test_fallback_drops_a_bad_correction_and_keeps_a_good_one():
     ws.frame(1, 5, learned=False)
     ws.begin_frame(2)
     ws.predict(0)
+    sim.synchronize()  # the clone runs on torch's current stream, not the engine's
     x_pred = sim._pos4.clone()
     # a network with a large random output layer: centimetre-scale non-rigid
     # cage corrections raise the cage's ARAP residual and are dropped (a rigid
@@ -105,3 +106,42 @@ def test_trained_network_gains_over_plain():
     print(f"weights {meta}; per-frame max error plain {np.round(p, 3)} learned {np.round(q, 3)} mm; "
           f"rms plain {rms['plain'][20].mean():.4f} learned {rms['learned'][20].mean():.4f} mm")
     assert q[1:].sum() < 0.85 * p[1:].sum()
+
+
+def test_residual_checked_fallback_takes_the_plain_solve():
+    """fallback="residual": a network with a large random output layer gives
+    a warm start whose post-iteration residual is above the plain solver's, so
+    the substep ends on the plain solve from x_pred, bit for bit, and the
+    choice is counted; with a zero network (no correction) the learned result
+    is kept, and it equals the plain one."""
+    sim, ws = _small()
+    ws.reset(reseed_motion(sim.scene, 9))
+    ws.frame(1, 5, learned=False)
+    ws.begin_frame(2)
+    ws.predict(0)
+    sim.synchronize()  # clones run on torch's current stream, not the engine's
+    x_pred = sim._pos4.clone()
+    ws.iterate(4)
+    sim.synchronize()
+    x_plain = sim._pos4.clone()
+    with torch.cuda.stream(sim._stream):
+        sim._pos4.copy_(x_pred)
+    with torch.cuda.stream(ws.net.stream):
+        ws.net.W[4].normal_(0.0, 50.0)
+    ws.net.refresh_copies()
+    ws.set_norm(None, 1.0)
+    ws.plain_taken.zero_()
+    ws.plain_checked(4)
+    sim.synchronize()
+    assert int(ws.plain_taken.item()) == 1
+    torch.testing.assert_close(sim._pos4, x_plain, rtol=0, atol=0)
+    with torch.cuda.stream(ws.net.stream):
+        ws.net.W[4].zero_()
+        ws.net.b[4].zero_()
+    ws.net.refresh_copies()
+    with torch.cuda.stream(sim._stream):
+        sim._pos4.copy_(x_pred)
+    ws.plain_checked(4)
+    sim.synchronize()
+    assert int(ws.plain_taken.item()) == 1
+    assert float((sim._pos4 - x_plain).abs().max()) < 1e-6
