@@ -610,6 +610,18 @@ class XpbdEngine:
     def dPw(self) -> torch.Tensor:
         return torch.from_numpy(self._to_user(self._accum, 4)[:, 3].copy())
 
+    def __getattr__(self, name: str):
+        """The constraint table's columns as the reference engine's ``c_*``
+        attributes (engine.py:1179-1211: c_type, c_pts, c_stiffness,
+        c_compressionstiffness, c_dampingratio, c_tetid, c_L, c_restlength,
+        c_restvector, c_restdir), type-sorted rows with user vertex ids, as
+        device tensors.  They are copies of the table the engine was built
+        from: writing to them changes nothing (rebuild_constraints does)."""
+        table = self.__dict__.get("table")
+        if name.startswith("c_") and table is not None and name in table.__dataclass_fields__:
+            return torch.from_numpy(np.ascontiguousarray(getattr(table, name))).to(self.device)
+        raise AttributeError(f"{type(self).__name__!r} object has no attribute {name!r}")
+
     @property
     def mass(self) -> np.ndarray:
         return self._mass_user.copy()

@@ -117,7 +117,15 @@ def test_rebuild_constraints_keeps_state_and_adds_attach():
     tgt = m.verts[free] + np.array([0.0, 0.01, 0.0], np.float32)
     rows = [dict(type=int(ConstraintType.ATTACH), pts=[int(v), -1, -1, -1], stiffness=1e6, dampingratio=0.0,
                  restlength=0.0, restvector=[*map(float, t), 1.0]) for v, t in zip(free, tgt)]
+    n0 = int(c.c_type.shape[0])
     c.rebuild_constraints(rows)
+    # the c_* columns (engine.py:1179-1211) follow the rebuilt table
+    assert c.c_type.is_cuda and int(c.c_type.shape[0]) == n0 + len(rows)
+    at = (c.c_type == int(ConstraintType.ATTACH)).nonzero().flatten()
+    want = {int(v): t for v, t in zip(free, tgt)}
+    got_pts = c.c_pts[at, 0].tolist()
+    assert sorted(got_pts) == sorted(want)
+    np.testing.assert_array_equal(c.c_restvector[at, :3].cpu().numpy(), np.stack([want[v] for v in got_pts]))
     for s in (a, b, c):
         s.step()
     np.testing.assert_array_equal(a.positions_np(), b.positions_np())
