@@ -92,7 +92,11 @@ typedef struct XpbdParams {
                                     tiles of <= 768 vertices (default: compile-time offsets);
                                     bit 5: the per-iteration tile pass asks the copy engine for an L2
                                     prefetch of its tile's tet streams (cp.async.bulk.prefetch.L2)
-                                    before staging the tile's vertices */
+                                    before staging the tile's vertices;
+                                    bit 6: tets whose ARAP rotation needs the SVD (det F <= 1e-6 |F|^3)
+                                    are projected in a deferred pass of the whole CTA after the tile's
+                                    loop instead of where the loop meets them (same results bit for
+                                    bit; pays where such tets are common) */
     float acc_scale;             /* > 0: the tile passes sum each tet's corrections into shared memory as
                                     32-bit integers round(d * acc_scale) (native integer atomics; shared
                                     float atomics cost ~5x more) and read the sums back as float(sum) /

@@ -99,11 +99,14 @@ class BatchSim(MultiGridSim):
     # ------------------------------------------------------------- autotune
     def _candidates(self):
         """Persistent ranges without/with tet-stream prefetch; per-iteration
-        launches at the default and the flipped CTAs/SM, and with the bulk L2
-        prefetch of each tile's tet streams (tile_variant bit 5)."""
+        launches at the default and the flipped CTAs/SM, with the bulk L2
+        prefetch of each tile's tet streams (tile_variant bit 5), and with
+        that prefetch and the deferred pass for the tets that need the SVD
+        (bit 6)."""
         return [dict(persistent=True, variant=0), dict(persistent=True, variant=4),
                 dict(persistent=False, variant=0), dict(persistent=False, variant=1),
-                dict(persistent=False, variant=32), dict(persistent=False, variant=33)]
+                dict(persistent=False, variant=32), dict(persistent=False, variant=33),
+                dict(persistent=False, variant=96), dict(persistent=False, variant=97)]
 
     def _time_iterations(self, n_iters: int, reps: int) -> float:
         """ms per Jacobi iteration with the frame's own grouping: ``reps``

@@ -84,8 +84,10 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     const float4* pos4 = reinterpret_cast<const float4*>(V.pos);
     const float4* prev4 = reinterpret_cast<const float4*>(V.pprev);
     __shared__ float s_arap_at[XPBD_MAX_MATERIALS];
+    __shared__ int s_defer[2 + kDeferCap];
     // the tet streams are read after the vertex gather: ask for them first
     if ((prm.tile_variant & 32) && threadIdx.x == 0) prefetch_tile_tets(T, tile);
+    if (threadIdx.x == 0) s_defer[0] = s_defer[1] = 0;
     fill_arap_at(prm, s_arap_at);
     for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
         const int g = T.tile_verts[vbeg + i];
@@ -101,7 +103,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     if constexpr (X2 && CSET != CSET_FULL && !DAMP)
         project_tile_tets_x2<CSET == CSET_VOL>(prm, T, tile, s_pos, s_ax, s_ay, s_az, s_cnt, s_arap_at);
     else
-        project_tile_tets<DAMP, CSET>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at);
+        project_tile_tets<DAMP, CSET>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at, s_defer, 0);
     __syncthreads();
 
     float4* pos4w = reinterpret_cast<float4*>(V.pos);
@@ -502,7 +504,7 @@ int check_params(const XpbdParams* p) {
         p->n_attach_materials > XPBD_MAX_ATTACH_MATERIALS)
         return fail(XPBD_ERR_LIMIT, "XpbdParams: material count out of range");
     if (!(p->dt > 0.f)) return fail(XPBD_ERR_ARG, "XpbdParams: dt must be > 0");
-    if (p->tile_variant < 0 || p->tile_variant > 63) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..63");
+    if (p->tile_variant < 0 || p->tile_variant > 127) return fail(XPBD_ERR_ARG, "XpbdParams: tile_variant must be in 0..127");
     if (!(p->acc_scale > 0.f) || !(p->acc_scale < 3.0e38f))
         return fail(XPBD_ERR_ARG, "XpbdParams: acc_scale must be a finite value > 0 (xpbd_acc_scale_for_extent)");
     return XPBD_OK;

@@ -174,15 +174,29 @@ enum : uint32_t {
 // step on, the step of the unit-determinant iterates, (g/2)(g C - X), is
 // tested.  Returns false (caller falls back to the SVD) for det F <= tiny or
 // when 10 steps do not converge.
-__device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
-    float3 x0 = make_float3(F.m[0][0], F.m[1][0], F.m[2][0]);
-    float3 x1 = make_float3(F.m[0][1], F.m[1][1], F.m[2][1]);
-    float3 x2 = make_float3(F.m[0][2], F.m[1][2], F.m[2][2]);
+// The start test of polar_rotation: F's columns, the first cofactor column,
+// det F, and whether det F > 1e-6 |F|_F^3 (squared to avoid the square
+// root).  Tets that fail it take the SVD.
+__device__ __forceinline__ bool polar_start(const M3& F, float3& x0, float3& x1, float3& x2, float3& c0, float& det) {
+    x0 = make_float3(F.m[0][0], F.m[1][0], F.m[2][0]);
+    x1 = make_float3(F.m[0][1], F.m[1][1], F.m[2][1]);
+    x2 = make_float3(F.m[0][2], F.m[1][2], F.m[2][2]);
     const float n2 = dot(x0, x0) + dot(x1, x1) + dot(x2, x2);
-    float3 c0 = cross(x1, x2);
-    float det = dot(x0, c0);
-    // det > 1e-6 |F|_F^3, squared to avoid the square root
-    if (!(det > 0.f && det * det > 1e-12f * (n2 * n2 * n2))) return false;
+    c0 = cross(x1, x2);
+    det = dot(x0, c0);
+    return det > 0.f && det * det > 1e-12f * (n2 * n2 * n2);
+}
+
+__device__ __forceinline__ bool polar_start_ok(const M3& F) {
+    float3 x0, x1, x2, c0;
+    float det;
+    return polar_start(F, x0, x1, x2, c0, det);
+}
+
+__device__ __forceinline__ bool polar_rotation(const M3& F, M3& R) {
+    float3 x0, x1, x2, c0;
+    float det;
+    if (!polar_start(F, x0, x1, x2, c0, det)) return false;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const float3 c1 = cross(x2, x0), c2 = cross(x0, x1);

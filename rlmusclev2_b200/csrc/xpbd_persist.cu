@@ -95,6 +95,8 @@ __global__ void __launch_bounds__(kThreads, MINB)
     }
     const uint32_t ops = XPBD_APPLY_ATTACH | XPBD_APPLY_DIVIDE | XPBD_APPLY_PIN;
     __shared__ float s_arap_at[XPBD_MAX_MATERIALS];
+    __shared__ int s_defer[2 + kDeferCap];
+    if (threadIdx.x == 0) s_defer[0] = s_defer[1] = 0;
     fill_arap_at(prm, s_arap_at);
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = threadIdx.x; i < nvt; i += blockDim.x) {
@@ -145,7 +147,8 @@ __global__ void __launch_bounds__(kThreads, MINB)
         if constexpr (X2 && CSET != CSET_FULL && !DAMP)
             project_tile_tets_x2<CSET == CSET_VOL>(prm, T, tile, s_pos, s_ax, s_ay, s_az, s_cnt, s_arap_at);
         else
-            project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at);
+            project_tile_tets<DAMP, CSET, PF>(prm, T, tile, s_pos, s_prev, s_ax, s_ay, s_az, s_cnt, s_arap_at,
+                                              s_defer, it & 1);
         __syncthreads();
         // boundary partial sums first, so their L2 atomics overlap the interior finish
         for (int i = nint + threadIdx.x; i < nvt; i += blockDim.x) {

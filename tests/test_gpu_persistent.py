@@ -130,3 +130,39 @@ def test_tile_pass_with_l2_prefetch_is_bit_identical(base):
         out.append(sim.positions_np())
     assert np.array_equal(out[0], out[1])
     assert np.abs(out[0] - deformed).max() > 0
+
+
+@pytest.mark.parametrize("case", ["tangled", "flat"])
+def test_deferred_svd_pass_is_bit_identical(case):
+    """tile_variant bit 6 moves the tets whose rotation needs the SVD to a
+    pass after the tile's loop: the per-iteration and the persistent passes
+    give the same positions bit for bit.  "tangled": a jitter of 40 % of an
+    edge inverts many tets (56 of 384); "flat": every tet squashed to a
+    millionth of its height, so the one tile (all 384 tets) defers more than
+    the list's 128 and the rest run in place."""
+    verts, tets, table, mass, vf, act, tendon, deformed, prev = _mixed_problem()
+    rng = np.random.default_rng(7)
+    if case == "tangled":
+        deformed = verts + rng.normal(scale=0.004, size=verts.shape).astype(np.float32)
+    else:
+        deformed = (verts * np.array([1.0, 1.0, 1e-6], np.float32)).astype(np.float32)
+    kw = dict(dt=1.0 / 240.0, contraction_ratio=0.4, fiber_stiffness_scale=3.0)
+    for persistent in (False, True):
+        out = []
+        for tv in (0, 64):
+            sim = XpbdSolver(verts, tets, table, mass=mass, v_fiber=vf, tet_tendonmask=tendon, device="cuda:0",
+                             tile_tets=512 if case == "flat" else 64, **kw)
+            sim._prm.tile_variant = tv
+            sim.set_activation(act)
+            sim.set_positions(prev, also_prev=True)
+            sim.set_positions(deformed)
+            if persistent:
+                sim._fused_iterations(3)
+                assert sim.persistent_status() == 0
+            else:
+                for _ in range(3):
+                    sim._fused_iteration()
+            out.append(sim.positions_np())
+        assert np.isfinite(out[0]).all()
+        assert np.array_equal(out[0], out[1]), (case, persistent)
+        assert np.abs(out[0] - deformed).max() > 0
