@@ -833,8 +833,9 @@ def load_cage_npz(path, n_verts: int) -> Cage:
     the reference (mg/mg.py:774-779) it refuses a cage baked for another fine
     vertex count, and it checks that the block tables index inside the coarse
     vertex and Minv arrays, since the device restriction trusts them."""
-    d = np.load(path)
-    missing = [k for k in CAGE_NPZ_KEYS if k not in d.files]
+    with np.load(path) as z:
+        d = {k: z[k] for k in z.files}
+    missing = [k for k in CAGE_NPZ_KEYS if k not in d]
     if missing:
         raise ValueError(f"cage file {path} lacks {missing}")
     nv = int(d["mg_fine_nv"])
@@ -848,7 +849,7 @@ def load_cage_npz(path, n_verts: int) -> Cage:
                 blk_base=np.asarray(d["blk_base"], np.int32).reshape(-1),
                 blk_dim=np.asarray(d["blk_dim"], np.int32).reshape(-1),
                 blk_matoff=np.asarray(d["blk_matoff"], np.int32).reshape(-1),
-                mg_fine_nv=nv, lam=float(d["lam"]) if "lam" in d.files else 0.0)
+                mg_fine_nv=nv, lam=float(d["lam"]) if "lam" in d else 0.0)
     nc, nt = cage.coarse_pos.shape[0], cage.coarse_tet.shape[0]
     if cage.cage_idx.shape[0] != nv or cage.uvw.shape[0] != nv:
         raise ValueError(f"cage file {path}: cage_idx/uvw must have one row per fine vertex ({nv})")

@@ -152,11 +152,11 @@ class MultiGridSim(MuscleSim):
         # mg.py:1176-1198); without it the lbs targets are computed on the device
         self.lbs_target_npz = cfg.get("lbs_target_npz") if self.target_mode == "lbs" else None
         if self.lbs_target_npz:
-            z = np.load(self.lbs_target_npz)
-            self._lbs_pts = np.asarray(z["points"], np.float32)
+            with np.load(self.lbs_target_npz) as z:
+                self._lbs_pts = np.asarray(z["points"], np.float32)
+                self._lbs_f0 = int(np.asarray(z["frames"], np.int32)[0])
             if self._lbs_pts.ndim != 3 or self._lbs_pts.shape[1:] != (self.NV, 3):
                 raise ValueError(f"lbs_target_npz points {self._lbs_pts.shape} != (F, NV={self.NV}, 3)")
-            self._lbs_f0 = int(np.asarray(z["frames"], np.int32)[0])
         # targets that come from the host every frame (cons frames or the lbs file)
         self._host_tgt = self.target_mode == "points" or bool(self.lbs_target_npz)
         self.use_jacobi = True
