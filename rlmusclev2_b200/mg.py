@@ -159,6 +159,12 @@ class MultiGridSim(MuscleSim):
                 raise ValueError(f"lbs_target_npz points {self._lbs_pts.shape} != (F, NV={self.NV}, 3)")
         # targets that come from the host every frame (cons frames or the lbs file)
         self._host_tgt = self.target_mode == "points" or bool(self.lbs_target_npz)
+        # the solve is the Jacobi projection (mg.py:353-354 read use_jacobi,
+        # default true, and use_colored_gs, default false): the Gauss-Seidel
+        # variants are refused rather than silently replaced
+        if not bool(cfg.get("use_jacobi", True)) or bool(cfg.get("use_colored_gs", False)):
+            raise NotImplementedError("use_jacobi=false / use_colored_gs=true select the reference's Gauss-Seidel "
+                                      "solves, which are not on the sm_100a path (it runs the Jacobi projection)")
         self.use_jacobi = True
         self.use_colored_gs = False
         self.has_compressstiffness = False

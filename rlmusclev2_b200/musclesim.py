@@ -47,6 +47,11 @@ class MuscleSim(XpbdEngine):
         ``fiber_stiffness_scale``.  ``cfg`` is a dict or an attribute object
         (the reference's SimConfig)."""
         get = (lambda k, d=None: cfg.get(k, d)) if isinstance(cfg, dict) else (lambda k, d=None: getattr(cfg, k, d))
+        # musclesim.py:73-74: use_jacobi (default true on a GPU) and use_colored_gs;
+        # the Gauss-Seidel solves are refused rather than silently replaced
+        if not bool(get("use_jacobi", True)) or bool(get("use_colored_gs", False)):
+            raise NotImplementedError("use_jacobi=false / use_colored_gs=true select the reference's Gauss-Seidel "
+                                      "solves, which are not on the sm_100a path (it runs the Jacobi projection)")
         path = get("geo_path")
         if not path:
             raise ValueError("MuscleSim(cfg) needs cfg.geo_path (or use MuscleSim.from_procedural)")

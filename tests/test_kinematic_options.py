@@ -189,3 +189,19 @@ def test_restrict_modes_change_the_frames():
         print(key, np.isfinite(p).all(), np.abs(p - base).max())
         if key != ("direct", "galerkin"):
             assert not np.array_equal(p, base), key
+
+
+def test_gauss_seidel_options_are_refused():
+    """use_jacobi=false / use_colored_gs=true (mg.py:353-354,
+    musclesim.py:73-74) select Gauss-Seidel solves, which are not on this
+    path: both constructors refuse them before touching a device."""
+    import pytest
+    from rlmusclev2_b200 import MuscleSim
+    from rlmusclev2_b200.mg import MultiGridSim
+    for key, val in (("use_jacobi", False), ("use_colored_gs", True)):
+        cfg = _cfg()
+        cfg[key] = val
+        with pytest.raises(NotImplementedError, match="Gauss-Seidel"):
+            MultiGridSim(cfg, scene=_scene())
+        with pytest.raises(NotImplementedError, match="Gauss-Seidel"):
+            MuscleSim({key: val, "geo_path": "unused.geo"})
