@@ -116,6 +116,10 @@ class MultiGridSim(MuscleSim):
         if self.use_fiber and self.fiber_model != "aniso_arap":
             raise NotImplementedError(f"fiber_model={self.fiber_model!r} is not on the sm_100a path "
                                       "(supported: 'aniso_arap')")
+        # asset_scale (util/bone_source.py:60-66, 301-315; mg.py:299-305): a
+        # uniform scale of the USD rest mesh and of the bone_<frame>.geo
+        # surfaces on load (0.01 for a centimetre asset); a .geo rest is not scaled
+        self.asset_scale = float(cfg.get("asset_scale", 1.0))
         if scene is None and "synthetic" not in cfg and cfg.get("rest_path"):
             rp = Path(cfg["rest_path"])
             if rp.suffix.lower() not in (".geo", ".usda", ".usd"):
@@ -127,7 +131,12 @@ class MultiGridSim(MuscleSim):
                 scene = scene_from_geo(rp)
             else:
                 from .usd import scene_from_usda
-                scene = scene_from_usda(rp, cfg.get("rest_prim_path"))
+                if cfg.get("muscle_prim_root"):
+                    raise NotImplementedError("muscle_prim_root (merging every TetMesh under a root) is not read; "
+                                              "name one TetMesh with muscle_prim_path")
+                # the layer's points as authored (no xform ops are applied; usd_local_space)
+                scene = scene_from_usda(rp, cfg.get("muscle_prim_path") or cfg.get("rest_prim_path"))
+                scene.verts = self._asset_scaled(scene.verts)
         self.scene = scene if scene is not None else scene_from_cfg(cfg)
         sc = self.scene
         # kinematic targets (mg.py:436-446)
@@ -379,7 +388,7 @@ class MultiGridSim(MuscleSim):
             # positions of bone_<frame>.geo uploaded every frame
             from .geo import GeoFile
             g0 = GeoFile(Path(self._bone_dir) / f"bone_{self.start_frame}.geo")
-            bv = g0.positions
+            bv = self._asset_scaled(g0.positions)
             bt = np.asarray(g0.tet_indices, np.int32).reshape(-1, 3)
             bvb = np.zeros(bv.shape[0], np.int32)
             self._bone_frames = {}
@@ -547,11 +556,19 @@ class MultiGridSim(MuscleSim):
         self._solve_m2m_glue()
         self.apply_pintotarget()
 
+    def _asset_scaled(self, arr) -> np.ndarray:
+        """Positions times asset_scale in FP32 (unchanged at 1)."""
+        arr = np.asarray(arr, np.float32)
+        if self.asset_scale == 1.0:
+            return arr
+        return np.ascontiguousarray((arr * np.float32(self.asset_scale)).astype(np.float32))
+
     def _upload_bone_frame(self, frame: int) -> None:
         """bone_<frame>.geo positions into the bone-surface buffer (one pinned H2D copy)."""
         from .geo import read_geo_attr
         if frame not in self._bone_frames:
-            self._bone_frames[frame] = read_geo_attr(Path(self._bone_dir) / f"bone_{int(frame)}.geo", "P")
+            self._bone_frames[frame] = self._asset_scaled(
+                read_geo_attr(Path(self._bone_dir) / f"bone_{int(frame)}.geo", "P"))
         self._h2d_event.synchronize()
         self._bs_host.numpy()[:, :3] = self._bone_frames[frame]
         with torch.cuda.stream(self._stream):

@@ -205,3 +205,15 @@ def test_gauss_seidel_options_are_refused():
             MultiGridSim(cfg, scene=_scene())
         with pytest.raises(NotImplementedError, match="Gauss-Seidel"):
             MuscleSim({key: val, "geo_path": "unused.geo"})
+
+
+def test_asset_scale_is_an_fp32_product():
+    """asset_scale (util/bone_source.py:60-66): positions times the scale in
+    FP32, unchanged at 1."""
+    from types import SimpleNamespace
+    from rlmusclev2_b200.mg import MultiGridSim
+    x = np.random.default_rng(5).standard_normal((40, 3)).astype(np.float32) * 100
+    f = MultiGridSim._asset_scaled
+    assert np.array_equal(f(SimpleNamespace(asset_scale=1.0), x), x)
+    got = f(SimpleNamespace(asset_scale=0.01), x)
+    assert got.dtype == np.float32 and np.array_equal(got, x * np.float32(0.01))
